@@ -1,0 +1,295 @@
+#!/usr/bin/env python
+"""Benchmark: particle-steps/s of the FLIP sub-step on the obstacles-and-inflow workload.
+
+Workload (one GPU): 128×64(up)×64 cells at h = 1/64 m, ≈1.70M particles (bottom 26 layers at 8 per cell),
+a sphere, a turned box and a cylinder (face fractions from analytic SDFs), a 2 cm faucet at 1.5 m/s
+emitting 10 particles per sub-step, one floor drain, 100 SOR iterations at ω = 1.8, FLIP 0.95,
+dt = 1/240 s. A step is one sub-step of the liquid: binning, P2G, forces and divergence, the pressure
+solve, projection, G2P with collisions, drains and drop/whitewater logic. Synthetic seeded data.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl suiri|reference]
+
+Under torchrun each rank advances its own replica of the workload (tanks do not interact: no collective
+in the data path); the time is the max over ranks and the value counts every rank's particles.
+"""
+import argparse
+import importlib
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+METRIC = 'particle-steps/s'
+L2_FLUSH_BYTES = 256 << 20          # larger than the 126 MB L2; written between timed steps
+
+
+def pkg():
+    return importlib.import_module('hahenn-_b200')
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            p = json.load(f)
+        return float(p['hbm_gbs']), 'measured'
+    except Exception:
+        return 6650.0, 'fallback'
+
+
+def sor_traffic():
+    """DRAM bytes per SOR sweep launch from the committed ncu summary (null if none)."""
+    try:
+        with open(os.path.join(ROOT, 'profiles', 'sor_sweep_traffic.json')) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+    Q = 'clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,' \
+        'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap'
+
+    def __init__(self, device):
+        self.device, self.rows, self.proc = device, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', f'--query-gpu={self.Q}', '--format=csv,noheader,nounits',
+                                          '-lms', '200', '-i', str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(',')])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm = [float(r[0]) for r in self.rows if r and r[0].replace('.', '').isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) > 1 and r[1].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 2 + i and r[2 + i] == 'Active'})
+        return dict(sm_mhz=float(np.median(sm)) if sm else None, sm_max_mhz=max(mx) if mx else None,
+                    reasons=reasons, samples=len(sm))
+
+
+def make_tank(P, w, device, host_inflow=False):
+    prm = w['params']
+    t = P.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=prm['flip'], omega=prm['omega'], iters=prm['iters'],
+               gravity=prm['g'], whitewater=True, ripple=None, capacity=int(len(w['pos']) * 1.25) + 100000,
+               device=device, sdf_mode='analytic')
+    t.set_objects(w['objects'])
+    t.add_particles(w['pos'])
+    if not host_inflow:
+        t.set_emitters([dict(shape='disc', pos=e['pos'], dir=e['dir'], radius=e['radius'], speed=e['speed'],
+                             count=e['count']) for e in w['emitters']])
+    return t
+
+
+def faucet_particles(e, dt, rng):
+    """The faucet's particles of one sub-step generated on the host (for the end-to-end measurement)."""
+    n = e['count']
+    d = np.array(e['dir'], float); d /= np.linalg.norm(d)
+    ref = np.array([0.0, 1.0, 0.0]) if abs(d[1]) < 0.95 else np.array([1.0, 0.0, 0.0])
+    u = np.cross(d, ref); u /= np.linalg.norm(u)
+    w = np.cross(d, u)
+    rr = e['radius'] * np.sqrt(rng.random(n)); th = 2 * math.pi * rng.random(n)
+    p = np.array(e['pos']) + (np.cos(th)[:, None] * u + np.sin(th)[:, None] * w) * rr[:, None] \
+        + d * (rng.random(n) * e['speed'] * dt)[:, None]
+    v = d * e['speed'] + (rng.random((n, 3)) - 0.5) * (0.02 * e['speed'])
+    return p.astype(np.float32), v.astype(np.float32)
+
+
+def cpu_port_rate(w, steps):
+    """The CPU oracle (NumPy restatement of the reference solver, single core) on `steps` sub-steps of the
+    same workload: particle-steps/s."""
+    from oracle import flip as of
+    from oracle import sdf as sdfm
+    prm = w['params']
+    t = of.Tank(w['nx'], w['ny'], w['nz'], w['h'], origin=w['origin'], flip=prm['flip'], omega=prm['omega'],
+                iters=prm['iters'], g=prm['g'], whitewater=True, rng_mode='hash', sdf_mode='lattice')
+    objs = []
+    for it in w['objects']:
+        if it['kind'] == 'obstacle':
+            objs.append(sdfm.make_obstacle(it['shape'], it['pos'], tuple(it['rot']), **it['dims']))
+        else:
+            objs.append(sdfm.make_drain(it['pos'], it['r'], tuple(it['rot'])))
+    t.set_objects(objs)
+    t.add_particles(w['pos'].astype(np.float64))
+    rng = np.random.default_rng(1)
+    dt = prm['dt']
+    n_ps = 0
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for e in w['emitters']:
+            p, v = faucet_particles(e, dt, rng)
+            t.add_particles(p.astype(np.float64), v.astype(np.float64))
+        n_ps += len(t.pos)
+        t.frame += 1
+        t.substep(dt)
+    el = time.perf_counter() - t0
+    return n_ps / el, el
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    w = pkg().workloads.obstacles_inflow()
+    steps, warm = max(1, min(args.steps, 6)), min(args.warmup, 1)
+    if warm:
+        cpu_port_rate(w, warm)
+    rate, el = cpu_port_rate(w, steps)
+    line = dict(impl='reference', metric=METRIC, value=rate, unit=METRIC, n_gpus=args.gpus, steps=steps, warmup=warm,
+                ms_per_step=1000 * el / steps, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f64',
+                data='synthetic',
+                config=dict(workload=w['name'], particles=len(w['pos']), cells=w['nx'] * w['ny'] * w['nz'],
+                            sor_iters=w['params']['iters'], omega=w['params']['omega'], dt=w['params']['dt']),
+                cpu_baseline=dict(value=rate, unit=METRIC, cores=1, kind='port',
+                                  sample=f'{steps} sub-steps of the full workload (NumPy restatement of the reference '
+                                         f'solver, pinned bit-exact against it; NumPy runs on one core of {os.cpu_count()})'),
+                e2e=dict(value=rate, unit=METRIC, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='suiri', choices=['suiri', 'reference'])
+    ap.add_argument('--cpu-steps', type=int, default=2, help='sub-steps of the CPU baseline sample')
+    args = ap.parse_args()
+    rank, world = int(os.environ.get('RANK', 0)), int(os.environ.get('WORLD_SIZE', 1))
+    local = int(os.environ.get('LOCAL_RANK', 0))
+    if args.impl == 'reference':
+        return run_reference(args, rank)
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    P = pkg()
+    w = P.workloads.obstacles_inflow()
+    prm = w['params']
+    dt = prm['dt']
+    ncell = w['nx'] * w['ny'] * w['nz']
+    tank = make_tank(P, w, local)
+    tank.profile(True)
+    stream = torch.cuda.ExternalStream(tank.stream())
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f'cuda:{local}')
+    for _ in range(max(args.warmup, 3)):
+        tank.substep(dt)
+    tank.sync()
+    n0 = tank.stats()['count']
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    step_ms, sor_ms = [], []
+    clocks = Clocks(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()                          # L2 flush, outside the timed interval
+        ev[k][0].record(stream)
+        tank.substep(dt)
+        ev[k][1].record(stream)
+        sor_ms.append(tank.sor_phase_ms())
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if world > 1:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    n1 = tank.stats()['count']
+    ms = float(np.mean(step_ms))
+    particles = 0.5 * (n0 + n1)
+    sor_launch_ms = float(np.mean(sor_ms)) / (2 * prm['iters'])
+    if world > 1:
+        t = torch.tensor([ms, particles, sor_launch_ms], dtype=torch.float64, device=f'cuda:{local}')
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        tot = t.clone()
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        ms, sor_launch_ms = float(mx[0]), float(mx[2])
+        particles = float(tot[1])
+    value = particles * 1000.0 / ms
+
+    # end-to-end through the C ABI: host inflow particles (pinned) up, stats back, every step
+    e2e = None
+    if rank == 0 or world > 1:
+        t2 = make_tank(P, w, local, host_inflow=True)
+        rng = np.random.default_rng(7)
+        for _ in range(3):
+            for e in w['emitters']:
+                p, v = faucet_particles(e, dt, rng)
+                t2.add_particles(p, v)
+            t2.substep(dt)
+            t2.stats()
+        nA = t2.stats()['count']
+        h2d = d2h = 0
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            for e in w['emitters']:
+                p, v = faucet_particles(e, dt, rng)
+                t2.add_particles(p, v)
+                h2d += p.nbytes + v.nbytes
+            t2.substep(dt)
+            t2.stats()
+            d2h += 128
+        el = time.perf_counter() - t0
+        nB = t2.stats()['count']
+        e2e_rate = 0.5 * (nA + nB) * args.steps / el
+        if world > 1:
+            x = torch.tensor([e2e_rate], dtype=torch.float64, device=f'cuda:{local}')
+            dist.all_reduce(x, op=dist.ReduceOp.MIN)
+            e2e_rate = float(x[0]) * world
+        e2e = dict(value=e2e_rate, unit=METRIC, h2d_bytes_per_step=h2d // args.steps, d2h_bytes_per_step=d2h // args.steps)
+        t2.close()
+
+    if rank == 0:
+        peak, kind = peaks()
+        alg_bytes = 20.0 * ncell                 # one colour sweep: read p 4 + 3 fractions 12 + rhs 2 + write p 2 per cell
+        achieved = alg_bytes / (sor_launch_ms * 1e-3) / 1e9
+        tr = sor_traffic()
+        cpu_rate, cpu_el = cpu_port_rate(w, args.cpu_steps)
+        launches_per_step = 13 + 2 * prm['iters']
+        line = dict(metric=METRIC, value=value, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
+                    ms_per_step=ms, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
+                    data='synthetic (seeded particles, analytic obstacles)',
+                    config=dict(workload=w['name'], particles=int(particles / world), cells=ncell,
+                                sor_iters=prm['iters'], omega=prm['omega'], flip=prm['flip'], dt=dt,
+                                inflow_per_step=w['emitters'][0]['count'], l2='flushed (256 MiB write) between timed steps',
+                                parallelism=f'replicas{world}'),
+                    roofline=dict(bound='hbm', kernel='k_sor (one colour sweep)', achieved=achieved, peak=peak,
+                                  unit='GB/s', frac=achieved / peak, peak_kind=kind,
+                                  traffic=None if tr is None else tr.get('dram_bytes_per_launch'),
+                                  alg_bytes_per_launch=alg_bytes, launch_ms=sor_launch_ms,
+                                  sor_share=float(np.mean(sor_ms)) / ms),
+                    cpu_baseline=dict(value=cpu_rate, unit=METRIC, cores=1, kind='port',
+                                      sample=f'{args.cpu_steps} sub-steps of the same workload on the host (NumPy '
+                                             f'restatement of the reference solver, {cpu_el:.1f} s, 1 core of {os.cpu_count()})'),
+                    e2e=e2e, gpu_launches=launches_per_step * args.steps, clocks=clk)
+        print(json.dumps(line), flush=True)
+    tank.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

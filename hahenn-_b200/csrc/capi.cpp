@@ -1,0 +1,535 @@
+// extern "C" surface of libsuiri_cuda.so (include/suiri.h): argument checks, error codes and messages,
+// no exception crosses the ABI.
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "../../include/suiri.h"
+#include "engine.h"
+
+using namespace suiri;
+
+struct suiri_tank {
+  std::unique_ptr<Tank> t;
+  std::string err;
+};
+struct suiri_batch {
+  std::unique_ptr<Group> g;
+  std::string err;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+template <class F>
+int guard(std::string* err, F&& f) {
+  try {
+    f();
+    return SUIRI_OK;
+  } catch (const Error& e) {
+    if (err) *err = e.what();
+    g_err = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    const char* m = "host out of memory";
+    if (err) *err = m;
+    g_err = m;
+    return SUIRI_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    if (err) *err = e.what();
+    g_err = e.what();
+    return SUIRI_ERR_INVALID;
+  }
+}
+
+struct Quality { const char* name; double h; long long cap, ww; int iters, ripple, wmap; };
+// quality presets (src/js/50-sim.js:4-8, solver.py:23-27)
+const Quality kQ[] = {{"low", 0.012, 140000, 60000, 28, 128, 256},
+                      {"standard", 0.0085, 320000, 140000, 40, 256, 256},
+                      {"high", 0.0065, 700000, 260000, 56, 512, 384}};
+
+const Quality& quality(const char* q) {
+  if (q)
+    for (const auto& x : kQ)
+      if (strcmp(x.name, q) == 0) return x;
+  if (q && *q) throw Error(SUIRI_ERR_INVALID, std::string("unknown quality '") + q + "'");
+  return kQ[1];
+}
+
+double js_round(double x) { return floor(x + 0.5); }
+
+void rotvec(const double R[9], double out[3]) {
+  // m3.log (src/js/00-util.js:53-60)
+  const double c = std::min(std::max((R[0] + R[4] + R[8] - 1) / 2, -1.0), 1.0);
+  const double ang = acos(c);
+  out[0] = out[1] = out[2] = 0;
+  if (ang < 1e-6) return;
+  const double s = 2 * sin(ang);
+  if (fabs(s) < 1e-6) return;
+  out[0] = (R[7] - R[5]) / s * ang;
+  out[1] = (R[2] - R[6]) / s * ang;
+  out[2] = (R[3] - R[1]) / s * ang;
+}
+
+// obstacles of a scene → device records with velocities from the previous transforms (src/js/50-sim.js:165-211)
+bool apply_solids(Tank& t, const std::vector<SceneItem>& items, double dt_move) {
+  std::vector<Obj> objs;
+  std::map<int, PrevXf> next;
+  bool moving = false;
+  for (const SceneItem& it : items) {
+    if (objs.size() >= (size_t)kMaxObj) break;
+    Obj o = it.obj;
+    double lin[3] = {0, 0, 0}, ang[3] = {0, 0, 0};
+    auto p = t.prev_xf.find(it.id);
+    if (p != t.prev_xf.end() && dt_move > 0) {
+      for (int a = 0; a < 3; ++a) lin[a] = (o.pos[a] - p->second.pos[a]) / dt_move;
+      double M[9];   // R · prevᵀ
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+          M[r * 3 + c] = it.R[r * 3] * p->second.R[c * 3] + it.R[r * 3 + 1] * p->second.R[c * 3 + 1] + it.R[r * 3 + 2] * p->second.R[c * 3 + 2];
+      rotvec(M, ang);
+      for (int a = 0; a < 3; ++a) ang[a] /= dt_move;
+      const double ll = sqrt(lin[0] * lin[0] + lin[1] * lin[1] + lin[2] * lin[2]);
+      const double la = sqrt(ang[0] * ang[0] + ang[1] * ang[1] + ang[2] * ang[2]);
+      if (ll > 1e-5 || la > 1e-4) moving = true;
+      if (ll > 4) for (double& v : lin) v *= 4 / ll;
+      if (la > 40) for (double& v : ang) v *= 40 / la;
+    }
+    PrevXf x;
+    memcpy(x.pos, o.pos, sizeof(x.pos));
+    memcpy(x.R, it.R, sizeof(x.R));
+    next[it.id] = x;
+    if (o.flag == 1) { memcpy(o.lin, lin, sizeof(lin)); memcpy(o.ang, ang, sizeof(ang)); }
+    objs.push_back(o);
+  }
+  t.prev_xf = next;
+  // a changed object list re-runs GEOM (the reference compares a signature of the packed records)
+  bool same = objs.size() == t.objs.size();
+  for (size_t i = 0; same && i < objs.size(); ++i) same = memcmp(&objs[i], &t.objs[i], sizeof(Obj)) == 0;
+  if (!same) t.set_objects(objs);
+  return moving;
+}
+
+Tank* T(suiri_tank* h) {
+  if (!h || !h->t) throw Error(SUIRI_ERR_INVALID, "null tank handle");
+  return h->t.get();
+}
+
+}  // namespace
+
+extern "C" {
+
+int suiri_params_default(suiri_params* p) {
+  if (!p) { g_err = "null params"; return SUIRI_ERR_INVALID; }
+  memset(p, 0, sizeof(*p));
+  p->size = sizeof(suiri_params);
+  p->quality = "standard";
+  p->clamp_tank = 1;
+  p->flip = 0.96; p->omega = 1.6; p->iters = 0; p->gravity = 9.81; p->friction = 0.03;
+  p->ppc = 8.0; p->drift = 6.0; p->ww_rate = 7.0; p->whitewater = 1;
+  p->capacity = 0; p->ww_capacity = 0; p->ripple_rx = 0; p->ripple_rz = 0; p->wmap = 0;
+  p->sdf_mode = 0; p->device = 0; p->seed = 1;
+  return SUIRI_OK;
+}
+
+int suiri_create(const char* scene_json, const suiri_params* params, suiri_tank** out) {
+  if (!out) { g_err = "null output handle"; return SUIRI_ERR_INVALID; }
+  *out = nullptr;
+  suiri_params p;
+  suiri_params_default(&p);
+  if (params) {
+    if (params->size != sizeof(suiri_params)) { g_err = "suiri_params.size mismatch (use suiri_params_default)"; return SUIRI_ERR_INVALID; }
+    p = *params;
+  }
+  std::unique_ptr<suiri_tank> h(new suiri_tank());
+  const int rc = guard(nullptr, [&] {
+    const Quality& q = quality(p.quality);
+    Scene sc;
+    std::string err;
+    if (scene_json) {
+      const bool ok = parse_scene(scene_json, p.clamp_tank != 0, sc, err);
+      if (!ok) throw Error(SUIRI_ERR_PARSE, err);
+    }
+    TankConfig c;
+    if (p.nx > 0 && p.ny > 0 && p.nz > 0 && p.h > 0) {
+      c.nx = p.nx; c.ny = p.ny; c.nz = p.nz; c.h = p.h;
+    } else if (p.nx != 0 || p.ny != 0 || p.nz != 0 || p.h != 0) {
+      throw Error(SUIRI_ERR_INVALID, "explicit grid needs nx, ny, nz and h all positive");
+    } else {
+      // FluidSim sizing (src/js/50-sim.js:33-38)
+      c.nx = (int)std::max(8.0, js_round(sc.tank[0] / q.h));
+      c.ny = (int)std::max(8.0, js_round(sc.tank[1] / q.h));
+      c.nz = (int)std::max(8.0, js_round(sc.tank[2] / q.h));
+      c.h = std::min(std::min(sc.tank[0] / c.nx, sc.tank[1] / c.ny), sc.tank[2] / c.nz);
+    }
+    c.origin[0] = -c.nx * c.h / 2; c.origin[1] = 0.0; c.origin[2] = -c.nz * c.h / 2;
+    c.nyl = c.ny + std::max(0, (int)ceil(p.extra_height / c.h));
+    c.flip = p.flip; c.omega = p.omega; c.g = p.gravity; c.friction = p.friction; c.ppc = p.ppc; c.drift = p.drift;
+    c.ww_rate = p.ww_rate; c.whitewater = p.whitewater ? 1 : 0;
+    c.iters = p.iters > 0 ? p.iters : q.iters;
+    c.cap = p.capacity > 0 ? p.capacity : q.cap;
+    c.ww_cap = p.ww_capacity > 0 ? p.ww_capacity : q.ww;
+    if (p.ripple_rx < 0 || p.ripple_rz < 0) { c.rx = c.rz = 0; }
+    else if (p.ripple_rx == 0 && p.ripple_rz == 0) { c.rx = c.rz = q.ripple; }
+    else { c.rx = p.ripple_rx; c.rz = p.ripple_rz; }
+    c.wmap = p.wmap > 0 ? p.wmap : q.wmap;
+    c.sdf_mode = p.sdf_mode;
+    c.device = p.device;
+    c.seed = p.seed;
+    if (!(c.omega > 0 && c.omega < 2)) throw Error(SUIRI_ERR_INVALID, "omega must be in (0, 2)");
+    if (c.cap > (1LL << 30)) throw Error(SUIRI_ERR_INVALID, "capacity above 2^30 particles");
+    h->t.reset(new Tank(c));
+    h->t->scene = sc;
+    apply_solids(*h->t, sc.solids, 0.0);
+    for (const WaterBlock& b : sc.blocks) h->t->emit_block(b.lo, b.hi, false);
+  });
+  if (rc != SUIRI_OK) return rc;
+  *out = h.release();
+  return SUIRI_OK;
+}
+
+int suiri_destroy(suiri_tank* t) {
+  if (!t) return SUIRI_ERR_INVALID;
+  const int rc = guard(nullptr, [&] { t->t.reset(); });
+  delete t;
+  return rc;
+}
+
+const char* suiri_last_error(const suiri_tank* t) {
+  if (t) return t->err.c_str();
+  return g_err.c_str();
+}
+
+int suiri_reset(suiri_tank* h) {
+  return guard(h ? &h->err : nullptr, [&] { T(h)->reset(); });
+}
+int suiri_clear(suiri_tank* h) {
+  return guard(h ? &h->err : nullptr, [&] { T(h)->clear(); });
+}
+
+int suiri_set_objects(suiri_tank* h, const char* items_json, double dt_move, int32_t* moving) {
+  return guard(h ? &h->err : nullptr, [&] {
+    Tank* t = T(h);
+    if (!items_json) throw Error(SUIRI_ERR_INVALID, "null items JSON");
+    JVal root;
+    std::string err;
+    if (!json_parse(items_json, root, err)) throw Error(SUIRI_ERR_PARSE, err);
+    const JVal* items = &root;
+    if (root.kind == JVal::Obj) {
+      const JVal* s = root.get("scene");
+      items = (s ? s : &root)->get("items");
+      if (!items) throw Error(SUIRI_ERR_PARSE, "scene JSON: no items");
+    }
+    Scene sc;
+    if (!parse_items(*items, sc, err)) throw Error(SUIRI_ERR_PARSE, err);
+    const bool mv = apply_solids(*t, sc.solids, dt_move);
+    t->scene.sources = sc.sources;
+    t->scene.blocks = sc.blocks;
+    if (moving) *moving = mv ? 1 : 0;
+  });
+}
+
+int suiri_set_obstacles(suiri_tank* h, const suiri_object* objs, int32_t n) {
+  return guard(h ? &h->err : nullptr, [&] {
+    Tank* t = T(h);
+    if (n < 0 || n > kMaxObj || (n > 0 && !objs)) throw Error(SUIRI_ERR_INVALID, "0..64 objects expected");
+    std::vector<Obj> v(n);
+    for (int i = 0; i < n; ++i) {
+      Obj& o = v[i];
+      memset(&o, 0, sizeof(o));
+      const suiri_object& s = objs[i];
+      if (s.flag != 1 && s.flag != 2) throw Error(SUIRI_ERR_INVALID, "object flag must be 1 (obstacle) or 2 (drain)");
+      o.type = s.type; o.flag = s.flag;
+      memcpy(o.pos, s.pos, sizeof(o.pos)); memcpy(o.rot, s.rot, sizeof(o.rot)); memcpy(o.dims, s.dims, sizeof(o.dims));
+      memcpy(o.lin, s.lin, sizeof(o.lin)); memcpy(o.ang, s.ang, sizeof(o.ang));
+      o.bound = s.flag == 1 ? bound_radius(o.type, o.dims) + 0.002 : o.dims[0] + 0.02;
+    }
+    t->set_objects(v);
+  });
+}
+
+int suiri_set_lattice(suiri_tank* h, const double* sdf, const int32_t* oid, int32_t lx, int32_t ly, int32_t lz) {
+  return guard(h ? &h->err : nullptr, [&] {
+    if (!sdf) throw Error(SUIRI_ERR_INVALID, "null lattice");
+    T(h)->set_lattice(sdf, oid, lx, ly, lz);
+  });
+}
+
+int suiri_add_particles(suiri_tank* h, const float* pos, const float* vel, const float* airborne, int64_t n, uint32_t* first_id) {
+  return guard(h ? &h->err : nullptr, [&] { T(h)->add_particles(pos, vel, airborne, n, first_id); });
+}
+
+int suiri_set_emitters(suiri_tank* h, const suiri_emitter* e, int32_t n) {
+  return guard(h ? &h->err : nullptr, [&] {
+    Tank* t = T(h);
+    if (n < 0 || n > kMaxEmitters || (n > 0 && !e)) throw Error(SUIRI_ERR_INVALID, "0..8 emitters expected");
+    std::vector<EmitterDev> v(n);
+    for (int i = 0; i < n; ++i) {
+      EmitterDev& d = v[i];
+      memset(&d, 0, sizeof(d));
+      if (e[i].shape != 0 && e[i].shape != 3) throw Error(SUIRI_ERR_INVALID, "emitter shape must be 0 (disc) or 3 (rain)");
+      if (!(e[i].per_substep >= 0) || !(e[i].radius >= 0)) throw Error(SUIRI_ERR_INVALID, "emitter rate and radius must be >= 0");
+      d.shape = e[i].shape; d.airborne = e[i].airborne ? 1 : 0;
+      d.radius = e[i].radius; d.speed = e[i].speed; d.per_substep = e[i].per_substep;
+      memcpy(d.pos, e[i].pos, sizeof(d.pos));
+      double l = sqrt(e[i].dir[0] * e[i].dir[0] + e[i].dir[1] * e[i].dir[1] + e[i].dir[2] * e[i].dir[2]);
+      if (!(l > 0)) { d.dir[1] = -1; l = 1; } else { for (int a = 0; a < 3; ++a) d.dir[a] = e[i].dir[a] / l; }
+      // basisOf (src/js/55-emit.js:4-9)
+      const double ref[3] = {fabs(d.dir[1]) < 0.95 ? 0.0 : 1.0, fabs(d.dir[1]) < 0.95 ? 1.0 : 0.0, 0.0};
+      double u[3] = {d.dir[1] * ref[2] - d.dir[2] * ref[1], d.dir[2] * ref[0] - d.dir[0] * ref[2], d.dir[0] * ref[1] - d.dir[1] * ref[0]};
+      const double ul = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+      for (int a = 0; a < 3; ++a) d.u[a] = u[a] / ul;
+      d.w[0] = d.dir[1] * d.u[2] - d.dir[2] * d.u[1];
+      d.w[1] = d.dir[2] * d.u[0] - d.dir[0] * d.u[2];
+      d.w[2] = d.dir[0] * d.u[1] - d.dir[1] * d.u[0];
+    }
+    t->set_emitters(v);
+  });
+}
+
+int suiri_emit_block(suiri_tank* h, const double lo[3], const double hi[3], int32_t fill) {
+  return guard(h ? &h->err : nullptr, [&] {
+    if (!lo || !hi) throw Error(SUIRI_ERR_INVALID, "null block corners");
+    T(h)->emit_block(lo, hi, fill != 0);
+  });
+}
+
+int suiri_substep(suiri_tank* h, double dt) {
+  return guard(h ? &h->err : nullptr, [&] {
+    if (!(dt > 0) || !std::isfinite(dt)) throw Error(SUIRI_ERR_INVALID, "dt must be positive");
+    T(h)->substep(dt);
+  });
+}
+
+int suiri_step(suiri_tank* h, double frame_dt, int32_t* substeps) {
+  return guard(h ? &h->err : nullptr, [&] {
+    if (!std::isfinite(frame_dt)) throw Error(SUIRI_ERR_INVALID, "frame_dt must be finite");
+    const int n = T(h)->step(frame_dt);
+    if (substeps) *substeps = n;
+  });
+}
+
+int suiri_sync(suiri_tank* h) {
+  return guard(h ? &h->err : nullptr, [&] { CK(cudaStreamSynchronize(T(h)->stream)); });
+}
+
+int suiri_read_particles(suiri_tank* h, float* pos4, float* vel4, int64_t cap, int64_t* n) {
+  return guard(h ? &h->err : nullptr, [&] {
+    const long long k = T(h)->read_particles(pos4, vel4, cap);
+    if (n) *n = k;
+  });
+}
+
+int suiri_read_whitewater(suiri_tank* h, float* pos4, float* vel4, int64_t cap, int64_t* n) {
+  return guard(h ? &h->err : nullptr, [&] {
+    const long long k = T(h)->read_whitewater(pos4, vel4, cap);
+    if (n) *n = k;
+  });
+}
+
+int suiri_read_grid(suiri_tank* h, int32_t field, void* out, size_t bytes) {
+  return guard(h ? &h->err : nullptr, [&] {
+    if (!out) throw Error(SUIRI_ERR_INVALID, "null output");
+    T(h)->read_grid(field, out, bytes);
+  });
+}
+
+int suiri_get_stats(suiri_tank* h, suiri_stats* s) {
+  return guard(h ? &h->err : nullptr, [&] {
+    Tank* t = T(h);
+    if (!s) throw Error(SUIRI_ERR_INVALID, "null stats");
+    t->read_counters();
+    const Counters& c = *t->h_ctr;
+    if (c.vmax_bits64 != 0ull) {
+      const unsigned long long b = c.vmax_bits64 - 1ull;
+      memcpy(&t->vmax, &b, 8);
+    }
+    long long alive = 0;
+    {
+      // alive = A without the dead flags + pending emissions: A's dead are only known after binning,
+      // n_sorted counts them out once the next sub-step (or a count pass) has run
+      alive = (long long)c.n_live + c.n_emit;
+    }
+    memset(s, 0, sizeof(*s));
+    s->count = alive;
+    s->ww_count = std::min<long long>(c.ww_count, t->d.ww_cap);
+    s->impacts = c.impacts;
+    s->vmax = t->vmax;
+    s->time = t->time;
+    s->liters = alive * t->d.vp * 1000;
+    s->full = c.full;
+    s->frame = c.frame;
+    s->nx = t->d.nx; s->ny = t->d.ny; s->nz = t->d.nz; s->h = t->d.h;
+    s->origin[0] = t->d.ox; s->origin[1] = t->d.oy; s->origin[2] = t->d.oz;
+  });
+}
+
+int suiri_snapshot(suiri_tank* h, int32_t* id) {
+  return guard(h ? &h->err : nullptr, [&] {
+    const int k = T(h)->snapshot();
+    if (id) *id = k;
+  });
+}
+
+int suiri_restore(suiri_tank* h, int32_t id) {
+  return guard(h ? &h->err : nullptr, [&] { T(h)->restore(id); });
+}
+
+int suiri_stream(suiri_tank* h, void** stream) {
+  return guard(h ? &h->err : nullptr, [&] {
+    if (!stream) throw Error(SUIRI_ERR_INVALID, "null output");
+    *stream = (void*)T(h)->stream;
+  });
+}
+
+int suiri_use_graphs(suiri_tank* h, int32_t on) {
+  return guard(h ? &h->err : nullptr, [&] { T(h)->use_graphs = on != 0; });
+}
+
+int suiri_batch_create(suiri_tank* const* tanks, int32_t n, suiri_batch** out) {
+  if (!out || !tanks || n <= 0) { g_err = "batch needs tanks"; return SUIRI_ERR_INVALID; }
+  *out = nullptr;
+  std::unique_ptr<suiri_batch> b(new suiri_batch());
+  const int rc = guard(nullptr, [&] {
+    std::vector<Tank*> v;
+    for (int i = 0; i < n; ++i) v.push_back(T(tanks[i]));
+    b->g.reset(new Group(v, nullptr));
+  });
+  if (rc != SUIRI_OK) return rc;
+  *out = b.release();
+  return SUIRI_OK;
+}
+
+int suiri_batch_destroy(suiri_batch* b) {
+  if (!b) return SUIRI_ERR_INVALID;
+  const int rc = guard(nullptr, [&] { b->g.reset(); });
+  delete b;
+  return rc;
+}
+
+int suiri_batch_substep(suiri_batch* b, double dt) {
+  return guard(b ? &b->err : nullptr, [&] {
+    if (!b || !b->g) throw Error(SUIRI_ERR_INVALID, "null batch");
+    if (!(dt > 0) || !std::isfinite(dt)) throw Error(SUIRI_ERR_INVALID, "dt must be positive");
+    b->g->substep(dt);
+  });
+}
+
+int suiri_batch_sync(suiri_batch* b) {
+  return guard(b ? &b->err : nullptr, [&] {
+    if (!b || !b->g) throw Error(SUIRI_ERR_INVALID, "null batch");
+    CK(cudaStreamSynchronize(b->g->stream));
+  });
+}
+
+int suiri_batch_tune(suiri_batch* b, int32_t particle_blocks_per_sm, int32_t sor_sweeps_per_launch) {
+  return guard(b ? &b->err : nullptr, [&] {
+    if (!b || !b->g) throw Error(SUIRI_ERR_INVALID, "null batch");
+    if (particle_blocks_per_sm < 1 || particle_blocks_per_sm > 32) throw Error(SUIRI_ERR_INVALID, "blocks per SM in 1..32");
+    if (sor_sweeps_per_launch < 1) throw Error(SUIRI_ERR_INVALID, "sweeps per launch >= 1");
+    Group& g = *b->g;
+    g.blocks_per_sm = particle_blocks_per_sm;
+    g.ctx.particle_blocks = particle_blocks_per_sm * g.sm_count;
+    g.drop_graph();
+  });
+}
+
+int suiri_batch_stream(suiri_batch* b, void** stream) {
+  return guard(b ? &b->err : nullptr, [&] {
+    if (!b || !b->g || !stream) throw Error(SUIRI_ERR_INVALID, "null batch or output");
+    *stream = (void*)b->g->stream;
+  });
+}
+
+int suiri_time_substeps(suiri_tank* h, double dt, int32_t steps, double* ms) {
+  return guard(h ? &h->err : nullptr, [&] {
+    Tank* t = T(h);
+    if (!ms || steps <= 0) throw Error(SUIRI_ERR_INVALID, "bad timing arguments");
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    t->substep(dt);                        // make sure GEOM and graph capture are outside the timed region
+    CK(cudaEventRecord(a, t->stream));
+    for (int i = 0; i < steps; ++i) t->substep(dt);
+    CK(cudaEventRecord(b, t->stream));
+    CK(cudaEventSynchronize(b));
+    float f = 0;
+    CK(cudaEventElapsedTime(&f, a, b));
+    *ms = f;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  });
+}
+
+int suiri_batch_time_substeps(suiri_batch* bt, double dt, int32_t steps, double* ms) {
+  return guard(bt ? &bt->err : nullptr, [&] {
+    if (!bt || !bt->g || !ms || steps <= 0) throw Error(SUIRI_ERR_INVALID, "bad timing arguments");
+    Group& g = *bt->g;
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    g.substep(dt);
+    CK(cudaEventRecord(a, g.stream));
+    for (int i = 0; i < steps; ++i) g.substep(dt);
+    CK(cudaEventRecord(b, g.stream));
+    CK(cudaEventSynchronize(b));
+    float f = 0;
+    CK(cudaEventElapsedTime(&f, a, b));
+    *ms = f;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  });
+}
+
+int suiri_profile(suiri_tank* h, int32_t on) {
+  return guard(h ? &h->err : nullptr, [&] { T(h)->solo->set_profile(on != 0); });
+}
+
+int suiri_sor_phase_ms(suiri_tank* h, double* ms) {
+  return guard(h ? &h->err : nullptr, [&] {
+    if (!ms) throw Error(SUIRI_ERR_INVALID, "null output");
+    *ms = T(h)->solo->sor_phase_ms();
+  });
+}
+
+int suiri_batch_profile(suiri_batch* b, int32_t on) {
+  return guard(b ? &b->err : nullptr, [&] {
+    if (!b || !b->g) throw Error(SUIRI_ERR_INVALID, "null batch");
+    b->g->set_profile(on != 0);
+  });
+}
+
+int suiri_batch_sor_phase_ms(suiri_batch* b, double* ms) {
+  return guard(b ? &b->err : nullptr, [&] {
+    if (!b || !b->g || !ms) throw Error(SUIRI_ERR_INVALID, "null batch or output");
+    *ms = b->g->sor_phase_ms();
+  });
+}
+
+int suiri_time_sor(suiri_tank* h, int32_t iters, double* ms) {
+  return guard(h ? &h->err : nullptr, [&] {
+    Tank* t = T(h);
+    if (!ms || iters <= 0) throw Error(SUIRI_ERR_INVALID, "bad timing arguments");
+    Group& g = *t->solo;
+    g.ensure_uploaded();
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    CK(cudaEventRecord(a, g.stream));
+    for (int it = 0; it < iters; ++it) {
+      launch_sor_sweep(g.ctx, 0, 0);
+      launch_sor_sweep(g.ctx, 1, 0);
+    }
+    CK(cudaEventRecord(b, g.stream));
+    CK(cudaEventSynchronize(b));
+    CK(cudaGetLastError());
+    float f = 0;
+    CK(cudaEventElapsedTime(&f, a, b));
+    *ms = f / (2.0 * iters);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,887 @@
+// Host engine: tank state on the device, batched groups, the sub-step and frame sequence, emission,
+// read-back and snapshots.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "sdf.cuh"
+
+namespace suiri {
+
+uint32_t hash_host(uint32_t x) {
+  x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+  return x;
+}
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    if (e == cudaErrorMemoryAllocation) throw Error(-3, std::string("CUDA out of memory in ") + what);
+    throw Error(-2, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+// ------------------------------------------------------------------------------------ small kernels
+__global__ void k_set_dt(TankDev* tanks, int n, double dt) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) tanks[t].dt = dt;
+}
+__global__ void k_set_emit(Counters* c, int n) { c->n_emit = n; }
+
+__device__ __forceinline__ uint32_t hash32(uint32_t x) {
+  x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+  return x;
+}
+__device__ __forceinline__ double rnd01(uint32_t& s) {
+  s = hash32(s);
+  return (double)(s >> 8) / 16777216.0;
+}
+
+// Emission record: shape 0 disc outlet (stream/shower), 1 sphere (drop/burst), 2 jittered lattice (water
+// block), 3 rain area — the records of src/js/55-emit.js:13-106, emitted as src/js/31-wgsl-sim2.js:262-315 does.
+struct EmitRec {
+  double a[4], b[4], c[4], d[4];
+  int shape, count, base;     // particles, first slot in E
+  uint32_t seed, first_id;
+  int pad;
+};
+
+__global__ void k_emit(TankDev T, const EmitRec* __restrict__ recs, int nrec, int total) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= total) return;
+  int r = 0, acc = 0;
+  for (int i = 0; i < nrec; ++i) {
+    if (q < acc + recs[i].count) { r = i; break; }
+    acc += recs[i].count;
+  }
+  const EmitRec& e = recs[r];
+  const int local = q - acc;
+  uint32_t s = hash32((uint32_t)local * 747796405u + e.seed * 2891336453u + 1u);
+  double p[3] = {0, 0, 0}, v[3] = {0, 0, 0};
+  double mark = 0.0;
+  bool alive = true;
+  if (e.shape == 0) {
+    const double rr = e.a[3] * sqrt(rnd01(s));
+    const double th = 6.283185307179586 * rnd01(s);
+    const double ct = cos(th), st = sin(th);
+    const double along = rnd01(s) * e.d[3];
+    for (int k = 0; k < 3; ++k) p[k] = e.a[k] + (e.c[k] * ct + e.d[k] * st) * rr + e.b[k] * along;
+    double dv[3] = {e.b[0], e.b[1], e.b[2]};
+    if (e.c[3] > 0.0) {
+      const double ca = 1.0 - rnd01(s) * (1.0 - cos(e.c[3]));
+      const double sa = sqrt(fmax(1.0 - ca * ca, 0.0));
+      const double ph = 6.283185307179586 * rnd01(s);
+      for (int k = 0; k < 3; ++k) dv[k] = e.b[k] * ca + (e.c[k] * cos(ph) + e.d[k] * sin(ph)) * sa;
+    }
+    const double j0 = rnd01(s) - 0.5, j1 = rnd01(s) - 0.5, j2 = rnd01(s) - 0.5;
+    v[0] = dv[0] * e.b[3] + j0 * (0.02 * e.b[3]);
+    v[1] = dv[1] * e.b[3] + j1 * (0.02 * e.b[3]);
+    v[2] = dv[2] * e.b[3] + j2 * (0.02 * e.b[3]);
+  } else if (e.shape == 1) {
+    double dd[3] = {rnd01(s) * 2 - 1 + 1e-4, rnd01(s) * 2 - 1 + 1e-4, rnd01(s) * 2 - 1 + 1e-4};
+    const double l = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
+    const double rad = e.a[3] * pow(rnd01(s), 1.0 / 3.0);
+    for (int k = 0; k < 3; ++k) { p[k] = e.a[k] + dd[k] / l * rad; v[k] = e.b[k]; }
+    mark = e.b[3];
+  } else if (e.shape == 2) {
+    const int nx = (int)e.b[0], ny = (int)e.b[1];
+    const int i = local % nx, j = (local / nx) % ny, k = local / (nx * ny);
+    const double ji[3] = {(rnd01(s) - 0.5) * 0.3, (rnd01(s) - 0.5) * 0.3, (rnd01(s) - 0.5) * 0.3};
+    p[0] = e.a[0] + (i + 0.5 + ji[0]) * e.a[3];
+    p[1] = e.a[1] + (j + 0.5 + ji[1]) * e.a[3];
+    p[2] = e.a[2] + (k + 0.5 + ji[2]) * e.a[3];
+    for (int c = 0; c < 3; ++c) v[c] = e.c[c];
+    if (e.b[3] > 0.5) {            // pouring into running water: skip cells at least half full
+      double g[3];
+      grid_pos(T, p[0], p[1], p[2], g[0], g[1], g[2]);
+      if (in_grid(T, g[0], g[1], g[2])) {
+        const int c = cell_idx(T, (int)g[0], (int)g[1], (int)g[2]);
+        if ((double)(T.off[c + 1] - T.off[c]) >= 0.5 * T.ppc) alive = false;
+      }
+    }
+  } else {
+    p[0] = e.a[0] + (rnd01(s) * 2 - 1) * e.a[3];
+    p[1] = e.a[1] - rnd01(s) * e.d[3];
+    p[2] = e.a[2] + (rnd01(s) * 2 - 1) * e.a[3];
+    for (int c = 0; c < 3; ++c) v[c] = e.b[c];
+    mark = 1.0;
+  }
+  if (alive && T.has_obst && tank_sdf(T, p[0], p[1], p[2]) < 0.0) alive = false;
+  const int flags = (mark > 0.5 ? kFlagAir : 0) | (alive ? 0 : kFlagDead);
+  const int slot = e.base + local;
+  T.pE[slot] = make_float4((float)p[0], (float)p[1], (float)p[2], (float)flags);
+  T.vE[slot] = make_float4((float)v[0], (float)v[1], (float)v[2], __uint_as_float(e.first_id + (uint32_t)local));
+}
+
+// Fixed-rate emitters, one block per tank, inside the captured sub-step: a disc outlet emits as the
+// stream source of src/js/31-wgsl-sim2.js:276-288, the rain area as :307-310. Ids of device-emitted
+// particles carry the top bit so they never meet host-assigned ids.
+__global__ void k_emit_fixed(const TankDev* __restrict__ tanks) {
+  const TankDev& T = tanks[blockIdx.x];
+  if (T.nemit == 0) return;
+  __shared__ int s_base, s_total, s_first[kMaxEmitters + 1];
+  __shared__ unsigned s_id;
+  Counters* c = T.ctr;
+  if (threadIdx.x == 0) {
+    const int base = c->n_emit;
+    long long room = (long long)T.cap - (c->n_live + c->n_emit) - 64;
+    room = min(room, (long long)T.emit_cap - c->n_emit);
+    int total = 0;
+    for (int e = 0; e < T.nemit; ++e) {
+      const double acc = c->emit_acc[e] + T.emitters[e].per_substep;
+      const double fl = floor(acc);
+      c->emit_acc[e] = acc - fl;
+      int n = (int)fl;
+      if (n > room - total) { n = (int)max(0LL, room - total); c->full = 1; }
+      s_first[e] = total;
+      total += n;
+    }
+    s_first[T.nemit] = total;
+    s_base = base;
+    s_total = total;
+    s_id = c->next_id;
+  }
+  __syncthreads();
+  const int frame = c->frame + 1;
+  for (int q = threadIdx.x; q < s_total; q += blockDim.x) {
+    int e = 0;
+    while (q >= s_first[e + 1]) ++e;
+    const EmitterDev& E = T.emitters[e];
+    const int local = q - s_first[e];
+    uint32_t s = hash32((uint32_t)local * 747796405u + hash32(T.seed * 2891336453u + (uint32_t)frame * 97u + (uint32_t)e) + 1u);
+    double p[3], v[3];
+    if (E.shape == 0) {
+      const double rr = E.radius * sqrt(rnd01(s));
+      const double th = 6.283185307179586 * rnd01(s);
+      const double ct = cos(th), st = sin(th);
+      const double along = rnd01(s) * (E.speed * T.dt);
+      const double j0 = rnd01(s) - 0.5, j1 = rnd01(s) - 0.5, j2 = rnd01(s) - 0.5;
+      for (int k = 0; k < 3; ++k) p[k] = E.pos[k] + (E.u[k] * ct + E.w[k] * st) * rr + E.dir[k] * along;
+      v[0] = E.dir[0] * E.speed + j0 * (0.02 * E.speed);
+      v[1] = E.dir[1] * E.speed + j1 * (0.02 * E.speed);
+      v[2] = E.dir[2] * E.speed + j2 * (0.02 * E.speed);
+    } else {
+      p[0] = E.pos[0] + (rnd01(s) * 2 - 1) * E.radius;
+      p[1] = E.pos[1] - rnd01(s) * (E.speed * T.dt);
+      p[2] = E.pos[2] + (rnd01(s) * 2 - 1) * E.radius;
+      v[0] = 0.0; v[1] = -E.speed; v[2] = 0.0;
+    }
+    const bool alive = !(T.has_obst && tank_sdf(T, p[0], p[1], p[2]) < 0.0);
+    const int flags = (E.airborne ? kFlagAir : 0) | (alive ? 0 : kFlagDead);
+    const int slot = s_base + q;
+    T.pE[slot] = make_float4((float)p[0], (float)p[1], (float)p[2], (float)flags);
+    T.vE[slot] = make_float4((float)v[0], (float)v[1], (float)v[2], __uint_as_float(0x80000000u | (s_id + (unsigned)q)));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    c->n_emit = s_base + s_total;
+    c->next_id = s_id + (unsigned)s_total;
+  }
+}
+
+// ------------------------------------------------------------------------------------ Tank
+Tank::Tank(const TankConfig& c) : cfg(c) {
+  if (cfg.nx < 2 || cfg.ny < 2 || cfg.nz < 2 || !(cfg.h > 0)) throw Error(-1, "grid must be at least 2×2×2 with h > 0");
+  if ((long long)cfg.nx * cfg.ny * cfg.nz > (1LL << 30)) throw Error(-1, "grid too large");
+  if (cfg.cap < 1) throw Error(-1, "capacity must be positive");
+  CK(cudaSetDevice(cfg.device));
+  CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  TankDev& D = d;
+  D.nx = cfg.nx; D.ny = cfg.ny; D.nz = cfg.nz; D.hx = (cfg.nx + 1) / 2;
+  D.sx = cfg.nx + 1; D.sxy = (cfg.nx + 1) * (cfg.ny + 1);
+  D.nnodes = (cfg.nx + 1) * (cfg.ny + 1) * (cfg.nz + 1);
+  D.ncells = cfg.nx * cfg.ny * cfg.nz;
+  D.nhalf = D.hx * cfg.ny * cfg.nz;
+  D.nyl = std::max(cfg.nyl, cfg.ny);
+  D.h = cfg.h; D.ox = cfg.origin[0]; D.oy = cfg.origin[1]; D.oz = cfg.origin[2];
+  D.rim = cfg.ny * cfg.h;
+  D.g = cfg.g; D.flip = cfg.flip; D.friction = cfg.friction; D.ppc = cfg.ppc; D.drift = cfg.drift; D.ww_rate = cfg.ww_rate;
+  D.dt = 1.0 / 60;
+  D.vp = pow(cfg.h / 2, 3);
+  D.drop_mass = 998.0 * pow(0.5 * cfg.h, 3.0);
+  D.omega = (float)cfg.omega;
+  D.iters = cfg.iters; D.whitewater = cfg.whitewater;
+  D.sdf_mode = cfg.sdf_mode;
+  D.seed = cfg.seed;
+  D.cap = (int)cfg.cap;
+  emit_cap = cfg.cap;
+  D.emit_cap = (int)emit_cap;
+  D.ww_cap = (int)std::max(1LL, cfg.ww_cap);
+  D.rx = std::max(0, cfg.rx); D.rz = std::max(0, cfg.rz);
+  const size_t nn = D.nnodes, nc = D.ncells, nh = D.nhalf, cap = cfg.cap;
+  D.pA = (float4*)alloc(cap * 16); D.vA = (float4*)alloc(cap * 16);
+  D.pE = (float4*)alloc(emit_cap * 16); D.vE = (float4*)alloc(emit_cap * 16);
+  D.pB = (float4*)alloc(cap * 16); D.vB = (float4*)alloc(cap * 16);
+  D.rank = (uint32_t*)alloc((cap + emit_cap) * 4);
+  D.cnt = (int*)alloc((nc + 1) * 4);
+  D.off = (int*)alloc((nc + 2) * 4);
+  D.acc = (long long*)alloc(6 * nn * 8);
+  D.vel = (float4*)alloc(nn * 16); D.velold = (float4*)alloc(nn * 16);
+  D.frac = (float4*)alloc(nn * 16); D.svel = (float4*)alloc(nn * 16);
+  D.fracd = (double*)alloc(3 * nn * 8); D.flux = (double*)alloc(3 * nn * 8);
+  D.pres = (float*)alloc(2 * nh * 4); D.rhs = (float*)alloc(2 * nh * 4); D.code = (uint32_t*)alloc(2 * nh * 4);
+  d_objs = (Obj*)alloc(kMaxObj * sizeof(Obj));
+  D.objs = d_objs;
+  D.ctr = (Counters*)alloc(sizeof(Counters));
+  D.wpos = (float4*)alloc(2 * (size_t)D.ww_cap * 16); D.wvel = (float4*)alloc(2 * (size_t)D.ww_cap * 16);
+  if (D.rx > 0) D.rsrc = (long long*)alloc((size_t)(D.rx + 1) * (D.rz + 1) * 8);
+  CK(cudaMallocHost(&h_ctr, sizeof(Counters)));
+  memset(h_ctr, 0, sizeof(Counters));
+  CK(cudaStreamSynchronize(stream));
+  solo = new Group({this}, stream);
+}
+
+Tank::~Tank() {
+  delete solo;
+  cudaSetDevice(cfg.device);
+  if (stream) cudaStreamSynchronize(stream);
+  for (void* p : dmem) cudaFree(p);
+  if (snap.p) { cudaFree(snap.p); cudaFree(snap.v); cudaFree(snap.wp); cudaFree(snap.wv); cudaFree(snap.pres); cudaFree(snap.ripple); }
+  free_ripple(*this);
+  if (h_ctr) cudaFreeHost(h_ctr);
+  if (h_stage_p) { cudaFreeHost(h_stage_p); cudaFreeHost(h_stage_v); }
+  if (stream) cudaStreamDestroy(stream);
+}
+
+void* Tank::alloc(size_t bytes) {
+  void* p = nullptr;
+  CK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+  dmem.push_back(p);
+  CK(cudaMemsetAsync(p, 0, std::max<size_t>(bytes, 16), stream));
+  return p;
+}
+
+void Tank::set_objects(const std::vector<Obj>& o) {
+  if (o.size() > (size_t)kMaxObj) throw Error(-1, "at most 64 obstacles and drains");
+  objs = o;
+  d.nobj = (int)objs.size();
+  d.has_obst = 0;
+  d.moving = 0;
+  for (const Obj& x : objs)
+    if (x.flag == 1) {
+      d.has_obst = 1;
+      for (int a = 0; a < 3; ++a)
+        if (x.lin[a] != 0.0 || x.ang[a] != 0.0) d.moving = 1;
+    }
+  if (d.sdf_mode == kSdfLattice && d_lattice) d.has_obst = 1;
+  if (!objs.empty()) CK(cudaMemcpyAsync(d_objs, objs.data(), objs.size() * sizeof(Obj), cudaMemcpyHostToDevice, stream));
+  CK(cudaStreamSynchronize(stream));
+  geom_dirty = true;
+  ++version;
+}
+
+void Tank::set_lattice(const double* sdf, const int* oid, int lx, int ly, int lz) {
+  if (lx != 2 * d.nx + 1 || lz != 2 * d.nz + 1 || ly < 2 * d.ny + 1 || (ly - 1) % 2)
+    throw Error(-1, "lattice must be (2nx+1) × (2nyl+1) × (2nz+1) with nyl >= ny");
+  d.nyl = (ly - 1) / 2;
+  const size_t n = (size_t)lx * ly * lz;
+  if (!d_lattice) { d_lattice = (double*)alloc(n * 8); d_oid = (int*)alloc(n * 4); }
+  CK(cudaMemcpyAsync(d_lattice, sdf, n * 8, cudaMemcpyHostToDevice, stream));
+  if (oid) CK(cudaMemcpyAsync(d_oid, oid, n * 4, cudaMemcpyHostToDevice, stream));
+  CK(cudaStreamSynchronize(stream));
+  d.lattice = d_lattice;
+  d.oid = oid ? d_oid : nullptr;
+  d.sdf_mode = kSdfLattice;
+  bool any = false;
+  for (const Obj& x : objs) any |= x.flag == 1;
+  d.has_obst = 1;
+  (void)any;
+  geom_dirty = true;
+  ++version;
+}
+
+void Tank::read_counters() {
+  CK(cudaMemcpyAsync(h_ctr, d.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  n_upper = h_ctr->n_live + h_ctr->n_emit;
+}
+
+void Tank::stage(const float4* p, const float4* v, long long n) {
+  if (n <= 0) return;
+  CK(cudaMemcpyAsync(d.pE + n_emit_host, p, n * 16, cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d.vE + n_emit_host, v, n * 16, cudaMemcpyHostToDevice, stream));
+  n_emit_host += n;
+  k_set_emit<<<1, 1, 0, stream>>>(d.ctr, (int)n_emit_host);
+  CK(cudaGetLastError());
+  n_upper += n;
+}
+
+void Tank::add_particles(const float* pos, const float* vel, const float* air, long long n, uint32_t* first) {
+  if (n < 0 || (n > 0 && !pos)) throw Error(-1, "add_particles: bad arrays");
+  if (first) *first = next_id;
+  if (n == 0) return;
+  long long room = std::min<long long>(cfg.cap - n_upper, emit_cap - n_emit_host);
+  if (n > room) {
+    read_counters();
+    room = std::min<long long>(cfg.cap - n_upper, emit_cap - n_emit_host);
+  }
+  long long take = std::max(0LL, std::min(n, room));
+  if ((size_t)take > stage_cap) {
+    if (h_stage_p) { CK(cudaStreamSynchronize(stream)); cudaFreeHost(h_stage_p); cudaFreeHost(h_stage_v); }
+    stage_cap = (size_t)take;
+    CK(cudaMallocHost(&h_stage_p, stage_cap * 16));
+    CK(cudaMallocHost(&h_stage_v, stage_cap * 16));
+  } else {
+    CK(cudaStreamSynchronize(stream));     // the staging buffer may still feed an earlier copy
+  }
+  for (long long i = 0; i < take; ++i) {
+    const float a = air ? air[i] : 0.f;
+    h_stage_p[i] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], a > 0.5f ? (float)kFlagAir : 0.f);
+    const float vx = vel ? vel[3 * i] : 0.f, vy = vel ? vel[3 * i + 1] : 0.f, vz = vel ? vel[3 * i + 2] : 0.f;
+    uint32_t id = next_id + (uint32_t)i;
+    float idf;
+    memcpy(&idf, &id, 4);
+    h_stage_v[i] = make_float4(vx, vy, vz, idf);
+  }
+  stage(h_stage_p, h_stage_v, take);
+  next_id += (uint32_t)take;
+  if (take < n) {
+    h_ctr->full = 1;
+    throw Error(-4, "particle capacity reached: " + std::to_string(take) + " of " + std::to_string(n) + " added");
+  }
+}
+
+namespace {
+void launch_emit(Tank& t, std::vector<EmitRec>& recs) {
+  if (recs.empty()) return;
+  int total = 0;
+  for (auto& r : recs) { r.base = (int)t.n_emit_host + total; total += r.count; }
+  EmitRec* d_recs = nullptr;
+  CK(cudaMallocAsync((void**)&d_recs, recs.size() * sizeof(EmitRec), t.stream));
+  CK(cudaMemcpyAsync(d_recs, recs.data(), recs.size() * sizeof(EmitRec), cudaMemcpyHostToDevice, t.stream));
+  k_emit<<<(total + 255) / 256, 256, 0, t.stream>>>(t.d, d_recs, (int)recs.size(), total);
+  CK(cudaGetLastError());
+  CK(cudaFreeAsync(d_recs, t.stream));
+  CK(cudaStreamSynchronize(t.stream));     // recs lives on the host stack
+  t.n_emit_host += total;
+  k_set_emit<<<1, 1, 0, t.stream>>>(t.d.ctr, (int)t.n_emit_host);
+  CK(cudaGetLastError());
+  t.n_upper += total;
+}
+
+// budget like writeEmits (src/js/50-sim.js:222-246): room = cap - count - 64
+int clip_to_room(Tank& t, std::vector<EmitRec>& recs) {
+  long long room = std::min<long long>(t.cfg.cap - t.n_upper - 64, t.emit_cap - t.n_emit_host);
+  bool full = false;
+  for (auto& r : recs) {
+    if (r.count > room) { r.count = (int)std::max(0LL, room); full = true; }
+    room -= r.count;
+  }
+  recs.erase(std::remove_if(recs.begin(), recs.end(), [](const EmitRec& r) { return r.count <= 0; }), recs.end());
+  if (full) t.h_ctr->full = 1;
+  return full;
+}
+}  // namespace
+
+void Tank::count_pass() {
+  solo->ensure_uploaded();
+  launch_begin_count(solo->ctx);
+  launch_bin(solo->ctx);
+  launch_scan(solo->ctx);
+  CK(cudaGetLastError());
+}
+
+void Tank::emit_block(const double lo_in[3], const double hi_in[3], bool fill) {
+  // blockEmits (src/js/55-emit.js:83-106) / emit_block (solver.py:317-343)
+  const double sp = d.h / 2;
+  double lo[3] = {lo_in[0], lo_in[1], lo_in[2]}, hi[3] = {hi_in[0], hi_in[1], hi_in[2]};
+  const double tlo[3] = {d.ox + sp * 0.5, 0.0005, d.oz + sp * 0.5};
+  const double thi[3] = {-d.ox - sp * 0.5, INFINITY, -d.oz - sp * 0.5};
+  if (lo[0] < thi[0] && hi[0] > tlo[0] && lo[2] < thi[2] && hi[2] > tlo[2]) {
+    for (int k : {0, 2}) { lo[k] = std::max(lo[k], tlo[k]); hi[k] = std::min(hi[k], thi[k]); }
+    lo[1] = std::max(lo[1], tlo[1]);
+  }
+  long long n[3];
+  for (int k = 0; k < 3; ++k) n[k] = (long long)std::max(0.0, floor((hi[k] - lo[k]) / sp));
+  const long long total = n[0] * n[1] * n[2];
+  if (total <= 0) return;
+  if (fill) count_pass();
+  EmitRec r{};
+  r.shape = 2;
+  for (int k = 0; k < 3; ++k) r.a[k] = lo[k] + ((hi[k] - lo[k]) - n[k] * sp) / 2;
+  r.a[3] = sp;
+  r.b[0] = (double)n[0]; r.b[1] = (double)n[1]; r.b[2] = (double)n[2]; r.b[3] = fill ? 1.0 : 0.0;
+  r.count = (int)std::min<long long>(total, 1LL << 30);
+  r.seed = hash_host(cfg.seed * 2654435761u + next_id * 40503u + 7u);
+  r.first_id = next_id;
+  std::vector<EmitRec> recs{r};
+  const bool full = clip_to_room(*this, recs);
+  if (!recs.empty()) {
+    next_id += (uint32_t)recs[0].count;
+    launch_emit(*this, recs);
+  }
+  if (full) throw Error(-4, "particle capacity reached while filling a water block");
+}
+
+void Tank::source_emits(double dt) {
+  // sourceEmits (src/js/55-emit.js:13-69): per source an accumulator of volume, drop timers, bursts, rain
+  if (scene.sources.empty()) return;
+  const double Vp = d.vp, DEG = M_PI / 180.0, RAIN_SPEED = 6.5;
+  std::vector<EmitRec> recs;
+  auto clampd = [](double x, double a, double b) { return std::min(std::max(x, a), b); };
+  auto jround = [](double x) { return floor(x + 0.5); };     // JavaScript Math.round
+  for (const SourceItem& src : scene.sources) {
+    if (!src.enabled) continue;
+    std::vector<double>& st = emit_state[src.id];
+    if (st.empty()) st.assign(4, 0.0);       // acc, liters, timer, fired
+    if (src.total > 0 && st[1] >= src.total) continue;
+    const double p = src.pitch * DEG, y = src.yaw * DEG;
+    const double dir[3] = {cos(p) * sin(y), sin(p), cos(p) * cos(y)};
+    const double ref[3] = {fabs(dir[1]) < 0.95 ? 0.0 : 1.0, fabs(dir[1]) < 0.95 ? 1.0 : 0.0, 0.0};
+    double u[3] = {dir[1] * ref[2] - dir[2] * ref[1], dir[2] * ref[0] - dir[0] * ref[2], dir[0] * ref[1] - dir[1] * ref[0]};
+    const double ul = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    for (double& c : u) c /= ul;
+    const double w[3] = {dir[1] * u[2] - dir[2] * u[1], dir[2] * u[0] - dir[0] * u[2], dir[0] * u[1] - dir[1] * u[0]};
+    EmitRec r{};
+    r.seed = hash_host(cfg.seed * 2654435761u + (uint32_t)src.id * 97u + (uint32_t)(h_ctr->frame + 1) * 7919u + (uint32_t)recs.size());
+    r.first_id = 0;
+    if (src.mode == "stream" || src.mode == "shower") {
+      const double Q = src.flow / 60000;
+      st[0] += (Q * dt) / Vp;
+      const double n = floor(st[0]);
+      st[0] -= n;
+      if (n <= 0) continue;
+      const bool shower = src.mode == "shower";
+      const double noz = sqrt(4 * Q / (M_PI * std::max(src.speed, 0.05)));
+      const double rr = shower ? std::max(noz / 2, 0.022) : std::max(noz / 2, 0.0005);
+      const double spread = shower ? clampd(src.spread, 0, 80) * DEG : 0;
+      r.shape = 0;
+      for (int k = 0; k < 3; ++k) { r.a[k] = src.pos[k] + dir[k] * 0.002; r.b[k] = dir[k]; r.c[k] = u[k]; r.d[k] = w[k]; }
+      r.a[3] = rr; r.b[3] = src.speed; r.c[3] = spread; r.d[3] = src.speed * dt;
+      r.count = (int)n;
+      st[1] += n * Vp * 1000;
+    } else if (src.mode == "drops") {
+      st[2] -= dt;
+      if (st[2] > 0) continue;
+      st[2] += 1 / clampd(src.drop_rate, 0.05, 60);
+      if (st[2] < 0) st[2] = 0;
+      const double dd = clampd(src.drop_d, 1, 40) / 1000;
+      const double V = M_PI / 6 * dd * dd * dd;
+      const double n = std::max(1.0, jround(V / Vp));
+      const double R = std::max(dd / 2, cbrt((3 * n * Vp) / (4 * M_PI)) * 0.9);
+      r.shape = 1;
+      for (int k = 0; k < 3; ++k) { r.a[k] = src.pos[k] + dir[k] * (R + 0.002); r.b[k] = dir[k] * src.speed; }
+      r.a[3] = n == 1 ? 0 : R; r.b[3] = n <= 8 ? 1 : 0;
+      r.count = (int)n;
+      st[1] += n * Vp * 1000;
+    } else if (src.mode == "burst") {
+      if (st[3] != 0) {
+        if (!(src.burst_every > 0)) continue;
+        st[2] -= dt;
+        if (st[2] > 0) continue;
+      }
+      st[3] = 1;
+      st[2] = src.burst_every > 0 ? src.burst_every : 0;
+      const double V = clampd(src.burst, 0.01, 50) / 1000;
+      const double n = std::max(1.0, jround(V / Vp));
+      const double R = cbrt((3 * V) / (4 * M_PI));
+      r.shape = 1;
+      for (int k = 0; k < 3; ++k) { r.a[k] = src.pos[k] + dir[k] * (R + 0.004); r.b[k] = dir[k] * src.speed; }
+      r.a[3] = R; r.b[3] = 0;
+      r.count = (int)n;
+      st[1] += n * Vp * 1000;
+    } else if (src.mode == "rain") {
+      const double side = clampd(src.rain_size, 0.05, 2);
+      const double flux = (clampd(src.rain_rate, 1, 500) / 3.6e6) * side * side;
+      st[0] += (flux * dt) / Vp;
+      const double n = floor(st[0]);
+      st[0] -= n;
+      if (n <= 0) continue;
+      r.shape = 3;
+      for (int k = 0; k < 3; ++k) r.a[k] = src.pos[k];
+      r.a[3] = side / 2;
+      r.b[0] = 0; r.b[1] = -RAIN_SPEED; r.b[2] = 0;
+      r.d[3] = RAIN_SPEED * dt;
+      r.count = (int)n;
+      st[1] += n * Vp * 1000;
+    } else {
+      continue;
+    }
+    recs.push_back(r);
+  }
+  if (recs.empty()) return;
+  clip_to_room(*this, recs);
+  for (EmitRec& r : recs) { r.first_id = next_id; next_id += (uint32_t)r.count; }
+  launch_emit(*this, recs);
+}
+
+void Tank::clear() {
+  // clearWater (src/js/50-sim.js:365-373)
+  CK(cudaStreamSynchronize(stream));
+  CK(cudaMemsetAsync(d.ctr, 0, sizeof(Counters), stream));
+  CK(cudaMemsetAsync(d.pres, 0, 2 * (size_t)d.nhalf * 4, stream));
+  if (d.rsrc) CK(cudaMemsetAsync(d.rsrc, 0, (size_t)(d.rx + 1) * (d.rz + 1) * 8, stream));
+  clear_ripple(*this);
+  CK(cudaStreamSynchronize(stream));
+  memset(h_ctr, 0, sizeof(Counters));
+  n_emit_host = 0; n_upper = 0; time = 0; vmax = 1.0;
+  emit_state.clear();
+}
+
+void Tank::reset() {
+  // restartWater (src/js/90-main.js:15-19): clear, objects again, refill the water blocks
+  clear();
+  for (const WaterBlock& b : scene.blocks) emit_block(b.lo, b.hi, false);
+}
+
+void Tank::substep(double dt) {
+  solo->use_graphs = use_graphs;
+  solo->substep(dt);
+}
+
+int Tank::step(double frame_dt) {
+  if (!(frame_dt > 0)) return 0;
+  read_counters();
+  if (h_ctr->vmax_bits64 != 0ull) {
+    const unsigned long long b = h_ctr->vmax_bits64 - 1ull;
+    double v;
+    memcpy(&v, &b, 8);
+    vmax = v;
+  }
+  const double vm = std::max(vmax, 0.4);
+  const int n = (int)std::min(std::max(ceil(frame_dt / (1.4 * d.h / vm)), 1.0), 6.0);
+  const double dt = frame_dt / n;
+  for (int s = 0; s < n; ++s) {
+    source_emits(dt);
+    substep(dt);
+  }
+  count_pass();
+  if (d.whitewater) launch_whitewater(solo->ctx, frame_dt);
+  ripple_frame(*this, frame_dt);
+  CK(cudaGetLastError());
+  return n;
+}
+
+long long Tank::read_particles(float* pos4, float* vel4, long long cap) {
+  read_counters();
+  const long long nl = h_ctr->n_live, ne = h_ctr->n_emit, tot = nl + ne;
+  std::vector<float4> P(tot), V(tot);
+  if (nl) {
+    CK(cudaMemcpyAsync(P.data(), d.pA, nl * 16, cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(V.data(), d.vA, nl * 16, cudaMemcpyDeviceToHost, stream));
+  }
+  if (ne) {
+    CK(cudaMemcpyAsync(P.data() + nl, d.pE, ne * 16, cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(V.data() + nl, d.vE, ne * 16, cudaMemcpyDeviceToHost, stream));
+  }
+  CK(cudaStreamSynchronize(stream));
+  long long k = 0;
+  for (long long i = 0; i < tot; ++i) {
+    const int fl = (int)P[i].w;
+    if (fl & kFlagDead) continue;
+    if (k < cap) {
+      if (pos4) { pos4[4 * k] = P[i].x; pos4[4 * k + 1] = P[i].y; pos4[4 * k + 2] = P[i].z; pos4[4 * k + 3] = (fl & kFlagAir) ? 1.f : 0.f; }
+      if (vel4) { vel4[4 * k] = V[i].x; vel4[4 * k + 1] = V[i].y; vel4[4 * k + 2] = V[i].z; vel4[4 * k + 3] = V[i].w; }
+    }
+    ++k;
+  }
+  return k;
+}
+
+long long Tank::read_whitewater(float* pos4, float* vel4, long long cap) {
+  read_counters();
+  const long long n = std::min<long long>(h_ctr->ww_count, d.ww_cap);
+  const size_t half = (h_ctr->ww_cur & 1) ? (size_t)d.ww_cap : 0;
+  const long long k = std::min(n, cap);
+  if (k > 0) {
+    if (pos4) CK(cudaMemcpyAsync(pos4, d.wpos + half, k * 16, cudaMemcpyDeviceToHost, stream));
+    if (vel4) CK(cudaMemcpyAsync(vel4, d.wvel + half, k * 16, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+  return n;
+}
+
+void Tank::read_grid(int field, void* out, size_t bytes) {
+  const size_t nn = d.nnodes, nc = d.ncells;
+  auto need = [&](size_t b) { if (bytes < b) throw Error(-1, "read_grid: output buffer too small (" + std::to_string(b) + " bytes needed)"); };
+  CK(cudaStreamSynchronize(stream));
+  if (field == 0) {
+    need(nc * 4);
+    std::vector<int> off(nc + 2);
+    CK(cudaMemcpy(off.data(), d.off, (nc + 2) * 4, cudaMemcpyDeviceToHost));
+    int* o = (int*)out;
+    for (size_t c = 0; c < nc; ++c) o[c] = off[c + 1] - off[c];
+  } else if (field >= 1 && field <= 4) {
+    const float4* src = field == 1 ? d.frac : (field == 2 ? d.vel : d.velold);
+    std::vector<float4> v(nn);
+    CK(cudaMemcpy(v.data(), src, nn * 16, cudaMemcpyDeviceToHost));
+    if (field == 4) {
+      need(3 * nn);
+      uint8_t* o = (uint8_t*)out;
+      for (size_t n = 0; n < nn; ++n) {
+        const int m = (int)v[n].w;
+        for (int a = 0; a < 3; ++a) o[a * nn + n] = (m >> a) & 1;
+      }
+    } else {
+      need(3 * nn * 4);
+      float* o = (float*)out;
+      for (size_t n = 0; n < nn; ++n) { o[n] = v[n].x; o[nn + n] = v[n].y; o[2 * nn + n] = v[n].z; }
+    }
+  } else if (field == 5 || field == 6) {
+    need(nc * 4);
+    std::vector<float> h(2 * (size_t)d.nhalf);
+    CK(cudaMemcpy(h.data(), field == 5 ? d.pres : d.rhs, h.size() * 4, cudaMemcpyDeviceToHost));
+    float* o = (float*)out;
+    for (int k = 0; k < d.nz; ++k)
+      for (int j = 0; j < d.ny; ++j)
+        for (int i = 0; i < d.nx; ++i) {
+          const size_t c = i + (size_t)d.nx * (j + (size_t)d.ny * k);
+          const size_t s = (size_t)((i + j + k) & 1) * d.nhalf + (i >> 1) + (size_t)d.hx * (j + (size_t)d.ny * k);
+          o[c] = h[s];
+        }
+  } else {
+    read_ripple_field(*this, field, out, bytes);
+  }
+}
+
+int Tank::snapshot() {
+  // saveWater (src/js/50-sim.js:111-125)
+  read_counters();
+  const size_t cap = cfg.cap;
+  if (!snap.p) {
+    CK(cudaMalloc(&snap.p, cap * 16)); CK(cudaMalloc(&snap.v, cap * 16));
+    CK(cudaMalloc(&snap.wp, 2 * (size_t)d.ww_cap * 16)); CK(cudaMalloc(&snap.wv, 2 * (size_t)d.ww_cap * 16));
+    CK(cudaMalloc(&snap.pres, 2 * (size_t)d.nhalf * 4));
+    snap.ripple_bytes = ripple_state_bytes(*this);
+    if (snap.ripple_bytes) CK(cudaMalloc(&snap.ripple, snap.ripple_bytes));
+  }
+  // pending emissions are kept by folding them into the copy: copy A then E behind it
+  const long long nl = h_ctr->n_live, ne = h_ctr->n_emit;
+  if (nl + ne > (long long)cap) throw Error(-4, "snapshot: more particles than capacity");
+  CK(cudaMemcpyAsync(snap.p, d.pA, nl * 16, cudaMemcpyDeviceToDevice, stream));
+  CK(cudaMemcpyAsync(snap.v, d.vA, nl * 16, cudaMemcpyDeviceToDevice, stream));
+  CK(cudaMemcpyAsync(snap.p + nl, d.pE, ne * 16, cudaMemcpyDeviceToDevice, stream));
+  CK(cudaMemcpyAsync(snap.v + nl, d.vE, ne * 16, cudaMemcpyDeviceToDevice, stream));
+  CK(cudaMemcpyAsync(snap.wp, d.wpos, 2 * (size_t)d.ww_cap * 16, cudaMemcpyDeviceToDevice, stream));
+  CK(cudaMemcpyAsync(snap.wv, d.wvel, 2 * (size_t)d.ww_cap * 16, cudaMemcpyDeviceToDevice, stream));
+  CK(cudaMemcpyAsync(snap.pres, d.pres, 2 * (size_t)d.nhalf * 4, cudaMemcpyDeviceToDevice, stream));
+  if (snap.ripple_bytes) copy_ripple_state(*this, snap.ripple, true);
+  CK(cudaStreamSynchronize(stream));
+  snap.ctr = *h_ctr;
+  snap.ctr.n_live = (int)(nl + ne);
+  snap.ctr.n_emit = 0;
+  snap.n = nl + ne;
+  snap.time = time; snap.vmax = vmax; snap.next_id = next_id;
+  snap.emit_state = emit_state;
+  static int serial = 0;
+  snap.id = ++serial;
+  snap.valid = true;
+  return snap.id;
+}
+
+void Tank::restore(int id) {
+  // restoreWater (src/js/50-sim.js:127-141): only the latest copy, once
+  if (!snap.valid || snap.id != id) throw Error(-6, "no water copy with that id");
+  CK(cudaStreamSynchronize(stream));
+  CK(cudaMemcpyAsync(d.pA, snap.p, snap.n * 16, cudaMemcpyDeviceToDevice, stream));
+  CK(cudaMemcpyAsync(d.vA, snap.v, snap.n * 16, cudaMemcpyDeviceToDevice, stream));
+  CK(cudaMemcpyAsync(d.wpos, snap.wp, 2 * (size_t)d.ww_cap * 16, cudaMemcpyDeviceToDevice, stream));
+  CK(cudaMemcpyAsync(d.wvel, snap.wv, 2 * (size_t)d.ww_cap * 16, cudaMemcpyDeviceToDevice, stream));
+  CK(cudaMemcpyAsync(d.pres, snap.pres, 2 * (size_t)d.nhalf * 4, cudaMemcpyDeviceToDevice, stream));
+  if (snap.ripple_bytes) copy_ripple_state(*this, snap.ripple, false);
+  *h_ctr = snap.ctr;
+  CK(cudaMemcpyAsync(d.ctr, h_ctr, sizeof(Counters), cudaMemcpyHostToDevice, stream));
+  CK(cudaStreamSynchronize(stream));
+  n_emit_host = 0; n_upper = snap.n;
+  time = snap.time; vmax = snap.vmax; next_id = snap.next_id;
+  emit_state = snap.emit_state;
+  snap.valid = false;
+}
+
+// ------------------------------------------------------------------------------------ Group
+namespace {
+int blocks_for(int fam, const TankDev& D) {
+  switch (fam) {
+    case kFamNodes: return (D.nnodes + kThreads - 1) / kThreads;
+    case kFamCells: return (D.ncells + kThreads - 1) / kThreads;
+    case kFamHalf: return (D.nhalf + kThreads - 1) / kThreads;
+    case kFamBricks: return ((D.nx + kBrick - 1) / kBrick) * ((D.ny + kBrick - 1) / kBrick) * ((D.nz + kBrick - 1) / kBrick);
+    case kFamScan: return (D.ncells + 1 + kScanTile - 1) / kScanTile;
+  }
+  return 0;
+}
+}  // namespace
+
+Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
+  if (tanks.empty()) throw Error(-1, "a batch needs at least one tank");
+  device = tanks[0]->cfg.device;
+  for (Tank* x : tanks)
+    if (x->cfg.device != device) throw Error(-1, "all tanks of a batch must be on one device");
+  CK(cudaSetDevice(device));
+  if (s) { stream = s; } else { CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)); own_stream = true; }
+  CK(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device));
+  const int n = (int)tanks.size();
+  CK(cudaMalloc(&d_tanks, n * sizeof(TankDev)));
+  CK(cudaMallocHost(&h_tanks, n * sizeof(TankDev)));
+  CK(cudaMalloc(&d_bpfx, kFamCount * (n + 1) * sizeof(int)));
+  CK(cudaMalloc(&d_ppfx, 2 * (n + 1) * sizeof(int)));
+  CK(cudaMemsetAsync(d_ppfx, 0, 2 * (n + 1) * sizeof(int), stream));
+  std::vector<int> pf(kFamCount * (n + 1));
+  for (int f = 0; f < kFamCount; ++f) {
+    int acc = 0;
+    for (int i = 0; i < n; ++i) { pf[f * (n + 1) + i] = acc; acc += blocks_for(f, tanks[i]->d); }
+    pf[f * (n + 1) + n] = acc;
+    ctx.nblocks[f] = acc;
+    ctx.bpfx[f] = d_bpfx + f * (n + 1);
+  }
+  CK(cudaMalloc(&d_bsum, std::max(1, ctx.nblocks[kFamScan]) * sizeof(long long)));
+  CK(cudaMemcpyAsync(d_bpfx, pf.data(), pf.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+  CK(cudaStreamSynchronize(stream));
+  ctx.stream = stream;
+  ctx.tanks = d_tanks;
+  ctx.ntanks = n;
+  ctx.ppfx_in = d_ppfx;
+  ctx.ppfx_sorted = d_ppfx + (n + 1);
+  ctx.scan_bsum = d_bsum;
+  ctx.particle_blocks = blocks_per_sm * sm_count;
+  uploaded.assign(n, 0);
+}
+
+Group::~Group() {
+  cudaSetDevice(device);
+  cudaStreamSynchronize(stream);
+  drop_graph();
+  if (ev_sor[0]) { cudaEventDestroy(ev_sor[0]); cudaEventDestroy(ev_sor[1]); }
+  cudaFree(d_tanks); cudaFreeHost(h_tanks); cudaFree(d_bpfx); cudaFree(d_ppfx); cudaFree(d_bsum);
+  if (own_stream) cudaStreamDestroy(stream);
+}
+
+void Group::set_profile(bool on) {
+  if (on == profile) return;
+  if (on && !ev_sor[0]) {
+    CK(cudaEventCreate(&ev_sor[0]));
+    CK(cudaEventCreate(&ev_sor[1]));
+  }
+  profile = on;
+  CK(cudaStreamSynchronize(stream));
+  drop_graph();
+}
+
+double Group::sor_phase_ms() {
+  if (!profile) throw Error(-6, "profiling is off");
+  CK(cudaEventSynchronize(ev_sor[1]));
+  float f = 0;
+  CK(cudaEventElapsedTime(&f, ev_sor[0], ev_sor[1]));
+  return f;
+}
+
+void Group::drop_graph() {
+  if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+  if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+}
+
+void Group::ensure_uploaded() {
+  bool stale = false;
+  for (size_t i = 0; i < tanks.size(); ++i) stale |= uploaded[i] != tanks[i]->version;
+  if (!stale) return;
+  CK(cudaStreamSynchronize(stream));
+  int mi = 0;
+  for (size_t i = 0; i < tanks.size(); ++i) {
+    h_tanks[i] = tanks[i]->d;
+    uploaded[i] = tanks[i]->version;
+    mi = std::max(mi, tanks[i]->d.iters);
+  }
+  CK(cudaMemcpyAsync(d_tanks, h_tanks, tanks.size() * sizeof(TankDev), cudaMemcpyHostToDevice, stream));
+  CK(cudaStreamSynchronize(stream));
+  bool em = false;
+  for (Tank* t : tanks) em |= t->d.nemit > 0;
+  if (mi != max_iters || em != graph_emitters) { max_iters = mi; graph_emitters = em; drop_graph(); }
+}
+
+void Tank::set_emitters(const std::vector<EmitterDev>& e) {
+  if (e.size() > (size_t)kMaxEmitters) throw Error(-1, "at most 8 fixed emitters");
+  if (!d_emitters) d_emitters = (EmitterDev*)alloc(kMaxEmitters * sizeof(EmitterDev));
+  CK(cudaStreamSynchronize(stream));
+  if (!e.empty()) CK(cudaMemcpyAsync(d_emitters, e.data(), e.size() * sizeof(EmitterDev), cudaMemcpyHostToDevice, stream));
+  CK(cudaStreamSynchronize(stream));
+  d.emitters = d_emitters;
+  d.nemit = (int)e.size();
+  emit_per_substep = 0;
+  for (const auto& x : e) emit_per_substep += x.per_substep;
+  ++version;
+}
+
+void Group::set_dt(double dt) {
+  const int n = (int)tanks.size();
+  k_set_dt<<<(n + 127) / 128, 128, 0, stream>>>(d_tanks, n, dt);
+  CK(cudaGetLastError());
+}
+
+void Group::enqueue_body() {
+  bool emitters = false;
+  for (Tank* t : tanks) emitters |= t->d.nemit > 0;
+  if (emitters) k_emit_fixed<<<(int)tanks.size(), 128, 0, stream>>>(d_tanks);
+  launch_begin_substep(ctx);
+  launch_bin(ctx);
+  launch_scan(ctx);
+  launch_scatter(ctx);
+  launch_sorted_prefix(ctx);
+  launch_p2g(ctx);
+  launch_grid_nodes(ctx);
+  launch_grid_cells(ctx);
+  // inside a capture an event record must be an external event node to be replayed with the graph
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (profile) CK(cudaStreamIsCapturing(stream, &cap));
+  const unsigned evflags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
+  if (profile) CK(cudaEventRecordWithFlags(ev_sor[0], stream, evflags));
+  for (int it = 0; it < max_iters; ++it) {
+    launch_sor_sweep(ctx, 0, it);
+    launch_sor_sweep(ctx, 1, it);
+  }
+  if (profile) CK(cudaEventRecordWithFlags(ev_sor[1], stream, evflags));
+  launch_project(ctx);
+  launch_g2p(ctx);
+}
+
+void Group::substep(double dt) {
+  CK(cudaSetDevice(device));
+  // particle staging of every tank goes through its own stream; order it before this one
+  for (Tank* t : tanks)
+    if (t->stream != stream) {
+      cudaEvent_t e;
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      CK(cudaEventRecord(e, t->stream));
+      CK(cudaStreamWaitEvent(stream, e, 0));
+      CK(cudaEventDestroy(e));
+    }
+  ensure_uploaded();
+  bool geom = false;
+  for (Tank* t : tanks) geom |= t->geom_dirty;
+  if (geom) {
+    launch_geom(ctx);
+    CK(cudaGetLastError());
+    for (Tank* t : tanks) t->geom_dirty = false;
+  }
+  set_dt(dt);
+  if (use_graphs) {
+    if (!exec) {
+      CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      enqueue_body();
+      cudaError_t e = cudaStreamEndCapture(stream, &graph);
+      CK(e);
+      CK(cudaGetLastError());
+      CK(cudaGraphInstantiate(&exec, graph, 0));
+    }
+    CK(cudaGraphLaunch(exec, stream));
+  } else {
+    enqueue_body();
+    CK(cudaGetLastError());
+  }
+  for (Tank* t : tanks) {
+    t->time += dt;
+    t->n_emit_host = 0;
+    t->n_upper += (long long)ceil(t->emit_per_substep);
+  }
+  // later work on a tank's own stream (reads, emission) must follow this sub-step
+  for (Tank* t : tanks)
+    if (t->stream != stream) {
+      cudaEvent_t e;
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      CK(cudaEventRecord(e, stream));
+      CK(cudaStreamWaitEvent(t->stream, e, 0));
+      CK(cudaEventDestroy(e));
+    }
+}
+
+}  // namespace suiri

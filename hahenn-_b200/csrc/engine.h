@@ -1,0 +1,150 @@
+// Host-side engine: tanks (device state of one scene), groups (tanks stepped by shared batched launches)
+// and the sub-step / frame sequence. The C ABI (capi.cpp) is a thin layer over this.
+#pragma once
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "launch.cuh"
+#include "scene.h"
+
+namespace suiri {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t e, const char* what);
+#define CK(x) ::suiri::cuda_check((x), #x)
+
+struct Group;
+struct Tank;
+
+// ripple layer and top-view height map (ripple.cu)
+size_t ripple_state_bytes(Tank& t);
+void clear_ripple(Tank& t);
+void ripple_frame(Tank& t, double frame_dt);
+void read_ripple_field(Tank& t, int field, void* out, size_t bytes);
+void copy_ripple_state(Tank& t, void* dst_or_src, bool save);
+void free_ripple(Tank& t);
+
+uint32_t hash_host(uint32_t x);
+
+struct TankConfig {
+  int nx = 0, ny = 0, nz = 0, nyl = 0;
+  double h = 0, origin[3] = {0, 0, 0};
+  double flip = 0.96, omega = 1.6, g = 9.81, friction = 0.03, ppc = 8.0, drift = 6.0, ww_rate = 7.0;
+  int iters = 40, whitewater = 1;
+  long long cap = 320000, ww_cap = 140000;
+  int rx = 256, rz = 256, wmap = 256;
+  int sdf_mode = kSdfAnalytic, device = 0;
+  uint32_t seed = 1;
+};
+
+struct PrevXf { double pos[3]; double R[9]; };
+
+struct Snapshot {
+  int id = 0;
+  bool valid = false;
+  float4 *p = nullptr, *v = nullptr, *wp = nullptr, *wv = nullptr;
+  float* pres = nullptr;
+  void* ripple = nullptr;
+  size_t ripple_bytes = 0;
+  Counters ctr{};
+  long long n = 0;
+  double time = 0, vmax = 1;
+  uint32_t next_id = 0;
+  std::map<int, std::vector<double>> emit_state;
+};
+
+struct Tank {
+  TankConfig cfg;
+  TankDev d{};                    // host image of the device descriptor
+  Counters* h_ctr = nullptr;      // pinned mirror for reads
+  cudaStream_t stream = nullptr;
+  std::vector<void*> dmem;        // device allocations owned by the tank
+  Obj* d_objs = nullptr;
+  double* d_lattice = nullptr;
+  int* d_oid = nullptr;
+  Scene scene;                    // water blocks and sources of the scene (reset, step)
+  std::vector<Obj> objs;
+  std::map<int, PrevXf> prev_xf;
+  std::map<int, std::vector<double>> emit_state;   // per source: acc, liters, timer, fired
+  bool geom_dirty = true;
+  int version = 1;                // bumps when the descriptor changes
+  double time = 0, vmax = 1.0;
+  uint32_t next_id = 0;
+  long long n_emit_host = 0;      // particles staged in E for the next sub-step
+  long long n_upper = 0;          // upper bound of live particles (exact after a stats read)
+  float4 *h_stage_p = nullptr, *h_stage_v = nullptr;
+  size_t stage_cap = 0;
+  std::string err;
+  Group* solo = nullptr;
+  bool use_graphs = true;
+  void* ripple = nullptr;          // ripple.cu state
+  Snapshot snap;
+  long long emit_cap = 0;
+  EmitterDev* d_emitters = nullptr;
+  double emit_per_substep = 0;    // fixed emitters, particles per sub-step (host bound tracking)
+
+  void set_emitters(const std::vector<EmitterDev>& e);
+
+  explicit Tank(const TankConfig& c);
+  ~Tank();
+  void* alloc(size_t bytes);
+  void upload_objects();
+  void set_objects(const std::vector<Obj>& o);
+  void set_lattice(const double* sdf, const int* oid, int lx, int ly, int lz);
+  void read_counters();           // synchronous
+  void add_particles(const float* pos, const float* vel, const float* air, long long n, uint32_t* first);
+  void stage(const float4* p, const float4* v, long long n);
+  void emit_block(const double lo[3], const double hi[3], bool fill);
+  void clear();
+  void reset();
+  void substep(double dt);
+  int step(double frame_dt);
+  void count_pass();
+  void source_emits(double dt);
+  long long read_particles(float* pos4, float* vel4, long long cap);
+  long long read_whitewater(float* pos4, float* vel4, long long cap);
+  void read_grid(int field, void* out, size_t bytes);
+  int snapshot();
+  void restore(int id);
+};
+
+struct Group {
+  std::vector<Tank*> tanks;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  TankDev* d_tanks = nullptr;
+  TankDev* h_tanks = nullptr;     // pinned
+  int* d_bpfx = nullptr;
+  int* d_ppfx = nullptr;          // [0, n+1) in, [n+1, 2n+2) sorted
+  long long* d_bsum = nullptr;
+  LaunchCtx ctx{};
+  std::vector<int> uploaded;      // tank versions last uploaded
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int max_iters = 0;
+  bool graph_emitters = false;
+  bool profile = false;           // record events around the SOR phase (inside the graph too)
+  cudaEvent_t ev_sor[2] = {nullptr, nullptr};
+  int blocks_per_sm = 4;
+  void set_profile(bool on);
+  double sor_phase_ms();          // SOR phase of the last sub-step (waits for it)
+  bool use_graphs = true;
+  int sm_count = 148;
+
+  Group(const std::vector<Tank*>& t, cudaStream_t s);
+  ~Group();
+  void ensure_uploaded();
+  void set_dt(double dt);
+  void enqueue_body();            // the sub-step without GEOM
+  void substep(double dt);
+  void drop_graph();
+};
+
+}  // namespace suiri

@@ -1,0 +1,384 @@
+// Grid-to-particle update and the whitewater advance.
+//
+// k_g2p walks the particles in cell order (B) and writes the new state back to A at the same slot:
+// FLIP/PIC blend over valid faces, explicit Euler advection, obstacle collision with friction, the glass
+// walls and floor, drains, the free-flight mark of sub-grid drops, their merging with the pool (ripple
+// impulse + crown splash at K = We·Oh^-0.4) and whitewater spawning.
+// Reference: blender_addon/suiri_lab/solver.py:527-673 and src/js/31-wgsl-sim2.js:9-251. Positions,
+// weights and velocities are float64 inside the kernel, stored as float32.
+//
+// Spawning randomness is the reference WGSL's integer hash (src/js/30-wgsl-sim.js:36-37) seeded by the
+// particle's carried id and the sub-step number, so it does not depend on particle order.
+#include "launch.cuh"
+#include "sdf.cuh"
+
+namespace suiri {
+
+__device__ __forceinline__ uint32_t hash_u32(uint32_t x) {
+  x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+  return x;
+}
+__device__ __forceinline__ double rnd(uint32_t& s) {
+  s = hash_u32(s);
+  return (double)(s >> 8) / 16777216.0;
+}
+
+struct Fp { double lx, lz, hx, hz; };
+__device__ __forceinline__ Fp footprint(const TankDev& T) {
+  Fp f;
+  f.lx = T.ox; f.lz = T.oz;
+  f.hx = T.ox + T.nx * T.h; f.hz = T.oz + T.nz * T.h;
+  return f;
+}
+__device__ __forceinline__ bool in_fp(const Fp& f, double x, double z) { return x > f.lx && x < f.hx && z > f.lz && z < f.hz; }
+
+// glass walls below the rim, floor, re-entry from outside (solver.py:290-301, 31-wgsl-sim2.js:66-80)
+__device__ inline void tank_clamp(const TankDev& T, const double x0[3], double x[3], double v[3], double r) {
+  const Fp f = footprint(T);
+  const bool was = in_fp(f, x0[0], x0[2]);
+  if (was && x[1] < T.rim) {
+    if (x[0] < f.lx + r) { x[0] = f.lx + r; v[0] = fmax(v[0], 0.0); }
+    if (x[0] > f.hx - r) { x[0] = f.hx - r; v[0] = fmin(v[0], 0.0); }
+    if (x[2] < f.lz + r) { x[2] = f.lz + r; v[2] = fmax(v[2], 0.0); }
+    if (x[2] > f.hz - r) { x[2] = f.hz - r; v[2] = fmin(v[2], 0.0); }
+  }
+  if (was && x[1] < T.oy + r) { x[1] = T.oy + r; v[1] = fmax(v[1], 0.0); }
+  if (!was && x[1] < T.rim && in_fp(f, x[0], x[2])) {
+    x[0] = x0[0]; x[2] = x0[2];
+    v[0] *= -0.2; v[2] *= -0.2;
+  }
+}
+
+__device__ __forceinline__ int count_at(const TankDev& T, int i, int j, int k) {
+  if (i < 0 || j < 0 || k < 0 || i >= T.nx || j >= T.ny || k >= T.nz) return 0;
+  const int c = cell_idx(T, i, j, k);
+  return T.off[c + 1] - T.off[c];
+}
+__device__ __forceinline__ bool air_at(const TankDev& T, int i, int j, int k) {
+  if (j >= T.ny) return true;
+  if (i < 0 || j < 0 || k < 0 || i >= T.nx || k >= T.nz) return false;
+  return count_at(T, i, j, k) == 0;
+}
+
+// PIC and FLIP velocity of one component from faces that took weight this step (solver.py:236-249)
+__device__ inline void transfer(const TankDev& T, const double g[3], int comp, double vp, double& pic, double& flip) {
+  const double qx = g[0] - (comp == 0 ? 0.0 : 0.5), qy = g[1] - (comp == 1 ? 0.0 : 0.5), qz = g[2] - (comp == 2 ? 0.0 : 0.5);
+  const int bx = (int)floor(qx), by = (int)floor(qy), bz = (int)floor(qz);
+  const double fx = qx - bx, fy = qy - by, fz = qz - bz;
+  const double wx[2] = {1 - fx, fx}, wy[2] = {1 - fy, fy}, wz[2] = {1 - fz, fz};
+  double sn = 0.0, so = 0.0, sw = 0.0;
+  const int bit = 1 << comp;
+  for (int dx = 0; dx < 2; ++dx) {
+    const int ix = bx + dx;
+    if (ix < 0 || ix > T.nx) continue;
+    for (int dy = 0; dy < 2; ++dy) {
+      const int iy = by + dy;
+      if (iy < 0 || iy > T.ny) continue;
+      const double wxy = wx[dx] * wy[dy];
+      for (int dz = 0; dz < 2; ++dz) {
+        const int iz = bz + dz;
+        if (iz < 0 || iz > T.nz) continue;
+        const int n = node_idx(T, ix, iy, iz);
+        const float4 vo = __ldg(T.velold + n);
+        if (!((int)vo.w & bit)) continue;
+        const float4 vn = __ldg(T.vel + n);
+        const double w = wxy * wz[dz];
+        const float a = comp == 0 ? vn.x : (comp == 1 ? vn.y : vn.z);
+        const float b = comp == 0 ? vo.x : (comp == 1 ? vo.y : vo.z);
+        sn += w * (double)a;
+        so += w * (double)b;
+        sw += w;
+      }
+    }
+  }
+  if (sw >= 1e-6) {
+    pic = sn / sw;
+    flip = vp + (sn - so) / sw;
+  } else {
+    pic = vp;
+    flip = vp;
+  }
+}
+
+__device__ inline void ripple_deposit(const TankDev& T, double x, double z, double impulse, double cap) {
+  if (T.rx <= 0) return;
+  const Fp f = footprint(T);
+  const double u = (x - f.lx) / (f.hx - f.lx), w = (z - f.lz) / (f.hz - f.lz);
+  const int i = (int)fmin(fmax(rint(u * T.rx), 0.0), (double)T.rx);
+  const int j = (int)fmin(fmax(rint(w * T.rz), 0.0), (double)T.rz);
+  const double imp = fmin(fmax(impulse, 0.0), cap);
+  atomicAdd((unsigned long long*)&T.rsrc[(size_t)j * (T.rx + 1) + i], (unsigned long long)__double2ll_rn(imp * kRippleFix));
+}
+
+__device__ inline void ww_write(const TankDev& T, int k, double px, double py, double pz, double life, double vx, double vy, double vz) {
+  const int cur = T.ctr->ww_cur & 1;
+  float4* wp = cur ? T.wpos + T.ww_cap : T.wpos;
+  float4* wv = cur ? T.wvel + T.ww_cap : T.wvel;
+  wp[k] = make_float4((float)px, (float)py, (float)pz, (float)life);
+  wv[k] = make_float4((float)vx, (float)vy, (float)vz, 0.f);
+}
+
+// crown splash of a drop of mass m at speed U (solver.py:632-657, 31-wgsl-sim2.js:119-148)
+__device__ inline void crown(const TankDev& T, double cx, double cy, double cz, double U, double m, uint32_t id, int frame) {
+  if (!T.whitewater) return;
+  const double D = pow(6 * m / (M_PI * 998.0), 1.0 / 3.0);
+  const double We = 998.0 * U * U * D / 0.0728;
+  const double Oh = 0.001 / sqrt(998.0 * 0.0728 * D);
+  const double K = We * pow(Oh, -0.4);
+  const int n = (int)fmin(fmax(rint(4 * (K / 2100 - 1)), 0.0), 24.0);
+  const int nj = K > 700 ? (K > 2100 ? 2 : 1) : 0;
+  if (n + nj == 0) return;
+  uint32_t s = hash_u32(id * 2654435761u + (uint32_t)frame * 97u + 3u);
+  const int base = atomicAdd(&T.ctr->ww_count, n + nj);
+  const double r0 = 0.6 * D;
+  const double ph0 = rnd(s) * 2 * M_PI;
+  for (int i = 0; i < n; ++i) {
+    const double ph = ph0 + 2 * M_PI * (i + 0.3 * rnd(s)) / n;
+    const double el = 0.9 + 0.45 * rnd(s);
+    const double sp = U * (0.15 + 0.2 * rnd(s));
+    const double life = 0.5 + 0.4 * rnd(s);
+    const double dx = cos(ph), dz = sin(ph);
+    if (base + i < T.ww_cap)
+      ww_write(T, base + i, cx + dx * r0, cy, cz + dz * r0, life, dx * cos(el) * sp, sin(el) * sp, dz * cos(el) * sp);
+  }
+  for (int j = 0; j < nj; ++j) {
+    const double sp = U * (0.22 + 0.04 * j) * (0.9 + 0.2 * rnd(s));
+    const double vx = (rnd(s) - 0.5) * 0.05;
+    const double vz = (rnd(s) - 0.5) * 0.05;
+    if (base + n + j < T.ww_cap) ww_write(T, base + n + j, cx, cy + 0.001 * j, cz, 0.7, vx, sp, vz);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ pfx) {
+  const int total = pfx[ntanks];
+  const int stride = gridDim.x * blockDim.x;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
+    const int t = find_slot(pfx, ntanks, idx);
+    const TankDev& T = tanks[t];
+    const int local = idx - pfx[t];
+    const float4 P = T.pB[local];
+    const float4 V = T.vB[local];
+    const int flags = flags_of(P.w);
+    const uint32_t id = __float_as_uint(V.w);
+    const double dt = T.dt, h = T.h;
+    const double x0[3] = {(double)P.x, (double)P.y, (double)P.z};
+    const double vold[3] = {(double)V.x, (double)V.y, (double)V.z};
+    double g[3];
+    grid_pos(T, x0[0], x0[1], x0[2], g[0], g[1], g[2]);
+    const bool ing = in_grid(T, g[0], g[1], g[2]);
+    double v[3] = {vold[0], vold[1], vold[2]};
+    if (ing) {
+      for (int a = 0; a < 3; ++a) {
+        double pic, flip;
+        transfer(T, g, a, vold[a], pic, flip);
+        v[a] = pic + T.flip * (flip - pic);
+      }
+    } else {
+      v[1] -= T.g * dt;
+    }
+    double x[3] = {x0[0] + v[0] * dt, x0[1] + v[1] * dt, x0[2] + v[2] * dt};
+    const double rc = 0.32 * h;
+    if (T.has_obst) {
+      const double d = tank_sdf(T, x[0], x[1], x[2]);
+      if (d < rc) {
+        double nx, ny, nz;
+        tank_normal(T, x[0], x[1], x[2], nx, ny, nz);
+        x[0] += nx * (rc - d); x[1] += ny * (rc - d); x[2] += nz * (rc - d);
+        double vs[3];
+        tank_solid_vel(T, x[0], x[1], x[2], vs[0], vs[1], vs[2]);
+        const double rel[3] = {v[0] - vs[0], v[1] - vs[1], v[2] - vs[2]};
+        const double vn = rel[0] * nx + rel[1] * ny + rel[2] * nz;
+        if (vn < 0) {
+          const double kf = 1 - T.friction;
+          v[0] = vs[0] + (rel[0] - nx * vn) * kf;
+          v[1] = vs[1] + (rel[1] - ny * vn) * kf;
+          v[2] = vs[2] + (rel[2] - nz * vn) * kf;
+        }
+      }
+    }
+    tank_clamp(T, x0, x, v, rc);
+    const Fp fp = footprint(T);
+    bool alive = true;
+    if (T.nobj && in_drain(T.objs, T.nobj, x[0], x[1], x[2])) alive = false;
+    if (!in_fp(fp, x[0], x[2]) && x[1] < 0.002) alive = false;
+    if (fabs(x[0]) > 20 || fabs(x[2]) > 20 || x[1] < -1 || x[1] > 30) alive = false;
+    // free-flight mark of sub-grid drops (solver.py:565-583)
+    const int c0[3] = {(int)floor(g[0]), (int)floor(g[1]), (int)floor(g[2])};
+    bool air = flags & kFlagAir;
+    if (ing) {
+      const int n0 = count_at(T, c0[0], c0[1], c0[2]);
+      if (n0 >= 4) {
+        air = false;
+      } else if (n0 <= 2 && c0[1] + 2 < T.ny) {
+        int around = 0, above = 0;
+        for (int dz = -1; dz <= 1; ++dz)
+          for (int dx = -1; dx <= 1; ++dx) {
+            for (int dy = -1; dy <= 1; ++dy) around += count_at(T, c0[0] + dx, c0[1] + dy, c0[2] + dz);
+            above += count_at(T, c0[0] + dx, c0[1] + 1, c0[2] + dz) + count_at(T, c0[0] + dx, c0[1] + 2, c0[2] + dz);
+          }
+        if (around <= 4 && above == 0) air = true;
+      }
+    }
+    // merging with the pool (solver.py:584-606)
+    const int frame = T.ctr->frame;
+    double g1[3];
+    grid_pos(T, x[0], x[1], x[2], g1[0], g1[1], g1[2]);
+    if (air && vold[1] < -0.3 && in_grid(T, g1[0], g1[1], g1[2])) {
+      const int c1[3] = {(int)floor(g1[0]), (int)floor(g1[1]), (int)floor(g1[2])};
+      const int same = (c1[0] == c0[0] && c1[1] == c0[1] && c1[2] == c0[2]) ? 1 : 0;
+      const int cnt1 = count_at(T, c1[0], c1[1], c1[2]);
+      if (cnt1 - same >= 3) {
+        double vl[3];
+        for (int a = 0; a < 3; ++a) {
+          double pic, flip;
+          transfer(T, g1, a, v[a], pic, flip);
+          vl[a] = pic;
+        }
+        const double dv = vl[1] - vold[1];
+        if (dv > 0.3) {
+          v[0] = vl[0]; v[1] = vl[1]; v[2] = vl[2];
+          air = false;
+          atomicAdd(&T.ctr->impacts, 1);
+          const double m = T.drop_mass;
+          ripple_deposit(T, x[0], x[2], 2.0 * m * fmin(dv, 8.0), 2e-3);
+          const double level = T.oy + (c1[1] + fmin(cnt1 / T.ppc, 1.0)) * h;
+          crown(T, x[0], level + 0.25 * h, x[2], -vold[1], m, id, frame);
+        }
+      }
+    }
+    if (ing) {
+      const double sp = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      // stored +1 so that 0 means "no in-grid particle this sub-step" (the reference keeps vmax then)
+      atomicMax((unsigned long long*)&T.ctr->vmax_bits64, (unsigned long long)__double_as_longlong(fmin(sp, 60.0)) + 1ull);
+      if (T.whitewater && sp > 0.75) {
+        bool near = false;
+        for (int a = 0; a < 3 && !near; ++a)
+          for (int sg = -1; sg <= 1 && !near; sg += 2)
+            near = air_at(T, c0[0] + (a == 0 ? sg : 0), c0[1] + (a == 1 ? sg : 0), c0[2] + (a == 2 ? sg : 0));
+        if (near) {
+          uint32_t s = hash_u32(id * 9781u + (uint32_t)frame * 6271u + 17u);
+          const double e = fmin(fmax((sp - 0.75) / 1.6, 0.0), 1.0);
+          if (rnd(s) < T.ww_rate * e * e * dt) {
+            const double j0 = rnd(s) - 0.5, j1 = rnd(s) - 0.5, j2 = rnd(s) - 0.5;
+            const double life = 1.0 + 2.5 * rnd(s);
+            const double f = 0.8 + 0.35 * rnd(s);
+            atomicAdd(&T.ctr->ww_spawned, 1);
+            const int k = atomicAdd(&T.ctr->ww_count, 1);
+            if (k < T.ww_cap)
+              ww_write(T, k, x[0] + j0 * h * 0.6, x[1] + j1 * h * 0.6, x[2] + j2 * h * 0.6, life,
+                       v[0] * f + j0 * 0.35, v[1] * f + j1 * 0.35, v[2] * f + j2 * 0.35);
+          }
+        }
+      }
+    }
+    const float fl = (float)((air ? kFlagAir : 0) | (alive ? 0 : kFlagDead));
+    T.pA[local] = make_float4((float)x[0], (float)x[1], (float)x[2], fl);
+    T.vA[local] = make_float4((float)v[0], (float)v[1], (float)v[2], __uint_as_float(id));
+  }
+}
+
+// ---------------------------------------------------------------------------------------- whitewater
+// spray falls with drag, foam rides the surface, bubbles rise (solver.py:675-713, 31-wgsl-sim2.js:361-409)
+__device__ inline double sample_vel(const TankDev& T, const double g[3], int comp) {
+  const double qx = g[0] - (comp == 0 ? 0.0 : 0.5), qy = g[1] - (comp == 1 ? 0.0 : 0.5), qz = g[2] - (comp == 2 ? 0.0 : 0.5);
+  const double fbx = floor(qx), fby = floor(qy), fbz = floor(qz);
+  const int bx = (int)fbx, by = (int)fby, bz = (int)fbz;
+  const double fx = qx - fbx, fy = qy - fby, fz = qz - fbz;
+  double s = 0.0;
+  for (int dx = 0; dx < 2; ++dx) {
+    const double wx = dx ? fx : 1 - fx;
+    const int ix = min(max(bx + dx, 0), T.nx);
+    for (int dy = 0; dy < 2; ++dy) {
+      const double wy = dy ? fy : 1 - fy;
+      const int iy = min(max(by + dy, 0), T.ny);
+      for (int dz = 0; dz < 2; ++dz) {
+        const double wz = dz ? fz : 1 - fz;
+        const int iz = min(max(bz + dz, 0), T.nz);
+        const float4 vn = __ldg(T.vel + node_idx(T, ix, iy, iz));
+        s += wx * wy * wz * (double)(comp == 0 ? vn.x : (comp == 1 ? vn.y : vn.z));
+      }
+    }
+  }
+  return s;
+}
+
+__global__ void __launch_bounds__(kThreads) k_whitewater(const TankDev* __restrict__ tanks, int ntanks, double frame_dt) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int t = 0; t < ntanks; ++t) {
+    const TankDev& T = tanks[t];
+    const int cur = T.ctr->ww_cur & 1;
+    const int n = min(T.ctr->ww_count, T.ww_cap);
+    const float4* wp = cur ? T.wpos + T.ww_cap : T.wpos;
+    const float4* wv = cur ? T.wvel + T.ww_cap : T.wvel;
+    float4* op = cur ? T.wpos : T.wpos + T.ww_cap;
+    float4* ov = cur ? T.wvel : T.wvel + T.ww_cap;
+    const double dt = frame_dt;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+      const float4 P = wp[q], V = wv[q];
+      double x[3] = {(double)P.x, (double)P.y, (double)P.z};
+      double v[3] = {(double)V.x, (double)V.y, (double)V.z};
+      double life = (double)P.w;
+      const double kind0 = (double)V.w;
+      double g[3];
+      grid_pos(T, x[0], x[1], x[2], g[0], g[1], g[2]);
+      double kind = 0.0;
+      if (in_grid(T, g[0], g[1], g[2])) {
+        const int c[3] = {(int)g[0], (int)g[1], (int)g[2]};
+        const int nc = count_at(T, c[0], c[1], c[2]);
+        const int up = count_at(T, c[0], c[1] + 1, c[2]);
+        if (nc > 0) kind = up > 0 ? 2.0 : ((g[1] - c[1] < fmin(nc / T.ppc, 1.0)) ? 1.0 : 0.0);
+      }
+      if (kind0 < 0.5 && kind > 0.5 && (double)V.y < -0.3) ripple_deposit(T, x[0], x[2], 4.2e-6 * -(double)V.y, 1e-4);
+      if (kind == 0.0) {
+        v[1] -= T.g * dt;
+        const double damp = 1.0 / (1.0 + 0.6 * dt);
+        v[0] *= damp; v[1] *= damp; v[2] *= damp;
+        life -= dt * 0.7;
+      } else {
+        const double vf[3] = {sample_vel(T, g, 0), sample_vel(T, g, 1), sample_vel(T, g, 2)};
+        if (kind == 1.0) { v[0] = vf[0] * 1; v[1] = vf[1] * 0.2; v[2] = vf[2] * 1; life -= dt * 0.5; }
+        else { v[0] = vf[0] + 0; v[1] = vf[1] + 0.16; v[2] = vf[2] + 0; life -= dt * 0.3; }
+      }
+      const double x0[3] = {x[0], x[1], x[2]};
+      x[0] = x0[0] + v[0] * dt; x[1] = x0[1] + v[1] * dt; x[2] = x0[2] + v[2] * dt;
+      if (T.has_obst) {
+        const double d = tank_sdf(T, x[0], x[1], x[2]);
+        if (d < 0) {
+          double nx, ny, nz;
+          tank_normal(T, x[0], x[1], x[2], nx, ny, nz);
+          x[0] -= nx * d; x[1] -= ny * d; x[2] -= nz * d;
+        }
+      }
+      tank_clamp(T, x0, x, v, 0.001);
+      const Fp fp = footprint(T);
+      const bool outside = !in_fp(fp, x[0], x[2]) && x[1] < 0.001;
+      const bool drained = T.nobj && in_drain(T.objs, T.nobj, x[0], x[1], x[2]);
+      if (life > 0 && !outside && x[1] > -0.5 && !drained) {
+        const int k = atomicAdd(&T.ctr->ww_next, 1);
+        if (k < T.ww_cap) {
+          op[k] = make_float4((float)x[0], (float)x[1], (float)x[2], (float)life);
+          ov[k] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)kind);
+        }
+      }
+    }
+  }
+}
+
+__global__ void k_whitewater_end(const TankDev* __restrict__ tanks, int ntanks) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntanks) return;
+  Counters* c = tanks[t].ctr;
+  c->ww_count = min(c->ww_next, tanks[t].ww_cap);
+  c->ww_next = 0;
+  c->ww_cur ^= 1;
+}
+
+void launch_g2p(const LaunchCtx& L) {
+  k_g2p<<<L.particle_blocks, kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_sorted);
+}
+void launch_whitewater(const LaunchCtx& L, double frame_dt) {
+  k_whitewater<<<L.particle_blocks, kThreads, 0, L.stream>>>(L.tanks, L.ntanks, frame_dt);
+  k_whitewater_end<<<(L.ntanks + 127) / 128, 128, 0, L.stream>>>(L.tanks, L.ntanks);
+}
+
+}  // namespace suiri

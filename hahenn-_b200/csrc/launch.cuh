@@ -1,0 +1,43 @@
+// Host-side launch context shared by the kernel files: which tanks a launch covers and how its blocks
+// map onto them.
+#pragma once
+#include "common.cuh"
+
+namespace suiri {
+
+constexpr int kThreads = 256;
+constexpr int kScanTile = 2048;          // cells per scan block (256 threads × 8)
+constexpr int kBrick = 8;                // P2G brick edge in cells
+
+// block families: blocks of one launch are laid out tank after tank; pfx[t] = first block of tank t
+enum Family { kFamNodes = 0, kFamCells, kFamHalf, kFamBricks, kFamScan, kFamCount };
+
+struct LaunchCtx {
+  cudaStream_t stream;
+  const TankDev* tanks;     // device array of ntanks descriptors
+  int ntanks;
+  const int* bpfx[kFamCount];   // device: ntanks+1 block prefixes per family
+  int nblocks[kFamCount];       // host copy of the totals
+  int* ppfx_in;             // device: ntanks+1 prefix of particles in A∪E
+  int* ppfx_sorted;         // device: ntanks+1 prefix of particles in B
+  long long* scan_bsum;     // device: one partial sum per scan block
+  int particle_blocks;      // persistent grid for particle kernels
+};
+
+// per-kernel launchers (bin.cu, grid.cu, sor.cu, g2p.cu)
+void launch_begin_substep(const LaunchCtx& L);
+void launch_begin_count(const LaunchCtx& L);   // prefix only, for a count pass between sub-steps
+void launch_bin(const LaunchCtx& L);
+void launch_scan(const LaunchCtx& L);
+void launch_scatter(const LaunchCtx& L);
+void launch_sorted_prefix(const LaunchCtx& L);
+void launch_geom(const LaunchCtx& L);
+void launch_p2g(const LaunchCtx& L);
+void launch_grid_nodes(const LaunchCtx& L);
+void launch_grid_cells(const LaunchCtx& L);
+void launch_sor_sweep(const LaunchCtx& L, int color, int sweep);
+void launch_project(const LaunchCtx& L);
+void launch_g2p(const LaunchCtx& L);
+void launch_whitewater(const LaunchCtx& L, double frame_dt);
+
+}  // namespace suiri

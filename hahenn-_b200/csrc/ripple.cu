@@ -1,0 +1,449 @@
+// Top-view water height map and the capillary-gravity ripple layer, once per frame.
+//
+// Height map (blender_addon/suiri_lab/solver.py:738-779): per texel the highest particle, every particle
+// widened to a sphere cap of radius 1.3125h (a dilation with the precomputed disc of cap heights), then a
+// separable Gaussian over wet texels only. Float64, with the same maxima and sums in the same order as
+// the reference, so the map agrees bit for bit.
+//
+// Ripple layer (solver.py:855-907, src/js/64-ripple.js): the impulses deposited by merging drops are
+// mirrored into a (2Rz)×(2Rx) cosine domain (reflecting walls), transformed, every mode advanced by the
+// exact damped oscillator of ω² = (gk + σ/ρ k³) tanh(kd) and kicked by the impulse, transformed back to
+// heights and slopes, multiplied by the absorption mask (obstacle walls at the water line, dry floor)
+// and transformed forward again. The reference's square layer is Rx = Rz; here the layer may be
+// rectangular. The 2D FFTs are written here: rows, then columns, each line in shared memory, in-place
+// radix-2 decimation in time from a bit-reversed load, twiddles from a float64 table (as the reference's
+// WGSL does, 64-ripple.js:32-33, :175-178), complex64 data.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "engine.h"
+#include "sdf.cuh"
+
+namespace suiri {
+
+struct RippleState {
+  int W = 0, Mx = 0, Mz = 0, lx = 0, lz = 0;
+  double Lx = 0, Lz = 0;
+  double sigma_rho = 0.0728 / 998.0, rho = 998.0, g = 9.81;
+  unsigned* topkey = nullptr;   // W² ordered float keys of the highest particle
+  double* hA = nullptr;         // W² float64 work maps
+  double* hB = nullptr;
+  double* top = nullptr;        // W² final height map, -1 dry
+  float* mask = nullptr;        // (rz+1)(rx+1)
+  float4* field = nullptr;      // (rz+1)(rx+1): h, slope x, slope z
+  float2* S = nullptr;          // Mz×Mx spectral state
+  float2* A = nullptr;          // Mz×Mx work
+  float2* twx = nullptr;        // Mx twiddles (cos, sin)(2πt/Mx)
+  float2* twz = nullptr;
+  double* mx_coord = nullptr;   // rx+1 x coordinates of the ripple vertices
+  double* mz_coord = nullptr;
+  int4* disc = nullptr;         // dilation offsets (ox, oy) with cap height index
+  double* disc_h = nullptr;
+  int ndisc = 0;
+  double* blur_w = nullptr;
+  int blur_rad = 0;
+  double texel[2] = {0, 0};
+  std::vector<void*> mem;
+};
+
+namespace {
+
+RippleState* rs(Tank& t) { return (RippleState*)t.ripple; }
+
+__device__ __forceinline__ unsigned fkey(float f) {
+  const unsigned b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float funkey(unsigned k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+__global__ void k_top_scatter(TankDev T, unsigned* __restrict__ key, int W, double tx, double tz) {
+  const int n = T.ctr->n_live;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const float4 p = T.pA[q];
+    if (flags_of(p.w) & kFlagDead) continue;
+    if (!((double)p.y <= T.rim + 0.01)) continue;
+    const double fx = floor(((double)p.x - T.ox) / tx), fz = floor(((double)p.z - T.oz) / tz);
+    if (fx < 0 || fz < 0 || fx >= W || fz >= W) continue;
+    atomicMax(key + (size_t)fz * W + (int)fx, fkey(p.y));
+  }
+}
+
+// H = max(-1, max over the disc of (top[y+oy][x+ox] + cap)) ; dry where nothing reaches
+__global__ void k_top_dilate(const unsigned* __restrict__ key, double* __restrict__ H, int W, const int4* __restrict__ disc,
+                             const double* __restrict__ cap, int ndisc, int any) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= W * W) return;
+  const int x = e % W, y = e / W;
+  double h = -1.0;
+  if (any) {
+    for (int d = 0; d < ndisc; ++d) {
+      const int xs = x + disc[d].x, ys = y + disc[d].y;
+      if (xs < 0 || ys < 0 || xs >= W || ys >= W) continue;
+      const unsigned k = key[(size_t)ys * W + xs];
+      if (k == 0u) continue;
+      h = fmax(h, (double)funkey(k) + cap[d]);
+    }
+  }
+  H[e] = h;
+}
+
+// wet-only Gaussian along x (axis 0) or z (axis 1); wet = the unblurred map >= 0 (wet0)
+__global__ void k_top_blur(const double* __restrict__ in, const double* __restrict__ wet0, double* __restrict__ out, int W,
+                           const double* __restrict__ w, int rad, int along_z) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= W * W) return;
+  const int x = e % W, y = e / W;
+  if (!(wet0[e] >= 0.0)) { out[e] = -1.0; return; }
+  double s = 0.0, ws = 0.0;
+  for (int i = -rad; i <= rad; ++i) {
+    int xi = x, yi = y;
+    if (along_z) yi = min(max(y + i, 0), W - 1); else xi = min(max(x + i, 0), W - 1);
+    const size_t o = (size_t)yi * W + xi;
+    const double k = w[i + rad];
+    if (wet0[o] >= 0.0) { s += in[o] * k; ws += k; } else { s += 0.0; ws += 0.0; }
+  }
+  out[e] = s / fmax(ws, 1e-12);
+}
+
+__global__ void k_ripple_mask(TankDev T, const double* __restrict__ top, int W, const double* __restrict__ X,
+                              const double* __restrict__ Z, float* __restrict__ mask) {
+  const int rx = T.rx, rz = T.rz;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (rx + 1) * (rz + 1)) return;
+  const int i = e % (rx + 1), j = e / (rx + 1);
+  const double lx = T.ox, lz = T.oz, hx = T.ox + T.nx * T.h, hz = T.oz + T.nz * T.h;
+  const double x = X[i], z = Z[j];
+  const int ti = (int)fmin(fmax((x - lx) / (hx - lx) * W, 0.0), (double)(W - 1));
+  const int tj = (int)fmin(fmax((z - lz) / (hz - lz) * W, 0.0), (double)(W - 1));
+  const double h = top[(size_t)tj * W + ti];
+  double m = 0.75;
+  if (h >= 0) {
+    const double d = tank_sdf(T, x, h - 0.002, z);
+    double t = (d - -0.003) / (0.006 - -0.003);
+    t = fmin(fmax(t, 0.0), 1.0);
+    m = t * t * (3.0 - 2.0 * t);
+  }
+  mask[e] = (float)m;
+}
+
+// mirrored source (impulse density) → complex input of the forward transform (64-ripple.js:18-31)
+__global__ void k_ripple_src(TankDev T, const long long* __restrict__ src, float2* __restrict__ out, int Mx, int Mz, double inv_area) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= Mx * Mz) return;
+  const int i = e % Mx, j = e / Mx;
+  const int pi = i <= T.rx ? i : Mx - i, pj = j <= T.rz ? j : Mz - j;
+  const double v = (double)src[(size_t)pj * (T.rx + 1) + pi] * (1.0 / kRippleFix) * inv_area;
+  out[e] = make_float2((float)v, 0.f);
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+
+// one line per block: rows of length M (stride 1) starting at data + line*M
+__global__ void k_fft_rows(float2* __restrict__ data, int M, int logM, const float2* __restrict__ tw, float sign) {
+  extern __shared__ float2 s[];
+  float2* row = data + (size_t)blockIdx.x * M;
+  for (int i = threadIdx.x; i < M; i += blockDim.x) s[__brev(i) >> (32 - logM)] = row[i];
+  __syncthreads();
+  for (int half = 1; half < M; half <<= 1) {
+    const int step = M / (2 * half);
+    for (int k = threadIdx.x; k < M / 2; k += blockDim.x) {
+      const int pos = k & (half - 1);
+      const int i = ((k - pos) << 1) + pos, j = i + half;
+      float2 w = tw[pos * step];
+      w.y *= sign;
+      const float2 t = cmul(w, s[j]);
+      const float2 a = s[i];
+      s[j] = make_float2(a.x - t.x, a.y - t.y);
+      s[i] = make_float2(a.x + t.x, a.y + t.y);
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < M; i += blockDim.x) row[i] = s[i];
+}
+
+// C columns per block: columns of length M with row stride `ld`
+__global__ void k_fft_cols(float2* __restrict__ data, int M, int logM, int ld, int C, const float2* __restrict__ tw, float sign) {
+  extern __shared__ float2 s[];
+  const int c0 = blockIdx.x * C;
+  for (int e = threadIdx.x; e < M * C; e += blockDim.x) {
+    const int r = e / C, cl = e % C;
+    s[cl * M + (__brev(r) >> (32 - logM))] = data[(size_t)r * ld + c0 + cl];
+  }
+  __syncthreads();
+  for (int half = 1; half < M; half <<= 1) {
+    const int step = M / (2 * half);
+    for (int e = threadIdx.x; e < (M / 2) * C; e += blockDim.x) {
+      const int cl = e / (M / 2), k = e % (M / 2);
+      const int pos = k & (half - 1);
+      const int i = cl * M + ((k - pos) << 1) + pos, j = i + half;
+      float2 w = tw[pos * step];
+      w.y *= sign;
+      const float2 t = cmul(w, s[j]);
+      const float2 a = s[i];
+      s[j] = make_float2(a.x - t.x, a.y - t.y);
+      s[i] = make_float2(a.x + t.x, a.y + t.y);
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < M * C; e += blockDim.x) {
+    const int r = e / C, cl = e % C;
+    data[(size_t)r * ld + c0 + cl] = s[cl * M + r];
+  }
+}
+
+// exact damped oscillator per mode plus the impulse kick (solver.py:882-899, 64-ripple.js:58-90)
+__global__ void k_ripple_evolve(TankDev T, float2* __restrict__ S, const float2* __restrict__ hat, int Mx, int Mz, double Lx,
+                                double Lz, double dt, double g, double sigma_rho, double rho) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= Mx * Mz) return;
+  const int i = e % Mx, j = e / Mx;
+  const int Rx = T.rx, Rz = T.rz;
+  const int mx = i < Rx ? i : i - Mx, mz = j < Rz ? j : j - Mz;
+  if ((mx == 0 && mz == 0) || mx == -Rx || mz == -Rz) { S[e] = make_float2(0.f, 0.f); return; }
+  const double n = (double)T.ctr->n_sorted;
+  const double depth = fmin(fmax(n * T.vp / (T.nx * T.nz * T.h * T.h), 0.003), T.rim);
+  const double kx = mx * M_PI / Lx, kz = mz * M_PI / Lz;
+  const double kk = sqrt(kx * kx + kz * kz);
+  const double D = fmax(depth, 0.002);
+  const double kd = fmin(kk * D, 15.0);
+  const double th = tanh(kd);
+  const double nu = 1.0e-6, film = 0.3;
+  const double w2 = (g * kk + sigma_rho * kk * kk * kk) * th;
+  const double w = sqrt(w2);
+  const double gam = 2 * nu * kk * kk + film * kk * sqrt(nu * w * 0.125) + kk * sqrt(nu * w * 0.5) / fmax(sinh(fmin(2 * kd, 30.0)), 1e-4);
+  const double wd = sqrt(fmax(w2 - gam * gam, 1e-6));
+  double Hs = S[e].x, Vs = S[e].y;
+  if (dt > 0) {
+    const double c = cos(wd * dt), sn = sin(wd * dt), ex = exp(-gam * dt);
+    const double H2 = ex * (Hs * c + (Vs + gam * Hs) / wd * sn);
+    const double V2 = ex * (Vs * c - (w2 * Hs + gam * Vs) / wd * sn);
+    Hs = H2; Vs = V2;
+  }
+  const double kh = 2 * M_PI / 0.12;
+  const double hp = 1 - exp(-(kk * kk) / (kh * kh));
+  const double sw = fmax(1.2 * Lx / Rx, 0.003);
+  const double spread = exp(-0.5 * kk * kk * sw * sw);
+  Vs = Vs - (kk * th / rho) * (double)hat[e].x * hp * spread;
+  S[e] = make_float2((float)Hs, (float)Vs);
+}
+
+// field = ifft (already in S, unnormalised) → heights and slopes; masked = field · mirrored mask → A
+__global__ void k_ripple_field(TankDev T, const float2* __restrict__ S, float2* __restrict__ A, const float* __restrict__ mask,
+                               float4* __restrict__ field, int Mx, int Mz, double dx, double dz) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= Mx * Mz) return;
+  const int i = e % Mx, j = e / Mx;
+  const double inv = 1.0 / ((double)Mx * Mz);
+  const int pi = i <= T.rx ? i : Mx - i, pj = j <= T.rz ? j : Mz - j;
+  const float m = mask[(size_t)pj * (T.rx + 1) + pi];
+  const float2 v = S[e];
+  A[e] = make_float2((float)(v.x * inv) * m, (float)(v.y * inv) * m);
+  if (i <= T.rx && j <= T.rz) {
+    const double h = v.x * inv;
+    const double hl = S[(size_t)j * Mx + (i + Mx - 1) % Mx].x * inv, hr = S[(size_t)j * Mx + (i + 1) % Mx].x * inv;
+    const double hd = S[(size_t)((j + Mz - 1) % Mz) * Mx + i].x * inv, hu = S[(size_t)((j + 1) % Mz) * Mx + i].x * inv;
+    field[(size_t)j * (T.rx + 1) + i] = make_float4((float)h, (float)((hr - hl) / (2 * dx)), (float)((hu - hd) / (2 * dz)), 0.f);
+  }
+}
+
+int ilog2(int x) { int l = 0; while ((1 << l) < x) ++l; return l; }
+
+void fft2(Tank& t, float2* data, float sign) {
+  RippleState& r = *rs(t);
+  const int lx = ilog2(r.Mx), lz = ilog2(r.Mz);
+  k_fft_rows<<<r.Mz, 256, r.Mx * sizeof(float2), t.stream>>>(data, r.Mx, lx, r.twx, sign);
+  int C = 8;
+  while (C > 1 && (size_t)r.Mz * C * sizeof(float2) > 96 * 1024) C >>= 1;
+  while (r.Mx % C) C >>= 1;
+  k_fft_cols<<<r.Mx / C, 256, r.Mz * C * sizeof(float2), t.stream>>>(data, r.Mz, lz, r.Mx, C, r.twz, sign);
+  CK(cudaGetLastError());
+}
+
+void* ralloc(Tank& t, RippleState& r, size_t bytes) {
+  void* p = nullptr;
+  CK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+  CK(cudaMemsetAsync(p, 0, std::max<size_t>(bytes, 16), t.stream));
+  r.mem.push_back(p);
+  return p;
+}
+
+RippleState& ensure(Tank& t) {
+  if (t.ripple) return *rs(t);
+  const TankDev& D = t.d;
+  auto pow2 = [](int x) { return x > 0 && (x & (x - 1)) == 0; };
+  if (!pow2(D.rx) || !pow2(D.rz)) throw Error(-1, "ripple layer sizes must be powers of two");
+  RippleState* r = new RippleState();
+  t.ripple = r;
+  r->W = t.cfg.wmap;
+  r->Mx = 2 * D.rx; r->Mz = 2 * D.rz;
+  r->Lx = D.nx * D.h; r->Lz = D.nz * D.h;
+  const int W = r->W;
+  static_assert(sizeof(float2) == 8, "");
+  CK(cudaFuncSetAttribute(k_fft_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  CK(cudaFuncSetAttribute(k_fft_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  if ((size_t)r->Mx * 8 > 200 * 1024 || (size_t)r->Mz * 8 > 200 * 1024) throw Error(-1, "ripple layer too large");
+  r->topkey = (unsigned*)ralloc(t, *r, (size_t)W * W * 4);
+  r->hA = (double*)ralloc(t, *r, (size_t)W * W * 8);
+  r->hB = (double*)ralloc(t, *r, (size_t)W * W * 8);
+  r->top = (double*)ralloc(t, *r, (size_t)W * W * 8);
+  r->mask = (float*)ralloc(t, *r, (size_t)(D.rx + 1) * (D.rz + 1) * 4);
+  r->field = (float4*)ralloc(t, *r, (size_t)(D.rx + 1) * (D.rz + 1) * 16);
+  r->S = (float2*)ralloc(t, *r, (size_t)r->Mx * r->Mz * 8);
+  r->A = (float2*)ralloc(t, *r, (size_t)r->Mx * r->Mz * 8);
+  r->twx = (float2*)ralloc(t, *r, (size_t)r->Mx * 8);
+  r->twz = (float2*)ralloc(t, *r, (size_t)r->Mz * 8);
+  r->mx_coord = (double*)ralloc(t, *r, (size_t)(D.rx + 1) * 8);
+  r->mz_coord = (double*)ralloc(t, *r, (size_t)(D.rz + 1) * 8);
+  // host tables
+  std::vector<float2> tw(std::max(r->Mx, r->Mz));
+  for (int pass = 0; pass < 2; ++pass) {
+    const int M = pass ? r->Mz : r->Mx;
+    for (int k = 0; k < M; ++k) tw[k] = make_float2((float)cos(2 * M_PI * k / M), (float)sin(2 * M_PI * k / M));
+    CK(cudaMemcpy(pass ? r->twz : r->twx, tw.data(), M * 8, cudaMemcpyHostToDevice));
+  }
+  // ripple vertex coordinates: lo + linspace(0, 1, R+1)·(hi - lo) as NumPy forms them (solver.py:784-785)
+  const double lo[2] = {D.ox, D.oz}, hi[2] = {D.ox + D.nx * D.h, D.oz + D.nz * D.h};
+  for (int a = 0; a < 2; ++a) {
+    const int R = a ? D.rz : D.rx;
+    std::vector<double> c(R + 1);
+    const double step = 1.0 / R;
+    for (int i = 0; i <= R; ++i) {
+      const double u = i == R ? 1.0 : i * step + 0.0;
+      c[i] = lo[a] + u * (hi[a] - lo[a]);
+    }
+    CK(cudaMemcpy(a ? r->mz_coord : r->mx_coord, c.data(), (R + 1) * 8, cudaMemcpyHostToDevice));
+  }
+  // dilation disc and blur weights (solver.py:752-768)
+  r->texel[0] = (hi[0] - lo[0]) / W;
+  r->texel[1] = (hi[1] - lo[1]) / W;
+  const double rad = (0.5 * D.h * 1.05) * 1.25;
+  const int ri = (int)ceil(rad / std::min(r->texel[0], r->texel[1]));
+  std::vector<int4> disc;
+  std::vector<double> cap;
+  for (int oy = -ri; oy <= ri; ++oy)
+    for (int ox = -ri; ox <= ri; ++ox) {
+      const double q = rad * rad - (ox * r->texel[0]) * (ox * r->texel[0]) - (oy * r->texel[1]) * (oy * r->texel[1]);
+      if (q <= 0) continue;
+      disc.push_back(make_int4(ox, oy, 0, 0));     // H[y][x] takes top[y + oy][x + ox] (solver.py:759-763)
+      cap.push_back(sqrt(q));
+    }
+  r->ndisc = (int)disc.size();
+  r->disc = (int4*)ralloc(t, *r, disc.size() * 16);
+  r->disc_h = (double*)ralloc(t, *r, cap.size() * 8);
+  CK(cudaMemcpy(r->disc, disc.data(), disc.size() * 16, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(r->disc_h, cap.data(), cap.size() * 8, cudaMemcpyHostToDevice));
+  const double sigma = 1.5 * D.h / std::min(r->texel[0], r->texel[1]);
+  r->blur_rad = (int)ceil(2.5 * sigma);
+  std::vector<double> bw(2 * r->blur_rad + 1);
+  for (int i = -r->blur_rad; i <= r->blur_rad; ++i) {
+    const double x = i / sigma;
+    bw[i + r->blur_rad] = exp(-0.5 * (x * x));
+  }
+  r->blur_w = (double*)ralloc(t, *r, bw.size() * 8);
+  CK(cudaMemcpy(r->blur_w, bw.data(), bw.size() * 8, cudaMemcpyHostToDevice));
+  CK(cudaStreamSynchronize(t.stream));
+  return *r;
+}
+
+}  // namespace
+
+size_t ripple_state_bytes(Tank& t) {
+  if (t.d.rx <= 0) return 0;
+  return (size_t)(2 * t.d.rx) * (2 * t.d.rz) * 8;
+}
+
+void clear_ripple(Tank& t) {
+  if (t.d.rx <= 0 || !t.ripple) return;
+  RippleState& r = *rs(t);
+  CK(cudaMemsetAsync(r.S, 0, (size_t)r.Mx * r.Mz * 8, t.stream));
+  CK(cudaMemsetAsync(r.field, 0, (size_t)(t.d.rx + 1) * (t.d.rz + 1) * 16, t.stream));
+}
+
+void free_ripple(Tank& t) {
+  if (!t.ripple) return;
+  RippleState* r = rs(t);
+  for (void* p : r->mem) cudaFree(p);
+  delete r;
+  t.ripple = nullptr;
+}
+
+void copy_ripple_state(Tank& t, void* buf, bool save) {
+  if (t.d.rx <= 0) return;
+  RippleState& r = ensure(t);
+  const size_t b = (size_t)r.Mx * r.Mz * 8;
+  if (save) CK(cudaMemcpyAsync(buf, r.S, b, cudaMemcpyDeviceToDevice, t.stream));
+  else CK(cudaMemcpyAsync(r.S, buf, b, cudaMemcpyDeviceToDevice, t.stream));
+}
+
+void compute_top_height(Tank& t) {
+  RippleState& r = ensure(t);
+  const int W = r.W;
+  const int nb = (W * W + 255) / 256;
+  CK(cudaMemsetAsync(r.topkey, 0, (size_t)W * W * 4, t.stream));
+  k_top_scatter<<<t.solo->sm_count * 4, 256, 0, t.stream>>>(t.d, r.topkey, W, r.texel[0], r.texel[1]);
+  k_top_dilate<<<nb, 256, 0, t.stream>>>(r.topkey, r.hA, W, r.disc, r.disc_h, r.ndisc, 1);
+  k_top_blur<<<nb, 256, 0, t.stream>>>(r.hA, r.hA, r.hB, W, r.blur_w, r.blur_rad, 0);
+  k_top_blur<<<nb, 256, 0, t.stream>>>(r.hB, r.hA, r.top, W, r.blur_w, r.blur_rad, 1);
+  CK(cudaGetLastError());
+}
+
+void ripple_frame(Tank& t, double frame_dt) {
+  if (t.d.rx <= 0) return;
+  RippleState& r = ensure(t);
+  compute_top_height(t);
+  const int nv = (t.d.rx + 1) * (t.d.rz + 1);
+  k_ripple_mask<<<(nv + 255) / 256, 256, 0, t.stream>>>(t.d, r.top, r.W, r.mx_coord, r.mz_coord, r.mask);
+  const int nm = r.Mx * r.Mz, nb = (nm + 255) / 256;
+  const double dx = r.Lx / t.d.rx, dz = r.Lz / t.d.rz;
+  k_ripple_src<<<nb, 256, 0, t.stream>>>(t.d, t.d.rsrc, r.A, r.Mx, r.Mz, 1.0 / (dx * dz));
+  CK(cudaMemsetAsync(t.d.rsrc, 0, (size_t)nv * 8, t.stream));
+  fft2(t, r.A, -1.f);
+  k_ripple_evolve<<<nb, 256, 0, t.stream>>>(t.d, r.S, r.A, r.Mx, r.Mz, r.Lx, r.Lz, frame_dt, r.g, r.sigma_rho, r.rho);
+  fft2(t, r.S, 1.f);
+  k_ripple_field<<<nb, 256, 0, t.stream>>>(t.d, r.S, r.A, r.mask, r.field, r.Mx, r.Mz, dx, dz);
+  fft2(t, r.A, -1.f);
+  std::swap(r.S, r.A);
+  CK(cudaGetLastError());
+}
+
+void read_ripple_field(Tank& t, int field, void* out, size_t bytes) {
+  const TankDev& D = t.d;
+  if (D.rx <= 0) throw Error(-6, "this tank has no ripple layer");
+  RippleState& r = ensure(t);
+  CK(cudaStreamSynchronize(t.stream));
+  const size_t nv = (size_t)(D.rx + 1) * (D.rz + 1);
+  auto need = [&](size_t b) { if (bytes < b) throw Error(-1, "read_grid: output buffer too small (" + std::to_string(b) + " bytes needed)"); };
+  if (field == 7) {
+    need(nv * 8);
+    std::vector<long long> v(nv);
+    CK(cudaMemcpy(v.data(), D.rsrc, nv * 8, cudaMemcpyDeviceToHost));
+    double* o = (double*)out;
+    for (size_t i = 0; i < nv; ++i) o[i] = (double)v[i] / kRippleFix;
+  } else if (field == 8) {
+    need(nv * 12);
+    std::vector<float4> v(nv);
+    CK(cudaMemcpy(v.data(), r.field, nv * 16, cudaMemcpyDeviceToHost));
+    float* o = (float*)out;
+    for (size_t i = 0; i < nv; ++i) { o[3 * i] = v[i].x; o[3 * i + 1] = v[i].y; o[3 * i + 2] = v[i].z; }
+  } else if (field == 9) {
+    need((size_t)r.W * r.W * 4);
+    std::vector<double> v((size_t)r.W * r.W);
+    CK(cudaMemcpy(v.data(), r.top, v.size() * 8, cudaMemcpyDeviceToHost));
+    float* o = (float*)out;
+    for (size_t i = 0; i < v.size(); ++i) o[i] = (float)v[i];
+  } else if (field == 10) {
+    need((size_t)r.Mx * r.Mz * 8);
+    CK(cudaMemcpy(out, r.S, (size_t)r.Mx * r.Mz * 8, cudaMemcpyDeviceToHost));
+  } else if (field == 11) {
+    need(nv * 4);
+    CK(cudaMemcpy(out, r.mask, nv * 4, cudaMemcpyDeviceToHost));
+  } else {
+    throw Error(-1, "unknown grid field");
+  }
+}
+
+}  // namespace suiri

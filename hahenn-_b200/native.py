@@ -1,0 +1,115 @@
+"""ctypes binding of libsuiri_cuda.so (include/suiri.h).
+
+The library is the only implementation: there is no CPU fallback. Loading fails loudly when the in-tree
+build is missing; build it with ``python hahenn-_b200/build.py``.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'libsuiri_cuda.so')
+
+OK = 0
+ERR = {-1: 'invalid argument', -2: 'CUDA error', -3: 'out of memory', -4: 'capacity reached', -5: 'parse error',
+       -6: 'invalid state'}
+
+FIELD_CELL_COUNT, FIELD_FRAC, FIELD_VEL, FIELD_VELOLD, FIELD_MASK, FIELD_PRES, FIELD_RHS = range(7)
+FIELD_RIPPLE_SRC, FIELD_RIPPLE, FIELD_TOP, FIELD_RIPPLE_STATE, FIELD_RIPPLE_MASK = 7, 8, 9, 10, 11
+
+
+class Params(C.Structure):
+    _fields_ = [('size', C.c_uint32), ('nx', C.c_int32), ('ny', C.c_int32), ('nz', C.c_int32), ('h', C.c_double),
+                ('quality', C.c_char_p), ('clamp_tank', C.c_int32), ('extra_height', C.c_double),
+                ('flip', C.c_double), ('omega', C.c_double), ('iters', C.c_int32), ('gravity', C.c_double),
+                ('friction', C.c_double), ('ppc', C.c_double), ('drift', C.c_double), ('ww_rate', C.c_double),
+                ('whitewater', C.c_int32), ('capacity', C.c_int64), ('ww_capacity', C.c_int64),
+                ('ripple_rx', C.c_int32), ('ripple_rz', C.c_int32), ('wmap', C.c_int32), ('sdf_mode', C.c_int32),
+                ('device', C.c_int32), ('seed', C.c_uint32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [('count', C.c_int64), ('ww_count', C.c_int64), ('impacts', C.c_int64), ('vmax', C.c_double),
+                ('time', C.c_double), ('liters', C.c_double), ('full', C.c_int32), ('frame', C.c_int32),
+                ('nx', C.c_int32), ('ny', C.c_int32), ('nz', C.c_int32), ('h', C.c_double),
+                ('origin', C.c_double * 3)]
+
+
+class Object(C.Structure):
+    _fields_ = [('type', C.c_int32), ('flag', C.c_int32), ('pos', C.c_double * 3), ('rot', C.c_double * 9),
+                ('dims', C.c_double * 4), ('lin', C.c_double * 3), ('ang', C.c_double * 3)]
+
+
+class Emitter(C.Structure):
+    _fields_ = [('shape', C.c_int32), ('airborne', C.c_int32), ('pos', C.c_double * 3), ('dir', C.c_double * 3),
+                ('radius', C.c_double), ('speed', C.c_double), ('per_substep', C.c_double)]
+
+
+P = C.c_void_p
+# name: (restype, argtypes) for every entry point of include/suiri.h
+SIGNATURES = {
+    'suiri_set_emitters': (C.c_int, [P, C.POINTER(Emitter), C.c_int32]),
+    'suiri_profile': (C.c_int, [P, C.c_int32]),
+    'suiri_sor_phase_ms': (C.c_int, [P, C.POINTER(C.c_double)]),
+    'suiri_batch_profile': (C.c_int, [P, C.c_int32]),
+    'suiri_batch_sor_phase_ms': (C.c_int, [P, C.POINTER(C.c_double)]),
+    'suiri_params_default': (C.c_int, [C.POINTER(Params)]),
+    'suiri_create': (C.c_int, [C.c_char_p, C.POINTER(Params), C.POINTER(P)]),
+    'suiri_destroy': (C.c_int, [P]),
+    'suiri_last_error': (C.c_char_p, [P]),
+    'suiri_reset': (C.c_int, [P]),
+    'suiri_clear': (C.c_int, [P]),
+    'suiri_set_objects': (C.c_int, [P, C.c_char_p, C.c_double, C.POINTER(C.c_int32)]),
+    'suiri_set_obstacles': (C.c_int, [P, C.POINTER(Object), C.c_int32]),
+    'suiri_set_lattice': (C.c_int, [P, P, P, C.c_int32, C.c_int32, C.c_int32]),
+    'suiri_add_particles': (C.c_int, [P, P, P, P, C.c_int64, C.POINTER(C.c_uint32)]),
+    'suiri_emit_block': (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int32]),
+    'suiri_substep': (C.c_int, [P, C.c_double]),
+    'suiri_step': (C.c_int, [P, C.c_double, C.POINTER(C.c_int32)]),
+    'suiri_sync': (C.c_int, [P]),
+    'suiri_read_particles': (C.c_int, [P, P, P, C.c_int64, C.POINTER(C.c_int64)]),
+    'suiri_read_whitewater': (C.c_int, [P, P, P, C.c_int64, C.POINTER(C.c_int64)]),
+    'suiri_read_grid': (C.c_int, [P, C.c_int32, P, C.c_size_t]),
+    'suiri_get_stats': (C.c_int, [P, C.POINTER(Stats)]),
+    'suiri_snapshot': (C.c_int, [P, C.POINTER(C.c_int32)]),
+    'suiri_restore': (C.c_int, [P, C.c_int32]),
+    'suiri_stream': (C.c_int, [P, C.POINTER(P)]),
+    'suiri_use_graphs': (C.c_int, [P, C.c_int32]),
+    'suiri_batch_create': (C.c_int, [C.POINTER(P), C.c_int32, C.POINTER(P)]),
+    'suiri_batch_destroy': (C.c_int, [P]),
+    'suiri_batch_substep': (C.c_int, [P, C.c_double]),
+    'suiri_batch_sync': (C.c_int, [P]),
+    'suiri_batch_tune': (C.c_int, [P, C.c_int32, C.c_int32]),
+    'suiri_batch_stream': (C.c_int, [P, C.POINTER(P)]),
+    'suiri_time_substeps': (C.c_int, [P, C.c_double, C.c_int32, C.POINTER(C.c_double)]),
+    'suiri_batch_time_substeps': (C.c_int, [P, C.c_double, C.c_int32, C.POINTER(C.c_double)]),
+    'suiri_time_sor': (C.c_int, [P, C.c_int32, C.POINTER(C.c_double)]),
+}
+
+_lib = None
+
+
+class SuiriError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f'{ERR.get(code, code)}: {msg}')
+        self.code = code
+
+
+def lib():
+    """The loaded library (declares every signature on first use)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f'{LIB_PATH} is missing: build it with `python hahenn-_b200/build.py`')
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype, f.argtypes = res, args
+        _lib = L
+    return _lib
+
+
+def check(rc, handle=None):
+    if rc != OK:
+        msg = lib().suiri_last_error(handle)
+        raise SuiriError(rc, msg.decode(errors='replace') if msg else '')
+    return rc

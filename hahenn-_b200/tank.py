@@ -1,0 +1,290 @@
+"""Python host API over libsuiri_cuda.so, mirroring the reference's two front-ends for the liquid step:
+
+* the web version's ``FluidSim`` (``src/js/50-sim.js:28-376``): construction from a scene, ``set_objects``,
+  ``step(frame_dt)``, ``clear_water``, ``save_water``/``restore_water``, ``stats``, ``water_liters``;
+* the Blender add-on's ``Solver`` (``blender_addon/suiri_lab/solver.py:58-794``): ``emit_block``, ``step``,
+  ``set_solids`` (a distance lattice), and ``pos``/``vel``/``air`` arrays, ``liters``.
+
+Every call goes through the C ABI; all state lives on the GPU.
+"""
+import ctypes as C
+import json
+
+import numpy as np
+
+from . import native as N
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+class Tank:
+    """One tank on the GPU (the plain drop-in path)."""
+
+    def __init__(self, scene=None, *, nx=0, ny=0, nz=0, h=0.0, quality='standard', clamp_tank=True,
+                 extra_height=0.0, flip=0.96, omega=1.6, iters=0, gravity=9.81, friction=0.03, ppc=8.0, drift=6.0,
+                 ww_rate=7.0, whitewater=True, capacity=0, ww_capacity=0, ripple=(0, 0), wmap=0, sdf_mode='analytic',
+                 device=0, seed=1):
+        L = N.lib()
+        p = N.Params()
+        N.check(L.suiri_params_default(C.byref(p)))
+        p.nx, p.ny, p.nz, p.h = int(nx), int(ny), int(nz), float(h)
+        self._quality = quality.encode()
+        p.quality = self._quality
+        p.clamp_tank = 1 if clamp_tank else 0
+        p.extra_height = float(extra_height)
+        p.flip, p.omega, p.iters, p.gravity, p.friction = float(flip), float(omega), int(iters), float(gravity), float(friction)
+        p.ppc, p.drift, p.ww_rate, p.whitewater = float(ppc), float(drift), float(ww_rate), 1 if whitewater else 0
+        p.capacity, p.ww_capacity = int(capacity), int(ww_capacity)
+        if ripple is None:
+            p.ripple_rx = p.ripple_rz = -1
+        else:
+            p.ripple_rx, p.ripple_rz = int(ripple[0]), int(ripple[1])
+        p.wmap = int(wmap)
+        p.sdf_mode = {'analytic': 0, 'lattice': 1}[sdf_mode]
+        p.device, p.seed = int(device), int(seed)
+        if scene is not None and not isinstance(scene, (str, bytes)):
+            scene = json.dumps(scene)
+        h_ = C.c_void_p()
+        N.check(L.suiri_create(scene.encode() if isinstance(scene, str) else scene, C.byref(p), C.byref(h_)))
+        self._h = h_
+        st = self.stats()
+        self.nx, self.ny, self.nz, self.h = st['nx'], st['ny'], st['nz'], st['h']
+        self.origin = np.array(st['origin'])
+        self.ns = (self.nx + 1, self.ny + 1, self.nz + 1)
+
+    # ------------------------------------------------------------------ lifecycle
+    def close(self):
+        if getattr(self, '_h', None):
+            N.lib().suiri_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc):
+        return N.check(rc, self._h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ------------------------------------------------------------------ scene
+    def set_objects(self, items, dt_move=0.0):
+        """setObjects (``50-sim.js:165-211``): obstacles and drains from scene items; returns 'moving'."""
+        mv = C.c_int32()
+        self._c(N.lib().suiri_set_objects(self._h, json.dumps(items).encode(), float(dt_move), C.byref(mv)))
+        return bool(mv.value)
+
+    def set_obstacles(self, objs):
+        """Binary obstacle records: dicts with type, flag, pos, rot (3x3), dims (4), lin, ang."""
+        arr = (N.Object * max(1, len(objs)))()
+        for i, o in enumerate(objs):
+            r = arr[i]
+            r.type, r.flag = int(o['type']), int(o['flag'])
+            r.pos[:] = [float(v) for v in o['pos']]
+            r.rot[:] = [float(v) for v in np.asarray(o['rot'], float).ravel()]
+            r.dims[:] = [float(v) for v in o['dims']]
+            r.lin[:] = [float(v) for v in o.get('lin', (0, 0, 0))]
+            r.ang[:] = [float(v) for v in o.get('ang', (0, 0, 0))]
+        self._c(N.lib().suiri_set_obstacles(self._h, arr, len(objs)))
+
+    def set_lattice(self, sdf, oid=None):
+        """Solids lattice [i, j, k] (``solver.py:47-56``) — switches to lattice mode."""
+        sdf = np.asarray(sdf, np.float64)
+        lx, ly, lz = sdf.shape
+        s = np.ascontiguousarray(sdf.transpose(2, 1, 0))
+        o = None if oid is None else np.ascontiguousarray(np.asarray(oid, np.int32).transpose(2, 1, 0))
+        self._c(N.lib().suiri_set_lattice(self._h, _ptr(s), _ptr(o), lx, ly, lz))
+
+    # ------------------------------------------------------------------ water
+    def add_particles(self, pos, vel=None, air=None):
+        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        vel = None if vel is None else np.ascontiguousarray(vel, np.float32).reshape(-1, 3)
+        air = None if air is None else np.ascontiguousarray(air, np.float32).reshape(-1)
+        first = C.c_uint32()
+        self._c(N.lib().suiri_add_particles(self._h, _ptr(pos), _ptr(vel), _ptr(air), len(pos), C.byref(first)))
+        return first.value
+
+    def set_emitters(self, emitters):
+        """Fixed-rate device emitters: dicts with shape ('disc' | 'rain'), pos, dir, radius, speed,
+        count (particles per sub-step) and airborne."""
+        arr = (N.Emitter * max(1, len(emitters)))()
+        for i, e in enumerate(emitters):
+            r = arr[i]
+            r.shape = {'disc': 0, 'rain': 3}[e.get('shape', 'disc')]
+            r.airborne = 1 if e.get('airborne', False) else 0
+            r.pos[:] = [float(v) for v in e['pos']]
+            r.dir[:] = [float(v) for v in e.get('dir', (0.0, -1.0, 0.0))]
+            r.radius, r.speed, r.per_substep = float(e['radius']), float(e['speed']), float(e['count'])
+        self._c(N.lib().suiri_set_emitters(self._h, arr, len(emitters)))
+
+    def emit_block(self, lo, hi, fill=False):
+        lo_ = (C.c_double * 3)(*[float(v) for v in lo])
+        hi_ = (C.c_double * 3)(*[float(v) for v in hi])
+        self._c(N.lib().suiri_emit_block(self._h, lo_, hi_, 1 if fill else 0))
+
+    def reset(self):
+        self._c(N.lib().suiri_reset(self._h))
+
+    def clear_water(self):
+        self._c(N.lib().suiri_clear(self._h))
+
+    def save_water(self):
+        i = C.c_int32()
+        self._c(N.lib().suiri_snapshot(self._h, C.byref(i)))
+        return i.value
+
+    def restore_water(self, copy_id):
+        try:
+            self._c(N.lib().suiri_restore(self._h, int(copy_id)))
+            return True
+        except N.SuiriError as e:
+            if e.code == -6:
+                return False
+            raise
+
+    # ------------------------------------------------------------------ time stepping
+    def substep(self, dt):
+        self._c(N.lib().suiri_substep(self._h, float(dt)))
+
+    def step(self, frame_dt):
+        n = C.c_int32()
+        self._c(N.lib().suiri_step(self._h, float(frame_dt), C.byref(n)))
+        return n.value
+
+    def sync(self):
+        self._c(N.lib().suiri_sync(self._h))
+
+    def use_graphs(self, on=True):
+        self._c(N.lib().suiri_use_graphs(self._h, 1 if on else 0))
+
+    def time_substeps(self, dt, steps):
+        ms = C.c_double()
+        self._c(N.lib().suiri_time_substeps(self._h, float(dt), int(steps), C.byref(ms)))
+        return ms.value
+
+    def time_sor(self, iters):
+        ms = C.c_double()
+        self._c(N.lib().suiri_time_sor(self._h, int(iters), C.byref(ms)))
+        return ms.value
+
+    def stream(self):
+        s = C.c_void_p()
+        self._c(N.lib().suiri_stream(self._h, C.byref(s)))
+        return s.value
+
+    def profile(self, on=True):
+        self._c(N.lib().suiri_profile(self._h, 1 if on else 0))
+
+    def sor_phase_ms(self):
+        ms = C.c_double()
+        self._c(N.lib().suiri_sor_phase_ms(self._h, C.byref(ms)))
+        return ms.value
+
+    # ------------------------------------------------------------------ read-back
+    def particles(self):
+        """(pos (N,3), vel (N,3), air (N,), id (N,) uint32) of the liquid particles."""
+        n = C.c_int64()
+        self._c(N.lib().suiri_read_particles(self._h, None, None, 0, C.byref(n)))
+        P = np.empty((n.value, 4), np.float32)
+        V = np.empty((n.value, 4), np.float32)
+        self._c(N.lib().suiri_read_particles(self._h, _ptr(P), _ptr(V), n.value, C.byref(n)))
+        return P[:, :3].copy(), V[:, :3].copy(), P[:, 3].copy(), V[:, 3].copy().view(np.uint32)
+
+    @property
+    def pos(self):
+        return self.particles()[0].astype(np.float64)
+
+    @property
+    def vel(self):
+        return self.particles()[1].astype(np.float64)
+
+    @property
+    def air(self):
+        return self.particles()[2].astype(np.float64)
+
+    def whitewater(self):
+        n = C.c_int64()
+        self._c(N.lib().suiri_read_whitewater(self._h, None, None, 0, C.byref(n)))
+        P = np.empty((n.value, 4), np.float32)
+        V = np.empty((n.value, 4), np.float32)
+        self._c(N.lib().suiri_read_whitewater(self._h, _ptr(P), _ptr(V), n.value, C.byref(n)))
+        return P, V
+
+    def grid(self, field):
+        """A grid field as the oracle indexes it: faces (3, nx+1, ny+1, nz+1), cells (nx, ny, nz)."""
+        nx, ny, nz = self.nx, self.ny, self.nz
+        L = N.lib()
+        if field in (N.FIELD_CELL_COUNT, N.FIELD_PRES, N.FIELD_RHS):
+            out = np.empty((nz, ny, nx), np.int32 if field == N.FIELD_CELL_COUNT else np.float32)
+            self._c(L.suiri_read_grid(self._h, field, _ptr(out), out.nbytes))
+            return out.transpose(2, 1, 0)
+        if field in (N.FIELD_FRAC, N.FIELD_VEL, N.FIELD_VELOLD, N.FIELD_MASK):
+            out = np.empty((3, nz + 1, ny + 1, nx + 1), np.uint8 if field == N.FIELD_MASK else np.float32)
+            self._c(L.suiri_read_grid(self._h, field, _ptr(out), out.nbytes))
+            out = out.transpose(0, 3, 2, 1)
+            return out.astype(bool) if field == N.FIELD_MASK else out
+        raise ValueError('use ripple_field / top_height for ripple fields')
+
+    def ripple_field(self, field, shape, dtype):
+        out = np.empty(shape, dtype)
+        self._c(N.lib().suiri_read_grid(self._h, field, _ptr(out), out.nbytes))
+        return out
+
+    def stats(self):
+        s = N.Stats()
+        self._c(N.lib().suiri_get_stats(self._h, C.byref(s)))
+        return dict(count=s.count, ww_count=s.ww_count, impacts=s.impacts, vmax=s.vmax, time=s.time, liters=s.liters,
+                    full=bool(s.full), frame=s.frame, nx=s.nx, ny=s.ny, nz=s.nz, h=s.h, origin=tuple(s.origin))
+
+    @property
+    def water_liters(self):
+        return self.stats()['liters']
+
+    liters = water_liters
+
+
+class Batch:
+    """Many tanks stepped by shared launches (one descriptor table, one CUDA graph per sub-step)."""
+
+    def __init__(self, tanks):
+        self.tanks = list(tanks)
+        arr = (C.c_void_p * len(self.tanks))(*[t.handle.value for t in self.tanks])
+        h = C.c_void_p()
+        N.check(N.lib().suiri_batch_create(arr, len(self.tanks), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, '_h', None):
+            N.lib().suiri_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def substep(self, dt):
+        N.check(N.lib().suiri_batch_substep(self._h, float(dt)))
+
+    def sync(self):
+        N.check(N.lib().suiri_batch_sync(self._h))
+
+    def tune(self, blocks_per_sm, sweeps_per_launch=1):
+        N.check(N.lib().suiri_batch_tune(self._h, int(blocks_per_sm), int(sweeps_per_launch)))
+
+    def time_substeps(self, dt, steps):
+        ms = C.c_double()
+        N.check(N.lib().suiri_batch_time_substeps(self._h, float(dt), int(steps), C.byref(ms)))
+        return ms.value
+
+    def stream(self):
+        s = C.c_void_p()
+        N.check(N.lib().suiri_batch_stream(self._h, C.byref(s)))
+        return s.value

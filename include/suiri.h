@@ -1,0 +1,213 @@
+/* libsuiri_cuda.so — B200-native FLIP liquid step of 水理ラボ (suiri-lab), C ABI.
+ *
+ * Plain pointers and sizes only; no CUDA or PyTorch types in the signatures. Every function returns
+ * SUIRI_OK (0) or a negative SUIRI_ERR_* code; the message of the last failure of a handle is
+ * suiri_last_error(handle) (suiri_last_error(NULL): the last failure of this thread without a handle).
+ * No exception crosses the ABI.
+ *
+ * Coordinates are the reference's solver coordinates: metres, y up, floor at y = 0, the tank centred on
+ * x = z = 0 (blender_addon/suiri_lab/solver.py:5-7, src/js/50-sim.js:38).
+ *
+ * Threading: a handle belongs to one host thread at a time. Each tank (and each batch) has its own CUDA
+ * stream; stepping functions enqueue work and return; reads, stats and suiri_sync block.
+ */
+#ifndef SUIRI_H
+#define SUIRI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SUIRI_OK 0
+#define SUIRI_ERR_INVALID (-1)   /* bad argument or handle */
+#define SUIRI_ERR_CUDA (-2)      /* a CUDA call failed (message names it) */
+#define SUIRI_ERR_NOMEM (-3)     /* device memory or HBM budget exhausted */
+#define SUIRI_ERR_CAPACITY (-4)  /* particle capacity reached (the particles that fit were kept) */
+#define SUIRI_ERR_PARSE (-5)     /* malformed scene JSON */
+#define SUIRI_ERR_STATE (-6)     /* call not valid now (e.g. restoring a consumed snapshot) */
+
+typedef struct suiri_tank suiri_tank;
+typedef struct suiri_batch suiri_batch;
+typedef struct suiri_server suiri_server;
+
+/* Construction parameters. Fill with suiri_params_default, then change what differs. */
+typedef struct suiri_params {
+  uint32_t size;           /* sizeof(suiri_params) */
+  /* grid: nx,ny,nz,h > 0 give it explicitly; otherwise it is derived from the scene's tank size and
+     the quality's cell size like FluidSim (src/js/50-sim.js:31-38): n = max(8, round(size/h)),
+     h = min(w/nx, h/ny, d/nz), origin (-nx h/2, 0, -nz h/2) */
+  int32_t nx, ny, nz;
+  double h;
+  const char* quality;     /* "low" | "standard" | "high" (src/js/50-sim.js:4-8) */
+  int32_t clamp_tank;      /* 1: the editor's tank limits apply to scene JSON (src/js/80-ui.js:459) */
+  double extra_height;     /* obstacle lattice above the rim [m] (solver.py:69-70) */
+  /* physics (src/js/50-sim.js:151-162, solver.py:11-21) */
+  double flip;             /* FLIP/PIC blend (0.96) */
+  double omega;            /* SOR over-relaxation (1.6) */
+  int32_t iters;           /* SOR iterations (quality) */
+  double gravity;          /* 9.81 */
+  double friction;         /* 0.03 */
+  double ppc;              /* particles per cell at rest (8) */
+  double drift;            /* drift correction strength (6) */
+  double ww_rate;          /* whitewater spawn rate (7) */
+  int32_t whitewater;      /* 1: spawn and advance whitewater */
+  /* capacities */
+  int64_t capacity;        /* particles (quality cap) */
+  int64_t ww_capacity;     /* whitewater particles (quality ww) */
+  /* ripple layer: (rx+1)×(rz+1) vertices over the footprint; 0,0 → quality R×R; -1 → none */
+  int32_t ripple_rx, ripple_rz;
+  int32_t wmap;            /* top-view height map texels per side (256/384) */
+  int32_t sdf_mode;        /* 0 analytic obstacle shapes (web version), 1 distance lattice (Blender) */
+  int32_t device;          /* CUDA device ordinal */
+  uint32_t seed;           /* emission jitter seed */
+} suiri_params;
+
+typedef struct suiri_stats {
+  int64_t count;           /* liquid particles */
+  int64_t ww_count;        /* whitewater particles */
+  int64_t impacts;         /* sub-grid drops merged so far */
+  double vmax;             /* max speed of in-grid particles in the last sub-step */
+  double time;             /* simulated time [s] */
+  double liters;           /* count · (h/2)³ · 1000 (src/js/50-sim.js:375) */
+  int32_t full;            /* capacity was reached */
+  int32_t frame;           /* sub-steps taken */
+  int32_t nx, ny, nz;
+  double h;
+  double origin[3];
+} suiri_stats;
+
+/* An obstacle or drain in binary form (instead of scene JSON items). */
+typedef struct suiri_object {
+  int32_t type;            /* 0 round box, 1 sphere, 2 cylinder, 3 cone, 4 torus, 5 cup, 6 container,
+                              7 gutter; 9 drain cylinder */
+  int32_t flag;            /* 1 obstacle, 2 drain */
+  double pos[3];
+  double rot[9];           /* world-from-local rotation, row major */
+  double dims[4];          /* shape parameters as src/js/10-scene.js:143-157 packs them */
+  double lin[3], ang[3];   /* solid velocity: linear and angular */
+} suiri_object;
+
+/* grid fields for suiri_read_grid (parity dumps; arrays x fastest) */
+enum suiri_field {
+  SUIRI_FIELD_CELL_COUNT = 0,  /* int32 [nz][ny][nx]: particles per cell */
+  SUIRI_FIELD_FRAC = 1,        /* float32 [3][nz+1][ny+1][nx+1]: face open fractions */
+  SUIRI_FIELD_VEL = 2,         /* float32 [3][nz+1][ny+1][nx+1]: face velocity (after projection) */
+  SUIRI_FIELD_VELOLD = 3,      /* float32 [3][nz+1][ny+1][nx+1]: P2G face velocity */
+  SUIRI_FIELD_MASK = 4,        /* uint8  [3][nz+1][ny+1][nx+1]: face took particle weight */
+  SUIRI_FIELD_PRES = 5,        /* float32 [nz][ny][nx]: pressure */
+  SUIRI_FIELD_RHS = 6,         /* float32 [nz][ny][nx]: h²·divergence (SOR right-hand side) */
+  SUIRI_FIELD_RIPPLE_SRC = 7,  /* float64 [rz+1][rx+1]: pending ripple impulses [N·s] */
+  SUIRI_FIELD_RIPPLE = 8,      /* float32 [rz+1][rx+1][3]: ripple height, slope x, slope z */
+  SUIRI_FIELD_TOP = 9,         /* float32 [wmap][wmap]: top-view water height, -1 dry */
+  SUIRI_FIELD_RIPPLE_STATE = 10, /* float32 [2rz][2rx][2]: spectral state (height + i·velocity) */
+  SUIRI_FIELD_RIPPLE_MASK = 11 /* float32 [rz+1][rx+1]: absorption mask of the last frame */
+};
+
+/* ---------------------------------------------------------------- one tank (the plain drop-in path) */
+
+int suiri_params_default(suiri_params* p);
+
+/* FluidSim constructor + setObjects + emitNow(blockEmits) (src/js/50-sim.js:29-89, src/js/90-main.js:5-13).
+   scene_json may be NULL: an empty tank with the explicit grid of `params`. */
+int suiri_create(const char* scene_json, const suiri_params* params, suiri_tank** out);
+int suiri_destroy(suiri_tank* t);
+const char* suiri_last_error(const suiri_tank* t);
+
+/* restartWater (src/js/90-main.js:15-19): clear, then refill the scene's water blocks */
+int suiri_reset(suiri_tank* t);
+/* clearWater (src/js/50-sim.js:365-373) */
+int suiri_clear(suiri_tank* t);
+
+/* setObjects (src/js/50-sim.js:165-211): obstacles and drains from scene items JSON ([…] or {items:[…]});
+   velocities from the previous transforms over dt_move; *moving = 1 if any moves (may be NULL) */
+int suiri_set_objects(suiri_tank* t, const char* items_json, double dt_move, int32_t* moving);
+/* the same from binary records */
+int suiri_set_obstacles(suiri_tank* t, const suiri_object* objs, int32_t n);
+/* Solids lattice of the Blender host (solver.py:47-56, bake.py:83-181): distances at the half-cell points
+   origin + h/2·(i,j,k), (2nx+1)(2nyl+1)(2nz+1), i fastest; oid (may be NULL) = obstacle index per point.
+   Switches the tank to lattice mode for face fractions and collisions. */
+int suiri_set_lattice(suiri_tank* t, const double* sdf, const int32_t* oid, int32_t lx, int32_t ly, int32_t lz);
+
+/* particles from host arrays, appended before the next sub-step (emit_block/_add, solver.py:304-343).
+   pos, vel: n×3 float32; airborne: n floats (0/1) or NULL. *first_id (may be NULL) = id of the first. */
+int suiri_add_particles(suiri_tank* t, const float* pos, const float* vel, const float* airborne, int64_t n,
+                        uint32_t* first_id);
+/* Fixed-rate emitters run on the device inside every sub-step (also inside a captured CUDA graph): shape 0
+   a disc outlet of `radius` at pos pointing along dir at `speed` (the stream source, src/js/31-wgsl-sim2.js:
+   276-288), shape 3 a square rain area of half side `radius` falling at `speed` (:307-310). per_substep
+   particles each sub-step, fractions carried over. At most 8; n = 0 removes them. */
+typedef struct suiri_emitter {
+  int32_t shape;
+  int32_t airborne;        /* 1: emitted particles carry the free-flight mark (sub-grid drops) */
+  double pos[3];
+  double dir[3];
+  double radius;
+  double speed;
+  double per_substep;
+} suiri_emitter;
+int suiri_set_emitters(suiri_tank* t, const suiri_emitter* e, int32_t n);
+
+/* a water block as a jittered half-cell lattice clipped to the tank (src/js/55-emit.js:83-106, solver.py:317-343);
+   fill = 1 skips cells already at least half full */
+int suiri_emit_block(suiri_tank* t, const double lo[3], const double hi[3], int32_t fill);
+
+/* one sub-step of fixed length dt (FluidSim.encodeSubstep, src/js/50-sim.js:276-297; solver.py:438-525) */
+int suiri_substep(suiri_tank* t, double dt);
+/* one frame: CFL sub-steps, scene sources, whitewater, top height and ripples
+   (FluidSim.step src/js/50-sim.js:300-336; Solver.step solver.py:716-728). *substeps may be NULL. */
+int suiri_step(suiri_tank* t, double frame_dt, int32_t* substeps);
+int suiri_sync(suiri_tank* t);
+
+/* liquid particles (alive) to host memory: pos4 = (x, y, z, airborne), vel4 = (vx, vy, vz, id as uint32 bits);
+   either pointer may be NULL; *n = number available (written even when cap is too small) */
+int suiri_read_particles(suiri_tank* t, float* pos4, float* vel4, int64_t cap, int64_t* n);
+/* whitewater: pos4 = (x, y, z, life), vel4 = (vx, vy, vz, kind) */
+int suiri_read_whitewater(suiri_tank* t, float* pos4, float* vel4, int64_t cap, int64_t* n);
+/* a grid field (enum suiri_field) into out (bytes long) */
+int suiri_read_grid(suiri_tank* t, int32_t field, void* out, size_t bytes);
+int suiri_get_stats(suiri_tank* t, suiri_stats* s);
+
+/* saveWater / restoreWater (src/js/50-sim.js:111-141): one copy slot per tank, on the device */
+int suiri_snapshot(suiri_tank* t, int32_t* id);
+int suiri_restore(suiri_tank* t, int32_t id);
+
+/* interop: the tank's cudaStream_t (as void*) and device ordinal */
+int suiri_stream(suiri_tank* t, void** stream);
+/* 1: capture the sub-step as a CUDA graph and replay it (default 1) */
+int suiri_use_graphs(suiri_tank* t, int32_t on);
+
+/* ---------------------------------------------------------------- batching: many tanks, one set of launches */
+
+/* a batch steps existing tanks (same device) together: every kernel of the sub-step covers all of them
+   in one launch, through per-tank descriptor and block-offset tables; the sub-step is one CUDA graph */
+int suiri_batch_create(suiri_tank* const* tanks, int32_t n, suiri_batch** out);
+int suiri_batch_destroy(suiri_batch* b);
+int suiri_batch_substep(suiri_batch* b, double dt);
+int suiri_batch_sync(suiri_batch* b);
+/* tuning knobs picked by the autotuner: particle-kernel blocks per SM, SOR sweeps per launch */
+int suiri_batch_tune(suiri_batch* b, int32_t particle_blocks_per_sm, int32_t sor_sweeps_per_launch);
+int suiri_batch_stream(suiri_batch* b, void** stream);
+
+/* ---------------------------------------------------------------- timing helpers (device events) */
+
+/* milliseconds of device time of `steps` sub-steps of dt, events on the tank's / batch's own stream */
+int suiri_time_substeps(suiri_tank* t, double dt, int32_t steps, double* ms);
+int suiri_batch_time_substeps(suiri_batch* b, double dt, int32_t steps, double* ms);
+/* milliseconds per launch of the SOR sweeps alone, timed over `iters` iterations on the current state
+   (this relaxes the current pressure further) */
+int suiri_time_sor(suiri_tank* t, int32_t iters, double* ms);
+/* 1: record device events around the pressure solve of every sub-step (inside the captured graph);
+   suiri_sor_phase_ms then gives the last sub-step's pressure-solve time (waits for it) */
+int suiri_profile(suiri_tank* t, int32_t on);
+int suiri_sor_phase_ms(suiri_tank* t, double* ms);
+int suiri_batch_profile(suiri_batch* b, int32_t on);
+int suiri_batch_sor_phase_ms(suiri_batch* b, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SUIRI_H */

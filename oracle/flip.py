@@ -388,26 +388,9 @@ class Tank:
         Non-liquid cells hold zero pressure, the outside of the grid reads as zero (its wall faces have
         coefficient 0, the open top has coefficient 1: Dirichlet p = 0). Equivalent to the reference's
         bounding-box form, whose extra margin only ever touches non-liquid cells."""
-        nx, ny, nz = self.nx, self.ny, self.nz
-        f32 = np.float32
         C, inv, U, rhs = self.sor_operands(self.div, fluid)
-        P = np.zeros((nx + 2, ny + 2, nz + 2), f32)
-        Pi = P[1:-1, 1:-1, 1:-1]
-        Pi[...] = np.where(fluid, self.pres, 0.0) if p_init is None else p_init
-        nbr = (P[:-2, 1:-1, 1:-1], P[2:, 1:-1, 1:-1], P[1:-1, :-2, 1:-1], P[1:-1, 2:, 1:-1], P[1:-1, 1:-1, :-2], P[1:-1, 1:-1, 2:])
-        num = np.empty((nx, ny, nz), f32); tmp = np.empty((nx, ny, nz), f32)
-        for _ in range(self.iters if iters is None else iters):
-            for Uc in U:
-                np.multiply(C[0], nbr[0], out=num)
-                for d in range(1, 6):
-                    np.multiply(C[d], nbr[d], out=tmp)
-                    num += tmp
-                num -= rhs
-                num *= inv
-                num -= Pi
-                num *= Uc
-                Pi += num
-        p = Pi.astype(np.float64)
+        p0 = np.where(fluid, self.pres, 0.0) if p_init is None else p_init
+        p = sor_f32(C, inv, U, rhs, p0, self.iters if iters is None else iters)
         p[~fluid] = 0
         self.pres = p
         return p
@@ -701,6 +684,46 @@ class Tank:
                + F[2][:nx, :ny, 1:nz + 1] - F[2][:nx, :ny, :nz]) / h
         fl = self.count > 0
         return float(np.abs(div[fl]).max()) if fl.any() else 0.0
+
+
+def sor_f32(C, inv, U, rhs, p_init, iters):
+    """The float32 red-black loop of ``solver.py:489-506`` on the whole grid: C the 6 coefficient arrays
+    (x-, x+, y-, y+, z-, z+), inv = 1/ΣC, U = (ω on active cells of colour 0, of colour 1), rhs = h²·div."""
+    f32 = np.float32
+    nx, ny, nz = rhs.shape
+    P = np.zeros((nx + 2, ny + 2, nz + 2), f32)
+    Pi = P[1:-1, 1:-1, 1:-1]
+    Pi[...] = p_init
+    nbr = (P[:-2, 1:-1, 1:-1], P[2:, 1:-1, 1:-1], P[1:-1, :-2, 1:-1], P[1:-1, 2:, 1:-1], P[1:-1, 1:-1, :-2], P[1:-1, 1:-1, 2:])
+    num = np.empty((nx, ny, nz), f32); tmp = np.empty((nx, ny, nz), f32)
+    for _ in range(iters):
+        for Uc in U:
+            np.multiply(C[0], nbr[0], out=num)
+            for d in range(1, 6):
+                np.multiply(C[d], nbr[d], out=tmp)
+                num += tmp
+            num -= rhs
+            num *= inv
+            num -= Pi
+            num *= Uc
+            Pi += num
+    return Pi.astype(np.float64)
+
+
+def sor_operands_from(frac32, rhs32, fluid, omega):
+    """SOR operands from float32 face fractions (3, nx+1, ny+1, nz+1) and a float32 right-hand side, formed
+    as ``solver.py:478-487`` does."""
+    f32 = np.float32
+    nx, ny, nz = rhs32.shape
+    fx, fy, fz = (np.asarray(frac32[a], f32) for a in range(3))
+    C = [np.ascontiguousarray(a) for a in (fx[0:nx, :ny, :nz], fx[1:nx + 1, :ny, :nz], fy[:nx, 0:ny, :nz],
+                                           fy[:nx, 1:ny + 1, :nz], fz[:nx, :ny, 0:nz], fz[:nx, :ny, 1:nz + 1])]
+    den = C[0] + C[1] + C[2] + C[3] + C[4] + C[5]
+    inv = np.where(den > 0, 1.0 / np.maximum(den, 1e-30), 0.0).astype(f32)
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing='ij', sparse=True)
+    color = (ii + jj + kk) & 1
+    U = [(fluid & (den > 0) & (color == c)).astype(f32) * f32(omega) for c in (0, 1)]
+    return C, inv, U, np.asarray(rhs32, f32)
 
 
 def residual_f64(C, rhs, fluid, p):

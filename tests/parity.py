@@ -1,0 +1,89 @@
+"""Helpers shared by the parity tests: the same seeded inputs to the CUDA path and to the oracle, and the
+comparisons with their tolerances.
+
+Tolerances (stated once, used everywhere):
+  * binning / cell counts / classification / valid-face masks: bit-exact;
+  * face fractions: float32 of the same float64 value — bit-exact;
+  * P2G face velocities, pressure, projected velocities: |a - b| <= 1e-5·|b| + 1e-5·max|b| (the GPU sums
+    in 64-bit fixed point and stores float32; the CPU solver sums in float64);
+  * particles after a sub-step (matched by id): positions within 1e-6 m + 1e-6 relative,
+    velocities within 1e-5 relative + 1e-5·max|v|;
+  * ripple layer (float32 FFT against float64 numpy.fft): 1e-4 relative to the field's max.
+"""
+import numpy as np
+
+from oracle import flip as of
+from oracle import sdf as sdfm
+
+RTOL = 1e-5
+
+
+def f32(a):
+    return np.asarray(a, np.float32).astype(np.float64)
+
+
+def oracle_from(nx, ny, nz, h, origin, *, flip, omega, iters, g=9.81, whitewater=False, rng_mode='hash', sdf_mode='analytic',
+                ripple=(16, 16), wmap=32, seed=1, ww_cap=140000):
+    return of.Tank(nx, ny, nz, h, origin=origin, flip=flip, omega=omega, iters=iters, g=g, whitewater=whitewater,
+                   rng_mode=rng_mode, sdf_mode=sdf_mode, ripple=ripple, wmap=wmap, seed=seed, ww_cap=ww_cap)
+
+
+def gpu_from(pkg, nx, ny, nz, h, *, flip, omega, iters, g=9.81, whitewater=False, ripple=None, wmap=32, capacity=None,
+             sdf_mode='analytic', ww_capacity=140000, seed=1):
+    n = capacity or max(64, nx * ny * nz * 12)
+    return pkg.Tank(nx=nx, ny=ny, nz=nz, h=h, flip=flip, omega=omega, iters=iters, gravity=g, whitewater=whitewater,
+                    capacity=n, ripple=ripple, wmap=wmap, sdf_mode=sdf_mode, ww_capacity=ww_capacity, seed=seed)
+
+
+def assert_close_field(a, b, rtol=RTOL, what=''):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    assert a.shape == b.shape, (what, a.shape, b.shape)
+    scale = max(float(np.abs(b).max()) if b.size else 0.0, 1e-30)
+    err = np.abs(a - b)
+    lim = rtol * np.abs(b) + rtol * scale
+    bad = err > lim
+    assert not bad.any(), f'{what}: {int(bad.sum())} of {b.size} beyond tolerance, max err {err.max():.3e} (scale {scale:.3e})'
+
+
+def by_id(pos, vel, air, ids):
+    o = np.argsort(ids, kind='stable')
+    return pos[o], vel[o], air[o], ids[o]
+
+
+def assert_particles(gpu, ora, what=''):
+    gp, gv, ga, gi = gpu.particles()
+    gp, gv, ga, gi = by_id(gp, gv, ga, gi.astype(np.int64))
+    op, ov, oa, oi = by_id(ora.pos, ora.vel, ora.air, ora.pid)
+    assert len(gi) == len(oi), f'{what}: {len(gi)} particles on the GPU, {len(oi)} in the oracle'
+    np.testing.assert_array_equal(gi, oi)
+    np.testing.assert_array_equal(ga, oa, err_msg=f'{what}: airborne marks')
+    err = np.abs(gp - op)
+    assert np.all(err <= 1e-6 + 1e-6 * np.abs(op)), f'{what}: position err {err.max():.3e}'
+    assert_close_field(gv, ov, what=f'{what}: velocity')
+
+
+def sync_oracle_particles(gpu, ora):
+    """Continue the oracle from the GPU's float32 particle state (step-wise parity over many steps)."""
+    gp, gv, ga, gi = gpu.particles()
+    o = np.argsort(gi)
+    ora.pos, ora.vel, ora.air, ora.pid = gp[o].astype(np.float64), gv[o].astype(np.float64), ga[o].astype(np.float64), gi[o].astype(np.int64)
+
+
+def obstacle_items():
+    """Scene items (JSON form) with the oracle objects made from them."""
+    items = [dict(kind='obstacle', shape='sphere', pos=[0.15, 0.18, 0.0], rot=[0, 0, 0], dims=dict(r=0.09)),
+             dict(kind='obstacle', shape='box', pos=[-0.25, 0.1, 0.12], rot=[0, 30, 0], dims=dict(w=0.16, h=0.1, d=0.12)),
+             dict(kind='obstacle', shape='cone', pos=[-0.05, 0.1, -0.2], rot=[10, 0, 20], dims=dict(r=0.08, h=0.14)),
+             dict(kind='drain', pos=[0.38, 0.0, -0.28], rot=[0, 0, 0], r=0.06)]
+    return items, objs_from_items(items)
+
+
+def objs_from_items(items):
+    out = []
+    for it in items:
+        if it['kind'] == 'obstacle':
+            out.append(sdfm.make_obstacle(it['shape'], it['pos'], tuple(it['rot']), **it['dims']))
+        elif it['kind'] == 'drain':
+            out.append(sdfm.make_drain(it['pos'], it['r'], tuple(it['rot'])))
+    return out
