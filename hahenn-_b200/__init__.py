@@ -4,3 +4,4 @@
 """
 from . import native, workloads  # noqa: F401
 from .tank import Batch, Tank  # noqa: F401
+from .serve import Server  # noqa: F401

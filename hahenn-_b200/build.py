@@ -18,7 +18,7 @@ BUILD = os.path.join(HERE, '_build')
 NVCC = os.environ.get('NVCC', 'nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 FLAGS = ['-O3', '-lineinfo', '-std=c++17', '-fmad=false', '-Xcompiler', '-fPIC,-O3', '--expt-relaxed-constexpr']
-SOURCES = ['bin.cu', 'grid.cu', 'sor.cu', 'g2p.cu', 'ripple.cu', 'engine.cu', 'scene.cpp', 'capi.cpp']
+SOURCES = ['bin.cu', 'grid.cu', 'sor.cu', 'g2p.cu', 'ripple.cu', 'engine.cu', 'scene.cpp', 'server.cpp', 'capi.cpp']
 
 
 def _compile(src, verbose):

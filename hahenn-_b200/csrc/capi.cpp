@@ -6,6 +6,7 @@
 
 #include "../../include/suiri.h"
 #include "engine.h"
+#include "server.h"
 
 using namespace suiri;
 
@@ -17,6 +18,15 @@ struct suiri_batch {
   std::unique_ptr<Group> g;
   std::string err;
 };
+struct suiri_server {
+  std::unique_ptr<Server> s;
+  std::string err;
+};
+
+// tank configuration from parameters and an optional scene (FluidSim sizing, quality presets)
+TankConfig make_config(const suiri_params& p, const char* scene_json, Scene& sc);
+// device records of fixed-rate emitters (direction normalised, outlet basis as basisOf, src/js/55-emit.js:4-9)
+std::vector<EmitterDev> emitters_from(const suiri_emitter* e, int n);
 
 namespace {
 
@@ -144,8 +154,22 @@ int suiri_create(const char* scene_json, const suiri_params* params, suiri_tank*
   }
   std::unique_ptr<suiri_tank> h(new suiri_tank());
   const int rc = guard(nullptr, [&] {
-    const Quality& q = quality(p.quality);
     Scene sc;
+    const TankConfig c = make_config(p, scene_json, sc);
+    h->t.reset(new Tank(c));
+    h->t->scene = sc;
+    apply_solids(*h->t, sc.solids, 0.0);
+    for (const WaterBlock& b : sc.blocks) h->t->emit_block(b.lo, b.hi, false);
+  });
+  if (rc != SUIRI_OK) return rc;
+  *out = h.release();
+  return SUIRI_OK;
+}
+
+}  // extern "C"
+
+TankConfig make_config(const suiri_params& p, const char* scene_json, Scene& sc) {
+    const Quality& q = quality(p.quality);
     std::string err;
     if (scene_json) {
       const bool ok = parse_scene(scene_json, p.clamp_tank != 0, sc, err);
@@ -179,15 +203,10 @@ int suiri_create(const char* scene_json, const suiri_params* params, suiri_tank*
     c.seed = p.seed;
     if (!(c.omega > 0 && c.omega < 2)) throw Error(SUIRI_ERR_INVALID, "omega must be in (0, 2)");
     if (c.cap > (1LL << 30)) throw Error(SUIRI_ERR_INVALID, "capacity above 2^30 particles");
-    h->t.reset(new Tank(c));
-    h->t->scene = sc;
-    apply_solids(*h->t, sc.solids, 0.0);
-    for (const WaterBlock& b : sc.blocks) h->t->emit_block(b.lo, b.hi, false);
-  });
-  if (rc != SUIRI_OK) return rc;
-  *out = h.release();
-  return SUIRI_OK;
+    return c;
 }
+
+extern "C" {
 
 int suiri_destroy(suiri_tank* t) {
   if (!t) return SUIRI_ERR_INVALID;
@@ -261,8 +280,12 @@ int suiri_add_particles(suiri_tank* h, const float* pos, const float* vel, const
 }
 
 int suiri_set_emitters(suiri_tank* h, const suiri_emitter* e, int32_t n) {
-  return guard(h ? &h->err : nullptr, [&] {
-    Tank* t = T(h);
+  return guard(h ? &h->err : nullptr, [&] { T(h)->set_emitters(emitters_from(e, n)); });
+}
+
+}  // extern "C"
+
+std::vector<EmitterDev> emitters_from(const suiri_emitter* e, int n) {
     if (n < 0 || n > kMaxEmitters || (n > 0 && !e)) throw Error(SUIRI_ERR_INVALID, "0..8 emitters expected");
     std::vector<EmitterDev> v(n);
     for (int i = 0; i < n; ++i) {
@@ -284,9 +307,10 @@ int suiri_set_emitters(suiri_tank* h, const suiri_emitter* e, int32_t n) {
       d.w[1] = d.dir[2] * d.u[0] - d.dir[0] * d.u[2];
       d.w[2] = d.dir[0] * d.u[1] - d.dir[1] * d.u[0];
     }
-    t->set_emitters(v);
-  });
+    return v;
 }
+
+extern "C" {
 
 int suiri_emit_block(suiri_tank* h, const double lo[3], const double hi[3], int32_t fill) {
   return guard(h ? &h->err : nullptr, [&] {
@@ -504,6 +528,103 @@ int suiri_batch_sor_phase_ms(suiri_batch* b, double* ms) {
   return guard(b ? &b->err : nullptr, [&] {
     if (!b || !b->g || !ms) throw Error(SUIRI_ERR_INVALID, "null batch or output");
     *ms = b->g->sor_phase_ms();
+  });
+}
+
+int suiri_server_create(int32_t device, double budget_bytes, double dt, suiri_server** out) {
+  if (!out) { g_err = "null output handle"; return SUIRI_ERR_INVALID; }
+  *out = nullptr;
+  std::unique_ptr<suiri_server> s(new suiri_server());
+  const int rc = guard(nullptr, [&] {
+    if (!(budget_bytes > 0) || !(dt > 0)) throw Error(SUIRI_ERR_INVALID, "budget and dt must be positive");
+    s->s.reset(new Server(device, budget_bytes, dt));
+  });
+  if (rc != SUIRI_OK) return rc;
+  *out = s.release();
+  return SUIRI_OK;
+}
+
+int suiri_server_destroy(suiri_server* s) {
+  if (!s) return SUIRI_ERR_INVALID;
+  const int rc = guard(nullptr, [&] { s->s.reset(); });
+  delete s;
+  return rc;
+}
+
+int suiri_server_submit(suiri_server* s, const suiri_request* r, int64_t* id) {
+  return guard(s ? &s->err : nullptr, [&] {
+    if (!s || !s->s || !r || !id) throw Error(SUIRI_ERR_INVALID, "null server, request or output");
+    if (r->size != sizeof(suiri_request)) throw Error(SUIRI_ERR_INVALID, "suiri_request.size mismatch");
+    if (r->steps <= 0) throw Error(SUIRI_ERR_INVALID, "steps must be positive");
+    suiri_params p;
+    suiri_params_default(&p);
+    if (r->params) {
+      if (r->params->size != sizeof(suiri_params)) throw Error(SUIRI_ERR_INVALID, "suiri_params.size mismatch");
+      p = *r->params;
+    }
+    std::unique_ptr<Request> q(new Request());
+    q->cfg = make_config(p, r->scene_json, q->scene);
+    q->emitters = emitters_from(r->emitters, r->n_emitters);
+    q->steps = r->steps;
+    q->keep_result = r->keep_result != 0;
+    *id = s->s->submit(std::move(q));
+  });
+}
+
+int suiri_server_poll(suiri_server* s, int64_t id, int32_t* state, double* latency_ms, int64_t* count) {
+  return guard(s ? &s->err : nullptr, [&] {
+    if (!s || !s->s) throw Error(SUIRI_ERR_INVALID, "null server");
+    Server& S = *s->s;
+    std::lock_guard<std::mutex> g(S.m);
+    auto it = S.reqs.find(id);
+    if (it == S.reqs.end()) throw Error(SUIRI_ERR_INVALID, "unknown request id");
+    const Request& q = *it->second;
+    if (state) *state = q.state;
+    if (latency_ms) *latency_ms = q.state >= kDone ? 1000.0 * (q.t_done - q.t_submit) : 0.0;
+    if (count) *count = q.final_count;
+    if (q.state == kFailed) s->err = q.err;
+  });
+}
+
+int suiri_server_wait(suiri_server* s, int64_t id, double timeout_s) {
+  return guard(s ? &s->err : nullptr, [&] {
+    if (!s || !s->s) throw Error(SUIRI_ERR_INVALID, "null server");
+    Server& S = *s->s;
+    std::unique_lock<std::mutex> g(S.m);
+    auto it = S.reqs.find(id);
+    if (it == S.reqs.end()) throw Error(SUIRI_ERR_INVALID, "unknown request id");
+    Request* q = it->second.get();
+    const bool ok = S.cv.wait_for(g, std::chrono::duration<double>(timeout_s), [&] { return q->state >= kDone; });
+    if (!ok) throw Error(SUIRI_ERR_STATE, "request not finished within the timeout");
+    if (q->state == kFailed) throw Error(SUIRI_ERR_STATE, "request failed: " + q->err);
+  });
+}
+
+int suiri_server_result(suiri_server* s, int64_t id, float* pos4, float* vel4, int64_t cap, int64_t* n) {
+  return guard(s ? &s->err : nullptr, [&] {
+    if (!s || !s->s) throw Error(SUIRI_ERR_INVALID, "null server");
+    Server& S = *s->s;
+    std::lock_guard<std::mutex> g(S.m);
+    auto it = S.reqs.find(id);
+    if (it == S.reqs.end()) throw Error(SUIRI_ERR_INVALID, "unknown request id");
+    const Request& q = *it->second;
+    if (q.state != kDone || !q.keep_result) throw Error(SUIRI_ERR_STATE, "no result (not done, or submitted without keep_result)");
+    const long long k = (long long)q.res_pos.size() / 4;
+    const long long m = std::min<long long>(k, cap);
+    if (pos4 && m) memcpy(pos4, q.res_pos.data(), m * 16);
+    if (vel4 && m) memcpy(vel4, q.res_vel.data(), m * 16);
+    if (n) *n = k;
+  });
+}
+
+int suiri_server_get_stats(suiri_server* s, suiri_server_stats* st) {
+  return guard(s ? &s->err : nullptr, [&] {
+    if (!s || !s->s || !st) throw Error(SUIRI_ERR_INVALID, "null server or output");
+    const ServerStats x = s->s->stats();
+    st->completed = x.completed; st->queued = x.queued; st->running = x.running; st->failed = x.failed;
+    st->rebuilds = x.rebuilds; st->substeps = x.substeps; st->particle_steps = x.particle_steps;
+    st->elapsed_s = x.elapsed_s; st->used_bytes = x.used_bytes; st->budget_bytes = x.budget_bytes;
+    st->p50_ms = x.p50_ms; st->p99_ms = x.p99_ms; st->mean_active = x.mean_active;
   });
 }
 

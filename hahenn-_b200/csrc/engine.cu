@@ -186,7 +186,9 @@ Tank::Tank(const TankConfig& c) : cfg(c) {
   if ((long long)cfg.nx * cfg.ny * cfg.nz > (1LL << 30)) throw Error(-1, "grid too large");
   if (cfg.cap < 1) throw Error(-1, "capacity must be positive");
   CK(cudaSetDevice(cfg.device));
-  CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  if (cfg.stream) { stream = cfg.stream; own_stream = false; }
+  else CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&ev_own, cudaEventDisableTiming));
   TankDev& D = d;
   D.nx = cfg.nx; D.ny = cfg.ny; D.nz = cfg.nz; D.hx = (cfg.nx + 1) / 2;
   D.sx = cfg.nx + 1; D.sxy = (cfg.nx + 1) * (cfg.ny + 1);
@@ -241,7 +243,32 @@ Tank::~Tank() {
   free_ripple(*this);
   if (h_ctr) cudaFreeHost(h_ctr);
   if (h_stage_p) { cudaFreeHost(h_stage_p); cudaFreeHost(h_stage_v); }
-  if (stream) cudaStreamDestroy(stream);
+  if (ev_own) cudaEventDestroy(ev_own);
+  if (stream && own_stream) cudaStreamDestroy(stream);
+}
+
+void Tank::join() {
+  if (dep) {
+    CK(cudaStreamWaitEvent(stream, dep, 0));
+    dep = nullptr;
+  }
+  dirty = true;
+}
+
+size_t tank_bytes(const TankConfig& c) {
+  const size_t nn = (size_t)(c.nx + 1) * (c.ny + 1) * (c.nz + 1), nc = (size_t)c.nx * c.ny * c.nz;
+  const size_t nh = (size_t)((c.nx + 1) / 2) * c.ny * c.nz, cap = (size_t)c.cap;
+  size_t b = cap * 16 * 6 + cap * 2 * 4;                      // A, E, B (pos, vel), ranks
+  b += (nc + 1) * 4 + (nc + 2) * 4;                           // counts, offsets
+  b += nn * (6 * 8 + 4 * 16 + 2 * 3 * 8);                     // accumulator, vel/velold/frac/svel, fracd/flux
+  b += 2 * nh * 12;                                           // pressure, rhs, code
+  b += kMaxObj * sizeof(Obj) + sizeof(Counters) + kMaxEmitters * sizeof(EmitterDev);
+  b += 2 * (size_t)std::max(1LL, c.ww_cap) * 32;
+  if (c.rx > 0) {
+    const size_t nv = (size_t)(c.rx + 1) * (c.rz + 1), W = (size_t)c.wmap;
+    b += nv * 8 + nv * 20 + (size_t)(2 * c.rx) * (2 * c.rz) * 16 + W * W * 28 + (size_t)(2 * c.rx + 2 * c.rz) * 8;
+  }
+  return b + (64 << 10) * 24;                                 // allocation granularity
 }
 
 void* Tank::alloc(size_t bytes) {
@@ -253,6 +280,7 @@ void* Tank::alloc(size_t bytes) {
 }
 
 void Tank::set_objects(const std::vector<Obj>& o) {
+  join();
   if (o.size() > (size_t)kMaxObj) throw Error(-1, "at most 64 obstacles and drains");
   objs = o;
   d.nobj = (int)objs.size();
@@ -272,6 +300,7 @@ void Tank::set_objects(const std::vector<Obj>& o) {
 }
 
 void Tank::set_lattice(const double* sdf, const int* oid, int lx, int ly, int lz) {
+  join();
   if (lx != 2 * d.nx + 1 || lz != 2 * d.nz + 1 || ly < 2 * d.ny + 1 || (ly - 1) % 2)
     throw Error(-1, "lattice must be (2nx+1) × (2nyl+1) × (2nz+1) with nyl >= ny");
   d.nyl = (ly - 1) / 2;
@@ -292,12 +321,14 @@ void Tank::set_lattice(const double* sdf, const int* oid, int lx, int ly, int lz
 }
 
 void Tank::read_counters() {
+  join();
   CK(cudaMemcpyAsync(h_ctr, d.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
   n_upper = h_ctr->n_live + h_ctr->n_emit;
 }
 
 void Tank::stage(const float4* p, const float4* v, long long n) {
+  join();
   if (n <= 0) return;
   CK(cudaMemcpyAsync(d.pE + n_emit_host, p, n * 16, cudaMemcpyHostToDevice, stream));
   CK(cudaMemcpyAsync(d.vE + n_emit_host, v, n * 16, cudaMemcpyHostToDevice, stream));
@@ -308,6 +339,7 @@ void Tank::stage(const float4* p, const float4* v, long long n) {
 }
 
 void Tank::add_particles(const float* pos, const float* vel, const float* air, long long n, uint32_t* first) {
+  join();
   if (n < 0 || (n > 0 && !pos)) throw Error(-1, "add_particles: bad arrays");
   if (first) *first = next_id;
   if (n == 0) return;
@@ -375,6 +407,7 @@ int clip_to_room(Tank& t, std::vector<EmitRec>& recs) {
 }  // namespace
 
 void Tank::count_pass() {
+  join();
   solo->ensure_uploaded();
   launch_begin_count(solo->ctx);
   launch_bin(solo->ctx);
@@ -383,6 +416,7 @@ void Tank::count_pass() {
 }
 
 void Tank::emit_block(const double lo_in[3], const double hi_in[3], bool fill) {
+  join();
   // blockEmits (src/js/55-emit.js:83-106) / emit_block (solver.py:317-343)
   const double sp = d.h / 2;
   double lo[3] = {lo_in[0], lo_in[1], lo_in[2]}, hi[3] = {hi_in[0], hi_in[1], hi_in[2]};
@@ -415,6 +449,7 @@ void Tank::emit_block(const double lo_in[3], const double hi_in[3], bool fill) {
 }
 
 void Tank::source_emits(double dt) {
+  join();
   // sourceEmits (src/js/55-emit.js:13-69): per source an accumulator of volume, drop timers, bursts, rain
   if (scene.sources.empty()) return;
   const double Vp = d.vp, DEG = M_PI / 180.0, RAIN_SPEED = 6.5;
@@ -507,6 +542,7 @@ void Tank::source_emits(double dt) {
 }
 
 void Tank::clear() {
+  join();
   // clearWater (src/js/50-sim.js:365-373)
   CK(cudaStreamSynchronize(stream));
   CK(cudaMemsetAsync(d.ctr, 0, sizeof(Counters), stream));
@@ -526,11 +562,13 @@ void Tank::reset() {
 }
 
 void Tank::substep(double dt) {
+  join();
   solo->use_graphs = use_graphs;
   solo->substep(dt);
 }
 
 int Tank::step(double frame_dt) {
+  join();
   if (!(frame_dt > 0)) return 0;
   read_counters();
   if (h_ctr->vmax_bits64 != 0ull) {
@@ -593,6 +631,7 @@ long long Tank::read_whitewater(float* pos4, float* vel4, long long cap) {
 }
 
 void Tank::read_grid(int field, void* out, size_t bytes) {
+  join();
   const size_t nn = d.nnodes, nc = d.ncells;
   auto need = [&](size_t b) { if (bytes < b) throw Error(-1, "read_grid: output buffer too small (" + std::to_string(b) + " bytes needed)"); };
   CK(cudaStreamSynchronize(stream));
@@ -671,6 +710,7 @@ int Tank::snapshot() {
 }
 
 void Tank::restore(int id) {
+  join();
   // restoreWater (src/js/50-sim.js:127-141): only the latest copy, once
   if (!snap.valid || snap.id != id) throw Error(-6, "no water copy with that id");
   CK(cudaStreamSynchronize(stream));
@@ -743,6 +783,11 @@ Group::~Group() {
   cudaStreamSynchronize(stream);
   drop_graph();
   if (ev_sor[0]) { cudaEventDestroy(ev_sor[0]); cudaEventDestroy(ev_sor[1]); }
+  if (ev_done) {
+    for (Tank* t : tanks)
+      if (t->dep == ev_done) { cudaStreamWaitEvent(t->stream, ev_done, 0); t->dep = nullptr; }
+    cudaEventDestroy(ev_done);
+  }
   cudaFree(d_tanks); cudaFreeHost(h_tanks); cudaFree(d_bpfx); cudaFree(d_ppfx); cudaFree(d_bsum);
   if (own_stream) cudaStreamDestroy(stream);
 }
@@ -790,6 +835,7 @@ void Group::ensure_uploaded() {
 }
 
 void Tank::set_emitters(const std::vector<EmitterDev>& e) {
+  join();
   if (e.size() > (size_t)kMaxEmitters) throw Error(-1, "at most 8 fixed emitters");
   if (!d_emitters) d_emitters = (EmitterDev*)alloc(kMaxEmitters * sizeof(EmitterDev));
   CK(cudaStreamSynchronize(stream));
@@ -836,14 +882,12 @@ void Group::enqueue_body() {
 
 void Group::substep(double dt) {
   CK(cudaSetDevice(device));
-  // particle staging of every tank goes through its own stream; order it before this one
+  // work a tank enqueued on its own stream (staging, emission) must come first
   for (Tank* t : tanks)
-    if (t->stream != stream) {
-      cudaEvent_t e;
-      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-      CK(cudaEventRecord(e, t->stream));
-      CK(cudaStreamWaitEvent(stream, e, 0));
-      CK(cudaEventDestroy(e));
+    if (t->stream != stream && t->dirty) {
+      CK(cudaEventRecord(t->ev_own, t->stream));
+      CK(cudaStreamWaitEvent(stream, t->ev_own, 0));
+      t->dirty = false;
     }
   ensure_uploaded();
   bool geom = false;
@@ -873,15 +917,15 @@ void Group::substep(double dt) {
     t->n_emit_host = 0;
     t->n_upper += (long long)ceil(t->emit_per_substep);
   }
-  // later work on a tank's own stream (reads, emission) must follow this sub-step
-  for (Tank* t : tanks)
-    if (t->stream != stream) {
-      cudaEvent_t e;
-      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-      CK(cudaEventRecord(e, stream));
-      CK(cudaStreamWaitEvent(t->stream, e, 0));
-      CK(cudaEventDestroy(e));
-    }
+  // later work on a tank's own stream (reads, emission) must follow this sub-step: it waits on ev_done
+  bool others = false;
+  for (Tank* t : tanks) others |= t->stream != stream;
+  if (others) {
+    if (!ev_done) CK(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev_done, stream));
+    for (Tank* t : tanks)
+      if (t->stream != stream) t->dep = ev_done;
+  }
 }
 
 }  // namespace suiri

@@ -41,7 +41,11 @@ struct TankConfig {
   int rx = 256, rz = 256, wmap = 256;
   int sdf_mode = kSdfAnalytic, device = 0;
   uint32_t seed = 1;
+  cudaStream_t stream = nullptr;  // use this stream instead of creating one (not owned)
 };
+
+// device bytes a tank of this configuration allocates (admission by HBM budget)
+size_t tank_bytes(const TankConfig& c);
 
 struct PrevXf { double pos[3]; double R[9]; };
 
@@ -88,6 +92,11 @@ struct Tank {
   long long emit_cap = 0;
   EmitterDev* d_emitters = nullptr;
   double emit_per_substep = 0;    // fixed emitters, particles per sub-step (host bound tracking)
+  bool own_stream = true;
+  cudaEvent_t ev_own = nullptr;   // marks this tank's own-stream work for a batch to wait on
+  cudaEvent_t dep = nullptr;      // a batch's event this tank's own stream must wait for
+  bool dirty = false;             // own-stream work enqueued since the last batch sub-step
+  void join();                    // order own-stream work after the last batch sub-step
 
   void set_emitters(const std::vector<EmitterDev>& e);
 
@@ -130,6 +139,7 @@ struct Group {
   cudaGraphExec_t exec = nullptr;
   int max_iters = 0;
   bool graph_emitters = false;
+  cudaEvent_t ev_done = nullptr;  // recorded after every sub-step (tanks on other streams wait for it)
   bool profile = false;           // record events around the SOR phase (inside the graph too)
   cudaEvent_t ev_sor[2] = {nullptr, nullptr};
   int blocks_per_sm = 4;

@@ -1,0 +1,202 @@
+// Serving: a request loop that admits scene solves by HBM budget and advances every resident scene with
+// shared batched launches (continuous batching). Requests arriving while others run are admitted at the
+// next sub-step boundary as memory frees up; finished ones leave at a boundary and their memory returns
+// to the budget. All device work runs on one worker thread and one stream; the state of a request stays
+// on the device from admission to completion.
+#include "server.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+namespace suiri {
+
+namespace {
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+}  // namespace
+
+Server::Server(int device, double budget_bytes, double dt_) : budget(budget_bytes), dt(dt_), dev(device) {
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  t_start = now_s();
+  worker = std::thread([this] { loop(); });
+}
+
+Server::~Server() {
+  {
+    std::lock_guard<std::mutex> g(m);
+    stop = true;
+  }
+  cv.notify_all();
+  if (worker.joinable()) worker.join();
+  cudaSetDevice(dev);
+  group.reset();
+  for (auto& kv : reqs) kv.second->tank.reset();
+  cudaStreamDestroy(stream);
+}
+
+long long Server::submit(std::unique_ptr<Request> r) {
+  r->t_submit = now_s();
+  r->bytes = tank_bytes(r->cfg);
+  std::lock_guard<std::mutex> g(m);
+  const long long id = ++next_id;
+  r->id = id;
+  if ((double)r->bytes > budget) {
+    r->state = kFailed;
+    r->err = "request needs " + std::to_string(r->bytes) + " bytes, more than the whole budget";
+    r->t_done = r->t_submit;
+  } else {
+    queue.push_back(r.get());
+  }
+  reqs[id] = std::move(r);
+  cv.notify_all();
+  return id;
+}
+
+void Server::admit_locked(std::vector<Request*>& admitted) {
+  // FIFO admission: the head waits until it fits, so large scenes are not starved by small ones
+  while (!queue.empty()) {
+    Request* r = queue.front();
+    if (used + (double)r->bytes > budget) break;
+    queue.pop_front();
+    used += (double)r->bytes;
+    r->state = kRunning;
+    admitted.push_back(r);
+  }
+}
+
+void Server::start_request(Request* r) {
+  try {
+    r->cfg.stream = stream;
+    r->cfg.device = dev;
+    r->tank.reset(new Tank(r->cfg));
+    Tank& t = *r->tank;
+    t.scene = r->scene;
+    apply(t, r->scene);
+    for (const WaterBlock& b : r->scene.blocks) t.emit_block(b.lo, b.hi, false);
+    if (!r->emitters.empty()) t.set_emitters(r->emitters);
+    r->t_admit = now_s();
+  } catch (const Error& e) {
+    r->tank.reset();
+    r->state = kFailed;
+    r->err = e.what();
+    r->t_done = now_s();
+    std::lock_guard<std::mutex> g(m);
+    used -= (double)r->bytes;
+  }
+}
+
+void Server::finish_request(Request* r) {
+  Tank& t = *r->tank;
+  t.read_counters();
+  r->final_count = t.h_ctr->n_live;
+  r->particle_steps = (double)r->final_count * r->steps;    // liquid particles × sub-steps
+  if (r->keep_result) {
+    const long long n = t.read_particles(nullptr, nullptr, 0);
+    r->res_pos.resize(4 * n);
+    r->res_vel.resize(4 * n);
+    t.read_particles(r->res_pos.data(), r->res_vel.data(), n);
+  }
+  r->tank.reset();
+  const double tdone = now_s();
+  std::lock_guard<std::mutex> g(m);
+  used -= (double)r->bytes;
+  r->t_done = tdone;
+  r->state = kDone;
+  lat_ms.push_back(1000.0 * (r->t_done - r->t_submit));
+  total_particle_steps += r->particle_steps;
+  ++completed;
+  cv.notify_all();
+}
+
+void Server::loop() {
+  cudaSetDevice(dev);
+  std::vector<Request*> active;
+  bool changed = false;
+  while (true) {
+    std::vector<Request*> admitted;
+    {
+      std::unique_lock<std::mutex> g(m);
+      if (active.empty() && queue.empty()) cv.wait_for(g, std::chrono::milliseconds(20));
+      if (stop) break;
+      admit_locked(admitted);
+    }
+    for (Request* r : admitted) {
+      start_request(r);
+      if (r->state == kRunning) { active.push_back(r); changed = true; }
+    }
+    if (active.empty()) continue;
+    if (changed || !group) {
+      group.reset();
+      std::vector<Tank*> ts;
+      for (Request* r : active) ts.push_back(r->tank.get());
+      group.reset(new Group(ts, stream));
+      ++rebuilds;
+      changed = false;
+    }
+    try {
+      group->substep(dt);
+    } catch (const Error& e) {
+      // a failed launch ends every request of this batch with the message; the server keeps serving
+      for (Request* r : active) {
+        r->state = kFailed;
+        r->err = e.what();
+        r->t_done = now_s();
+        r->tank.reset();
+        std::lock_guard<std::mutex> g(m);
+        used -= (double)r->bytes;
+      }
+      active.clear();
+      group.reset();
+      continue;
+    }
+    ++substeps;
+    sum_active += (double)active.size();
+    std::vector<Request*> still, done;
+    for (Request* r : active) (++r->steps_done >= r->steps ? done : still).push_back(r);
+    if (!done.empty()) {
+      group.reset();                 // the batch refers to the tanks that are about to be freed
+      for (Request* r : done) finish_request(r);
+      changed = true;
+    }
+    active.swap(still);
+  }
+}
+
+void Server::apply(Tank& t, const Scene& sc) {
+  std::vector<Obj> objs;
+  for (const SceneItem& it : sc.solids) objs.push_back(it.obj);
+  if (!objs.empty()) t.set_objects(objs);
+}
+
+ServerStats Server::stats() {
+  std::lock_guard<std::mutex> g(m);
+  ServerStats s;
+  s.completed = completed;
+  s.queued = (long long)queue.size();
+  long long running = 0, failed = 0;
+  for (auto& kv : reqs) {
+    running += kv.second->state == kRunning;
+    failed += kv.second->state == kFailed;
+  }
+  s.running = running;
+  s.failed = failed;
+  s.particle_steps = total_particle_steps;
+  s.elapsed_s = now_s() - t_start;
+  s.used_bytes = used;
+  s.budget_bytes = budget;
+  s.rebuilds = rebuilds;
+  s.substeps = substeps;
+  s.mean_active = substeps ? sum_active / substeps : 0.0;
+  std::vector<double> l = lat_ms;
+  std::sort(l.begin(), l.end());
+  auto pct = [&](double q) { return l.empty() ? 0.0 : l[std::min(l.size() - 1, (size_t)floor(q * (l.size() - 1) + 0.5))]; };
+  s.p50_ms = pct(0.50);
+  s.p99_ms = pct(0.99);
+  return s;
+}
+
+}  // namespace suiri

@@ -44,9 +44,29 @@ class Emitter(C.Structure):
                 ('radius', C.c_double), ('speed', C.c_double), ('per_substep', C.c_double)]
 
 
+class Request(C.Structure):
+    _fields_ = [('size', C.c_uint32), ('params', C.POINTER(Params)), ('scene_json', C.c_char_p),
+                ('emitters', C.POINTER(Emitter)), ('n_emitters', C.c_int32), ('steps', C.c_int32),
+                ('keep_result', C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [('completed', C.c_int64), ('queued', C.c_int64), ('running', C.c_int64), ('failed', C.c_int64),
+                ('rebuilds', C.c_int64), ('substeps', C.c_int64), ('particle_steps', C.c_double),
+                ('elapsed_s', C.c_double), ('used_bytes', C.c_double), ('budget_bytes', C.c_double),
+                ('p50_ms', C.c_double), ('p99_ms', C.c_double), ('mean_active', C.c_double)]
+
+
 P = C.c_void_p
 # name: (restype, argtypes) for every entry point of include/suiri.h
 SIGNATURES = {
+    'suiri_server_create': (C.c_int, [C.c_int32, C.c_double, C.c_double, C.POINTER(P)]),
+    'suiri_server_destroy': (C.c_int, [P]),
+    'suiri_server_submit': (C.c_int, [P, C.POINTER(Request), C.POINTER(C.c_int64)]),
+    'suiri_server_poll': (C.c_int, [P, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    'suiri_server_wait': (C.c_int, [P, C.c_int64, C.c_double]),
+    'suiri_server_result': (C.c_int, [P, C.c_int64, P, P, C.c_int64, C.POINTER(C.c_int64)]),
+    'suiri_server_get_stats': (C.c_int, [P, C.POINTER(ServerStats)]),
     'suiri_set_emitters': (C.c_int, [P, C.POINTER(Emitter), C.c_int32]),
     'suiri_profile': (C.c_int, [P, C.c_int32]),
     'suiri_sor_phase_ms': (C.c_int, [P, C.POINTER(C.c_double)]),

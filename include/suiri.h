@@ -191,6 +191,42 @@ int suiri_batch_sync(suiri_batch* b);
 int suiri_batch_tune(suiri_batch* b, int32_t particle_blocks_per_sm, int32_t sor_sweeps_per_launch);
 int suiri_batch_stream(suiri_batch* b, void** stream);
 
+/* ---------------------------------------------------------------- serving: continuous batching under an HBM budget */
+
+/* A scene solve: grid and physics as in suiri_create, the scene JSON (tank, obstacles, drains, water
+   blocks), fixed-rate emitters, and the number of sub-steps. No reference counterpart: the reference runs
+   one scene per page (src/js/90-main.js) or per Blender bake (bake.py). */
+typedef struct suiri_request {
+  uint32_t size;                    /* sizeof(suiri_request) */
+  const suiri_params* params;       /* may be NULL: defaults */
+  const char* scene_json;
+  const suiri_emitter* emitters;
+  int32_t n_emitters;
+  int32_t steps;
+  int32_t keep_result;              /* 1: keep the final particles for suiri_server_result */
+} suiri_request;
+
+typedef struct suiri_server_stats {
+  int64_t completed, queued, running, failed, rebuilds, substeps;
+  double particle_steps;            /* liquid particles × sub-steps of completed requests */
+  double elapsed_s, used_bytes, budget_bytes;
+  double p50_ms, p99_ms;            /* request latency: submit → results ready */
+  double mean_active;               /* resident scenes per batched sub-step */
+} suiri_server_stats;
+
+/* a worker thread admits requests FIFO while their device memory fits the budget, advances all resident
+   scenes with one batched sub-step of length dt at a time, and retires finished ones at sub-step boundaries */
+int suiri_server_create(int32_t device, double budget_bytes, double dt, suiri_server** out);
+int suiri_server_destroy(suiri_server* s);
+int suiri_server_submit(suiri_server* s, const suiri_request* r, int64_t* id);
+/* state: 0 queued, 1 running, 2 done, 3 failed; latency_ms (done/failed); count = final liquid particles */
+int suiri_server_poll(suiri_server* s, int64_t id, int32_t* state, double* latency_ms, int64_t* count);
+/* block until the request is done or failed, at most timeout_s seconds (SUIRI_ERR_STATE on timeout) */
+int suiri_server_wait(suiri_server* s, int64_t id, double timeout_s);
+/* final particles of a finished request submitted with keep_result (as suiri_read_particles) */
+int suiri_server_result(suiri_server* s, int64_t id, float* pos4, float* vel4, int64_t cap, int64_t* n);
+int suiri_server_get_stats(suiri_server* s, suiri_server_stats* st);
+
 /* ---------------------------------------------------------------- timing helpers (device events) */
 
 /* milliseconds of device time of `steps` sub-steps of dt, events on the tank's / batch's own stream */
