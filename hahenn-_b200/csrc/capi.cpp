@@ -275,6 +275,27 @@ int suiri_set_lattice(suiri_tank* h, const double* sdf, const int32_t* oid, int3
   });
 }
 
+int suiri_eval_sdf(suiri_tank* h, const double* pts, int64_t n, double* out) {
+  return guard(h ? &h->err : nullptr, [&] {
+    if (n < 0 || (n > 0 && (!pts || !out))) throw Error(SUIRI_ERR_INVALID, "bad point arrays");
+    T(h)->eval_sdf(pts, n, out);
+  });
+}
+
+int suiri_estimate_bytes(const char* scene_json, const suiri_params* params, double* bytes) {
+  return guard(nullptr, [&] {
+    if (!bytes) throw Error(SUIRI_ERR_INVALID, "null output");
+    suiri_params p;
+    suiri_params_default(&p);
+    if (params) {
+      if (params->size != sizeof(suiri_params)) throw Error(SUIRI_ERR_INVALID, "suiri_params.size mismatch");
+      p = *params;
+    }
+    Scene sc;
+    *bytes = (double)tank_bytes(make_config(p, scene_json, sc));
+  });
+}
+
 int suiri_add_particles(suiri_tank* h, const float* pos, const float* vel, const float* airborne, int64_t n, uint32_t* first_id) {
   return guard(h ? &h->err : nullptr, [&] { T(h)->add_particles(pos, vel, airborne, n, first_id); });
 }
@@ -384,6 +405,7 @@ int suiri_get_stats(suiri_tank* h, suiri_stats* s) {
     s->liters = alive * t->d.vp * 1000;
     s->full = c.full;
     s->frame = c.frame;
+    s->errors = c.err;
     s->nx = t->d.nx; s->ny = t->d.ny; s->nz = t->d.nz; s->h = t->d.h;
     s->origin[0] = t->d.ox; s->origin[1] = t->d.oy; s->origin[2] = t->d.oz;
   });
@@ -447,16 +469,25 @@ int suiri_batch_sync(suiri_batch* b) {
   });
 }
 
-int suiri_batch_tune(suiri_batch* b, int32_t particle_blocks_per_sm, int32_t sor_sweeps_per_launch) {
+static void tune_group(Group& g, int32_t particle_blocks_per_sm, int32_t sor_persistent) {
+  if (particle_blocks_per_sm < 1 || particle_blocks_per_sm > 32) throw Error(SUIRI_ERR_INVALID, "blocks per SM in 1..32");
+  if (sor_persistent != 0 && sor_persistent != 1) throw Error(SUIRI_ERR_INVALID, "sor_persistent is 0 or 1");
+  CK(cudaStreamSynchronize(g.stream));
+  g.blocks_per_sm = particle_blocks_per_sm;
+  g.ctx.particle_blocks = particle_blocks_per_sm * g.sm_count;
+  g.sor_persistent = sor_persistent;
+  g.drop_graph();
+}
+
+int suiri_batch_tune(suiri_batch* b, int32_t particle_blocks_per_sm, int32_t sor_persistent) {
   return guard(b ? &b->err : nullptr, [&] {
     if (!b || !b->g) throw Error(SUIRI_ERR_INVALID, "null batch");
-    if (particle_blocks_per_sm < 1 || particle_blocks_per_sm > 32) throw Error(SUIRI_ERR_INVALID, "blocks per SM in 1..32");
-    if (sor_sweeps_per_launch < 1) throw Error(SUIRI_ERR_INVALID, "sweeps per launch >= 1");
-    Group& g = *b->g;
-    g.blocks_per_sm = particle_blocks_per_sm;
-    g.ctx.particle_blocks = particle_blocks_per_sm * g.sm_count;
-    g.drop_graph();
+    tune_group(*b->g, particle_blocks_per_sm, sor_persistent);
   });
+}
+
+int suiri_tune(suiri_tank* h, int32_t particle_blocks_per_sm, int32_t sor_persistent) {
+  return guard(h ? &h->err : nullptr, [&] { tune_group(*T(h)->solo, particle_blocks_per_sm, sor_persistent); });
 }
 
 int suiri_batch_stream(suiri_batch* b, void** stream) {

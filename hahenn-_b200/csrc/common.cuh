@@ -107,6 +107,13 @@ struct TankDev {
 
 constexpr int kMaxEmitters = 8;
 
+// grid barrier of a persistent (cooperative) launch; err is set when a bounded wait gave up
+struct GridBarrier {
+  unsigned count, gen;
+  int err, pad;
+};
+constexpr int kErrBarrier = 1;    // Counters::err bit: a grid barrier wait ran out
+
 constexpr int kFlagAir = 1;
 constexpr int kFlagDead = 2;
 

@@ -180,6 +180,27 @@ __global__ void k_emit_fixed(const TankDev* __restrict__ tanks) {
   }
 }
 
+__global__ void k_eval_sdf(TankDev T, const double* __restrict__ pts, double* __restrict__ out, long long n) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  out[q] = tank_sdf(T, pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+}
+
+void Tank::eval_sdf(const double* pts, long long n, double* out) {
+  join();
+  if (n <= 0) return;
+  double *dp = nullptr, *dout = nullptr;
+  CK(cudaMallocAsync((void**)&dp, n * 24, stream));
+  CK(cudaMallocAsync((void**)&dout, n * 8, stream));
+  CK(cudaMemcpyAsync(dp, pts, n * 24, cudaMemcpyHostToDevice, stream));
+  k_eval_sdf<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(d, dp, dout, n);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, dout, n * 8, cudaMemcpyDeviceToHost, stream));
+  CK(cudaFreeAsync(dp, stream));
+  CK(cudaFreeAsync(dout, stream));
+  CK(cudaStreamSynchronize(stream));
+}
+
 // ------------------------------------------------------------------------------------ Tank
 Tank::Tank(const TankConfig& c) : cfg(c) {
   if (cfg.nx < 2 || cfg.ny < 2 || cfg.nz < 2 || !(cfg.h > 0)) throw Error(-1, "grid must be at least 2×2×2 with h > 0");
@@ -767,7 +788,16 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
   }
   CK(cudaMalloc(&d_bsum, std::max(1, ctx.nblocks[kFamScan]) * sizeof(long long)));
   CK(cudaMemcpyAsync(d_bpfx, pf.data(), pf.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+  std::vector<int> hp(n + 1, 0);
+  for (int i = 0; i < n; ++i) hp[i + 1] = hp[i] + tanks[i]->d.nhalf;
+  CK(cudaMalloc(&d_hpfx, (n + 1) * sizeof(int)));
+  CK(cudaMemcpyAsync(d_hpfx, hp.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
+  CK(cudaMalloc(&d_barrier, sizeof(GridBarrier)));
+  CK(cudaMemsetAsync(d_barrier, 0, sizeof(GridBarrier), stream));
+  sor_blocks = std::min(sor_persist_max_blocks(device), std::max(1, (hp[n] + kThreads - 1) / kThreads));
   CK(cudaStreamSynchronize(stream));
+  ctx.hpfx = d_hpfx;
+  ctx.barrier = d_barrier;
   ctx.stream = stream;
   ctx.tanks = d_tanks;
   ctx.ntanks = n;
@@ -788,6 +818,7 @@ Group::~Group() {
       if (t->dep == ev_done) { cudaStreamWaitEvent(t->stream, ev_done, 0); t->dep = nullptr; }
     cudaEventDestroy(ev_done);
   }
+  cudaFree(d_hpfx); cudaFree(d_barrier);
   cudaFree(d_tanks); cudaFreeHost(h_tanks); cudaFree(d_bpfx); cudaFree(d_ppfx); cudaFree(d_bsum);
   if (own_stream) cudaStreamDestroy(stream);
 }
@@ -871,9 +902,14 @@ void Group::enqueue_body() {
   if (profile) CK(cudaStreamIsCapturing(stream, &cap));
   const unsigned evflags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
   if (profile) CK(cudaEventRecordWithFlags(ev_sor[0], stream, evflags));
-  for (int it = 0; it < max_iters; ++it) {
-    launch_sor_sweep(ctx, 0, it);
-    launch_sor_sweep(ctx, 1, it);
+  if (sor_persistent && max_iters > 0) {
+    launch_sor_persist(ctx, max_iters, sor_blocks);
+    CK(cudaGetLastError());
+  } else {
+    for (int it = 0; it < max_iters; ++it) {
+      launch_sor_sweep(ctx, 0, it);
+      launch_sor_sweep(ctx, 1, it);
+    }
   }
   if (profile) CK(cudaEventRecordWithFlags(ev_sor[1], stream, evflags));
   launch_project(ctx);

@@ -99,6 +99,7 @@ struct Tank {
   void join();                    // order own-stream work after the last batch sub-step
 
   void set_emitters(const std::vector<EmitterDev>& e);
+  void eval_sdf(const double* pts, long long n, double* out);
 
   explicit Tank(const TankConfig& c);
   ~Tank();
@@ -140,6 +141,10 @@ struct Group {
   int max_iters = 0;
   bool graph_emitters = false;
   cudaEvent_t ev_done = nullptr;  // recorded after every sub-step (tanks on other streams wait for it)
+  int* d_hpfx = nullptr;          // colour-slot prefix for the persistent SOR
+  GridBarrier* d_barrier = nullptr;
+  int sor_persistent = 0;         // 0: one launch per colour sweep, 1: one cooperative launch per solve
+  int sor_blocks = 0;
   bool profile = false;           // record events around the SOR phase (inside the graph too)
   cudaEvent_t ev_sor[2] = {nullptr, nullptr};
   int blocks_per_sm = 4;

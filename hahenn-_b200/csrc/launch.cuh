@@ -22,6 +22,8 @@ struct LaunchCtx {
   int* ppfx_sorted;         // device: ntanks+1 prefix of particles in B
   long long* scan_bsum;     // device: one partial sum per scan block
   int particle_blocks;      // persistent grid for particle kernels
+  int* hpfx;                // device: ntanks+1 prefix of colour slots (nhalf) for the persistent SOR
+  GridBarrier* barrier;     // device: grid barrier of the persistent SOR
 };
 
 // per-kernel launchers (bin.cu, grid.cu, sor.cu, g2p.cu)
@@ -36,6 +38,8 @@ void launch_p2g(const LaunchCtx& L);
 void launch_grid_nodes(const LaunchCtx& L);
 void launch_grid_cells(const LaunchCtx& L);
 void launch_sor_sweep(const LaunchCtx& L, int color, int sweep);
+void launch_sor_persist(const LaunchCtx& L, int max_iters, int blocks);   // whole solve, one cooperative launch
+int sor_persist_max_blocks(int device);                                  // co-resident blocks of k_sor_persist
 void launch_project(const LaunchCtx& L);
 void launch_g2p(const LaunchCtx& L);
 void launch_whitewater(const LaunchCtx& L, double frame_dt);

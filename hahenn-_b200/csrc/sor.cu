@@ -1,31 +1,31 @@
 // Red-black SOR pressure sweep.
 //
-// One launch relaxes one colour of every tank. Cells are stored split by colour (slot = (i>>1) + hx·row),
-// so a thread's own pressure, right-hand side and code load coalesced, and its six neighbours come from
-// the other colour's array (two of them in the same slot column, coalesced as well).
+// Cells are stored split by colour (slot = (i>>1) + hx·row), so a thread's own pressure, right-hand side
+// and code load coalesced, and its six neighbours come from the other colour's array (two of them in the
+// same slot column, coalesced as well).
 //
 // Arithmetic is float32 in exactly the order of the reference's NumPy solve
 // (blender_addon/suiri_lab/solver.py:494-505):
 //   num = C0·p(x-) + C1·p(x+) + C2·p(y-) + C3·p(y+) + C4·p(z-) + C5·p(z+)    (each product rounded, summed left to right)
 //   p  += ω·(((num − rhs)·inv) − p),   inv = 1/(C0+…+C5) correctly rounded
-// with the library built without FMA contraction, so the pressures equal the reference's bit for bit
-// given the same operands. Faces on the tank walls and floor have C = 0 (Neumann); the open top has
-// C = 1 with p = 0 above (Dirichlet); non-liquid cells hold 0 and are not updated
-// (src/js/30-wgsl-sim.js:267-297 is the same update as a WGSL `mix`).
+// with explicit round-to-nearest intrinsics, so the pressures equal the reference's bit for bit given the
+// same operands. Faces on the tank walls and floor have C = 0 (Neumann); the open top has C = 1 with p = 0
+// above (Dirichlet); non-liquid cells hold 0 and are not updated (src/js/30-wgsl-sim.js:267-297 is the
+// same update as a WGSL `mix`).
 //
 // Most cells have every face either closed or fully open; their coefficients come from the 6 "open"
 // bits of the code and the float fractions are only read for cut cells next to obstacles.
+//
+// Two launch forms:
+//   k_sor          one colour of every tank per launch (2·iters launches per solve, in the sub-step graph)
+//   k_sor_persist  the whole solve in one cooperative launch: all blocks resident, a grid barrier after
+//                  every colour sweep. The barrier's wait is bounded: after kSpinLimit polls it records
+//                  an error in the tank counters and every block returns.
 #include "launch.cuh"
 
 namespace suiri {
 
-__global__ void __launch_bounds__(kThreads) k_sor(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx,
-                                                  int color, int sweep) {
-  const int t = find_slot(bpfx, ntanks, blockIdx.x);
-  const TankDev& T = tanks[t];
-  if (sweep >= T.iters) return;
-  const int s = (blockIdx.x - bpfx[t]) * blockDim.x + threadIdx.x;
-  if (s >= T.nhalf) return;
+__device__ __forceinline__ void sor_cell(const TankDev& T, int color, int s) {
   const int hx = T.hx, nx = T.nx, ny = T.ny, nz = T.nz;
   const int ti = s % hx, row = s / hx;
   const int j = row % ny, k = row / ny;
@@ -70,8 +70,87 @@ __global__ void __launch_bounds__(kThreads) k_sor(const TankDev* __restrict__ ta
   T.pres[own] = p;
 }
 
+__global__ void __launch_bounds__(kThreads) k_sor(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx,
+                                                  int color, int sweep) {
+  const int t = find_slot(bpfx, ntanks, blockIdx.x);
+  const TankDev& T = tanks[t];
+  if (sweep >= T.iters) return;
+  const int s = (blockIdx.x - bpfx[t]) * blockDim.x + threadIdx.x;
+  if (s >= T.nhalf) return;
+  sor_cell(T, color, s);
+}
+
+constexpr unsigned kSpinLimit = 1u << 22;
+
+// sense-free generation barrier over all blocks of a cooperative launch; false if the wait gave up
+__device__ __forceinline__ bool grid_barrier(GridBarrier* b, unsigned nblocks) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned g = *(volatile unsigned*)&b->gen;
+    __threadfence();
+    if (atomicAdd(&b->count, 1u) == nblocks - 1) {
+      b->count = 0;
+      __threadfence();
+      atomicAdd(&b->gen, 1u);
+    } else {
+      unsigned spins = 0;
+      while (*(volatile unsigned*)&b->gen == g) {
+        if (++spins > kSpinLimit || *(volatile int*)&b->err) { ok = 0; break; }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    if (!ok) atomicExch(&b->err, 1);
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok;
+}
+
+__global__ void __launch_bounds__(kThreads) k_sor_persist(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ hpfx,
+                                                          int max_iters, GridBarrier* bar) {
+  const int total = hpfx[ntanks];
+  const int stride = gridDim.x * blockDim.x;
+  for (int sweep = 0; sweep < 2 * max_iters; ++sweep) {
+    const int color = sweep & 1, it = sweep >> 1;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += stride) {
+      const int t = find_slot(hpfx, ntanks, q);
+      const TankDev& T = tanks[t];
+      if (it < T.iters) sor_cell(T, color, q - hpfx[t]);
+    }
+    if (sweep + 1 < 2 * max_iters && !grid_barrier(bar, gridDim.x)) {
+      if (threadIdx.x == 0 && blockIdx.x == 0)
+        for (int t = 0; t < ntanks; ++t) atomicOr(&tanks[t].ctr->err, kErrBarrier);
+      return;
+    }
+  }
+}
+
 void launch_sor_sweep(const LaunchCtx& L, int color, int sweep) {
   k_sor<<<L.nblocks[kFamHalf], kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.bpfx[kFamHalf], color, sweep);
+}
+
+int sor_persist_max_blocks(int device) {
+  int per_sm = 0, sms = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sor_persist, kThreads, 0);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  return per_sm * sms;
+}
+
+void launch_sor_persist(const LaunchCtx& L, int max_iters, int blocks) {
+  // cooperative launch: the runtime refuses it unless every block can be resident at once
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(kThreads);
+  cfg.stream = L.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_sor_persist, L.tanks, L.ntanks, (const int*)L.hpfx, max_iters, L.barrier);
 }
 
 }  // namespace suiri

@@ -30,7 +30,7 @@ class Params(C.Structure):
 class Stats(C.Structure):
     _fields_ = [('count', C.c_int64), ('ww_count', C.c_int64), ('impacts', C.c_int64), ('vmax', C.c_double),
                 ('time', C.c_double), ('liters', C.c_double), ('full', C.c_int32), ('frame', C.c_int32),
-                ('nx', C.c_int32), ('ny', C.c_int32), ('nz', C.c_int32), ('h', C.c_double),
+                ('errors', C.c_int32), ('pad', C.c_int32), ('nx', C.c_int32), ('ny', C.c_int32), ('nz', C.c_int32), ('h', C.c_double),
                 ('origin', C.c_double * 3)]
 
 
@@ -68,6 +68,9 @@ SIGNATURES = {
     'suiri_server_result': (C.c_int, [P, C.c_int64, P, P, C.c_int64, C.POINTER(C.c_int64)]),
     'suiri_server_get_stats': (C.c_int, [P, C.POINTER(ServerStats)]),
     'suiri_set_emitters': (C.c_int, [P, C.POINTER(Emitter), C.c_int32]),
+    'suiri_tune': (C.c_int, [P, C.c_int32, C.c_int32]),
+    'suiri_eval_sdf': (C.c_int, [P, P, C.c_int64, P]),
+    'suiri_estimate_bytes': (C.c_int, [C.c_char_p, C.POINTER(Params), C.POINTER(C.c_double)]),
     'suiri_profile': (C.c_int, [P, C.c_int32]),
     'suiri_sor_phase_ms': (C.c_int, [P, C.POINTER(C.c_double)]),
     'suiri_batch_profile': (C.c_int, [P, C.c_int32]),

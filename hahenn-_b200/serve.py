@@ -20,6 +20,23 @@ from . import native as N
 AXES_SERVE = (16, 24, 32, 48, 64, 96, 128)
 
 
+def estimate_bytes(scene, params=None):
+    """Device bytes a scene solve would take (the server admits by this figure)."""
+    L = N.lib()
+    p = N.Params()
+    N.check(L.suiri_params_default(C.byref(p)))
+    keep = []
+    for k, v in (params or {}).items():
+        if k == 'quality':
+            v = v.encode()
+            keep.append(v)
+        setattr(p, k, v)
+    b = C.c_double()
+    js = (scene if isinstance(scene, str) else json.dumps(scene)).encode()
+    N.check(L.suiri_estimate_bytes(js, C.byref(p), C.byref(b)))
+    return b.value
+
+
 class Server:
     def __init__(self, budget_bytes=150e9, dt=1 / 240, device=0):
         h = C.c_void_p()

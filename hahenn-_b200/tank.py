@@ -101,6 +101,13 @@ class Tank:
         o = None if oid is None else np.ascontiguousarray(np.asarray(oid, np.int32).transpose(2, 1, 0))
         self._c(N.lib().suiri_set_lattice(self._h, _ptr(s), _ptr(o), lx, ly, lz))
 
+    def eval_sdf(self, pts):
+        """Distance to the nearest obstacle at points (N,3), as the step sees it (analytic or lattice)."""
+        p = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
+        out = np.empty(len(p))
+        self._c(N.lib().suiri_eval_sdf(self._h, _ptr(p), len(p), _ptr(out)))
+        return out
+
     # ------------------------------------------------------------------ water
     def add_particles(self, pos, vel=None, air=None):
         pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
@@ -181,6 +188,9 @@ class Tank:
     def profile(self, on=True):
         self._c(N.lib().suiri_profile(self._h, 1 if on else 0))
 
+    def tune(self, blocks_per_sm=4, sor_persistent=False):
+        self._c(N.lib().suiri_tune(self._h, int(blocks_per_sm), 1 if sor_persistent else 0))
+
     def sor_phase_ms(self):
         ms = C.c_double()
         self._c(N.lib().suiri_sor_phase_ms(self._h, C.byref(ms)))
@@ -240,7 +250,7 @@ class Tank:
         s = N.Stats()
         self._c(N.lib().suiri_get_stats(self._h, C.byref(s)))
         return dict(count=s.count, ww_count=s.ww_count, impacts=s.impacts, vmax=s.vmax, time=s.time, liters=s.liters,
-                    full=bool(s.full), frame=s.frame, nx=s.nx, ny=s.ny, nz=s.nz, h=s.h, origin=tuple(s.origin))
+                    full=bool(s.full), frame=s.frame, errors=s.errors, nx=s.nx, ny=s.ny, nz=s.nz, h=s.h, origin=tuple(s.origin))
 
     @property
     def water_liters(self):
@@ -276,8 +286,16 @@ class Batch:
     def sync(self):
         N.check(N.lib().suiri_batch_sync(self._h))
 
-    def tune(self, blocks_per_sm, sweeps_per_launch=1):
-        N.check(N.lib().suiri_batch_tune(self._h, int(blocks_per_sm), int(sweeps_per_launch)))
+    def tune(self, blocks_per_sm=4, sor_persistent=False):
+        N.check(N.lib().suiri_batch_tune(self._h, int(blocks_per_sm), 1 if sor_persistent else 0))
+
+    def profile(self, on=True):
+        N.check(N.lib().suiri_batch_profile(self._h, 1 if on else 0))
+
+    def sor_phase_ms(self):
+        ms = C.c_double()
+        N.check(N.lib().suiri_batch_sor_phase_ms(self._h, C.byref(ms)))
+        return ms.value
 
     def time_substeps(self, dt, steps):
         ms = C.c_double()

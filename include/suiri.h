@@ -74,6 +74,8 @@ typedef struct suiri_stats {
   double liters;           /* count · (h/2)³ · 1000 (src/js/50-sim.js:375) */
   int32_t full;            /* capacity was reached */
   int32_t frame;           /* sub-steps taken */
+  int32_t errors;          /* device error bits: 1 = a grid-barrier wait of the persistent solve gave up */
+  int32_t pad;
   int32_t nx, ny, nz;
   double h;
   double origin[3];
@@ -131,6 +133,13 @@ int suiri_set_obstacles(suiri_tank* t, const suiri_object* objs, int32_t n);
    Switches the tank to lattice mode for face fractions and collisions. */
 int suiri_set_lattice(suiri_tank* t, const double* sdf, const int32_t* oid, int32_t lx, int32_t ly, int32_t lz);
 
+/* distance to the nearest obstacle at n points (host arrays, n×3 → n), as the step sees it: analytic
+   shapes or the lattice (sceneSdf, src/js/30-wgsl-sim.js:78-87; sdf_at, solver.py:116-140; the editor's
+   mirror for picking and placement, src/js/10-scene.js:124-176). 1e9 where there is no obstacle. */
+int suiri_eval_sdf(suiri_tank* t, const double* pts, int64_t n, double* out);
+/* device bytes a tank of these parameters and scene would take (admission planning) */
+int suiri_estimate_bytes(const char* scene_json, const suiri_params* params, double* bytes);
+
 /* particles from host arrays, appended before the next sub-step (emit_block/_add, solver.py:304-343).
    pos, vel: n×3 float32; airborne: n floats (0/1) or NULL. *first_id (may be NULL) = id of the first. */
 int suiri_add_particles(suiri_tank* t, const float* pos, const float* vel, const float* airborne, int64_t n,
@@ -187,8 +196,11 @@ int suiri_batch_create(suiri_tank* const* tanks, int32_t n, suiri_batch** out);
 int suiri_batch_destroy(suiri_batch* b);
 int suiri_batch_substep(suiri_batch* b, double dt);
 int suiri_batch_sync(suiri_batch* b);
-/* tuning knobs picked by the autotuner: particle-kernel blocks per SM, SOR sweeps per launch */
-int suiri_batch_tune(suiri_batch* b, int32_t particle_blocks_per_sm, int32_t sor_sweeps_per_launch);
+/* tuning knobs picked by the autotuner: blocks per SM of the persistent particle kernels, and the form of
+   the pressure solve (0: one launch per colour sweep, 1: the whole solve in one cooperative launch with a
+   grid barrier between sweeps) */
+int suiri_batch_tune(suiri_batch* b, int32_t particle_blocks_per_sm, int32_t sor_persistent);
+int suiri_tune(suiri_tank* t, int32_t particle_blocks_per_sm, int32_t sor_persistent);
 int suiri_batch_stream(suiri_batch* b, void** stream);
 
 /* ---------------------------------------------------------------- serving: continuous batching under an HBM budget */

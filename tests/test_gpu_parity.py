@@ -113,6 +113,38 @@ def test_obstacles_face_fractions_and_substep(pkg, mode):
     gpu.close()
 
 
+ALL_SHAPES = [
+    dict(kind='obstacle', shape='box', pos=[-0.2, 0.1, -0.1], rot=[10, 30, 0], dims=dict(w=0.1, h=0.06, d=0.08)),
+    dict(kind='obstacle', shape='plate', pos=[0.0, 0.25, 0.1], rot=[0, 0, 15], dims=dict(w=0.22, d=0.1, t=0.012)),
+    dict(kind='obstacle', shape='sphere', pos=[0.2, 0.1, 0.1], rot=[0, 0, 0], dims=dict(r=0.05)),
+    dict(kind='obstacle', shape='cylinder', pos=[0.1, 0.08, -0.15], rot=[0, 0, 20], dims=dict(r=0.03, h=0.12)),
+    dict(kind='obstacle', shape='cone', pos=[-0.15, 0.05, 0.15], rot=[0, 45, 0], dims=dict(r=0.04, h=0.08)),
+    dict(kind='obstacle', shape='torus', pos=[0.05, 0.18, -0.02], rot=[30, 0, 0], dims=dict(R=0.05, r=0.014)),
+    dict(kind='obstacle', shape='cup', pos=[-0.05, 0.06, 0.0], rot=[0, 0, 0], dims=dict(r=0.04, h=0.1, t=0.006)),
+    dict(kind='obstacle', shape='container', pos=[0.2, 0.04, -0.1], rot=[0, 20, 0], dims=dict(w=0.14, h=0.06, d=0.1, t=0.008)),
+    dict(kind='obstacle', shape='gutter', pos=[-0.1, 0.2, -0.05], rot=[0, 0, -14], dims=dict(len=0.28, r=0.03, t=0.006))]
+
+
+@pytest.mark.parametrize('mode', ['analytic', 'lattice'])
+def test_obstacle_distances_every_shape(pkg, mode):
+    """The device's distances equal the oracle's bit for bit: the analytic shape library (all eight shapes,
+    turned) and the trilinear lattice."""
+    from parity import objs_from_items
+    nx, ny, nz, h = 24, 12, 16, 1 / 40
+    t = pkg.Tank(nx=nx, ny=ny, nz=nz, h=h, whitewater=False, ripple=None, capacity=1024, sdf_mode=mode)
+    t.set_objects(ALL_SHAPES)
+    ora = oracle_from(nx, ny, nz, h, t.origin, flip=0.96, omega=1.6, iters=1, sdf_mode=mode)
+    ora.set_objects(objs_from_items(ALL_SHAPES))
+    if mode == 'lattice':
+        t.set_lattice(ora.lat)
+    rng = np.random.default_rng(9)
+    pts = t.origin + rng.random((20000, 3)) * np.array([nx, ny, nz]) * h
+    np.testing.assert_array_equal(t.eval_sdf(pts), ora.sdf_at(pts))
+    t.substep(1 / 240)                     # face fractions are computed at the first sub-step
+    np.testing.assert_array_equal(t.grid(pkg.native.FIELD_FRAC), ora.frac.astype(np.float32))
+    t.close()
+
+
 def test_drops_merge_ripple_impulse_crown_and_spawn(pkg):
     d = load('drops')
     nx, ny, nz, h = int(d['nx']), int(d['ny']), int(d['nz']), float(d['h'])
@@ -177,7 +209,7 @@ def test_frame_step_whitewater_top_height_and_ripples(pkg):
 def test_ripple_layer_spectral_update(pkg):
     """One ripple frame with a known impulse pattern and no particles (dry floor: mask 0.75)."""
     R = 32
-    gpu = pkg.Tank(nx=24, ny=8, nz=16, h=0.025, iters=4, whitewater=False, ripple=(R, R), wmap=32, capacity=4096)
+    gpu = pkg.Tank(nx=24, ny=8, nz=16, h=0.025, iters=4, whitewater=False, ripple=(R, R), wmap=32, capacity=16384)
     # drops landing put impulses into the source grid; here: add a few airborne particles that merge
     rng = np.random.default_rng(3)
     pool = gpu.origin + (np.stack(np.meshgrid(np.arange(24), np.arange(3), np.arange(16), indexing='ij'), -1).reshape(-1, 3)
@@ -233,6 +265,28 @@ def test_batch_equals_solo_bit_for_bit(pkg):
     b.close()
     for t in solo + batched:
         t.close()
+
+
+def test_persistent_solve_equals_per_sweep_launches(pkg):
+    """The whole-solve cooperative launch relaxes the same colours in the same order: identical pressures
+    and particles, bit for bit, and no barrier error."""
+    w = pkg.workloads.obstacles_inflow(scale=4)
+    out = []
+    for persistent in (False, True):
+        t = pkg.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=0.95, omega=1.8, iters=40, whitewater=True,
+                     ripple=None, capacity=len(w['pos']) * 2)
+        t.set_objects(w['objects'])
+        t.add_particles(w['pos'])
+        t.tune(4, persistent)
+        for _ in range(3):
+            t.substep(1 / 240)
+        assert t.stats()['errors'] == 0
+        pos, vel, air, ids = t.particles()
+        o = np.argsort(ids)
+        out.append((t.grid(pkg.native.FIELD_PRES), pos[o], vel[o]))
+        t.close()
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
 
 
 def test_snapshot_restore(pkg):

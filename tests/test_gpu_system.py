@@ -84,7 +84,7 @@ def test_serving_budget_admission(pkg):
     from importlib import import_module
     serve = import_module('hahenn-_b200.serve')
     sc, prm, em, info = serve.scene_request(5, axes=(16,))
-    one = 1.5 * 64 * 2 ** 20
+    one = 1.5 * serve.estimate_bytes(sc, prm)
     srv = serve.Server(budget_bytes=one)
     ids = [srv.submit(sc, prm, em, steps=4) for _ in range(3)]
     for i in ids:
