@@ -90,6 +90,7 @@ struct TankDev {
   float4* frac;             // face open fractions, float32
   double* fracd;            // 3*nnodes, float64 (divergence)
   float4* svel;             // solid velocity at faces
+  float2* vv;               // 3*nnodes: per component (projected v, P2G v or NaN where the face took no weight)
   double* flux;             // 3*nnodes cut-cell face fluxes (divergence operand)
   float* pres;              // 2*nhalf colour-split pressure
   float* rhs;               // 2*nhalf h²·div

@@ -243,6 +243,7 @@ Tank::Tank(const TankConfig& c) : cfg(c) {
   D.vel = (float4*)alloc(nn * 16); D.velold = (float4*)alloc(nn * 16);
   D.frac = (float4*)alloc(nn * 16); D.svel = (float4*)alloc(nn * 16);
   D.fracd = (double*)alloc(3 * nn * 8); D.flux = (double*)alloc(3 * nn * 8);
+  D.vv = (float2*)alloc(3 * nn * 8);
   D.pres = (float*)alloc(2 * nh * 4); D.rhs = (float*)alloc(2 * nh * 4); D.code = (uint32_t*)alloc(2 * nh * 4);
   d_objs = (Obj*)alloc(kMaxObj * sizeof(Obj));
   D.objs = d_objs;
@@ -281,7 +282,7 @@ size_t tank_bytes(const TankConfig& c) {
   const size_t nh = (size_t)((c.nx + 1) / 2) * c.ny * c.nz, cap = (size_t)c.cap;
   size_t b = cap * 16 * 6 + cap * 2 * 4;                      // A, E, B (pos, vel), ranks
   b += (nc + 1) * 4 + (nc + 2) * 4;                           // counts, offsets
-  b += nn * (6 * 8 + 4 * 16 + 2 * 3 * 8);                     // accumulator, vel/velold/frac/svel, fracd/flux
+  b += nn * (6 * 8 + 4 * 16 + 2 * 3 * 8 + 3 * 8);            // accumulator, vel/velold/frac/svel, fracd/flux, vv
   b += 2 * nh * 12;                                           // pressure, rhs, code
   b += kMaxObj * sizeof(Obj) + sizeof(Counters) + kMaxEmitters * sizeof(EmitterDev);
   b += 2 * (size_t)std::max(1LL, c.ww_cap) * 32;
@@ -794,7 +795,8 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
   CK(cudaMemcpyAsync(d_hpfx, hp.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
   CK(cudaMalloc(&d_barrier, sizeof(GridBarrier)));
   CK(cudaMemsetAsync(d_barrier, 0, sizeof(GridBarrier), stream));
-  sor_blocks = std::min(sor_persist_max_blocks(device), std::max(1, (hp[n] + kThreads - 1) / kThreads));
+  // one block per SM: the grid barrier's cost grows with the number of arriving blocks
+  sor_blocks = std::min(std::min(sor_persist_max_blocks(device), sm_count), std::max(1, (hp[n] + kThreads - 1) / kThreads));
   CK(cudaStreamSynchronize(stream));
   ctx.hpfx = d_hpfx;
   ctx.barrier = d_barrier;

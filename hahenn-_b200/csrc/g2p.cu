@@ -60,36 +60,32 @@ __device__ __forceinline__ bool air_at(const TankDev& T, int i, int j, int k) {
   return count_at(T, i, j, k) == 0;
 }
 
-// PIC and FLIP velocity of one component from faces that took weight this step (solver.py:236-249)
-__device__ inline void transfer(const TankDev& T, const double g[3], int comp, double vp, double& pic, double& flip) {
-  const double qx = g[0] - (comp == 0 ? 0.0 : 0.5), qy = g[1] - (comp == 1 ? 0.0 : 0.5), qz = g[2] - (comp == 2 ? 0.0 : 0.5);
+// PIC and FLIP velocity of one component from faces that took weight this step (solver.py:236-249).
+// The 8 corner loads are issued together (one float2 each: projected v, P2G v or NaN), then summed in the
+// reference's corner order.
+__device__ __forceinline__ void transfer(const TankDev& T, double gx, double gy, double gz, int comp, double vp,
+                                         double& pic, double& flip) {
+  const double qx = gx - (comp == 0 ? 0.0 : 0.5), qy = gy - (comp == 1 ? 0.0 : 0.5), qz = gz - (comp == 2 ? 0.0 : 0.5);
   const int bx = (int)floor(qx), by = (int)floor(qy), bz = (int)floor(qz);
   const double fx = qx - bx, fy = qy - by, fz = qz - bz;
   const double wx[2] = {1 - fx, fx}, wy[2] = {1 - fy, fy}, wz[2] = {1 - fz, fz};
+  const float2* __restrict__ vv = T.vv + (size_t)comp * T.nnodes;
+  float2 c[8];
+  bool ok[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    const int ix = bx + (e >> 2), iy = by + ((e >> 1) & 1), iz = bz + (e & 1);
+    ok[e] = ix >= 0 && ix <= T.nx && iy >= 0 && iy <= T.ny && iz >= 0 && iz <= T.nz;
+    c[e] = ok[e] ? __ldg(vv + node_idx(T, ix, iy, iz)) : make_float2(0.f, 0.f);
+  }
   double sn = 0.0, so = 0.0, sw = 0.0;
-  const int bit = 1 << comp;
-  for (int dx = 0; dx < 2; ++dx) {
-    const int ix = bx + dx;
-    if (ix < 0 || ix > T.nx) continue;
-    for (int dy = 0; dy < 2; ++dy) {
-      const int iy = by + dy;
-      if (iy < 0 || iy > T.ny) continue;
-      const double wxy = wx[dx] * wy[dy];
-      for (int dz = 0; dz < 2; ++dz) {
-        const int iz = bz + dz;
-        if (iz < 0 || iz > T.nz) continue;
-        const int n = node_idx(T, ix, iy, iz);
-        const float4 vo = __ldg(T.velold + n);
-        if (!((int)vo.w & bit)) continue;
-        const float4 vn = __ldg(T.vel + n);
-        const double w = wxy * wz[dz];
-        const float a = comp == 0 ? vn.x : (comp == 1 ? vn.y : vn.z);
-        const float b = comp == 0 ? vo.x : (comp == 1 ? vo.y : vo.z);
-        sn += w * (double)a;
-        so += w * (double)b;
-        sw += w;
-      }
-    }
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    if (!ok[e] || isnan(c[e].y)) continue;
+    const double w = (wx[e >> 2] * wy[(e >> 1) & 1]) * wz[e & 1];
+    sn += w * (double)c[e].x;
+    so += w * (double)c[e].y;
+    sw += w;
   }
   if (sw >= 1e-6) {
     pic = sn / sw;
@@ -170,7 +166,7 @@ __global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ ta
     if (ing) {
       for (int a = 0; a < 3; ++a) {
         double pic, flip;
-        transfer(T, g, a, vold[a], pic, flip);
+        transfer(T, g[0], g[1], g[2], a, vold[a], pic, flip);
         v[a] = pic + T.flip * (flip - pic);
       }
     } else {
@@ -231,7 +227,7 @@ __global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ ta
         double vl[3];
         for (int a = 0; a < 3; ++a) {
           double pic, flip;
-          transfer(T, g1, a, v[a], pic, flip);
+          transfer(T, g1[0], g1[1], g1[2], a, v[a], pic, flip);
           vl[a] = pic;
         }
         const double dv = vl[1] - vold[1];

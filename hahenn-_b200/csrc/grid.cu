@@ -16,14 +16,14 @@ __device__ __forceinline__ void node_coord(const TankDev& T, int n, int& i, int&
 // Open fraction of each staggered face from the obstacle distances at its 4 corners and (twice) its
 // centre (src/js/30-wgsl-sim.js:118-157; blender_addon/suiri_lab/solver.py:176-207). The sample points
 // are the half-cell lattice points origin + (h/2)·L; in lattice mode they are read from the lattice,
-// in analytic mode the shapes are evaluated there (float64, plain minimum over obstacles).
+// in analytic mode the web version's sceneSdf is evaluated there (float64, culled like the WGSL loop).
 __device__ __forceinline__ double lattice_at(const TankDev& T, int lx, int ly, int lz) {
   if (T.sdf_mode == kSdfLattice) {
     const int sx = 2 * T.nx + 1, sy = 2 * T.nyl + 1;
     return T.lattice[lx + sx * (ly + (size_t)sy * lz)];
   }
   const double hh = T.h / 2;
-  return scene_sdf(T.objs, T.nobj, T.ox + hh * lx, T.oy + hh * ly, T.oz + hh * lz, false);
+  return scene_sdf(T.objs, T.nobj, T.ox + hh * lx, T.oy + hh * ly, T.oz + hh * lz, true);
 }
 
 __device__ __forceinline__ double open_frac(double s0, double s1, double s2, double s3, double sc) {
@@ -112,6 +112,18 @@ __global__ void __launch_bounds__(kThreads) k_geom(const TankDev* __restrict__ t
 constexpr int kBN = kBrick + 2;              // nodes per brick edge, halo included
 constexpr int kBNodes = kBN * kBN * kBN;
 
+// exact sum of 64-bit integers over the lanes of `peers`: three 22-bit limbs, each summed with redux.sync
+// (at most 32 lanes: every limb sum stays below 2^27), recombined in 64-bit arithmetic
+__device__ __forceinline__ long long group_sum(unsigned peers, long long v) {
+  unsigned lo = (unsigned)(v & 0x3FFFFF);
+  unsigned mid = (unsigned)((v >> 22) & 0x3FFFFF);
+  unsigned hi = (unsigned)(int)(v >> 44);
+  lo = __reduce_add_sync(peers, lo);
+  mid = __reduce_add_sync(peers, mid);
+  hi = __reduce_add_sync(peers, hi);
+  return ((long long)(int)hi << 44) + ((long long)mid << 22) + (long long)lo;
+}
+
 __global__ void __launch_bounds__(kThreads) k_p2g(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx) {
   __shared__ long long s_acc[6][kBNodes];
   __shared__ int s_row0[kBrick * kBrick];
@@ -142,19 +154,27 @@ __global__ void __launch_bounds__(kThreads) k_p2g(const TankDev* __restrict__ ta
   __syncthreads();
   const int total = s_rowp[kBrick * kBrick];
   const int nsx = T.nx + 1, nsy = T.ny + 1, nsz = T.nz + 1;
-  for (int q = threadIdx.x; q < total; q += blockDim.x) {
-    int lo = 0, hi = kBrick * kBrick - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (s_rowp[mid] <= q) lo = mid; else hi = mid - 1;
+  const int lane = threadIdx.x & 31;
+  // warps walk consecutive sorted particles (the loop bound is uniform per warp: every lane takes part in
+  // the warp-wide match and reductions, lanes past the end with no node)
+  for (int qb = threadIdx.x & ~31; qb < total; qb += blockDim.x) {
+    const int q = qb + lane;
+    const bool valid = q < total;
+    double g[3] = {0.0, 0.0, 0.0}, vv[3] = {0.0, 0.0, 0.0};
+    if (valid) {
+      int lo = 0, hi = kBrick * kBrick - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_rowp[mid] <= q) lo = mid; else hi = mid - 1;
+      }
+      const int pi = s_row0[lo] + (q - s_rowp[lo]);
+      const float4 P = T.pB[pi];
+      const float4 V = T.vB[pi];
+      grid_pos(T, (double)P.x, (double)P.y, (double)P.z, g[0], g[1], g[2]);
+      vv[0] = fmin(fmax((double)V.x, -30.0), 30.0);
+      vv[1] = fmin(fmax((double)V.y, -30.0), 30.0);
+      vv[2] = fmin(fmax((double)V.z, -30.0), 30.0);
     }
-    const int pi = s_row0[lo] + (q - s_rowp[lo]);
-    const float4 P = T.pB[pi];
-    const float4 V = T.vB[pi];
-    double g[3];
-    grid_pos(T, (double)P.x, (double)P.y, (double)P.z, g[0], g[1], g[2]);
-    const double vv[3] = {fmin(fmax((double)V.x, -30.0), 30.0), fmin(fmax((double)V.y, -30.0), 30.0),
-                          fmin(fmax((double)V.z, -30.0), 30.0)};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const double qx = g[0] - (a == 0 ? 0.0 : 0.5), qy = g[1] - (a == 1 ? 0.0 : 0.5), qz = g[2] - (a == 2 ? 0.0 : 0.5);
@@ -162,24 +182,20 @@ __global__ void __launch_bounds__(kThreads) k_p2g(const TankDev* __restrict__ ta
       const double fx = qx - bx, fy = qy - by, fz = qz - bz;
       const double wx[2] = {1 - fx, fx}, wy[2] = {1 - fy, fy}, wz[2] = {1 - fz, fz};
 #pragma unroll
-      for (int dx = 0; dx < 2; ++dx) {
-        const int ix = bx + dx;
-        if (ix < 0 || ix >= nsx) continue;
-#pragma unroll
-        for (int dy = 0; dy < 2; ++dy) {
-          const int iy = by + dy;
-          if (iy < 0 || iy >= nsy) continue;
-          const double wxy = wx[dx] * wy[dy];
-#pragma unroll
-          for (int dz = 0; dz < 2; ++dz) {
-            const int iz = bz + dz;
-            if (iz < 0 || iz >= nsz) continue;
-            const double w = wxy * wz[dz];
-            if (!(w > 0.0)) continue;
-            const int ln = (ix - i0 + 1) + kBN * ((iy - j0 + 1) + kBN * (iz - k0 + 1));
-            atomicAdd((unsigned long long*)&s_acc[a][ln], (unsigned long long)__double2ll_rn(w * vv[a] * kFix));
-            atomicAdd((unsigned long long*)&s_acc[3 + a][ln], (unsigned long long)__double2ll_rn(w * kFix));
-          }
+      for (int e = 0; e < 8; ++e) {
+        const int dx = e >> 2, dy = (e >> 1) & 1, dz = e & 1;
+        const int ix = bx + dx, iy = by + dy, iz = bz + dz;
+        const double w = (wx[dx] * wy[dy]) * wz[dz];
+        const bool use = valid && ix >= 0 && ix < nsx && iy >= 0 && iy < nsy && iz >= 0 && iz < nsz && w > 0.0;
+        const int ln = use ? (ix - i0 + 1) + kBN * ((iy - j0 + 1) + kBN * (iz - k0 + 1)) : -1;
+        const long long m = use ? __double2ll_rn(w * vv[a] * kFix) : 0LL;
+        const long long wt = use ? __double2ll_rn(w * kFix) : 0LL;
+        const unsigned peers = __match_any_sync(0xffffffffu, ln);
+        const long long M = group_sum(peers, m);
+        const long long Wt = group_sum(peers, wt);
+        if (ln >= 0 && lane == __ffs(peers) - 1) {
+          atomicAdd((unsigned long long*)&s_acc[a][ln], (unsigned long long)M);
+          atomicAdd((unsigned long long*)&s_acc[3 + a][ln], (unsigned long long)Wt);
         }
       }
     }
@@ -322,6 +338,15 @@ __global__ void __launch_bounds__(kThreads) k_project(const TankDev* __restrict_
       v.z = (float)((double)v.z - (cell_pres(T, i, j, k) - cell_pres(T, i, j, k - 1)) / h);
   }
   T.vel[n] = v;
+  // compact per-component pairs for the G2P gathers: one 8-byte load per corner; NaN marks a face that
+  // took no particle weight (it is skipped, solver.py:240-245)
+  const float4 vo = T.velold[n];
+  const int m = (int)vo.w;
+  const float qnan = __int_as_float(0x7fc00000);
+  const size_t nn = T.nnodes;
+  T.vv[n] = make_float2(v.x, (m & 1) ? vo.x : qnan);
+  T.vv[nn + n] = make_float2(v.y, (m & 2) ? vo.y : qnan);
+  T.vv[2 * nn + n] = make_float2(v.z, (m & 4) ? vo.z : qnan);
 }
 
 void launch_geom(const LaunchCtx& L) {

@@ -263,6 +263,13 @@ void fft2(Tank& t, float2* data, float sign) {
   CK(cudaGetLastError());
 }
 
+// host table → device, ordered on the tank's stream after the zero-fill of the same buffer (the tank's
+// stream does not synchronise with the legacy default stream), complete before the host buffer is reused
+void upload(Tank& t, void* dst, const void* src, size_t bytes) {
+  CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, t.stream));
+  CK(cudaStreamSynchronize(t.stream));
+}
+
 void* ralloc(Tank& t, RippleState& r, size_t bytes) {
   void* p = nullptr;
   CK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
@@ -303,7 +310,7 @@ RippleState& ensure(Tank& t) {
   for (int pass = 0; pass < 2; ++pass) {
     const int M = pass ? r->Mz : r->Mx;
     for (int k = 0; k < M; ++k) tw[k] = make_float2((float)cos(2 * M_PI * k / M), (float)sin(2 * M_PI * k / M));
-    CK(cudaMemcpy(pass ? r->twz : r->twx, tw.data(), M * 8, cudaMemcpyHostToDevice));
+    upload(t, pass ? r->twz : r->twx, tw.data(), M * 8);
   }
   // ripple vertex coordinates: lo + linspace(0, 1, R+1)·(hi - lo) as NumPy forms them (solver.py:784-785)
   const double lo[2] = {D.ox, D.oz}, hi[2] = {D.ox + D.nx * D.h, D.oz + D.nz * D.h};
@@ -315,7 +322,7 @@ RippleState& ensure(Tank& t) {
       const double u = i == R ? 1.0 : i * step + 0.0;
       c[i] = lo[a] + u * (hi[a] - lo[a]);
     }
-    CK(cudaMemcpy(a ? r->mz_coord : r->mx_coord, c.data(), (R + 1) * 8, cudaMemcpyHostToDevice));
+    upload(t, a ? r->mz_coord : r->mx_coord, c.data(), (R + 1) * 8);
   }
   // dilation disc and blur weights (solver.py:752-768)
   r->texel[0] = (hi[0] - lo[0]) / W;
@@ -334,8 +341,8 @@ RippleState& ensure(Tank& t) {
   r->ndisc = (int)disc.size();
   r->disc = (int4*)ralloc(t, *r, disc.size() * 16);
   r->disc_h = (double*)ralloc(t, *r, cap.size() * 8);
-  CK(cudaMemcpy(r->disc, disc.data(), disc.size() * 16, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(r->disc_h, cap.data(), cap.size() * 8, cudaMemcpyHostToDevice));
+  upload(t, r->disc, disc.data(), disc.size() * 16);
+  upload(t, r->disc_h, cap.data(), cap.size() * 8);
   const double sigma = 1.5 * D.h / std::min(r->texel[0], r->texel[1]);
   r->blur_rad = (int)ceil(2.5 * sigma);
   std::vector<double> bw(2 * r->blur_rad + 1);
@@ -344,7 +351,7 @@ RippleState& ensure(Tank& t) {
     bw[i + r->blur_rad] = exp(-0.5 * (x * x));
   }
   r->blur_w = (double*)ralloc(t, *r, bw.size() * 8);
-  CK(cudaMemcpy(r->blur_w, bw.data(), bw.size() * 8, cudaMemcpyHostToDevice));
+  upload(t, r->blur_w, bw.data(), bw.size() * 8);
   CK(cudaStreamSynchronize(t.stream));
   return *r;
 }

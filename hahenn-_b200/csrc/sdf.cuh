@@ -66,9 +66,9 @@ __device__ inline double shape_sdf(const Obj& o, double px, double py, double pz
   }
 }
 
-// minimum over obstacles; `cull` skips objects whose bounding sphere is farther than the current best
-// (only used where the result feeds a tolerance check: the skip never changes the minimum of exact
-// distance bounds, but the plain loop is what the bit-exact face fractions use)
+// minimum over obstacles; `cull` skips objects whose bounding sphere is farther than the current best,
+// as the WGSL loop does (src/js/30-wgsl-sim.js:83). For shapes whose distance is bounded by their
+// bounding sphere that changes nothing; the gutter's is not, so the culled value is the web version's.
 __device__ inline double scene_sdf(const Obj* __restrict__ objs, int n, double px, double py, double pz, bool cull) {
   double best = kBig;
   for (int i = 0; i < n; ++i) {
@@ -91,6 +91,7 @@ __device__ inline void solid_vel_analytic(const Obj* __restrict__ objs, int n, d
   for (int i = 0; i < n; ++i) {
     const Obj& o = objs[i];
     if (o.flag != 1) continue;
+    if (len3(px - o.pos[0], py - o.pos[1], pz - o.pos[2]) - o.bound > best) continue;
     const double d = shape_sdf(o, px, py, pz);
     if (d < best) {
       best = d;

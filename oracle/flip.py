@@ -83,7 +83,9 @@ class Tank:
         self.objs = list(objs)
         obst = [o for o in self.objs if o['flag'] == 1]
         if obst:
-            self.lat = sdfm.lattice(obst, self.origin, self.h, self.lattice_shape()) if lattice is None else lattice
+            # analytic mode: the face fractions sample the web version's culled sceneSdf (30-wgsl-sim.js:127-129)
+            self.lat = (sdfm.lattice(obst, self.origin, self.h, self.lattice_shape(), cull=self.sdf_mode == 'analytic')
+                        if lattice is None else lattice)
             # nearest obstacle per lattice point, for solid velocities (solver.py:153-165)
             hh = self.h / 2
             s = self.lattice_shape()
@@ -107,7 +109,7 @@ class Tank:
         if not obst or n == 0:
             return np.full(n, 1e9)
         if self.sdf_mode == 'analytic':
-            return sdfm.scene_sdf(obst, p)
+            return sdfm.scene_sdf(obst, p, cull=True)
         lat = self.lat
         g = (p - self.origin) / (self.h / 2)
         s = np.array(lat.shape)
@@ -149,8 +151,15 @@ class Tank:
         if not obst or len(p) == 0:
             return v
         if self.sdf_mode == 'analytic':
-            ds = np.stack([sdfm.shape_sdf(o, p) for o in obst], 0)
-            ids = np.argmin(ds, 0)
+            # solidVelAt (30-wgsl-sim.js:96-106): culled like sceneSdf, the first strict minimum wins
+            best = np.full(len(p), 1e9)
+            ids = np.full(len(p), -1)
+            for k, o in enumerate(obst):
+                c = np.linalg.norm(p - o['pos'], axis=1) - o['bound']
+                d = sdfm.shape_sdf(o, p)
+                take = ~(c > best) & (d < best)
+                best = np.where(take, d, best)
+                ids = np.where(take, k, ids)
         else:
             g = np.rint((p - self.origin) / (self.h / 2)).astype(np.int64)
             g = np.clip(g, 0, np.array(self.oid.shape) - 1)

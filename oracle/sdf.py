@@ -165,16 +165,22 @@ def shape_sdf(o, p):
     return np.full(len(p), BIG)
 
 
-def scene_sdf(objs, p):
+def scene_sdf(objs, p, cull=False):
     """Minimum over obstacles (flag 1) of the shape distance (``sceneSdf`` ``30-wgsl-sim.js:78-87``).
 
-    The bounding-sphere skip of the WGSL loop only drops objects that cannot lower the minimum,
-    so the plain minimum is the same value."""
+    cull=True is the WGSL loop exactly: an object whose bounding sphere is farther than the running
+    minimum is skipped (``:83``). For most shapes that never changes the result, but the gutter's distance
+    can be smaller than the distance to its bounding sphere, so the web version's value differs from the
+    true minimum there. cull=False is the true minimum (what a mesh distance lattice holds)."""
     best = np.full(len(p), BIG)
     for o in objs:
         if o['flag'] != 1:
             continue
-        best = np.minimum(best, shape_sdf(o, p))
+        d = shape_sdf(o, p)
+        if cull:
+            c = _len3(p[:, 0] - o['pos'][0], p[:, 1] - o['pos'][1], p[:, 2] - o['pos'][2]) - o['bound']
+            d = np.where(c > best, best, d)
+        best = np.minimum(best, d)
     return best
 
 
@@ -188,15 +194,16 @@ def in_drain_analytic(objs, p):
     return out
 
 
-def lattice(objs, origin, h, shape):
+def lattice(objs, origin, h, shape, cull=False):
     """Obstacle distances on the half-cell lattice origin + h/2·index (``solver.py:103-110``).
 
-    shape = (2nx+1, 2nyl+1, 2nz+1). Returns float64 of that shape (BIG where no obstacle)."""
+    shape = (2nx+1, 2nyl+1, 2nz+1). Returns float64 of that shape (BIG where no obstacle). cull: the web
+    version's culled minimum (see scene_sdf)."""
     hh = h / 2
     axes = [origin[a] + hh * np.arange(shape[a]) for a in range(3)]
     X, Y, Z = np.meshgrid(*axes, indexing='ij')
     pts = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
-    return scene_sdf(objs, pts).reshape(shape)
+    return scene_sdf(objs, pts, cull).reshape(shape)
 
 
 def drains_for_solver(objs):
