@@ -140,6 +140,7 @@ int suiri_params_default(suiri_params* p) {
   p->ppc = 8.0; p->drift = 6.0; p->ww_rate = 7.0; p->whitewater = 1;
   p->capacity = 0; p->ww_capacity = 0; p->ripple_rx = 0; p->ripple_rz = 0; p->wmap = 0;
   p->sdf_mode = 0; p->device = 0; p->seed = 1;
+  p->ripple_sigma = 0.0728; p->ripple_rho = 998.0; p->ripple_depth = 0.0;
   return SUIRI_OK;
 }
 
@@ -201,6 +202,9 @@ TankConfig make_config(const suiri_params& p, const char* scene_json, Scene& sc)
     c.sdf_mode = p.sdf_mode;
     c.device = p.device;
     c.seed = p.seed;
+    if (!(p.ripple_sigma >= 0) || !(p.ripple_rho > 0) || !(p.ripple_depth >= 0))
+      throw Error(SUIRI_ERR_INVALID, "ripple sigma >= 0, rho > 0, depth >= 0");
+    c.ripple_sigma = p.ripple_sigma; c.ripple_rho = p.ripple_rho; c.ripple_depth = p.ripple_depth;
     if (!(c.omega > 0 && c.omega < 2)) throw Error(SUIRI_ERR_INVALID, "omega must be in (0, 2)");
     if (c.cap > (1LL << 30)) throw Error(SUIRI_ERR_INVALID, "capacity above 2^30 particles");
     return c;
@@ -316,6 +320,7 @@ std::vector<EmitterDev> emitters_from(const suiri_emitter* e, int n) {
       if (!(e[i].per_substep >= 0) || !(e[i].radius >= 0)) throw Error(SUIRI_ERR_INVALID, "emitter rate and radius must be >= 0");
       d.shape = e[i].shape; d.airborne = e[i].airborne ? 1 : 0;
       d.radius = e[i].radius; d.speed = e[i].speed; d.per_substep = e[i].per_substep;
+      d.radius_z = e[i].radius_z > 0 ? e[i].radius_z : e[i].radius;
       memcpy(d.pos, e[i].pos, sizeof(d.pos));
       double l = sqrt(e[i].dir[0] * e[i].dir[0] + e[i].dir[1] * e[i].dir[1] + e[i].dir[2] * e[i].dir[2]);
       if (!(l > 0)) { d.dir[1] = -1; l = 1; } else { for (int a = 0; a < 3; ++a) d.dir[a] = e[i].dir[a] / l; }

@@ -43,6 +43,7 @@ struct Obj {
 struct EmitterDev {
   double pos[3], dir[3], u[3], w[3];
   double radius, speed, per_substep;   // particles per sub-step (fractional parts accumulate)
+  double radius_z;                     // rain: half extent along z
   int shape, airborne;
 };
 

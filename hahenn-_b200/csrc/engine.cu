@@ -164,7 +164,7 @@ __global__ void k_emit_fixed(const TankDev* __restrict__ tanks) {
     } else {
       p[0] = E.pos[0] + (rnd01(s) * 2 - 1) * E.radius;
       p[1] = E.pos[1] - rnd01(s) * (E.speed * T.dt);
-      p[2] = E.pos[2] + (rnd01(s) * 2 - 1) * E.radius;
+      p[2] = E.pos[2] + (rnd01(s) * 2 - 1) * E.radius_z;
       v[0] = 0.0; v[1] = -E.speed; v[2] = 0.0;
     }
     const bool alive = !(T.has_obst && tank_sdf(T, p[0], p[1], p[2]) < 0.0);

@@ -41,6 +41,7 @@ struct TankConfig {
   int rx = 256, rz = 256, wmap = 256;
   int sdf_mode = kSdfAnalytic, device = 0;
   uint32_t seed = 1;
+  double ripple_sigma = 0.0728, ripple_rho = 998.0, ripple_depth = 0.0;
   cudaStream_t stream = nullptr;  // use this stream instead of creating one (not owned)
 };
 

@@ -148,8 +148,16 @@ __device__ inline void crown(const TankDev& T, double cx, double cy, double cz, 
 __global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ pfx) {
   const int total = pfx[ntanks];
   const int stride = gridDim.x * blockDim.x;
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
+  const int lane = threadIdx.x & 31;
+  // warp-uniform loop: the speed maximum is reduced over the warp before its one atomic (one global
+  // address per tank would otherwise take an atomic from every particle)
+  for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < total; base += stride) {
+    const int idx = base + lane;
+    unsigned long long vbits = 0ull;
+    int tt = -1;
+    if (idx < total) {
     const int t = find_slot(pfx, ntanks, idx);
+    tt = t;
     const TankDev& T = tanks[t];
     const int local = idx - pfx[t];
     const float4 P = T.pB[local];
@@ -245,7 +253,7 @@ __global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ ta
     if (ing) {
       const double sp = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
       // stored +1 so that 0 means "no in-grid particle this sub-step" (the reference keeps vmax then)
-      atomicMax((unsigned long long*)&T.ctr->vmax_bits64, (unsigned long long)__double_as_longlong(fmin(sp, 60.0)) + 1ull);
+      vbits = (unsigned long long)__double_as_longlong(fmin(sp, 60.0)) + 1ull;
       if (T.whitewater && sp > 0.75) {
         bool near = false;
         for (int a = 0; a < 3 && !near; ++a)
@@ -270,6 +278,20 @@ __global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ ta
     const float fl = (float)((air ? kFlagAir : 0) | (alive ? 0 : kFlagDead));
     T.pA[local] = make_float4((float)x[0], (float)x[1], (float)x[2], fl);
     T.vA[local] = make_float4((float)v[0], (float)v[1], (float)v[2], __uint_as_float(id));
+    }
+    // non-negative doubles order like their bit patterns: a warp max, then one atomic per warp and tank
+    const int t0 = __shfl_sync(0xffffffffu, tt, 0);
+    if (__all_sync(0xffffffffu, tt == t0 || tt < 0)) {
+      unsigned long long m = vbits;
+#pragma unroll
+      for (int o = 16; o; o >>= 1) {
+        const unsigned long long x = __shfl_xor_sync(0xffffffffu, m, o);
+        m = x > m ? x : m;
+      }
+      if (lane == 0 && m && t0 >= 0) atomicMax((unsigned long long*)&tanks[t0].ctr->vmax_bits64, m);
+    } else if (vbits) {
+      atomicMax((unsigned long long*)&tanks[tt].ctr->vmax_bits64, vbits);
+    }
   }
 }
 

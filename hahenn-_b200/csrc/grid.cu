@@ -112,18 +112,6 @@ __global__ void __launch_bounds__(kThreads) k_geom(const TankDev* __restrict__ t
 constexpr int kBN = kBrick + 2;              // nodes per brick edge, halo included
 constexpr int kBNodes = kBN * kBN * kBN;
 
-// exact sum of 64-bit integers over the lanes of `peers`: three 22-bit limbs, each summed with redux.sync
-// (at most 32 lanes: every limb sum stays below 2^27), recombined in 64-bit arithmetic
-__device__ __forceinline__ long long group_sum(unsigned peers, long long v) {
-  unsigned lo = (unsigned)(v & 0x3FFFFF);
-  unsigned mid = (unsigned)((v >> 22) & 0x3FFFFF);
-  unsigned hi = (unsigned)(int)(v >> 44);
-  lo = __reduce_add_sync(peers, lo);
-  mid = __reduce_add_sync(peers, mid);
-  hi = __reduce_add_sync(peers, hi);
-  return ((long long)(int)hi << 44) + ((long long)mid << 22) + (long long)lo;
-}
-
 __global__ void __launch_bounds__(kThreads) k_p2g(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx) {
   __shared__ long long s_acc[6][kBNodes];
   __shared__ int s_row0[kBrick * kBrick];
@@ -154,27 +142,33 @@ __global__ void __launch_bounds__(kThreads) k_p2g(const TankDev* __restrict__ ta
   __syncthreads();
   const int total = s_rowp[kBrick * kBrick];
   const int nsx = T.nx + 1, nsy = T.ny + 1, nsz = T.nz + 1;
-  const int lane = threadIdx.x & 31;
-  // warps walk consecutive sorted particles (the loop bound is uniform per warp: every lane takes part in
-  // the warp-wide match and reductions, lanes past the end with no node)
-  for (int qb = threadIdx.x & ~31; qb < total; qb += blockDim.x) {
-    const int q = qb + lane;
-    const bool valid = q < total;
-    double g[3] = {0.0, 0.0, 0.0}, vv[3] = {0.0, 0.0, 0.0};
-    if (valid) {
-      int lo = 0, hi = kBrick * kBrick - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (s_rowp[mid] <= q) lo = mid; else hi = mid - 1;
-      }
-      const int pi = s_row0[lo] + (q - s_rowp[lo]);
-      const float4 P = T.pB[pi];
-      const float4 V = T.vB[pi];
-      grid_pos(T, (double)P.x, (double)P.y, (double)P.z, g[0], g[1], g[2]);
-      vv[0] = fmin(fmax((double)V.x, -30.0), 30.0);
-      vv[1] = fmin(fmax((double)V.y, -30.0), 30.0);
-      vv[2] = fmin(fmax((double)V.z, -30.0), 30.0);
+  // Walk the brick's particles in a strided permutation q = j·P mod total (P coprime to total, about a
+  // warp's share apart): consecutive lanes of a warp then take particles of cells far apart, so their
+  // shared-memory atomics hit different nodes instead of the same 8 (sorted neighbours share a cell).
+  __shared__ int s_P;
+  if (threadIdx.x == 0) {
+    int P = (total / 32) | 1;
+    if (P < 1) P = 1;
+    auto gcd = [](int a, int b) { while (b) { const int t = a % b; a = b; b = t; } return a; };
+    while (total > 1 && gcd(P, total) != 1) ++P;
+    s_P = P;
+  }
+  __syncthreads();
+  const long long P = s_P;
+  for (int j = threadIdx.x; j < total; j += blockDim.x) {
+    const int q = (int)((j * P) % total);
+    int lo = 0, hi = kBrick * kBrick - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (s_rowp[mid] <= q) lo = mid; else hi = mid - 1;
     }
+    const int pi = s_row0[lo] + (q - s_rowp[lo]);
+    const float4 Pp = T.pB[pi];
+    const float4 V = T.vB[pi];
+    double g[3];
+    grid_pos(T, (double)Pp.x, (double)Pp.y, (double)Pp.z, g[0], g[1], g[2]);
+    const double vv[3] = {fmin(fmax((double)V.x, -30.0), 30.0), fmin(fmax((double)V.y, -30.0), 30.0),
+                          fmin(fmax((double)V.z, -30.0), 30.0)};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const double qx = g[0] - (a == 0 ? 0.0 : 0.5), qy = g[1] - (a == 1 ? 0.0 : 0.5), qz = g[2] - (a == 2 ? 0.0 : 0.5);
@@ -185,18 +179,12 @@ __global__ void __launch_bounds__(kThreads) k_p2g(const TankDev* __restrict__ ta
       for (int e = 0; e < 8; ++e) {
         const int dx = e >> 2, dy = (e >> 1) & 1, dz = e & 1;
         const int ix = bx + dx, iy = by + dy, iz = bz + dz;
+        if (ix < 0 || ix >= nsx || iy < 0 || iy >= nsy || iz < 0 || iz >= nsz) continue;
         const double w = (wx[dx] * wy[dy]) * wz[dz];
-        const bool use = valid && ix >= 0 && ix < nsx && iy >= 0 && iy < nsy && iz >= 0 && iz < nsz && w > 0.0;
-        const int ln = use ? (ix - i0 + 1) + kBN * ((iy - j0 + 1) + kBN * (iz - k0 + 1)) : -1;
-        const long long m = use ? __double2ll_rn(w * vv[a] * kFix) : 0LL;
-        const long long wt = use ? __double2ll_rn(w * kFix) : 0LL;
-        const unsigned peers = __match_any_sync(0xffffffffu, ln);
-        const long long M = group_sum(peers, m);
-        const long long Wt = group_sum(peers, wt);
-        if (ln >= 0 && lane == __ffs(peers) - 1) {
-          atomicAdd((unsigned long long*)&s_acc[a][ln], (unsigned long long)M);
-          atomicAdd((unsigned long long*)&s_acc[3 + a][ln], (unsigned long long)Wt);
-        }
+        if (!(w > 0.0)) continue;
+        const int ln = (ix - i0 + 1) + kBN * ((iy - j0 + 1) + kBN * (iz - k0 + 1));
+        atomicAdd((unsigned long long*)&s_acc[a][ln], (unsigned long long)__double2ll_rn(w * vv[a] * kFix));
+        atomicAdd((unsigned long long*)&s_acc[3 + a][ln], (unsigned long long)__double2ll_rn(w * kFix));
       }
     }
   }

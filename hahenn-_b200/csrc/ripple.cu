@@ -27,6 +27,7 @@ struct RippleState {
   int W = 0, Mx = 0, Mz = 0, lx = 0, lz = 0;
   double Lx = 0, Lz = 0;
   double sigma_rho = 0.0728 / 998.0, rho = 998.0, g = 9.81;
+  double depth = 0.0;           // fixed dispersion depth; 0: mean depth of the liquid each frame
   unsigned* topkey = nullptr;   // W² ordered float keys of the highest particle
   double* hA = nullptr;         // W² float64 work maps
   double* hB = nullptr;
@@ -197,7 +198,7 @@ __global__ void k_fft_cols(float2* __restrict__ data, int M, int logM, int ld, i
 
 // exact damped oscillator per mode plus the impulse kick (solver.py:882-899, 64-ripple.js:58-90)
 __global__ void k_ripple_evolve(TankDev T, float2* __restrict__ S, const float2* __restrict__ hat, int Mx, int Mz, double Lx,
-                                double Lz, double dt, double g, double sigma_rho, double rho) {
+                                double Lz, double dt, double g, double sigma_rho, double rho, double fixed_depth) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= Mx * Mz) return;
   const int i = e % Mx, j = e / Mx;
@@ -205,7 +206,7 @@ __global__ void k_ripple_evolve(TankDev T, float2* __restrict__ S, const float2*
   const int mx = i < Rx ? i : i - Mx, mz = j < Rz ? j : j - Mz;
   if ((mx == 0 && mz == 0) || mx == -Rx || mz == -Rz) { S[e] = make_float2(0.f, 0.f); return; }
   const double n = (double)T.ctr->n_sorted;
-  const double depth = fmin(fmax(n * T.vp / (T.nx * T.nz * T.h * T.h), 0.003), T.rim);
+  const double depth = fixed_depth > 0 ? fixed_depth : fmin(fmax(n * T.vp / (T.nx * T.nz * T.h * T.h), 0.003), T.rim);
   const double kx = mx * M_PI / Lx, kz = mz * M_PI / Lz;
   const double kk = sqrt(kx * kx + kz * kz);
   const double D = fmax(depth, 0.002);
@@ -287,6 +288,10 @@ RippleState& ensure(Tank& t) {
   t.ripple = r;
   r->W = t.cfg.wmap;
   r->Mx = 2 * D.rx; r->Mz = 2 * D.rz;
+  r->sigma_rho = t.cfg.ripple_sigma / t.cfg.ripple_rho;
+  r->rho = t.cfg.ripple_rho;
+  r->g = t.cfg.g;
+  r->depth = t.cfg.ripple_depth;
   r->Lx = D.nx * D.h; r->Lz = D.nz * D.h;
   const int W = r->W;
   static_assert(sizeof(float2) == 8, "");
@@ -409,7 +414,7 @@ void ripple_frame(Tank& t, double frame_dt) {
   k_ripple_src<<<nb, 256, 0, t.stream>>>(t.d, t.d.rsrc, r.A, r.Mx, r.Mz, 1.0 / (dx * dz));
   CK(cudaMemsetAsync(t.d.rsrc, 0, (size_t)nv * 8, t.stream));
   fft2(t, r.A, -1.f);
-  k_ripple_evolve<<<nb, 256, 0, t.stream>>>(t.d, r.S, r.A, r.Mx, r.Mz, r.Lx, r.Lz, frame_dt, r.g, r.sigma_rho, r.rho);
+  k_ripple_evolve<<<nb, 256, 0, t.stream>>>(t.d, r.S, r.A, r.Mx, r.Mz, r.Lx, r.Lz, frame_dt, r.g, r.sigma_rho, r.rho, r.depth);
   fft2(t, r.S, 1.f);
   k_ripple_field<<<nb, 256, 0, t.stream>>>(t.d, r.S, r.A, r.mask, r.field, r.Mx, r.Mz, dx, dz);
   fft2(t, r.A, -1.f);

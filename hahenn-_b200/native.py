@@ -24,7 +24,8 @@ class Params(C.Structure):
                 ('friction', C.c_double), ('ppc', C.c_double), ('drift', C.c_double), ('ww_rate', C.c_double),
                 ('whitewater', C.c_int32), ('capacity', C.c_int64), ('ww_capacity', C.c_int64),
                 ('ripple_rx', C.c_int32), ('ripple_rz', C.c_int32), ('wmap', C.c_int32), ('sdf_mode', C.c_int32),
-                ('device', C.c_int32), ('seed', C.c_uint32)]
+                ('device', C.c_int32), ('seed', C.c_uint32), ('ripple_sigma', C.c_double), ('ripple_rho', C.c_double),
+                ('ripple_depth', C.c_double)]
 
 
 class Stats(C.Structure):
@@ -41,7 +42,7 @@ class Object(C.Structure):
 
 class Emitter(C.Structure):
     _fields_ = [('shape', C.c_int32), ('airborne', C.c_int32), ('pos', C.c_double * 3), ('dir', C.c_double * 3),
-                ('radius', C.c_double), ('speed', C.c_double), ('per_substep', C.c_double)]
+                ('radius', C.c_double), ('speed', C.c_double), ('per_substep', C.c_double), ('radius_z', C.c_double)]
 
 
 class Request(C.Structure):

@@ -63,6 +63,10 @@ typedef struct suiri_params {
   int32_t sdf_mode;        /* 0 analytic obstacle shapes (web version), 1 distance lattice (Blender) */
   int32_t device;          /* CUDA device ordinal */
   uint32_t seed;           /* emission jitter seed */
+  /* ripple dispersion ω² = (g k + σ/ρ k³) tanh(k d) (solver.py:887; 64-ripple.js:74) */
+  double ripple_sigma;     /* surface tension σ [N/m] (0.0728) */
+  double ripple_rho;       /* density ρ [kg/m³] (998) */
+  double ripple_depth;     /* d [m]; 0: mean depth from the liquid volume each frame (solver.py:726) */
 } suiri_params;
 
 typedef struct suiri_stats {
@@ -153,9 +157,10 @@ typedef struct suiri_emitter {
   int32_t airborne;        /* 1: emitted particles carry the free-flight mark (sub-grid drops) */
   double pos[3];
   double dir[3];
-  double radius;
+  double radius;           /* disc radius; rain: half extent along x */
   double speed;
   double per_substep;
+  double radius_z;         /* rain: half extent along z (0: same as radius) */
 } suiri_emitter;
 int suiri_set_emitters(suiri_tank* t, const suiri_emitter* e, int32_t n);
 

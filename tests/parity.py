@@ -35,13 +35,13 @@ def gpu_from(pkg, nx, ny, nz, h, *, flip, omega, iters, g=9.81, whitewater=False
                     capacity=n, ripple=ripple, wmap=wmap, sdf_mode=sdf_mode, ww_capacity=ww_capacity, seed=seed)
 
 
-def assert_close_field(a, b, rtol=RTOL, what=''):
+def assert_close_field(a, b, rtol=RTOL, what='', atol=0.0):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     assert a.shape == b.shape, (what, a.shape, b.shape)
     scale = max(float(np.abs(b).max()) if b.size else 0.0, 1e-30)
     err = np.abs(a - b)
-    lim = rtol * np.abs(b) + rtol * scale
+    lim = rtol * np.abs(b) + rtol * scale + atol
     bad = err > lim
     assert not bad.any(), f'{what}: {int(bad.sum())} of {b.size} beyond tolerance, max err {err.max():.3e} (scale {scale:.3e})'
 
