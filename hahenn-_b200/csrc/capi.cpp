@@ -286,6 +286,13 @@ int suiri_eval_sdf(suiri_tank* h, const double* pts, int64_t n, double* out) {
   });
 }
 
+int suiri_eval_sdf_static(suiri_tank* h, const double* pts, int64_t n, double* out) {
+  return guard(h ? &h->err : nullptr, [&] {
+    if (n < 0 || (n > 0 && (!pts || !out))) throw Error(SUIRI_ERR_INVALID, "bad point arrays");
+    T(h)->eval_sdf_static(pts, n, out);
+  });
+}
+
 int suiri_estimate_bytes(const char* scene_json, const suiri_params* params, double* bytes) {
   return guard(nullptr, [&] {
     if (!bytes) throw Error(SUIRI_ERR_INVALID, "null output");

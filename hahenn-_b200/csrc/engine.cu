@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "sdf.cuh"
 
@@ -184,6 +185,45 @@ __global__ void k_eval_sdf(TankDev T, const double* __restrict__ pts, double* __
   const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (q >= n) return;
   out[q] = tank_sdf(T, pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+}
+
+// Staging for suiri_eval_sdf_static: the points (3 doubles each) followed by the distances, for at most
+// kSdfStaticMax points. 2 MiB that every GPU which loads the library holds until the process exits.
+constexpr long long kSdfStaticMax = 65536;
+static __device__ __align__(256) double g_sdf_static[4 * kSdfStaticMax];
+
+namespace {
+std::mutex g_static_mu;
+double* g_static_ptr[128] = {};
+
+// Device address of g_sdf_static on `dev` (host code cannot use the symbol itself: its host-side name is a
+// stand-in, not a device address). Looked up once per device, with that device current.
+double* sdf_static_scratch(int dev) {
+  if (dev < 0 || dev >= 128) throw Error(-1, "device ordinal out of range");
+  std::lock_guard<std::mutex> g(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    CK(cudaSetDevice(dev));
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_sdf_static));
+    g_static_ptr[dev] = (double*)p;
+  }
+  return g_static_ptr[dev];
+}
+}  // namespace
+
+void Tank::eval_sdf_static(const double* pts, long long n, double* out) {
+  if (n > kSdfStaticMax)
+    throw Error(-1, "suiri_eval_sdf_static: " + std::to_string(n) + " points, at most " + std::to_string(kSdfStaticMax) +
+                        " per call (the static staging array is fixed)");
+  join();
+  if (n <= 0) return;
+  double* s = sdf_static_scratch(cfg.device);
+  CK(cudaSetDevice(cfg.device));
+  CK(cudaMemcpyAsync(s, pts, n * 24, cudaMemcpyHostToDevice, stream));
+  k_eval_sdf<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(d, s, s + 3 * kSdfStaticMax, n);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, s + 3 * kSdfStaticMax, n * 8, cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
 }
 
 void Tank::eval_sdf(const double* pts, long long n, double* out) {

@@ -101,6 +101,7 @@ struct Tank {
 
   void set_emitters(const std::vector<EmitterDev>& e);
   void eval_sdf(const double* pts, long long n, double* out);
+  void eval_sdf_static(const double* pts, long long n, double* out);   // no device allocation
 
   explicit Tank(const TankConfig& c);
   ~Tank();

@@ -71,6 +71,7 @@ SIGNATURES = {
     'suiri_set_emitters': (C.c_int, [P, C.POINTER(Emitter), C.c_int32]),
     'suiri_tune': (C.c_int, [P, C.c_int32, C.c_int32]),
     'suiri_eval_sdf': (C.c_int, [P, P, C.c_int64, P]),
+    'suiri_eval_sdf_static': (C.c_int, [P, P, C.c_int64, P]),
     'suiri_estimate_bytes': (C.c_int, [C.c_char_p, C.POINTER(Params), C.POINTER(C.c_double)]),
     'suiri_profile': (C.c_int, [P, C.c_int32]),
     'suiri_sor_phase_ms': (C.c_int, [P, C.POINTER(C.c_double)]),

@@ -141,6 +141,18 @@ int suiri_set_lattice(suiri_tank* t, const double* sdf, const int32_t* oid, int3
    shapes or the lattice (sceneSdf, src/js/30-wgsl-sim.js:78-87; sdf_at, solver.py:116-140; the editor's
    mirror for picking and placement, src/js/10-scene.js:124-176). 1e9 where there is no obstacle. */
 int suiri_eval_sdf(suiri_tank* t, const double* pts, int64_t n, double* out);
+/* The same distances without allocating anything on the device. No counterpart in the reference: it is
+   for callers that cannot allocate device memory when they ask — a host whose device memory is fully
+   committed (a server that has admitted scenes up to its whole HBM budget, where a per-call allocation
+   could fail or take memory promised to resident scenes), or an interactive loop that queries distances
+   every frame (picking, placement) and must keep the allocator off that path. suiri_eval_sdf stages the
+   points and distances in memory it allocates per call; this one stages them in one fixed array inside
+   the library, at most 65536 points per call (more: SUIRI_ERR_INVALID). The array (2 MiB) exists on every
+   GPU that loads the library, until the process exits. The first call on a device looks up the array's
+   address there; make that first call before any stream capture. All calls share the one array: calls
+   that overlap on the GPU (two threads, two tanks on different streams) race on it, so serialise them.
+   Every call writes all the staging it reads, so nothing is left over from the previous call. */
+int suiri_eval_sdf_static(suiri_tank* t, const double* pts, int64_t n, double* out);
 /* device bytes a tank of these parameters and scene would take (admission planning) */
 int suiri_estimate_bytes(const char* scene_json, const suiri_params* params, double* bytes);
 
