@@ -208,7 +208,7 @@ def run_batch(args, local):
     line = dict(metric=METRIC, value=rate_b, unit=METRIC, n_gpus=1, steps=args.steps, warmup=args.warmup, ms_per_step=ms_batch,
                 higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32', data='synthetic',
                 config=dict(workload=f'batch_{len(specs)}_tanks', tanks=len(specs), particles=particles, cells=cells,
-                            sor_iters=80, omega=1.7, dt=dt, tuned=dict(blocks_per_sm=best[0], sor_persistent=best[1]),
+                            sor_iters=80, omega=1.7, dt=dt, tuned=dict(blocks_per_sm=best[0], sor_mode=best[1]),
                             tuning_ms={f'{k[0]}x{k[1]}': v for k, v in timings.items()}),
                 plain_sequential=dict(value=rate_p, ms_per_step=ms_plain), batched_over_plain=rate_b / rate_p)
     print(json.dumps(line), flush=True)

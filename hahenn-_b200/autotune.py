@@ -2,30 +2,32 @@
 
 Knobs (``suiri_tune`` / ``suiri_batch_tune``):
   * blocks per SM of the persistent particle kernels (binning, scatter, G2P);
-  * the form of the pressure solve: one launch per colour sweep inside the sub-step graph, or the whole
-    solve as one cooperative launch with a grid barrier between sweeps.
+  * the form of the pressure solve (sor_mode): 0 one launch per colour sweep inside the sub-step graph,
+    1 the whole solve as one cooperative launch with a grid barrier between sweeps, 2 four colour sweeps
+    per launch on shared-memory tiles with halos (temporal blocking).
 
 Each candidate is timed on the device (events on the tank's or batch's stream) over a few sub-steps of the
 real state, after one sub-step that captures its graph. Tuning advances the simulation by those
 sub-steps.
 """
 
-CANDIDATES = ((2, 0), (4, 0), (8, 0), (2, 1), (4, 1), (8, 1))
+CANDIDATES = ((2, 0), (4, 0), (8, 0), (2, 2), (4, 2), (8, 2), (4, 1))
 
 
 def autotune(target, dt, candidates=CANDIDATES, steps=3):
-    """Return ((blocks_per_sm, sor_persistent), {candidate: ms per sub-step}) and leave the best set."""
+    """Return ((blocks_per_sm, sor_mode), {candidate: ms per sub-step}) and leave the best set."""
     timings = {}
-    for bps, persistent in candidates:
+    last = None
+    for bps, mode in candidates:
         try:
-            target.tune(bps, bool(persistent))
+            target.tune(bps, mode)
             target.time_substeps(dt, 1)
-            timings[(bps, persistent)] = target.time_substeps(dt, steps) / steps
+            timings[(bps, mode)] = target.time_substeps(dt, steps) / steps
         except Exception as e:          # a shape the device cannot launch (e.g. too large to be co-resident)
-            timings[(bps, persistent)] = float('inf')
+            timings[(bps, mode)] = float('inf')
             last = e
     best = min(timings, key=timings.get)
     if timings[best] == float('inf'):
         raise last
-    target.tune(best[0], bool(best[1]))
+    target.tune(best[0], best[1])
     return best, timings

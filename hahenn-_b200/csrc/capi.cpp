@@ -481,25 +481,25 @@ int suiri_batch_sync(suiri_batch* b) {
   });
 }
 
-static void tune_group(Group& g, int32_t particle_blocks_per_sm, int32_t sor_persistent) {
+static void tune_group(Group& g, int32_t particle_blocks_per_sm, int32_t sor_mode) {
   if (particle_blocks_per_sm < 1 || particle_blocks_per_sm > 32) throw Error(SUIRI_ERR_INVALID, "blocks per SM in 1..32");
-  if (sor_persistent != 0 && sor_persistent != 1) throw Error(SUIRI_ERR_INVALID, "sor_persistent is 0 or 1");
+  if (sor_mode < 0 || sor_mode > 2) throw Error(SUIRI_ERR_INVALID, "sor_mode is 0, 1 or 2");
   CK(cudaStreamSynchronize(g.stream));
   g.blocks_per_sm = particle_blocks_per_sm;
   g.ctx.particle_blocks = particle_blocks_per_sm * g.sm_count;
-  g.sor_persistent = sor_persistent;
+  g.sor_mode = sor_mode;
   g.drop_graph();
 }
 
-int suiri_batch_tune(suiri_batch* b, int32_t particle_blocks_per_sm, int32_t sor_persistent) {
+int suiri_batch_tune(suiri_batch* b, int32_t particle_blocks_per_sm, int32_t sor_mode) {
   return guard(b ? &b->err : nullptr, [&] {
     if (!b || !b->g) throw Error(SUIRI_ERR_INVALID, "null batch");
-    tune_group(*b->g, particle_blocks_per_sm, sor_persistent);
+    tune_group(*b->g, particle_blocks_per_sm, sor_mode);
   });
 }
 
-int suiri_tune(suiri_tank* h, int32_t particle_blocks_per_sm, int32_t sor_persistent) {
-  return guard(h ? &h->err : nullptr, [&] { tune_group(*T(h)->solo, particle_blocks_per_sm, sor_persistent); });
+int suiri_tune(suiri_tank* h, int32_t particle_blocks_per_sm, int32_t sor_mode) {
+  return guard(h ? &h->err : nullptr, [&] { tune_group(*T(h)->solo, particle_blocks_per_sm, sor_mode); });
 }
 
 int suiri_batch_stream(suiri_batch* b, void** stream) {

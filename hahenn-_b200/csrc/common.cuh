@@ -13,9 +13,14 @@
 namespace suiri {
 
 // P2G sums are integer fixed point: order independent, so every run and every batch mix gives the same
-// bits. 2^40 keeps 9e-13 resolution per contribution and headroom for ~2.8e5 particles at 30 m/s per node.
-constexpr double kFix = 1099511627776.0;          // 2^40
-constexpr double kFixInv = 1.0 / 1099511627776.0;
+// bits. 2^38 keeps 3.6e-12 resolution per contribution (|w·v| ≤ 30 → |term| < 2^43), so a node's 64-bit
+// sum has headroom for 2^20 terms. Inside a P2G brick a term also splits exactly into a 22-bit remainder
+// and a signed quotient, which 32-bit shared atomics can sum without overflow while a node takes at most
+// kSplitMaxTerms terms (1023·(2^22 − 1) < 2^32 and 1023·2^21 < 2^31).
+constexpr double kFix = 274877906944.0;           // 2^38
+constexpr double kFixInv = 1.0 / 274877906944.0;
+constexpr int kSplit = 22;                        // remainder bits of the split shared-memory sums
+constexpr int kSplitMaxTerms = 1023;              // terms per node for which both halves stay exact
 constexpr double kRippleFix = 281474976710656.0;  // 2^48, ripple impulses [N·s]
 constexpr double kBig = 1e9;
 
@@ -94,6 +99,7 @@ struct TankDev {
   float2* vv;               // 3*nnodes: per component (projected v, P2G v or NaN where the face took no weight)
   double* flux;             // 3*nnodes cut-cell face fluxes (divergence operand)
   float* pres;              // 2*nhalf colour-split pressure
+  float* pres2;             // 2*nhalf, the other buffer of the temporal-blocked solve
   float* rhs;               // 2*nhalf h²·div
   uint32_t* code;           // 2*nhalf
   const Obj* objs;

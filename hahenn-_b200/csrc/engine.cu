@@ -285,6 +285,7 @@ Tank::Tank(const TankConfig& c) : cfg(c) {
   D.fracd = (double*)alloc(3 * nn * 8); D.flux = (double*)alloc(3 * nn * 8);
   D.vv = (float2*)alloc(3 * nn * 8);
   D.pres = (float*)alloc(2 * nh * 4); D.rhs = (float*)alloc(2 * nh * 4); D.code = (uint32_t*)alloc(2 * nh * 4);
+  D.pres2 = (float*)alloc(2 * nh * 4);
   d_objs = (Obj*)alloc(kMaxObj * sizeof(Obj));
   D.objs = d_objs;
   D.ctr = (Counters*)alloc(sizeof(Counters));
@@ -300,7 +301,8 @@ Tank::~Tank() {
   delete solo;
   cudaSetDevice(cfg.device);
   if (stream) cudaStreamSynchronize(stream);
-  for (void* p : dmem) cudaFree(p);
+  for (void* p : dmem) cudaFreeAsync(p, stream);
+  if (stream) cudaStreamSynchronize(stream);
   if (snap.p) { cudaFree(snap.p); cudaFree(snap.v); cudaFree(snap.wp); cudaFree(snap.wv); cudaFree(snap.pres); cudaFree(snap.ripple); }
   free_ripple(*this);
   if (h_ctr) cudaFreeHost(h_ctr);
@@ -323,7 +325,7 @@ size_t tank_bytes(const TankConfig& c) {
   size_t b = cap * 16 * 6 + cap * 2 * 4;                      // A, E, B (pos, vel), ranks
   b += (nc + 1) * 4 + (nc + 2) * 4;                           // counts, offsets
   b += nn * (6 * 8 + 4 * 16 + 2 * 3 * 8 + 3 * 8);            // accumulator, vel/velold/frac/svel, fracd/flux, vv
-  b += 2 * nh * 12;                                           // pressure, rhs, code
+  b += 2 * nh * 16;                                           // pressure (two buffers), rhs, code
   b += kMaxObj * sizeof(Obj) + sizeof(Counters) + kMaxEmitters * sizeof(EmitterDev);
   b += 2 * (size_t)std::max(1LL, c.ww_cap) * 32;
   if (c.rx > 0) {
@@ -333,9 +335,21 @@ size_t tank_bytes(const TankConfig& c) {
   return b + (64 << 10) * 24;                                 // allocation granularity
 }
 
+// Tank memory comes from the device's stream-ordered pool, which keeps freed blocks for reuse (release
+// threshold raised once per device): scenes that come and go (serving) then cost no driver allocation.
 void* Tank::alloc(size_t bytes) {
+  static std::once_flag once[128];
+  const int dev = cfg.device;
+  if (dev >= 0 && dev < 128)
+    std::call_once(once[dev], [dev] {
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        unsigned long long keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
+    });
   void* p = nullptr;
-  CK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+  CK(cudaMallocAsync(&p, std::max<size_t>(bytes, 16), stream));
   dmem.push_back(p);
   CK(cudaMemsetAsync(p, 0, std::max<size_t>(bytes, 16), stream));
   return p;
@@ -800,6 +814,8 @@ int blocks_for(int fam, const TankDev& D) {
     case kFamHalf: return (D.nhalf + kThreads - 1) / kThreads;
     case kFamBricks: return ((D.nx + kBrick - 1) / kBrick) * ((D.ny + kBrick - 1) / kBrick) * ((D.nz + kBrick - 1) / kBrick);
     case kFamScan: return (D.ncells + 1 + kScanTile - 1) / kScanTile;
+    case kFamSor: return (D.nhalf + kThreads * kSorPer - 1) / (kThreads * kSorPer);
+    case kFamTiles: return ((D.nx + kTbX - 1) / kTbX) * ((D.ny + kTbY - 1) / kTbY) * ((D.nz + kTbZ - 1) / kTbZ);
   }
   return 0;
 }
@@ -813,6 +829,7 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
   CK(cudaSetDevice(device));
   if (s) { stream = s; } else { CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)); own_stream = true; }
   CK(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device));
+  CK(sor_tb_prepare());
   const int n = (int)tanks.size();
   CK(cudaMalloc(&d_tanks, n * sizeof(TankDev)));
   CK(cudaMallocHost(&h_tanks, n * sizeof(TankDev)));
@@ -944,14 +961,21 @@ void Group::enqueue_body() {
   if (profile) CK(cudaStreamIsCapturing(stream, &cap));
   const unsigned evflags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
   if (profile) CK(cudaEventRecordWithFlags(ev_sor[0], stream, evflags));
-  if (sor_persistent && max_iters > 0) {
+  if (sor_mode == 1 && max_iters > 0) {
     launch_sor_persist(ctx, max_iters, sor_blocks);
+    CK(cudaGetLastError());
+  } else if (sor_mode == 2) {
+    // launch l reads pres (l even) or pres2 and writes the other; an odd count ends in pres2
+    const int sweeps = 2 * max_iters, nl = (sweeps + kTbSweeps - 1) / kTbSweeps;
+    for (int l = 0; l < nl; ++l) launch_sor_tb(ctx, l * kTbSweeps, std::min(kTbSweeps, sweeps - l * kTbSweeps), l & 1);
+    if (nl & 1) launch_sor_copy(ctx);
     CK(cudaGetLastError());
   } else {
     for (int it = 0; it < max_iters; ++it) {
       launch_sor_sweep(ctx, 0, it);
       launch_sor_sweep(ctx, 1, it);
     }
+    CK(cudaGetLastError());
   }
   if (profile) CK(cudaEventRecordWithFlags(ev_sor[1], stream, evflags));
   launch_project(ctx);

@@ -60,28 +60,31 @@ __device__ __forceinline__ bool air_at(const TankDev& T, int i, int j, int k) {
   return count_at(T, i, j, k) == 0;
 }
 
-// PIC and FLIP velocity of one component from faces that took weight this step (solver.py:236-249).
-// The 8 corner loads are issued together (one float2 each: projected v, P2G v or NaN), then summed in the
-// reference's corner order.
+// PIC and FLIP velocity of one component from faces that took weight this step (solver.py:236-249), at a
+// grid position inside the grid (0 ≤ g < n on every axis; both callers check). Along the component's own
+// axis both corner nodes then exist; on the other two axes the staggered lower corner is node −1 at the
+// first half cell, the only corners that can be missing. The 8 corner loads (one float2 each: projected
+// v, P2G v or NaN where the face took no weight) are issued together, then summed in the reference's
+// corner order.
 __device__ __forceinline__ void transfer(const TankDev& T, double gx, double gy, double gz, int comp, double vp,
                                          double& pic, double& flip) {
   const double qx = gx - (comp == 0 ? 0.0 : 0.5), qy = gy - (comp == 1 ? 0.0 : 0.5), qz = gz - (comp == 2 ? 0.0 : 0.5);
   const int bx = (int)floor(qx), by = (int)floor(qy), bz = (int)floor(qz);
   const double fx = qx - bx, fy = qy - by, fz = qz - bz;
   const double wx[2] = {1 - fx, fx}, wy[2] = {1 - fy, fy}, wz[2] = {1 - fz, fz};
-  const float2* __restrict__ vv = T.vv + (size_t)comp * T.nnodes;
+  const float2* __restrict__ vv = T.vv + (size_t)comp * T.nnodes + node_idx(T, bx, by, bz);
+  const bool lx = bx >= 0, ly = by >= 0, lz = bz >= 0;
   float2 c[8];
-  bool ok[8];
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
-    const int ix = bx + (e >> 2), iy = by + ((e >> 1) & 1), iz = bz + (e & 1);
-    ok[e] = ix >= 0 && ix <= T.nx && iy >= 0 && iy <= T.ny && iz >= 0 && iz <= T.nz;
-    c[e] = ok[e] ? __ldg(vv + node_idx(T, ix, iy, iz)) : make_float2(0.f, 0.f);
+    const int dx = e >> 2, dy = (e >> 1) & 1, dz = e & 1;
+    const bool ok = (dx || lx) && (dy || ly) && (dz || lz);
+    c[e] = ok ? __ldg(vv + dx + dy * T.sx + dz * T.sxy) : make_float2(0.f, __int_as_float(0x7fc00000));
   }
   double sn = 0.0, so = 0.0, sw = 0.0;
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
-    if (!ok[e] || isnan(c[e].y)) continue;
+    if (isnan(c[e].y)) continue;
     const double w = (wx[e >> 2] * wy[(e >> 1) & 1]) * wz[e & 1];
     sn += w * (double)c[e].x;
     so += w * (double)c[e].y;
@@ -171,7 +174,10 @@ __global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ ta
     grid_pos(T, x0[0], x0[1], x0[2], g[0], g[1], g[2]);
     const bool ing = in_grid(T, g[0], g[1], g[2]);
     double v[3] = {vold[0], vold[1], vold[2]};
+    const int c0[3] = {(int)floor(g[0]), (int)floor(g[1]), (int)floor(g[2])};
+    int n0 = 0;
     if (ing) {
+      n0 = count_at(T, c0[0], c0[1], c0[2]);
       for (int a = 0; a < 3; ++a) {
         double pic, flip;
         transfer(T, g[0], g[1], g[2], a, vold[a], pic, flip);
@@ -207,16 +213,17 @@ __global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ ta
     if (!in_fp(fp, x[0], x[2]) && x[1] < 0.002) alive = false;
     if (fabs(x[0]) > 20 || fabs(x[2]) > 20 || x[1] < -1 || x[1] > 30) alive = false;
     // free-flight mark of sub-grid drops (solver.py:565-583)
-    const int c0[3] = {(int)floor(g[0]), (int)floor(g[1]), (int)floor(g[2])};
     bool air = flags & kFlagAir;
     if (ing) {
-      const int n0 = count_at(T, c0[0], c0[1], c0[2]);
       if (n0 >= 4) {
         air = false;
       } else if (n0 <= 2 && c0[1] + 2 < T.ny) {
         int around = 0, above = 0;
+#pragma unroll
         for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
           for (int dx = -1; dx <= 1; ++dx) {
+#pragma unroll
             for (int dy = -1; dy <= 1; ++dy) around += count_at(T, c0[0] + dx, c0[1] + dy, c0[2] + dz);
             above += count_at(T, c0[0] + dx, c0[1] + 1, c0[2] + dz) + count_at(T, c0[0] + dx, c0[1] + 2, c0[2] + dz);
           }
@@ -255,10 +262,13 @@ __global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ ta
       // stored +1 so that 0 means "no in-grid particle this sub-step" (the reference keeps vmax then)
       vbits = (unsigned long long)__double_as_longlong(fmin(sp, 60.0)) + 1ull;
       if (T.whitewater && sp > 0.75) {
+        // the six face neighbours, loaded together
         bool near = false;
-        for (int a = 0; a < 3 && !near; ++a)
-          for (int sg = -1; sg <= 1 && !near; sg += 2)
-            near = air_at(T, c0[0] + (a == 0 ? sg : 0), c0[1] + (a == 1 ? sg : 0), c0[2] + (a == 2 ? sg : 0));
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int sg = -1; sg <= 1; sg += 2)
+            near |= air_at(T, c0[0] + (a == 0 ? sg : 0), c0[1] + (a == 1 ? sg : 0), c0[2] + (a == 2 ? sg : 0));
         if (near) {
           uint32_t s = hash_u32(id * 9781u + (uint32_t)frame * 6271u + 17u);
           const double e = fmin(fmax((sp - 0.75) / 1.6, 0.0), 1.0);

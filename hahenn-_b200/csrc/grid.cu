@@ -104,7 +104,8 @@ __global__ void __launch_bounds__(kThreads) k_geom(const TankDev* __restrict__ t
 // ------------------------------------------------------------------------------------------------ P2G
 // One block per 8×8×8-cell brick. The brick's particles are contiguous per (j,k) row in the sorted
 // array, so the block walks them coalesced and splats into a shared-memory copy of the 10×10×10 nodes
-// they can reach, as 64-bit fixed-point integers (exact, order independent), then adds the non-zero
+// they can reach, as fixed-point integers (exact, order independent; 32-bit halves while the brick's
+// cell counts allow, 64-bit otherwise), then adds the non-zero
 // node sums into the global accumulator. Weights follow blender_addon/suiri_lab/solver.py:443-460
 // (float64; per corner w = (wx·wy)·wz, zero weights skipped, velocity clamped to ±30) and
 // src/js/30-wgsl-sim.js:159-200 (fixed point). The global accumulator is zeroed by the node pass that
@@ -123,16 +124,27 @@ __global__ void __launch_bounds__(kThreads) k_p2g(const TankDev* __restrict__ ta
   const int bi = lb % bnx, bj = (lb / bnx) % bny, bk = lb / (bnx * bny);
   const int i0 = bi * kBrick, j0 = bj * kBrick, k0 = bk * kBrick;
   const int i1 = min(i0 + kBrick, T.nx);
+  __shared__ int s_maxc;
   for (int e = threadIdx.x; e < 6 * kBNodes; e += blockDim.x) (&s_acc[0][0])[e] = 0;
+  if (threadIdx.x == 0) s_maxc = 0;
+  __syncthreads();
   if (threadIdx.x < kBrick * kBrick) {
     const int j = j0 + (threadIdx.x % kBrick), k = k0 + (threadIdx.x / kBrick);
-    int a = 0, b = 0;
+    int a = 0, b = 0, mc = 0;
     if (j < T.ny && k < T.nz) {
-      a = T.off[cell_idx(T, i0, j, k)];
-      b = T.off[cell_idx(T, i0, j, k) + (i1 - i0)];
+      const int* o = T.off + cell_idx(T, i0, j, k);
+      a = o[0];
+      int prev = a;
+      for (int i = 1; i <= i1 - i0; ++i) {
+        const int x = o[i];
+        mc = max(mc, x - prev);
+        prev = x;
+      }
+      b = prev;
     }
     s_row0[threadIdx.x] = a;
     s_rowp[threadIdx.x + 1] = b - a;
+    if (mc > 0) atomicMax(&s_maxc, mc);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -155,6 +167,12 @@ __global__ void __launch_bounds__(kThreads) k_p2g(const TankDev* __restrict__ ta
   }
   __syncthreads();
   const long long P = s_P;
+  // A node takes terms from the particles of at most 2·3·3 cells of the brick (its own axis: the two cells
+  // either side; the other axes: three cells, half of the outer two), so at most 18·(largest cell count)
+  // terms. Within kSplitMaxTerms the split 32-bit sums are exact; above it the 64-bit shared atomics are used.
+  const bool split = 18 * s_maxc <= kSplitMaxTerms;
+  unsigned* s_lo = reinterpret_cast<unsigned*>(&s_acc[0][0]);
+  int* s_hi = reinterpret_cast<int*>(&s_acc[0][0]) + 6 * kBNodes;
   for (int j = threadIdx.x; j < total; j += blockDim.x) {
     const int q = (int)((j * P) % total);
     int lo = 0, hi = kBrick * kBrick - 1;
@@ -183,8 +201,17 @@ __global__ void __launch_bounds__(kThreads) k_p2g(const TankDev* __restrict__ ta
         const double w = (wx[dx] * wy[dy]) * wz[dz];
         if (!(w > 0.0)) continue;
         const int ln = (ix - i0 + 1) + kBN * ((iy - j0 + 1) + kBN * (iz - k0 + 1));
-        atomicAdd((unsigned long long*)&s_acc[a][ln], (unsigned long long)__double2ll_rn(w * vv[a] * kFix));
-        atomicAdd((unsigned long long*)&s_acc[3 + a][ln], (unsigned long long)__double2ll_rn(w * kFix));
+        const long long tm = __double2ll_rn(w * vv[a] * kFix), tw = __double2ll_rn(w * kFix);
+        if (split) {
+          // term = quotient·2^19 + remainder: two native 32-bit shared atomics, exact (see common.cuh)
+          atomicAdd(s_lo + a * kBNodes + ln, (unsigned)(tm & ((1LL << kSplit) - 1)));
+          atomicAdd(s_hi + a * kBNodes + ln, (int)(tm >> kSplit));
+          atomicAdd(s_lo + (3 + a) * kBNodes + ln, (unsigned)(tw & ((1LL << kSplit) - 1)));
+          atomicAdd(s_hi + (3 + a) * kBNodes + ln, (int)(tw >> kSplit));
+        } else {
+          atomicAdd((unsigned long long*)&s_acc[a][ln], (unsigned long long)tm);
+          atomicAdd((unsigned long long*)&s_acc[3 + a][ln], (unsigned long long)tw);
+        }
       }
     }
   }
@@ -196,10 +223,12 @@ __global__ void __launch_bounds__(kThreads) k_p2g(const TankDev* __restrict__ ta
     const int n = node_idx(T, ix, iy, iz);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const long long w = s_acc[3 + a][ln];
+      const long long w = split ? (long long)s_hi[(3 + a) * kBNodes + ln] * (1LL << kSplit) + (long long)s_lo[(3 + a) * kBNodes + ln]
+                                : s_acc[3 + a][ln];
       if (w == 0) continue;
       atomicAdd((unsigned long long*)&T.acc[(size_t)(3 + a) * T.nnodes + n], (unsigned long long)w);
-      const long long m = s_acc[a][ln];
+      const long long m = split ? (long long)s_hi[a * kBNodes + ln] * (1LL << kSplit) + (long long)s_lo[a * kBNodes + ln]
+                                : s_acc[a][ln];
       if (m != 0) atomicAdd((unsigned long long*)&T.acc[(size_t)a * T.nnodes + n], (unsigned long long)m);
     }
   }

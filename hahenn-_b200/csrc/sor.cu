@@ -25,35 +25,8 @@
 
 namespace suiri {
 
-__device__ __forceinline__ void sor_cell(const TankDev& T, int color, int s) {
-  const int hx = T.hx, nx = T.nx, ny = T.ny, nz = T.nz;
-  const int ti = s % hx, row = s / hx;
-  const int j = row % ny, k = row / ny;
-  const int i = 2 * ti + ((j + k + color) & 1);
-  if (i >= nx) return;
-  const size_t own = (size_t)color * T.nhalf + s;
-  const uint32_t code = T.code[own];
-  if (!(code & kCodeActive)) return;
-  const float* __restrict__ po = T.pres + (size_t)(1 - color) * T.nhalf;
-  const float rhs = T.rhs[own];
-  float p = T.pres[own];
-  const int rowb = hx * row;
-  float nb[6];
-  nb[0] = i > 0 ? po[((i - 1) >> 1) + rowb] : 0.f;
-  nb[1] = i + 1 < nx ? po[((i + 1) >> 1) + rowb] : 0.f;
-  nb[2] = j > 0 ? po[ti + rowb - hx] : 0.f;
-  nb[3] = j + 1 < ny ? po[ti + rowb + hx] : 0.f;
-  nb[4] = k > 0 ? po[ti + rowb - hx * ny] : 0.f;
-  nb[5] = k + 1 < nz ? po[ti + rowb + hx * ny] : 0.f;
-  float C[6];
-  if (code & kCodePartial) {
-    const int n = node_idx(T, i, j, k);
-    const float4 f0 = T.frac[n];
-    C[0] = f0.x; C[1] = T.frac[n + 1].x; C[2] = f0.y; C[3] = T.frac[n + T.sx].y; C[4] = f0.z; C[5] = T.frac[n + T.sxy].z;
-  } else {
-#pragma unroll
-    for (int d = 0; d < 6; ++d) C[d] = (code >> d) & 1u ? 1.0f : 0.0f;
-  }
+// p + ω·(((num − rhs)·inv) − p) with the reference's rounding steps (see the file comment)
+__device__ __forceinline__ float sor_update(const float C[6], const float nb[6], float rhs, float p, float omega) {
   float num = __fmul_rn(C[0], nb[0]);
   float den = C[0];
 #pragma unroll
@@ -65,19 +38,106 @@ __device__ __forceinline__ void sor_cell(const TankDev& T, int color, int s) {
   float r = __fsub_rn(num, rhs);
   r = __fmul_rn(r, inv);
   r = __fsub_rn(r, p);
-  r = __fmul_rn(r, T.omega);
-  p = __fadd_rn(p, r);
-  T.pres[own] = p;
+  r = __fmul_rn(r, omega);
+  return __fadd_rn(p, r);
 }
 
+// the six face coefficients of a cut cell: its own x, y, z face fractions and those of the +x, +y, +z
+// neighbours' faces
+__device__ __forceinline__ void cut_coeffs(const TankDev& T, int i, int j, int k, float C[6]) {
+  const int n = node_idx(T, i, j, k);
+  const float4 f0 = T.frac[n];
+  C[0] = f0.x; C[1] = T.frac[n + 1].x; C[2] = f0.y; C[3] = T.frac[n + T.sx].y; C[4] = f0.z; C[5] = T.frac[n + T.sxy].z;
+}
+
+__device__ __forceinline__ void sor_cell(const TankDev& T, int color, int s) {
+  const int hx = T.hx, nx = T.nx, ny = T.ny, nz = T.nz;
+  const int ti = s % hx, row = s / hx;
+  const int j = row % ny, k = row / ny;
+  const int i = 2 * ti + ((j + k + color) & 1);
+  if (i >= nx) return;
+  const size_t own = (size_t)color * T.nhalf + s;
+  const uint32_t code = T.code[own];
+  if (!(code & kCodeActive)) return;
+  const float* __restrict__ po = T.pres + (size_t)(1 - color) * T.nhalf;
+  const float rhs = T.rhs[own];
+  const float p = T.pres[own];
+  const int rowb = hx * row;
+  float nb[6];
+  nb[0] = i > 0 ? po[((i - 1) >> 1) + rowb] : 0.f;
+  nb[1] = i + 1 < nx ? po[((i + 1) >> 1) + rowb] : 0.f;
+  nb[2] = j > 0 ? po[ti + rowb - hx] : 0.f;
+  nb[3] = j + 1 < ny ? po[ti + rowb + hx] : 0.f;
+  nb[4] = k > 0 ? po[ti + rowb - hx * ny] : 0.f;
+  nb[5] = k + 1 < nz ? po[ti + rowb + hx * ny] : 0.f;
+  float C[6];
+  if (code & kCodePartial) {
+    cut_coeffs(T, i, j, k, C);
+  } else {
+#pragma unroll
+    for (int d = 0; d < 6; ++d) C[d] = (code >> d) & 1u ? 1.0f : 0.0f;
+  }
+  T.pres[own] = sor_update(C, nb, rhs, p, T.omega);
+}
+
+// Launched with programmatic stream serialisation (all but the first sweep of a solve): the next sweep's
+// blocks may start as soon as every block of this one has started. Before griddepcontrol.wait a block
+// reads only what no sweep writes (its tank descriptor, the cell's code, rhs and cut-cell fractions, all
+// written by kernels that completed before the first sweep, which is launched without the attribute), so
+// that part overlaps the previous sweep; after the wait, which returns once the previous sweep has
+// completed and its writes are visible, it reads the pressures, one round of loads, and writes its own.
 __global__ void __launch_bounds__(kThreads) k_sor(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx,
                                                   int color, int sweep) {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int t = find_slot(bpfx, ntanks, blockIdx.x);
   const TankDev& T = tanks[t];
-  if (sweep >= T.iters) return;
-  const int s = (blockIdx.x - bpfx[t]) * blockDim.x + threadIdx.x;
-  if (s >= T.nhalf) return;
-  sor_cell(T, color, s);
+  const int hx = T.hx, nx = T.nx, ny = T.ny, nz = T.nz, nhalf = T.nhalf;
+  const bool on = sweep < T.iters;
+  float* const pres = T.pres;
+  const float omega = T.omega;
+  // kSorPer slots per thread, a block's slots contiguous (kThreads apart per thread)
+  int ti[kSorPer], row[kSorPer], jj[kSorPer], kk[kSorPer], ii[kSorPer];
+  uint32_t code[kSorPer];
+  float rhs[kSorPer], C[kSorPer][6];
+#pragma unroll
+  for (int u = 0; u < kSorPer; ++u) {
+    const int s = (blockIdx.x - bpfx[t]) * (kThreads * kSorPer) + u * kThreads + threadIdx.x;
+    ti[u] = s % hx; row[u] = s / hx;
+    jj[u] = row[u] % ny; kk[u] = row[u] / ny;
+    ii[u] = 2 * ti[u] + ((jj[u] + kk[u] + color) & 1);
+    code[u] = 0; rhs[u] = 0.f;
+    if (on && s < nhalf && ii[u] < nx) {
+      code[u] = T.code[(size_t)color * nhalf + s];
+      rhs[u] = T.rhs[(size_t)color * nhalf + s];
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kSorPer; ++u) {
+    if (code[u] & kCodePartial) {
+      cut_coeffs(T, ii[u], jj[u], kk[u], C[u]);
+    } else {
+#pragma unroll
+      for (int d = 0; d < 6; ++d) C[u][d] = (code[u] >> d) & 1u ? 1.0f : 0.0f;
+    }
+  }
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const float* __restrict__ po = pres + (size_t)(1 - color) * nhalf;
+  float nb[kSorPer][6], p[kSorPer];
+#pragma unroll
+  for (int u = 0; u < kSorPer; ++u) {
+    if (!(code[u] & kCodeActive)) continue;
+    const int i = ii[u], j = jj[u], k = kk[u], rowb = hx * row[u];
+    nb[u][0] = i > 0 ? po[((i - 1) >> 1) + rowb] : 0.f;
+    nb[u][1] = i + 1 < nx ? po[((i + 1) >> 1) + rowb] : 0.f;
+    nb[u][2] = j > 0 ? po[ti[u] + rowb - hx] : 0.f;
+    nb[u][3] = j + 1 < ny ? po[ti[u] + rowb + hx] : 0.f;
+    nb[u][4] = k > 0 ? po[ti[u] + rowb - hx * ny] : 0.f;
+    nb[u][5] = k + 1 < nz ? po[ti[u] + rowb + hx * ny] : 0.f;
+    p[u] = pres[(size_t)color * nhalf + ti[u] + rowb];
+  }
+#pragma unroll
+  for (int u = 0; u < kSorPer; ++u)
+    if (code[u] & kCodeActive) pres[(size_t)color * nhalf + ti[u] + hx * row[u]] = sor_update(C[u], nb[u], rhs[u], p[u], omega);
 }
 
 constexpr unsigned kSpinLimit = 1u << 22;
@@ -128,8 +188,186 @@ __global__ void __launch_bounds__(kThreads) k_sor_persist(const TankDev* __restr
   }
 }
 
+// ------------------------------------------------------------------------------------------------
+// Temporal blocking: kTbSweeps colour sweeps per launch. A block owns a kTbX×kTbY×kTbZ tile of cells and
+// stages the tile plus a halo of kTbSweeps cells (clipped at the tank walls) in shared memory: pressure,
+// rhs and a 16-bit code per cell, split by colour like the global arrays. Sweep s (0-based, n sweeps in
+// the launch) updates the cells of its colour within n−1−s cells of the tile: a red-black sweep reads only
+// the other colour, so a cell updated there sees exactly the neighbour values the per-sweep launches would
+// give it, and after the n sweeps the tile itself holds exactly the per-sweep result. The tile is written
+// to the other pressure buffer (halos are read from the input buffer by neighbouring blocks while this one
+// writes), so launches alternate between pres and pres2.
+//
+// Cut cells keep their six coefficients in a shared table (kTbMaxCut entries; beyond that they are read
+// from the face fractions in global memory). The smem code: 0 inactive; 0x4000|open bits for a cell whose
+// faces are all closed or fully open; 0x8000|table index for a cut cell (0x7FFF: not in the table).
+constexpr int kTbRX = kTbX + 2 * kTbSweeps, kTbRY = kTbY + 2 * kTbSweeps, kTbRZ = kTbZ + 2 * kTbSweeps;
+constexpr int kTbHX = kTbRX / 2;
+constexpr int kTbSlots = kTbHX * kTbRY * kTbRZ;     // per colour
+constexpr int kTbMaxCut = 512;
+constexpr int kTbSmem = 2 * kTbSlots * 4 * 2 + 2 * kTbSlots * 2 + kTbMaxCut * 6 * 4;
+static_assert(kTbX % 2 == 0 && kTbSweeps % 2 == 0, "tile and halo keep the region's x origin even");
+static_assert(kTbSlots < 0x7FFF, "table index fits the code");
+
+__global__ void __launch_bounds__(kTbThreads, 2) k_sor_tb(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx,
+                                                          int sweep0, int nsweeps, int dir) {
+  extern __shared__ __align__(16) unsigned char tb_smem[];
+  float* sp = reinterpret_cast<float*>(tb_smem);               // [2][kTbSlots] pressure
+  float* srhs = sp + 2 * kTbSlots;                             // [2][kTbSlots]
+  uint16_t* scode = reinterpret_cast<uint16_t*>(srhs + 2 * kTbSlots);
+  float* stab = reinterpret_cast<float*>(scode + 2 * kTbSlots);  // [kTbMaxCut][6]
+  __shared__ int s_ncut;
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  const int t = find_slot(bpfx, ntanks, blockIdx.x);
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const TankDev& T = tanks[t];
+  const int nx = T.nx, ny = T.ny, nz = T.nz;
+  const int lb = blockIdx.x - bpfx[t];
+  const int tnx = (nx + kTbX - 1) / kTbX, tny = (ny + kTbY - 1) / kTbY;
+  const int x0 = (lb % tnx) * kTbX, y0 = ((lb / tnx) % tny) * kTbY, z0 = (lb / (tnx * tny)) * kTbZ;
+  const int rx0 = max(x0 - kTbSweeps, 0), ry0 = max(y0 - kTbSweeps, 0), rz0 = max(z0 - kTbSweeps, 0);
+  const int rx1 = min(x0 + kTbX + kTbSweeps, nx), ry1 = min(y0 + kTbY + kTbSweeps, ny), rz1 = min(z0 + kTbZ + kTbSweeps, nz);
+  const float* __restrict__ pin = dir ? T.pres2 : T.pres;
+  float* __restrict__ pout = dir ? T.pres : T.pres2;
+  const size_t nh = T.nhalf;
+  if (threadIdx.x == 0) s_ncut = 0;
+  __syncthreads();
+  for (int q = threadIdx.x; q < 2 * kTbSlots; q += kTbThreads) {
+    const int c = q >= kTbSlots;
+    const int ls = q - c * kTbSlots;
+    const int lti = ls % kTbHX, lrow = ls / kTbHX;
+    const int j = ry0 + lrow % kTbRY, k = rz0 + lrow / kTbRY;
+    const int i = rx0 + 2 * lti + ((j + k + c) & 1);
+    float p = 0.f, r = 0.f;
+    uint16_t cd = 0;
+    if (i < rx1 && j < ry1 && k < rz1) {
+      const size_t g = c * nh + (size_t)(i >> 1) + (size_t)T.hx * (j + (size_t)ny * k);
+      p = pin[g];
+      const uint32_t code = T.code[g];
+      if (code & kCodeActive) {
+        r = T.rhs[g];
+        if (code & kCodePartial) {
+          const int e = atomicAdd(&s_ncut, 1);
+          if (e < kTbMaxCut) {
+            float C[6];
+            cut_coeffs(T, i, j, k, C);
+#pragma unroll
+            for (int d = 0; d < 6; ++d) stab[6 * e + d] = C[d];
+            cd = (uint16_t)(0x8000 | e);
+          } else {
+            cd = 0xFFFF;
+          }
+        } else {
+          cd = (uint16_t)(0x4000 | (code & 0x3F));
+        }
+      }
+    }
+    sp[q] = p;
+    srhs[q] = r;
+    scode[q] = cd;
+  }
+  __syncthreads();
+  for (int s = 0; s < nsweeps; ++s) {
+    const int sw = sweep0 + s;
+    if (sw < 2 * T.iters) {
+      const int c = sw & 1, e = nsweeps - 1 - s;
+      const int bx0 = max(x0 - e, rx0), bx1 = min(x0 + kTbX + e, rx1);
+      const int by0 = max(y0 - e, ry0), by1 = min(y0 + kTbY + e, ry1);
+      const int bz0 = max(z0 - e, rz0), bz1 = min(z0 + kTbZ + e, rz1);
+      const int sx0 = (bx0 - rx0) >> 1, wsx = ((bx1 - rx0 + 1) >> 1) - sx0, wy = by1 - by0;
+      const int nq = wsx * wy * (bz1 - bz0);
+      const float* so = sp + (1 - c) * kTbSlots;
+      for (int q = threadIdx.x; q < nq; q += kTbThreads) {
+        const int lti = sx0 + q % wsx, rr = q / wsx;
+        const int j = by0 + rr % wy, k = bz0 + rr / wy;
+        const int i = rx0 + 2 * lti + ((j + k + c) & 1);
+        if (i < bx0 || i >= bx1) continue;
+        const int rowb = kTbHX * ((j - ry0) + kTbRY * (k - rz0));
+        const int own = c * kTbSlots + lti + rowb;
+        const unsigned cd = scode[own];
+        if (!cd) continue;
+        const int li = i - rx0;
+        float nb[6];
+        nb[0] = i > 0 ? so[((li - 1) >> 1) + rowb] : 0.f;
+        nb[1] = i + 1 < nx ? so[((li + 1) >> 1) + rowb] : 0.f;
+        nb[2] = j > 0 ? so[lti + rowb - kTbHX] : 0.f;
+        nb[3] = j + 1 < ny ? so[lti + rowb + kTbHX] : 0.f;
+        nb[4] = k > 0 ? so[lti + rowb - kTbHX * kTbRY] : 0.f;
+        nb[5] = k + 1 < nz ? so[lti + rowb + kTbHX * kTbRY] : 0.f;
+        float C[6];
+        if (cd & 0x8000) {
+          const unsigned x = cd & 0x7FFF;
+          if (x < kTbMaxCut) {
+#pragma unroll
+            for (int d = 0; d < 6; ++d) C[d] = stab[6 * x + d];
+          } else {
+            cut_coeffs(T, i, j, k, C);
+          }
+        } else {
+#pragma unroll
+          for (int d = 0; d < 6; ++d) C[d] = (cd >> d) & 1u ? 1.0f : 0.0f;
+        }
+        sp[own] = sor_update(C, nb, srhs[own], sp[own], T.omega);
+      }
+    }
+    __syncthreads();
+  }
+  constexpr int kTileSlots = (kTbX / 2) * kTbY * kTbZ;
+  for (int q = threadIdx.x; q < 2 * kTileSlots; q += kTbThreads) {
+    const int c = q >= kTileSlots;
+    const int r = q - c * kTileSlots;
+    const int mi = r % (kTbX / 2), rr = r / (kTbX / 2);
+    const int j = y0 + rr % kTbY, k = z0 + rr / kTbY;
+    const int i = x0 + 2 * mi + ((j + k + c) & 1);
+    if (i >= nx || j >= ny || k >= nz) continue;
+    const int ls = c * kTbSlots + ((i - rx0) >> 1) + kTbHX * ((j - ry0) + kTbRY * (k - rz0));
+    pout[c * nh + (size_t)(i >> 1) + (size_t)T.hx * (j + (size_t)ny * k)] = sp[ls];
+  }
+}
+
+// pres ← pres2 (after an odd number of temporal-blocked launches)
+__global__ void __launch_bounds__(kThreads) k_sor_copy(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx) {
+  const int t = find_slot(bpfx, ntanks, blockIdx.x);
+  const TankDev& T = tanks[t];
+  const int s = (blockIdx.x - bpfx[t]) * blockDim.x + threadIdx.x;
+  if (s >= T.nhalf) return;
+  T.pres[s] = T.pres2[s];
+  T.pres[T.nhalf + s] = T.pres2[T.nhalf + s];
+}
+
+cudaError_t sor_tb_prepare() {
+  return cudaFuncSetAttribute(k_sor_tb, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmem);
+}
+
+void launch_sor_tb(const LaunchCtx& L, int sweep0, int nsweeps, int dir) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(L.nblocks[kFamTiles]);
+  cfg.blockDim = dim3(kTbThreads);
+  cfg.dynamicSmemBytes = kTbSmem;
+  cfg.stream = L.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_sor_tb, L.tanks, L.ntanks, (const int*)L.bpfx[kFamTiles], sweep0, nsweeps, dir);
+}
+
+void launch_sor_copy(const LaunchCtx& L) {
+  k_sor_copy<<<L.nblocks[kFamHalf], kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.bpfx[kFamHalf]);
+}
+
 void launch_sor_sweep(const LaunchCtx& L, int color, int sweep) {
-  k_sor<<<L.nblocks[kFamHalf], kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.bpfx[kFamHalf], color, sweep);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(L.nblocks[kFamSor]);
+  cfg.blockDim = dim3(kThreads);
+  cfg.stream = L.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = (color | sweep) ? 1 : 0;     // the first sweep waits for the grid pass in full
+  cudaLaunchKernelEx(&cfg, k_sor, L.tanks, L.ntanks, (const int*)L.bpfx[kFamSor], color, sweep);
 }
 
 int sor_persist_max_blocks(int device) {

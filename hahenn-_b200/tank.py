@@ -190,8 +190,9 @@ class Tank:
     def profile(self, on=True):
         self._c(N.lib().suiri_profile(self._h, 1 if on else 0))
 
-    def tune(self, blocks_per_sm=4, sor_persistent=False):
-        self._c(N.lib().suiri_tune(self._h, int(blocks_per_sm), 1 if sor_persistent else 0))
+    def tune(self, blocks_per_sm=4, sor_mode=0):
+        """sor_mode: 0 one launch per colour sweep, 1 one cooperative launch, 2 temporal blocking."""
+        self._c(N.lib().suiri_tune(self._h, int(blocks_per_sm), int(sor_mode)))
 
     def sor_phase_ms(self):
         ms = C.c_double()
@@ -288,8 +289,8 @@ class Batch:
     def sync(self):
         N.check(N.lib().suiri_batch_sync(self._h))
 
-    def tune(self, blocks_per_sm=4, sor_persistent=False):
-        N.check(N.lib().suiri_batch_tune(self._h, int(blocks_per_sm), 1 if sor_persistent else 0))
+    def tune(self, blocks_per_sm=4, sor_mode=0):
+        N.check(N.lib().suiri_batch_tune(self._h, int(blocks_per_sm), int(sor_mode)))
 
     def profile(self, on=True):
         N.check(N.lib().suiri_batch_profile(self._h, 1 if on else 0))

@@ -60,12 +60,14 @@ def test_dam16_two_substeps(pkg):
     gpu.close()
 
 
-def test_sor_bit_exact_with_reference_operation_order(pkg):
+@pytest.mark.parametrize('sor_mode', [0, 2])
+def test_sor_bit_exact_with_reference_operation_order(pkg, sor_mode):
     """Given the GPU's own float32 operands, the reference's float32 SOR loop reproduces its pressure bit for
-    bit; the FP64 residual of the solve is stated."""
+    bit, for one launch per sweep and for temporal blocking; the FP64 residual of the solve is stated."""
     d = load('dam16')
     nx, ny, nz, h = int(d['nx']), int(d['ny']), int(d['nz']), float(d['h'])
     gpu = gpu_from(pkg, nx, ny, nz, h, flip=0.95, omega=1.7, iters=30)
+    gpu.tune(4, sor_mode)
     gpu.add_particles(f32(d['pos0']), f32(d['vel0']))
     gpu.substep(1 / 240)
     g = grid_fields(pkg, gpu)
@@ -267,26 +269,76 @@ def test_batch_equals_solo_bit_for_bit(pkg):
         t.close()
 
 
-def test_persistent_solve_equals_per_sweep_launches(pkg):
-    """The whole-solve cooperative launch relaxes the same colours in the same order: identical pressures
-    and particles, bit for bit, and no barrier error."""
+def _run_form(pkg, w, mode, iters, steps=3):
+    t = pkg.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=0.95, omega=1.8, iters=iters, whitewater=True,
+                 ripple=None, capacity=len(w['pos']) * 2)
+    t.set_objects(w['objects'])
+    t.add_particles(w['pos'])
+    t.tune(4, mode)
+    for _ in range(steps):
+        t.substep(1 / 240)
+    assert t.stats()['errors'] == 0
+    pos, vel, air, ids = t.particles()
+    o = np.argsort(ids)
+    out = (t.grid(pkg.native.FIELD_PRES), pos[o], vel[o])
+    t.close()
+    return out
+
+
+@pytest.mark.parametrize('mode', [1, 2])
+def test_solve_forms_equal_per_sweep_launches(pkg, mode):
+    """The cooperative whole-solve launch (1) and the temporal-blocked launches (2) relax the same colours
+    in the same order as one launch per sweep (0): identical pressures and particles, bit for bit."""
     w = pkg.workloads.obstacles_inflow(scale=4)
-    out = []
-    for persistent in (False, True):
-        t = pkg.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=0.95, omega=1.8, iters=40, whitewater=True,
-                     ripple=None, capacity=len(w['pos']) * 2)
-        t.set_objects(w['objects'])
-        t.add_particles(w['pos'])
-        t.tune(4, persistent)
-        for _ in range(3):
-            t.substep(1 / 240)
-        assert t.stats()['errors'] == 0
-        pos, vel, air, ids = t.particles()
-        o = np.argsort(ids)
-        out.append((t.grid(pkg.native.FIELD_PRES), pos[o], vel[o]))
-        t.close()
-    for a, b in zip(*out):
+    for a, b in zip(_run_form(pkg, w, 0, 40), _run_form(pkg, w, mode, 40)):
         np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize('iters', [6, 7, 1])
+def test_temporal_blocking_edges(pkg, iters):
+    """Temporal blocking on a grid that is no multiple of the tile (odd x), with an odd number of launches
+    (6 iterations: 3 launches, the result copied back), a short last launch (7: 4+4+4+2 sweeps) and a
+    single launch of two sweeps (1)."""
+    w = pkg.workloads.random_tank(5, axes=(21, 37, 19))
+    for a, b in zip(_run_form(pkg, w, 0, iters), _run_form(pkg, w, 2, iters)):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_temporal_blocking_batch_uneven_iterations(pkg):
+    """In a batch the tile launches run to the largest iteration count; tanks with fewer iterations stop
+    relaxing but keep being carried between the two pressure buffers: every tank equals its solo run."""
+    specs = [(pkg.workloads.random_tank(s, axes=(16, 24, 40)), it) for s, it in ((11, 5), (12, 12), (13, 9))]
+
+    def make(mode):
+        out = []
+        for w, it in specs:
+            t = pkg.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=0.95, omega=1.7, iters=it,
+                         whitewater=True, ripple=None, capacity=len(w['pos']) * 2)
+            t.set_objects(w['objects'])
+            t.add_particles(w['pos'])
+            if mode is not None:
+                t.tune(4, mode)
+            out.append(t)
+        return out
+
+    solo, batched = make(0), make(None)
+    b = pkg.Batch(batched)
+    b.tune(4, 2)
+    for _ in range(4):
+        for t in solo:
+            t.substep(1 / 240)
+        b.substep(1 / 240)
+    b.sync()
+    for a, c in zip(solo, batched):
+        np.testing.assert_array_equal(a.grid(pkg.native.FIELD_PRES), c.grid(pkg.native.FIELD_PRES))
+        pa, va, aa, ia = a.particles()
+        pc, vc, ac, ic = c.particles()
+        oa, oc = np.argsort(ia), np.argsort(ic)
+        np.testing.assert_array_equal(pa[oa], pc[oc])
+        np.testing.assert_array_equal(va[oa], vc[oc])
+    b.close()
+    for t in solo + batched:
+        t.close()
 
 
 def test_snapshot_restore(pkg):
