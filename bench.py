@@ -53,14 +53,40 @@ def sor_traffic():
 
 
 class Clocks:
-    """nvidia-smi samples during the timed region."""
+    """SM clock and throttle reasons sampled every 5 ms during the timed region (NVML reads only; the
+    nvidia-smi query loop is the fallback)."""
     Q = 'clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,' \
         'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap'
+    BITS = {'sw_power_cap': 0x4, 'hw_slowdown': 0x8, 'sw_thermal_slowdown': 0x20, 'hw_thermal_slowdown': 0x40}
 
     def __init__(self, device):
         self.device, self.rows, self.proc = device, [], None
+        self.stop_flag = threading.Event()
+        self.nv = None
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.device)
+            bus = f'{int(pr.pci_domain_id):08X}:{int(pr.pci_bus_id):02X}:{int(pr.pci_device_id):02X}.0'
+        except Exception:
+            bus = None
+        if bus is not None:      # the PCI id as NVML spells it ("00000000:1B:00.0"); a non-string here would crash NVML
+            try:
+                return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+            except Exception:
+                pass
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
 
     def start(self):
+        try:
+            self.nv = self._handle()
+            threading.Thread(target=self._poll, daemon=True).start()
+            return
+        except Exception:
+            self.nv = None
         try:
             self.proc = subprocess.Popen(['nvidia-smi', f'--query-gpu={self.Q}', '--format=csv,noheader,nounits',
                                           '-lms', '200', '-i', str(self.device)], stdout=subprocess.PIPE,
@@ -69,23 +95,40 @@ class Clocks:
         except Exception:
             self.proc = None
 
+    def _poll(self):
+        nv, h = self.nv
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop_flag.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            except Exception:
+                break
+            act = ['Active' if r & self.BITS[k] else 'Not Active'
+                   for k in ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')]
+            self.rows.append([str(sm), str(mx)] + act)
+            time.sleep(0.005)
+
     def _read(self):
         for line in self.proc.stdout:
             self.rows.append([x.strip() for x in line.split(',')])
 
     def stop(self):
+        self.stop_flag.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
-        sm = [float(r[0]) for r in self.rows if r and r[0].replace('.', '').isdigit()]
-        mx = [float(r[1]) for r in self.rows if len(r) > 1 and r[1].replace('.', '').isdigit()]
+        time.sleep(0.02)
+        rows = list(self.rows)
+        sm = [float(r[0]) for r in rows if r and r[0].replace('.', '').isdigit()]
+        mx = [float(r[1]) for r in rows if len(r) > 1 and r[1].replace('.', '').isdigit()]
         names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 2 + i and r[2 + i] == 'Active'})
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 2 + i and r[2 + i] == 'Active'})
         return dict(sm_mhz=float(np.median(sm)) if sm else None, sm_max_mhz=max(mx) if mx else None,
-                    reasons=reasons, samples=len(sm))
+                    reasons=reasons, samples=len(sm), source='nvml' if self.nv else 'nvidia-smi')
 
 
 def make_tank(P, w, device, host_inflow=False):
@@ -274,7 +317,7 @@ def run_serve(args, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--steps', type=int, default=200)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='suiri', choices=['suiri', 'reference'])
     ap.add_argument('--workload', default='obstacles_inflow', choices=['obstacles_inflow', 'batch', 'serve', 'full_scene'])
@@ -283,6 +326,8 @@ def main():
     ap.add_argument('--rate', type=float, default=200.0)
     ap.add_argument('--duration', type=float, default=60.0)
     ap.add_argument('--req-steps', type=int, default=120)
+    ap.add_argument('--ncu-steps', type=int, default=0,
+                    help='profiler run: 3 warm-up and N more sub-steps of the workload, no timing, no JSON line')
     args = ap.parse_args()
     rank, world = int(os.environ.get('RANK', 0)), int(os.environ.get('WORLD_SIZE', 1))
     local = int(os.environ.get('LOCAL_RANK', 0))
@@ -294,6 +339,8 @@ def main():
         return run_serve(args, local)
     if args.workload == 'full_scene':
         return run_full_scene(args, local)
+    if args.ncu_steps:
+        return run_for_profiler(args, local)
     import torch
     import torch.distributed as dist
     if world > 1:
@@ -405,6 +452,19 @@ def main():
     tank.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_for_profiler(args, local):
+    """The obstacles-and-inflow tank stepped 3 + N times and synchronised: a fixed launch sequence for ncu
+    (per sub-step: 13 kernels + 2 per SOR iteration)."""
+    P = pkg()
+    w = P.workloads.obstacles_inflow()
+    t = make_tank(P, w, local)
+    for _ in range(3 + args.ncu_steps):
+        t.substep(w['params']['dt'])
+    t.sync()
+    print('sub-steps', 3 + args.ncu_steps, 'particles', t.stats()['count'])
+    t.close()
 
 
 if __name__ == '__main__':

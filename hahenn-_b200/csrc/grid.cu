@@ -244,28 +244,41 @@ __global__ void __launch_bounds__(kThreads) k_grid_nodes(const TankDev* __restri
   const int n = (blockIdx.x - bpfx[t]) * blockDim.x + threadIdx.x;
   if (n >= T.nnodes) return;
   const size_t nn = T.nnodes;
+  // every load first (one round of memory latency), then the arithmetic, then the stores
+  long long* __restrict__ acc = T.acc;
+  const double* __restrict__ fracd = T.fracd;
+  long long W[3], M[3];
+  double f[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    W[a] = acc[(3 + a) * nn + n];
+    M[a] = acc[a * nn + n];
+    f[a] = fracd[a * nn + n];
+  }
+  const float4 s4 = T.svel[n];
   double v[3];
   int mask = 0;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const long long W = T.acc[(3 + a) * nn + n];
-    const long long M = T.acc[a * nn + n];
-    T.acc[(3 + a) * nn + n] = 0;
-    T.acc[a * nn + n] = 0;
-    const bool m = (double)W * kFixInv > 4e-6;
-    v[a] = m ? (double)M / (double)W : 0.0;
+    const bool m = (double)W[a] * kFixInv > 4e-6;
+    v[a] = m ? (double)M[a] / (double)W[a] : 0.0;
     mask |= m ? (1 << a) : 0;
   }
-  T.velold[n] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)mask);
+  const float4 vo = make_float4((float)v[0], (float)v[1], (float)v[2], (float)mask);
   v[1] -= T.g * T.dt;
-  const float4 s4 = T.svel[n];
   const double s[3] = {(double)s4.x, (double)s4.y, (double)s4.z};
+  double fl[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const double f = T.fracd[a * nn + n];
-    if (f <= 0.0) v[a] = s[a];
-    T.flux[a * nn + n] = f * v[a] + (1 - f) * s[a];
+    if (f[a] <= 0.0) v[a] = s[a];
+    fl[a] = f[a] * v[a] + (1 - f[a]) * s[a];
   }
+#pragma unroll
+  for (int a = 0; a < 6; ++a) acc[a * nn + n] = 0;
+  double* __restrict__ flux = T.flux;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) flux[a * nn + n] = fl[a];
+  T.velold[n] = vo;
   T.vel[n] = make_float4((float)v[0], (float)v[1], (float)v[2], 0.f);
 }
 
