@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ ta
     }
     double x[3] = {x0[0] + v[0] * dt, x0[1] + v[1] * dt, x0[2] + v[2] * dt};
     const double rc = 0.32 * h;
-    if (T.has_obst) {
+    if (maybe_within(T, x[0], x[1], x[2], rc)) {
       const double d = tank_sdf(T, x[0], x[1], x[2]);
       if (d < rc) {
         double nx, ny, nz;
@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(kThreads) k_whitewater(const TankDev* __restri
       }
       const double x0[3] = {x[0], x[1], x[2]};
       x[0] = x0[0] + v[0] * dt; x[1] = x0[1] + v[1] * dt; x[2] = x0[2] + v[2] * dt;
-      if (T.has_obst) {
+      if (maybe_within(T, x[0], x[1], x[2], 0.0)) {
         const double d = tank_sdf(T, x[0], x[1], x[2]);
         if (d < 0) {
           double nx, ny, nz;

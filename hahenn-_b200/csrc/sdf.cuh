@@ -107,6 +107,10 @@ __device__ inline bool in_drain(const Obj* __restrict__ objs, int n, double px, 
   for (int i = 0; i < n; ++i) {
     const Obj& o = objs[i];
     if (o.flag != 2) continue;
+    // a drain's cylinder (radius r, half height 0.012) lies within r + 0.0121 of its centre and its bound is
+    // r + 0.02: a point outside the bound sphere is not in it
+    const double ex = px - o.pos[0], ey = py - o.pos[1], ez = pz - o.pos[2];
+    if (ex * ex + ey * ey + ez * ez > o.bound * o.bound) continue;
     double qx, qy, qz;
     to_local(o, px, py, pz, qx, qy, qz);
     if (len2(qx, qz) < o.dims[0] && fabs(qy) < o.dims[1]) return true;
@@ -142,6 +146,25 @@ __device__ __forceinline__ double tank_sdf(const TankDev& T, double px, double p
   if (!T.has_obst) return kBig;
   if (T.sdf_mode == kSdfLattice) return lattice_sdf(T, px, py, pz);
   return scene_sdf(T.objs, T.nobj, px, py, pz, true);
+}
+
+// False only where the scene distance is certainly at least `r`: in analytic mode, when the point lies
+// beyond r (+1e-6, far above rounding) of every obstacle's bounding sphere. Every shape but the gutter
+// (type 7) lies inside its bounding sphere and its distance function is at least the distance to the shape
+// (exact, or the max of exact ones), so then every term of the scene minimum, culled or not, is ≥ r. Lattice
+// mode, or any gutter, always answers true.
+__device__ __forceinline__ bool maybe_within(const TankDev& T, double px, double py, double pz, double r) {
+  if (!T.has_obst) return false;
+  if (T.sdf_mode != kSdfAnalytic) return true;
+  for (int i = 0; i < T.nobj; ++i) {
+    const Obj& o = T.objs[i];
+    if (o.flag != 1) continue;
+    if (o.type == 7) return true;
+    const double ex = px - o.pos[0], ey = py - o.pos[1], ez = pz - o.pos[2];
+    const double lim = r + o.bound + 1e-6;
+    if (ex * ex + ey * ey + ez * ez < lim * lim) return true;
+  }
+  return false;
 }
 
 // central differences, e = 6e-4 (solver.py:142-151, 30-wgsl-sim.js:88-95)
