@@ -86,7 +86,7 @@ __device__ __forceinline__ void sor_cell(const TankDev& T, int color, int s) {
 // written by kernels that completed before the first sweep, which is launched without the attribute), so
 // that part overlaps the previous sweep; after the wait, which returns once the previous sweep has
 // completed and its writes are visible, it reads the pressures, one round of loads, and writes its own.
-__global__ void __launch_bounds__(kThreads) k_sor(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx,
+__global__ void __launch_bounds__(kSorThreads) k_sor(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx,
                                                   int color, int sweep) {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int t = find_slot(bpfx, ntanks, blockIdx.x);
@@ -95,13 +95,13 @@ __global__ void __launch_bounds__(kThreads) k_sor(const TankDev* __restrict__ ta
   const bool on = sweep < T.iters;
   float* const pres = T.pres;
   const float omega = T.omega;
-  // kSorPer slots per thread, a block's slots contiguous (kThreads apart per thread)
+  // kSorPer slots per thread, a block's slots contiguous (kSorThreads apart per thread)
   int ti[kSorPer], row[kSorPer], jj[kSorPer], kk[kSorPer], ii[kSorPer];
   uint32_t code[kSorPer];
   float rhs[kSorPer], C[kSorPer][6];
 #pragma unroll
   for (int u = 0; u < kSorPer; ++u) {
-    const int s = (blockIdx.x - bpfx[t]) * (kThreads * kSorPer) + u * kThreads + threadIdx.x;
+    const int s = (blockIdx.x - bpfx[t]) * (kSorThreads * kSorPer) + u * kSorThreads + threadIdx.x;
     ti[u] = s % hx; row[u] = s / hx;
     jj[u] = row[u] % ny; kk[u] = row[u] / ny;
     ii[u] = 2 * ti[u] + ((jj[u] + kk[u] + color) & 1);
@@ -360,7 +360,7 @@ void launch_sor_copy(const LaunchCtx& L) {
 void launch_sor_sweep(const LaunchCtx& L, int color, int sweep) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(L.nblocks[kFamSor]);
-  cfg.blockDim = dim3(kThreads);
+  cfg.blockDim = dim3(kSorThreads);
   cfg.stream = L.stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
