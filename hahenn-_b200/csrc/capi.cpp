@@ -205,6 +205,8 @@ TankConfig make_config(const suiri_params& p, const char* scene_json, Scene& sc)
     if (!(p.ripple_sigma >= 0) || !(p.ripple_rho > 0) || !(p.ripple_depth >= 0))
       throw Error(SUIRI_ERR_INVALID, "ripple sigma >= 0, rho > 0, depth >= 0");
     c.ripple_sigma = p.ripple_sigma; c.ripple_rho = p.ripple_rho; c.ripple_depth = p.ripple_depth;
+    if (p.advect != 0 && p.advect != 1) throw Error(SUIRI_ERR_INVALID, "advect is 0 (Euler) or 1 (RK2)");
+    c.advect = p.advect;
     if (!(c.omega > 0 && c.omega < 2)) throw Error(SUIRI_ERR_INVALID, "omega must be in (0, 2)");
     if (c.cap > (1LL << 30)) throw Error(SUIRI_ERR_INVALID, "capacity above 2^30 particles");
     return c;

@@ -83,6 +83,7 @@ struct TankDev {
   double vp, drop_mass;     // particle volume (h/2)³ and mass 998·(h/2)³ (host libm pow, as the reference)
   float omega;
   int iters, whitewater, nobj, sdf_mode, has_obst, moving;
+  int advect;               // 0 explicit Euler, 1 RK2 midpoint through the grid velocity
   int cap, emit_cap, ww_cap;
   int rx, rz;               // ripple vertices (rx+1)×(rz+1); 0 = no ripple layer
   // particles: A live, E emitted, B sorted; pos.w = flags (bit0 airborne, bit1 dead), vel.w = id bits

@@ -267,6 +267,7 @@ Tank::Tank(const TankConfig& c) : cfg(c) {
   D.iters = cfg.iters; D.whitewater = cfg.whitewater;
   D.sdf_mode = cfg.sdf_mode;
   D.seed = cfg.seed;
+  D.advect = cfg.advect;
   D.cap = (int)cfg.cap;
   emit_cap = cfg.cap;
   D.emit_cap = (int)emit_cap;

@@ -42,6 +42,7 @@ struct TankConfig {
   int sdf_mode = kSdfAnalytic, device = 0;
   uint32_t seed = 1;
   double ripple_sigma = 0.0728, ripple_rho = 998.0, ripple_depth = 0.0;
+  int advect = 0;                 // 0 explicit Euler (the reference), 1 RK2 midpoint through the grid velocity
   cudaStream_t stream = nullptr;  // use this stream instead of creating one (not owned)
 };
 

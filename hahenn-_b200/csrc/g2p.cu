@@ -176,17 +176,34 @@ __global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ ta
     double v[3] = {vold[0], vold[1], vold[2]};
     const int c0[3] = {(int)floor(g[0]), (int)floor(g[1]), (int)floor(g[2])};
     int n0 = 0;
+    double u0[3];      // interpolated grid velocity at x0 (RK2)
     if (ing) {
       n0 = count_at(T, c0[0], c0[1], c0[2]);
       for (int a = 0; a < 3; ++a) {
         double pic, flip;
         transfer(T, g[0], g[1], g[2], a, vold[a], pic, flip);
         v[a] = pic + T.flip * (flip - pic);
+        u0[a] = pic;
       }
     } else {
       v[1] -= T.g * dt;
     }
     double x[3] = {x0[0] + v[0] * dt, x0[1] + v[1] * dt, x0[2] + v[2] * dt};
+    if (T.advect && ing) {
+      // midpoint rule through the grid velocity (no reference counterpart): xm = x0 + u0·dt/2, x = x0 +
+      // u(xm)·dt; u falls back to u0 where no face took weight, Euler if the midpoint leaves the grid
+      const double hd = 0.5 * dt;
+      const double xm[3] = {x0[0] + u0[0] * hd, x0[1] + u0[1] * hd, x0[2] + u0[2] * hd};
+      double gm[3];
+      grid_pos(T, xm[0], xm[1], xm[2], gm[0], gm[1], gm[2]);
+      if (in_grid(T, gm[0], gm[1], gm[2])) {
+        for (int a = 0; a < 3; ++a) {
+          double pic, flip;
+          transfer(T, gm[0], gm[1], gm[2], a, u0[a], pic, flip);
+          x[a] = x0[a] + pic * dt;
+        }
+      }
+    }
     const double rc = 0.32 * h;
     if (maybe_within(T, x[0], x[1], x[2], rc)) {
       const double d = tank_sdf(T, x[0], x[1], x[2]);

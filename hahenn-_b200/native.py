@@ -25,7 +25,7 @@ class Params(C.Structure):
                 ('whitewater', C.c_int32), ('capacity', C.c_int64), ('ww_capacity', C.c_int64),
                 ('ripple_rx', C.c_int32), ('ripple_rz', C.c_int32), ('wmap', C.c_int32), ('sdf_mode', C.c_int32),
                 ('device', C.c_int32), ('seed', C.c_uint32), ('ripple_sigma', C.c_double), ('ripple_rho', C.c_double),
-                ('ripple_depth', C.c_double)]
+                ('ripple_depth', C.c_double), ('advect', C.c_int32)]
 
 
 class Stats(C.Structure):

@@ -25,7 +25,7 @@ class Tank:
     def __init__(self, scene=None, *, nx=0, ny=0, nz=0, h=0.0, quality='standard', clamp_tank=True,
                  extra_height=0.0, flip=0.96, omega=1.6, iters=0, gravity=9.81, friction=0.03, ppc=8.0, drift=6.0,
                  ww_rate=7.0, whitewater=True, capacity=0, ww_capacity=0, ripple=(0, 0), wmap=0, sdf_mode='analytic',
-                 device=0, seed=1, ripple_sigma=0.0728, ripple_rho=998.0, ripple_depth=0.0):
+                 device=0, seed=1, ripple_sigma=0.0728, ripple_rho=998.0, ripple_depth=0.0, advect='euler'):
         L = N.lib()
         p = N.Params()
         N.check(L.suiri_params_default(C.byref(p)))
@@ -45,6 +45,7 @@ class Tank:
         p.sdf_mode = {'analytic': 0, 'lattice': 1}[sdf_mode]
         p.device, p.seed = int(device), int(seed)
         p.ripple_sigma, p.ripple_rho, p.ripple_depth = float(ripple_sigma), float(ripple_rho), float(ripple_depth)
+        p.advect = {'euler': 0, 'rk2': 1}[advect]
         if scene is not None and not isinstance(scene, (str, bytes)):
             scene = json.dumps(scene)
         h_ = C.c_void_p()

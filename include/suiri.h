@@ -67,6 +67,10 @@ typedef struct suiri_params {
   double ripple_sigma;     /* surface tension σ [N/m] (0.0728) */
   double ripple_rho;       /* density ρ [kg/m³] (998) */
   double ripple_depth;     /* d [m]; 0: mean depth from the liquid volume each frame (solver.py:726) */
+  /* particle advection: 0 explicit Euler x0 + v·dt with the blended velocity, as the reference
+     (solver.py:545-550, 31-wgsl-sim2.js:168); 1 second-order midpoint (RK2) through the interpolated grid
+     velocity u for in-grid particles, x0 + u(x0 + u(x0)·dt/2)·dt (not in the reference) */
+  int32_t advect;
 } suiri_params;
 
 typedef struct suiri_stats {

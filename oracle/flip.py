@@ -31,7 +31,7 @@ OFF = (np.array([0.0, 0.5, 0.5]), np.array([0.5, 0.0, 0.5]), np.array([0.5, 0.5,
 class Tank:
     def __init__(self, nx, ny, nz, h, *, origin=None, extra_height=0.0, flip=0.96, omega=1.6, iters=40,
                  g=9.81, ppc=8.0, drift=6.0, friction=0.03, ww_rate=7.0, whitewater=True, ww_cap=140000,
-                 ripple=(128, 128), wmap=256, seed=1, rng_mode='numpy', sdf_mode='lattice'):
+                 ripple=(128, 128), wmap=256, seed=1, rng_mode='numpy', sdf_mode='lattice', advect='euler'):
         self.nx, self.ny, self.nz, self.h = int(nx), int(ny), int(nz), float(h)
         h = self.h
         self.origin = np.array([-self.nx * h / 2, 0.0, -self.nz * h / 2]) if origin is None else np.array(origin, float)
@@ -45,6 +45,9 @@ class Tank:
         self.radius = 0.5 * h * 1.05
         self.rng = np.random.default_rng(seed)
         self.rng_mode, self.sdf_mode = rng_mode, sdf_mode
+        if advect not in ('euler', 'rk2'):
+            raise ValueError('advect is euler or rk2')
+        self.advect = advect
         self.time, self.frame, self.vmax, self.impacts = 0.0, 0, 1.0, 0
         self.pos = np.zeros((0, 3)); self.vel = np.zeros((0, 3)); self.air = np.zeros(0)
         self.pid = np.zeros(0, np.int64)
@@ -436,7 +439,13 @@ class Tank:
     # ------------------------------------------------------------------ grid -> particles
     def g2p(self, dt):
         """FLIP/PIC blend, explicit Euler advection, obstacle collision with friction, tank walls,
-        drains, sub-grid drops and whitewater spawning (``solver.py:527-630``, ``31-wgsl-sim2.js:149-251``)."""
+        drains, sub-grid drops and whitewater spawning (``solver.py:527-630``, ``31-wgsl-sim2.js:149-251``).
+
+        ``advect='rk2'`` is not in the reference: in-grid particles move by the midpoint rule through the
+        interpolated grid velocity u (the PIC transfer, which falls back to the particle's blended velocity
+        where no face took weight): u0 = u(x0), xm = x0 + u0·(dt/2), x = x0 + u(xm)·dt, with u(xm) falling
+        back to u0; a particle whose midpoint leaves the grid, and every particle outside it, moves by
+        explicit Euler with its blended velocity. The stored velocity is the blended one either way."""
         h = self.h
         N = len(self.pos)
         self.spawned = 0
@@ -446,15 +455,29 @@ class Tank:
         v = self.vel.copy()
         g = self.grid_pos(x0)
         ing = self.in_grid(g)
+        u0 = None
         if ing.any():
             gi = g[ing]; vi = v[ing]
             new = np.empty_like(vi)
+            u0 = np.empty_like(vi)
             for comp in range(3):
                 pic, flip = self.transfer(gi, comp, vi[:, comp])
                 new[:, comp] = pic + self.FLIP * (flip - pic)
+                u0[:, comp] = pic
             v[ing] = new
         v[~ing, 1] -= self.G * dt
         x = x0 + v * dt
+        if self.advect == 'rk2' and u0 is not None:
+            xm = x0[ing] + u0 * (0.5 * dt)
+            gm = self.grid_pos(xm)
+            ok = self.in_grid(gm)
+            u1 = u0.copy()
+            for comp in range(3):
+                pic, _ = self.transfer(gm[ok], comp, u0[ok, comp])
+                u1[ok, comp] = pic
+            xi = x[ing]
+            xi[ok] = x0[ing][ok] + u1[ok] * dt
+            x[ing] = xi
         rc = 0.32 * h
         d = self.sdf_at(x)
         hit = d < rc

@@ -23,16 +23,18 @@ def f32(a):
 
 
 def oracle_from(nx, ny, nz, h, origin, *, flip, omega, iters, g=9.81, whitewater=False, rng_mode='hash', sdf_mode='analytic',
-                ripple=(16, 16), wmap=32, seed=1, ww_cap=140000):
+                ripple=(16, 16), wmap=32, seed=1, ww_cap=140000, advect='euler'):
     return of.Tank(nx, ny, nz, h, origin=origin, flip=flip, omega=omega, iters=iters, g=g, whitewater=whitewater,
-                   rng_mode=rng_mode, sdf_mode=sdf_mode, ripple=ripple, wmap=wmap, seed=seed, ww_cap=ww_cap)
+                   rng_mode=rng_mode, sdf_mode=sdf_mode, ripple=ripple, wmap=wmap, seed=seed, ww_cap=ww_cap,
+                   advect=advect)
 
 
 def gpu_from(pkg, nx, ny, nz, h, *, flip, omega, iters, g=9.81, whitewater=False, ripple=None, wmap=32, capacity=None,
-             sdf_mode='analytic', ww_capacity=140000, seed=1):
+             sdf_mode='analytic', ww_capacity=140000, seed=1, advect='euler'):
     n = capacity or max(64, nx * ny * nz * 12)
     return pkg.Tank(nx=nx, ny=ny, nz=nz, h=h, flip=flip, omega=omega, iters=iters, gravity=g, whitewater=whitewater,
-                    capacity=n, ripple=ripple, wmap=wmap, sdf_mode=sdf_mode, ww_capacity=ww_capacity, seed=seed)
+                    capacity=n, ripple=ripple, wmap=wmap, sdf_mode=sdf_mode, ww_capacity=ww_capacity, seed=seed,
+                    advect=advect)
 
 
 def assert_close_field(a, b, rtol=RTOL, what='', atol=0.0):
