@@ -309,7 +309,8 @@ def run_serve(args, local):
     line = dict(metric=METRIC, value=r['particle_steps_per_s'], unit=METRIC, n_gpus=1, steps=args.req_steps, warmup=0,
                 ms_per_step=None, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32', data='synthetic',
                 config=dict(workload='serving_poisson', rate_per_s=args.rate, duration_s=args.duration,
-                            steps_per_request=args.req_steps, budget_gb=150), latency=dict(p50_ms=r['p50_ms'], p99_ms=r['p99_ms']),
+                            steps_per_request=args.req_steps, budget_gb=150),
+                latency=dict(p50_ms=r['p50_ms'], p99_ms=r['p99_ms'], p50_all_ms=r['p50_all_ms'], p99_all_ms=r['p99_all_ms']),
                 serving=r)
     print(json.dumps(line), flush=True)
 

@@ -1,5 +1,6 @@
 // extern "C" surface of libsuiri_cuda.so (include/suiri.h): argument checks, error codes and messages,
 // no exception crosses the ABI.
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -625,7 +626,10 @@ int suiri_server_poll(suiri_server* s, int64_t id, int32_t* state, double* laten
     if (it == S.reqs.end()) throw Error(SUIRI_ERR_INVALID, "unknown request id");
     const Request& q = *it->second;
     if (state) *state = q.state;
-    if (latency_ms) *latency_ms = q.state >= kDone ? 1000.0 * (q.t_done - q.t_submit) : 0.0;
+    if (latency_ms) {
+      const double now = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+      *latency_ms = 1000.0 * ((q.state >= kDone ? q.t_done : now) - q.t_submit);
+    }
     if (count) *count = q.final_count;
     if (q.state == kFailed) s->err = q.err;
   });

@@ -78,6 +78,8 @@ void Server::start_request(Request* r) {
     apply(t, r->scene);
     for (const WaterBlock& b : r->scene.blocks) t.emit_block(b.lo, b.hi, false);
     if (!r->emitters.empty()) t.set_emitters(r->emitters);
+    t.read_counters();
+    r->start_count = t.h_ctr->n_live + t.h_ctr->n_emit;
     r->t_admit = now_s();
   } catch (const Error& e) {
     r->tank.reset();
@@ -93,7 +95,6 @@ void Server::finish_request(Request* r) {
   Tank& t = *r->tank;
   t.read_counters();
   r->final_count = t.h_ctr->n_live;
-  r->particle_steps = (double)r->final_count * r->steps;    // liquid particles × sub-steps
   if (r->keep_result) {
     const long long n = t.read_particles(nullptr, nullptr, 0);
     r->res_pos.resize(4 * n);
@@ -107,7 +108,6 @@ void Server::finish_request(Request* r) {
   r->t_done = tdone;
   r->state = kDone;
   lat_ms.push_back(1000.0 * (r->t_done - r->t_submit));
-  total_particle_steps += r->particle_steps;
   ++completed;
   cv.notify_all();
 }
@@ -155,6 +155,13 @@ void Server::loop() {
     }
     ++substeps;
     sum_active += (double)active.size();
+    {
+      // work done: every resident scene advanced one sub-step (particles counted at admission)
+      double w = 0;
+      for (Request* r : active) w += (double)r->start_count;
+      std::lock_guard<std::mutex> g(m);
+      total_particle_steps += w;
+    }
     std::vector<Request*> still, done;
     for (Request* r : active) (++r->steps_done >= r->steps ? done : still).push_back(r);
     if (!done.empty()) {

@@ -27,6 +27,7 @@ struct Request {
   std::string err;
   double t_submit = 0, t_admit = 0, t_done = 0;
   double acc_particle_steps = 0, particle_steps = 0;
+  long long start_count = 0;      // liquid particles at admission (after the scene's water blocks)
   long long final_count = 0;
   std::vector<float> res_pos, res_vel;
 };

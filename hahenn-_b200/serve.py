@@ -139,13 +139,19 @@ def scene_request(seed, axes=AXES_SERVE, faucet_p=0.1, iters=80, omega=1.7):
 def poisson_run(rate=200.0, duration=60.0, steps=120, budget_bytes=150e9, seed=0, axes=AXES_SERVE, faucet_p=0.1,
                 drain_timeout=10.0, device=0):
     """Submit requests at Poisson arrival times for `duration` seconds, give the outstanding ones up to
-    `drain_timeout` more seconds, and report over that window: latency percentiles of the completed
-    requests (requests still queued or running are counted, not timed), and particle-steps/s."""
+    `drain_timeout` more seconds, and report over that window:
+      * throughput: particle-steps/s done by the server (every resident scene's particles, counted at
+        admission, per batched sub-step), beside the load offered (the requests' fill particles × steps ÷
+        duration);
+      * latency: p50/p99 of the completed requests, and p50/p99 over every request with the unfinished ones
+        counted at the time they had waited when the window closed (a lower bound: under overload the queue
+        grows and this is what a client sees)."""
     srv = Server(budget_bytes=budget_bytes, device=device)
     rng = np.random.default_rng(seed)
     t0 = time.perf_counter()
     t_next = t0
     ids = []
+    offered = 0.0
     k = 0
     while True:
         t_next += rng.exponential(1.0 / rate)
@@ -153,8 +159,9 @@ def poisson_run(rate=200.0, duration=60.0, steps=120, budget_bytes=150e9, seed=0
             break
         while time.perf_counter() < t_next:
             time.sleep(min(0.002, max(0.0, t_next - time.perf_counter())))
-        scene, params, em, _ = scene_request(seed * 1000003 + k, axes, faucet_p)
+        scene, params, em, info = scene_request(seed * 1000003 + k, axes, faucet_p)
         ids.append(srv.submit(scene, params, em, steps))
+        offered += info['particles'] * steps
         k += 1
     submit_end = time.perf_counter()
     deadline = submit_end + drain_timeout
@@ -162,9 +169,10 @@ def poisson_run(rate=200.0, duration=60.0, steps=120, budget_bytes=150e9, seed=0
         time.sleep(0.05)
     el = time.perf_counter() - t0
     st = srv.stats()
-    lat, failed, pending = [], 0, 0
+    lat, all_lat, failed, pending = [], [], 0, 0
     for i in ids:
         s = srv.poll(i)
+        all_lat.append(s['latency_ms'])
         if s['state'] == 'done':
             lat.append(s['latency_ms'])
         elif s['state'] == 'failed':
@@ -172,9 +180,10 @@ def poisson_run(rate=200.0, duration=60.0, steps=120, budget_bytes=150e9, seed=0
         else:
             pending += 1
     srv.close()
-    lat = np.array(lat) if lat else np.zeros(1)
-    return dict(requests=len(ids), completed=len(lat) if len(ids) else 0, failed=failed, pending_at_end=pending, rate=rate,
-                duration_s=duration, wall_s=el, submit_s=submit_end - t0, p50_ms=float(np.percentile(lat, 50)),
-                p99_ms=float(np.percentile(lat, 99)), particle_steps=st['particle_steps'],
-                particle_steps_per_s=st['particle_steps'] / el, mean_active=st['mean_active'],
+    pc = lambda a, q: float(np.percentile(np.array(a), q)) if len(a) else None
+    return dict(requests=len(ids), completed=len(lat), failed=failed, pending_at_end=pending, rate=rate,
+                duration_s=duration, wall_s=el, submit_s=submit_end - t0,
+                p50_ms=pc(lat, 50), p99_ms=pc(lat, 99), p50_all_ms=pc(all_lat, 50), p99_all_ms=pc(all_lat, 99),
+                particle_steps=st['particle_steps'], particle_steps_per_s=st['particle_steps'] / el,
+                offered_particle_steps_per_s=offered / duration, mean_active=st['mean_active'],
                 rebuilds=int(st['rebuilds']), substeps=int(st['substeps']))

@@ -242,7 +242,8 @@ typedef struct suiri_request {
 
 typedef struct suiri_server_stats {
   int64_t completed, queued, running, failed, rebuilds, substeps;
-  double particle_steps;            /* liquid particles × sub-steps of completed requests */
+  double particle_steps;            /* work done so far: per batched sub-step, the liquid particles (counted at
+                                       admission) of every resident scene */
   double elapsed_s, used_bytes, budget_bytes;
   double p50_ms, p99_ms;            /* request latency: submit → results ready */
   double mean_active;               /* resident scenes per batched sub-step */
@@ -253,7 +254,8 @@ typedef struct suiri_server_stats {
 int suiri_server_create(int32_t device, double budget_bytes, double dt, suiri_server** out);
 int suiri_server_destroy(suiri_server* s);
 int suiri_server_submit(suiri_server* s, const suiri_request* r, int64_t* id);
-/* state: 0 queued, 1 running, 2 done, 3 failed; latency_ms (done/failed); count = final liquid particles */
+/* state: 0 queued, 1 running, 2 done, 3 failed; latency_ms: submit → done/failed, or the time waited so far
+   for a request still queued or running; count = final liquid particles */
 int suiri_server_poll(suiri_server* s, int64_t id, int32_t* state, double* latency_ms, int64_t* count);
 /* block until the request is done or failed, at most timeout_s seconds (SUIRI_ERR_STATE on timeout) */
 int suiri_server_wait(suiri_server* s, int64_t id, double timeout_s);
