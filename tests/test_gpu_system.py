@@ -179,3 +179,33 @@ def test_full_size_obstacles_inflow_properties(pkg):
     assert st['count'] <= n_first + 5 * 10 and st['count'] >= n_first - 5000
     assert np.isfinite(t.grid(N.FIELD_PRES)).all() and np.isfinite(vel).all()
     t.close()
+
+
+def test_empty_tank_steps_cleanly(pkg):
+    """A tank with no liquid steps without error: no particles, zero pressure, nothing spawned."""
+    t = pkg.Tank(nx=24, ny=16, nz=20, h=1 / 32, whitewater=True, ripple=None, capacity=1000, iters=10)
+    for _ in range(4):
+        t.substep(1 / 240)
+    st = t.stats()
+    assert st['count'] == 0 and st['ww_count'] == 0 and st['errors'] == 0 and st['full'] == 0
+    assert not np.any(t.grid(pkg.native.FIELD_PRES))
+    t.step(1 / 60)
+    assert t.stats()['count'] == 0
+    t.close()
+
+
+def test_capacity_reached_sets_full_and_caps_the_count(pkg):
+    """An emitter that outruns the particle capacity: emission stops at the capacity (minus its margin),
+    the full flag is raised, and the step keeps running."""
+    cap = 3000
+    t = pkg.Tank(nx=16, ny=16, nz=16, h=1 / 32, whitewater=False, ripple=None, capacity=cap, iters=10)
+    t.set_emitters([dict(shape='disc', pos=[0.0, 0.4, 0.0], dir=[0.0, -1.0, 0.0], radius=0.06, speed=1.0, count=400)])
+    for _ in range(20):
+        t.substep(1 / 240)
+    st = t.stats()
+    assert st['full'] == 1
+    assert 0.9 * cap < st['count'] <= cap
+    pos, vel, air, ids = t.particles()
+    assert len(ids) == st['count'] and len(np.unique(ids)) == len(ids)
+    assert np.all(np.isfinite(pos)) and np.all(np.isfinite(vel))
+    t.close()
