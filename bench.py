@@ -189,6 +189,28 @@ def cpu_port_rate(w, steps):
     return n_ps / el, el
 
 
+def reduce_ranks(ms, particles, sor_launch_ms, device):
+    """Whole-job figures of the replicas: the slowest rank's step and SOR-launch times (max over ranks) and
+    the particles of all ranks (sum), so value = all ranks' particle-steps ÷ the slowest rank's time."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms, particles, sor_launch_ms], dtype=torch.float64, device=device)
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    tot = t.clone()
+    dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    return float(mx[0]), float(tot[1]), float(mx[2])
+
+
+def reduce_e2e(rate, world, device):
+    """End-to-end rate of the whole job: the slowest rank's rate times the number of ranks."""
+    import torch
+    import torch.distributed as dist
+    x = torch.tensor([rate], dtype=torch.float64, device=device)
+    dist.all_reduce(x, op=dist.ReduceOp.MIN)
+    return float(x[0]) * world
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -385,13 +407,7 @@ def main():
     particles = 0.5 * (n0 + n1)
     sor_launch_ms = float(np.mean(sor_ms)) / (2 * prm['iters'])
     if world > 1:
-        t = torch.tensor([ms, particles, sor_launch_ms], dtype=torch.float64, device=f'cuda:{local}')
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        tot = t.clone()
-        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-        ms, sor_launch_ms = float(mx[0]), float(mx[2])
-        particles = float(tot[1])
+        ms, particles, sor_launch_ms = reduce_ranks(ms, particles, sor_launch_ms, f'cuda:{local}')
     value = particles * 1000.0 / ms
 
     # end-to-end through the C ABI: host inflow particles (pinned) up, stats back, every step
@@ -420,9 +436,7 @@ def main():
         nB = t2.stats()['count']
         e2e_rate = 0.5 * (nA + nB) * args.steps / el
         if world > 1:
-            x = torch.tensor([e2e_rate], dtype=torch.float64, device=f'cuda:{local}')
-            dist.all_reduce(x, op=dist.ReduceOp.MIN)
-            e2e_rate = float(x[0]) * world
+            e2e_rate = reduce_e2e(e2e_rate, world, f'cuda:{local}')
         e2e = dict(value=e2e_rate, unit=METRIC, h2d_bytes_per_step=h2d // args.steps, d2h_bytes_per_step=d2h // args.steps)
         t2.close()
 
