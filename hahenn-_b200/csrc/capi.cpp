@@ -486,7 +486,7 @@ int suiri_batch_sync(suiri_batch* b) {
 
 static void tune_group(Group& g, int32_t particle_blocks_per_sm, int32_t sor_mode) {
   if (particle_blocks_per_sm < 1 || particle_blocks_per_sm > 32) throw Error(SUIRI_ERR_INVALID, "blocks per SM in 1..32");
-  if (sor_mode < 0 || sor_mode > 2) throw Error(SUIRI_ERR_INVALID, "sor_mode is 0, 1 or 2");
+  if (sor_mode < 0 || sor_mode > 3) throw Error(SUIRI_ERR_INVALID, "sor_mode is 0, 1, 2 or 3");
   CK(cudaStreamSynchronize(g.stream));
   g.blocks_per_sm = particle_blocks_per_sm;
   g.ctx.particle_blocks = particle_blocks_per_sm * g.sm_count;

@@ -965,10 +965,11 @@ void Group::enqueue_body() {
   if (sor_mode == 1 && max_iters > 0) {
     launch_sor_persist(ctx, max_iters, sor_blocks);
     CK(cudaGetLastError());
-  } else if (sor_mode == 2) {
-    // launch l reads pres (l even) or pres2 and writes the other; an odd count ends in pres2
-    const int sweeps = 2 * max_iters, nl = (sweeps + kTbSweeps - 1) / kTbSweeps;
-    for (int l = 0; l < nl; ++l) launch_sor_tb(ctx, l * kTbSweeps, std::min(kTbSweeps, sweeps - l * kTbSweeps), l & 1);
+  } else if (sor_mode == 2 || sor_mode == 3) {
+    // S sweeps per launch; launch l reads pres (l even) or pres2 and writes the other; an odd count ends in pres2
+    const int S = sor_mode == 2 ? 2 : 4;
+    const int sweeps = 2 * max_iters, nl = (sweeps + S - 1) / S;
+    for (int l = 0; l < nl; ++l) launch_sor_tb(ctx, S, l * S, std::min(S, sweeps - l * S), l & 1);
     if (nl & 1) launch_sor_copy(ctx);
     CK(cudaGetLastError());
   } else {

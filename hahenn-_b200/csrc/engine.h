@@ -147,7 +147,7 @@ struct Group {
   int* d_hpfx = nullptr;          // colour-slot prefix for the persistent SOR
   GridBarrier* d_barrier = nullptr;
   int sor_mode = 0;               // 0: one launch per colour sweep, 1: one cooperative launch per solve,
-                                  // 2: kTbSweeps sweeps per launch (temporal blocking)
+                                  // 2, 3: 2 or 4 sweeps per launch (temporal blocking)
   int sor_blocks = 0;
   bool profile = false;           // record events around the SOR phase (inside the graph too)
   cudaEvent_t ev_sor[2] = {nullptr, nullptr};

@@ -9,7 +9,6 @@ constexpr int kThreads = 256;
 constexpr int kScanTile = 2048;          // cells per scan block (256 threads × 8)
 constexpr int kBrick = 8;                // P2G brick edge in cells
 constexpr int kTbX = 16, kTbY = 16, kTbZ = 8;   // temporal-blocked SOR tile (cells)
-constexpr int kTbSweeps = 4;             // colour sweeps per temporal-blocked SOR launch (= halo width)
 constexpr int kTbThreads = 512;
 
 // block families: blocks of one launch are laid out tank after tank; pfx[t] = first block of tank t
@@ -46,7 +45,7 @@ void launch_sor_sweep(const LaunchCtx& L, int color, int sweep);
 void launch_sor_persist(const LaunchCtx& L, int max_iters, int blocks);   // whole solve, one cooperative launch
 int sor_persist_max_blocks(int device);                                  // co-resident blocks of k_sor_persist
 cudaError_t sor_tb_prepare();                                            // once per device, outside capture
-void launch_sor_tb(const LaunchCtx& L, int sweep0, int nsweeps, int dir); // nsweeps ≤ kTbSweeps; dir 0: pres→pres2
+void launch_sor_tb(const LaunchCtx& L, int sweeps_per_launch, int sweep0, int nsweeps, int dir);  // 2 or 4; dir 0: pres→pres2
 void launch_sor_copy(const LaunchCtx& L);                                // pres ← pres2
 void launch_project(const LaunchCtx& L);
 void launch_g2p(const LaunchCtx& L);

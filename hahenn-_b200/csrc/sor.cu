@@ -189,115 +189,168 @@ __global__ void __launch_bounds__(kThreads) k_sor_persist(const TankDev* __restr
 }
 
 // ------------------------------------------------------------------------------------------------
-// Temporal blocking: kTbSweeps colour sweeps per launch. A block owns a kTbX×kTbY×kTbZ tile of cells and
-// stages the tile plus a halo of kTbSweeps cells (clipped at the tank walls) in shared memory: pressure,
-// rhs and a 16-bit code per cell, split by colour like the global arrays. Sweep s (0-based, n sweeps in
-// the launch) updates the cells of its colour within n−1−s cells of the tile: a red-black sweep reads only
-// the other colour, so a cell updated there sees exactly the neighbour values the per-sweep launches would
-// give it, and after the n sweeps the tile itself holds exactly the per-sweep result. The tile is written
-// to the other pressure buffer (halos are read from the input buffer by neighbouring blocks while this one
+// Temporal blocking: S colour sweeps per launch (S = 2 or 4). A block owns a kTbX×kTbY×kTbZ tile of cells and
+// stages the tile plus a halo of S cells (clipped at the tank walls) in shared memory: pressure, rhs and a
+// 16-bit code per cell, split by colour like the global arrays. Sweep s (0-based, n sweeps in the launch)
+// updates the cells of its colour within n−1−s cells of the tile: a red-black sweep reads only the other
+// colour, so a cell updated there sees exactly the neighbour values the per-sweep launches would give it,
+// and after the n sweeps the tile itself holds exactly the per-sweep result. The tile is written to the
+// other pressure buffer (halos are read from the input buffer by neighbouring blocks while this one
 // writes), so launches alternate between pres and pres2.
 //
-// Cut cells keep their six coefficients in a shared table (kTbMaxCut entries; beyond that they are read
-// from the face fractions in global memory). The smem code: 0 inactive; 0x4000|open bits for a cell whose
-// faces are all closed or fully open; 0x8000|table index for a cut cell (0x7FFF: not in the table).
-constexpr int kTbRX = kTbX + 2 * kTbSweeps, kTbRY = kTbY + 2 * kTbSweeps, kTbRZ = kTbZ + 2 * kTbSweeps;
-constexpr int kTbHX = kTbRX / 2;
-constexpr int kTbSlots = kTbHX * kTbRY * kTbRZ;     // per colour
-constexpr int kTbMaxCut = 512;
-constexpr int kTbSmem = 2 * kTbSlots * 4 * 2 + 2 * kTbSlots * 2 + kTbMaxCut * 6 * 4;
-static_assert(kTbX % 2 == 0 && kTbSweeps % 2 == 0, "tile and halo keep the region's x origin even");
-static_assert(kTbSlots < 0x7FFF, "table index fits the code");
+// Like k_sor, a block reads what the solve never writes (code, rhs, cut-cell fractions) before
+// griddepcontrol.wait, overlapping the previous launch, and the pressures after it, one batch of loads.
+// Cut cells keep their six coefficients in a shared table (kTbCut entries; beyond that they are read from
+// the face fractions in global memory). The smem code: 0 inactive; 0x4000|open bits for a cell whose faces
+// are all closed or fully open; 0x8000|table index for a cut cell (0x7FFF: not in the table).
+constexpr int kTbCut = 512;
+template <int S>
+struct TbShape {
+  static constexpr int RX = kTbX + 2 * S, RY = kTbY + 2 * S, RZ = kTbZ + 2 * S;
+  static constexpr int HX = RX / 2;
+  static constexpr int SLOTS = HX * RY * RZ;                              // per colour
+  static constexpr int PER = (2 * SLOTS + kTbThreads - 1) / kTbThreads;    // region slots per thread
+  static constexpr int SMEM = 2 * SLOTS * 4 * 2 + 2 * SLOTS * 2 + kTbCut * 6 * 4;
+  static_assert(kTbX % 2 == 0 && S % 2 == 0, "tile and halo keep the region's x origin even");
+  static_assert(SLOTS < 0x7FFF, "table index fits the code");
+};
 
+template <int S>
 __global__ void __launch_bounds__(kTbThreads, 2) k_sor_tb(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx,
                                                           int sweep0, int nsweeps, int dir) {
+  using G = TbShape<S>;
   extern __shared__ __align__(16) unsigned char tb_smem[];
-  float* sp = reinterpret_cast<float*>(tb_smem);               // [2][kTbSlots] pressure
-  float* srhs = sp + 2 * kTbSlots;                             // [2][kTbSlots]
-  uint16_t* scode = reinterpret_cast<uint16_t*>(srhs + 2 * kTbSlots);
-  float* stab = reinterpret_cast<float*>(scode + 2 * kTbSlots);  // [kTbMaxCut][6]
+  float* sp = reinterpret_cast<float*>(tb_smem);               // [2][SLOTS] pressure
+  float* srhs = sp + 2 * G::SLOTS;                             // [2][SLOTS]
+  uint16_t* scode = reinterpret_cast<uint16_t*>(srhs + 2 * G::SLOTS);
+  float* stab = reinterpret_cast<float*>(scode + 2 * G::SLOTS);  // [kTbCut][6]
   __shared__ int s_ncut;
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int t = find_slot(bpfx, ntanks, blockIdx.x);
-  asm volatile("griddepcontrol.wait;" ::: "memory");
   const TankDev& T = tanks[t];
-  const int nx = T.nx, ny = T.ny, nz = T.nz;
+  const int nx = T.nx, ny = T.ny, nz = T.nz, hx = T.hx;
+  const size_t nh = T.nhalf;
   const int lb = blockIdx.x - bpfx[t];
   const int tnx = (nx + kTbX - 1) / kTbX, tny = (ny + kTbY - 1) / kTbY;
   const int x0 = (lb % tnx) * kTbX, y0 = ((lb / tnx) % tny) * kTbY, z0 = (lb / (tnx * tny)) * kTbZ;
-  const int rx0 = max(x0 - kTbSweeps, 0), ry0 = max(y0 - kTbSweeps, 0), rz0 = max(z0 - kTbSweeps, 0);
-  const int rx1 = min(x0 + kTbX + kTbSweeps, nx), ry1 = min(y0 + kTbY + kTbSweeps, ny), rz1 = min(z0 + kTbZ + kTbSweeps, nz);
+  const int rx0 = max(x0 - S, 0), ry0 = max(y0 - S, 0), rz0 = max(z0 - S, 0);
+  const int rx1 = min(x0 + kTbX + S, nx), ry1 = min(y0 + kTbY + S, ny), rz1 = min(z0 + kTbZ + S, nz);
   const float* __restrict__ pin = dir ? T.pres2 : T.pres;
   float* __restrict__ pout = dir ? T.pres : T.pres2;
-  const size_t nh = T.nhalf;
+  const int iters = T.iters;
+  const float omega = T.omega;
+  // region slot q (colour q >= SLOTS) → global index within its colour, or −1 outside the tank
+  auto region = [&](int q, int& i, int& j, int& k) -> int {
+    const int c = q >= G::SLOTS;
+    const int ls = q - c * G::SLOTS;
+    const int lti = ls % G::HX, lrow = ls / G::HX;
+    j = ry0 + lrow % G::RY;
+    k = rz0 + lrow / G::RY;
+    i = rx0 + 2 * lti + ((j + k + c) & 1);
+    return (i < rx1 && j < ry1 && k < rz1) ? (i >> 1) + hx * (j + ny * k) : -1;
+  };
   if (threadIdx.x == 0) s_ncut = 0;
   __syncthreads();
-  for (int q = threadIdx.x; q < 2 * kTbSlots; q += kTbThreads) {
-    const int c = q >= kTbSlots;
-    const int ls = q - c * kTbSlots;
-    const int lti = ls % kTbHX, lrow = ls / kTbHX;
-    const int j = ry0 + lrow % kTbRY, k = rz0 + lrow / kTbRY;
-    const int i = rx0 + 2 * lti + ((j + k + c) & 1);
-    float p = 0.f, r = 0.f;
-    uint16_t cd = 0;
-    if (i < rx1 && j < ry1 && k < rz1) {
-      const size_t g = c * nh + (size_t)(i >> 1) + (size_t)T.hx * (j + (size_t)ny * k);
-      p = pin[g];
-      const uint32_t code = T.code[g];
-      if (code & kCodeActive) {
-        r = T.rhs[g];
-        if (code & kCodePartial) {
+  // constant operands, in chunks of loads issued together
+  constexpr int CH = 6;
+#pragma unroll
+  for (int u0 = 0; u0 < G::PER; u0 += CH) {
+    uint32_t cd[CH];
+    float rh[CH];
+#pragma unroll
+    for (int v = 0; v < CH; ++v) {
+      const int q = threadIdx.x + (u0 + v) * kTbThreads;
+      cd[v] = 0; rh[v] = 0.f;
+      if (u0 + v < G::PER && q < 2 * G::SLOTS) {
+        int i, j, k;
+        const int g = region(q, i, j, k);
+        if (g >= 0) {
+          const size_t gg = (q >= G::SLOTS ? nh : 0) + g;
+          cd[v] = T.code[gg];
+          rh[v] = T.rhs[gg];
+        }
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < CH; ++v) {
+      const int q = threadIdx.x + (u0 + v) * kTbThreads;
+      if (u0 + v >= G::PER || q >= 2 * G::SLOTS) continue;
+      uint16_t code16 = 0;
+      float r = 0.f;
+      if (cd[v] & kCodeActive) {
+        r = rh[v];
+        if (cd[v] & kCodePartial) {
           const int e = atomicAdd(&s_ncut, 1);
-          if (e < kTbMaxCut) {
+          if (e < kTbCut) {
+            int i, j, k;
+            region(q, i, j, k);
             float C[6];
             cut_coeffs(T, i, j, k, C);
 #pragma unroll
             for (int d = 0; d < 6; ++d) stab[6 * e + d] = C[d];
-            cd = (uint16_t)(0x8000 | e);
+            code16 = (uint16_t)(0x8000 | e);
           } else {
-            cd = 0xFFFF;
+            code16 = 0xFFFF;
           }
         } else {
-          cd = (uint16_t)(0x4000 | (code & 0x3F));
+          code16 = (uint16_t)(0x4000 | (cd[v] & 0x3F));
         }
       }
+      srhs[q] = r;
+      scode[q] = code16;
     }
-    sp[q] = p;
-    srhs[q] = r;
-    scode[q] = cd;
+  }
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  // pressures: every load of the thread in flight at once
+  {
+    float pv[G::PER];
+#pragma unroll
+    for (int u = 0; u < G::PER; ++u) {
+      const int q = threadIdx.x + u * kTbThreads;
+      pv[u] = 0.f;
+      if (q < 2 * G::SLOTS) {
+        int i, j, k;
+        const int g = region(q, i, j, k);
+        if (g >= 0) pv[u] = pin[(q >= G::SLOTS ? nh : 0) + g];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < G::PER; ++u) {
+      const int q = threadIdx.x + u * kTbThreads;
+      if (q < 2 * G::SLOTS) sp[q] = pv[u];
+    }
   }
   __syncthreads();
   for (int s = 0; s < nsweeps; ++s) {
     const int sw = sweep0 + s;
-    if (sw < 2 * T.iters) {
+    if (sw < 2 * iters) {
       const int c = sw & 1, e = nsweeps - 1 - s;
       const int bx0 = max(x0 - e, rx0), bx1 = min(x0 + kTbX + e, rx1);
       const int by0 = max(y0 - e, ry0), by1 = min(y0 + kTbY + e, ry1);
       const int bz0 = max(z0 - e, rz0), bz1 = min(z0 + kTbZ + e, rz1);
-      const int sx0 = (bx0 - rx0) >> 1, wsx = ((bx1 - rx0 + 1) >> 1) - sx0, wy = by1 - by0;
-      const int nq = wsx * wy * (bz1 - bz0);
-      const float* so = sp + (1 - c) * kTbSlots;
-      for (int q = threadIdx.x; q < nq; q += kTbThreads) {
-        const int lti = sx0 + q % wsx, rr = q / wsx;
-        const int j = by0 + rr % wy, k = bz0 + rr / wy;
+      const float* so = sp + (1 - c) * G::SLOTS;
+      for (int ls = threadIdx.x; ls < G::SLOTS; ls += kTbThreads) {
+        const int lti = ls % G::HX, lrow = ls / G::HX;
+        const int lj = lrow % G::RY, lk = lrow / G::RY;
+        const int j = ry0 + lj, k = rz0 + lk;
         const int i = rx0 + 2 * lti + ((j + k + c) & 1);
-        if (i < bx0 || i >= bx1) continue;
-        const int rowb = kTbHX * ((j - ry0) + kTbRY * (k - rz0));
-        const int own = c * kTbSlots + lti + rowb;
+        if (i < bx0 || i >= bx1 || j < by0 || j >= by1 || k < bz0 || k >= bz1) continue;
+        const int own = c * G::SLOTS + ls;
         const unsigned cd = scode[own];
         if (!cd) continue;
+        const int rowb = ls - lti;       // G::HX · (lj + G::RY · lk)
         const int li = i - rx0;
         float nb[6];
         nb[0] = i > 0 ? so[((li - 1) >> 1) + rowb] : 0.f;
         nb[1] = i + 1 < nx ? so[((li + 1) >> 1) + rowb] : 0.f;
-        nb[2] = j > 0 ? so[lti + rowb - kTbHX] : 0.f;
-        nb[3] = j + 1 < ny ? so[lti + rowb + kTbHX] : 0.f;
-        nb[4] = k > 0 ? so[lti + rowb - kTbHX * kTbRY] : 0.f;
-        nb[5] = k + 1 < nz ? so[lti + rowb + kTbHX * kTbRY] : 0.f;
+        nb[2] = j > 0 ? so[lti + rowb - G::HX] : 0.f;
+        nb[3] = j + 1 < ny ? so[lti + rowb + G::HX] : 0.f;
+        nb[4] = k > 0 ? so[lti + rowb - G::HX * G::RY] : 0.f;
+        nb[5] = k + 1 < nz ? so[lti + rowb + G::HX * G::RY] : 0.f;
         float C[6];
         if (cd & 0x8000) {
           const unsigned x = cd & 0x7FFF;
-          if (x < kTbMaxCut) {
+          if (x < kTbCut) {
 #pragma unroll
             for (int d = 0; d < 6; ++d) C[d] = stab[6 * x + d];
           } else {
@@ -307,7 +360,7 @@ __global__ void __launch_bounds__(kTbThreads, 2) k_sor_tb(const TankDev* __restr
 #pragma unroll
           for (int d = 0; d < 6; ++d) C[d] = (cd >> d) & 1u ? 1.0f : 0.0f;
         }
-        sp[own] = sor_update(C, nb, srhs[own], sp[own], T.omega);
+        sp[own] = sor_update(C, nb, srhs[own], sp[own], omega);
       }
     }
     __syncthreads();
@@ -320,8 +373,8 @@ __global__ void __launch_bounds__(kTbThreads, 2) k_sor_tb(const TankDev* __restr
     const int j = y0 + rr % kTbY, k = z0 + rr / kTbY;
     const int i = x0 + 2 * mi + ((j + k + c) & 1);
     if (i >= nx || j >= ny || k >= nz) continue;
-    const int ls = c * kTbSlots + ((i - rx0) >> 1) + kTbHX * ((j - ry0) + kTbRY * (k - rz0));
-    pout[c * nh + (size_t)(i >> 1) + (size_t)T.hx * (j + (size_t)ny * k)] = sp[ls];
+    const int ls = c * G::SLOTS + ((i - rx0) >> 1) + G::HX * ((j - ry0) + G::RY * (k - rz0));
+    pout[c * nh + (size_t)(i >> 1) + (size_t)hx * (j + (size_t)ny * k)] = sp[ls];
   }
 }
 
@@ -336,21 +389,26 @@ __global__ void __launch_bounds__(kThreads) k_sor_copy(const TankDev* __restrict
 }
 
 cudaError_t sor_tb_prepare() {
-  return cudaFuncSetAttribute(k_sor_tb, cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmem);
+  const cudaError_t e = cudaFuncSetAttribute(k_sor_tb<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, TbShape<2>::SMEM);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_sor_tb<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, TbShape<4>::SMEM);
 }
 
-void launch_sor_tb(const LaunchCtx& L, int sweep0, int nsweeps, int dir) {
+void launch_sor_tb(const LaunchCtx& L, int sweeps_per_launch, int sweep0, int nsweeps, int dir) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(L.nblocks[kFamTiles]);
   cfg.blockDim = dim3(kTbThreads);
-  cfg.dynamicSmemBytes = kTbSmem;
+  cfg.dynamicSmemBytes = sweeps_per_launch == 2 ? TbShape<2>::SMEM : TbShape<4>::SMEM;
   cfg.stream = L.stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k_sor_tb, L.tanks, L.ntanks, (const int*)L.bpfx[kFamTiles], sweep0, nsweeps, dir);
+  cfg.numAttrs = sweep0 > 0 ? 1 : 0;     // the first launch waits for the grid pass in full
+  if (sweeps_per_launch == 2)
+    cudaLaunchKernelEx(&cfg, k_sor_tb<2>, L.tanks, L.ntanks, (const int*)L.bpfx[kFamTiles], sweep0, nsweeps, dir);
+  else
+    cudaLaunchKernelEx(&cfg, k_sor_tb<4>, L.tanks, L.ntanks, (const int*)L.bpfx[kFamTiles], sweep0, nsweeps, dir);
 }
 
 void launch_sor_copy(const LaunchCtx& L) {

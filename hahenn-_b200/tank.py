@@ -192,7 +192,7 @@ class Tank:
         self._c(N.lib().suiri_profile(self._h, 1 if on else 0))
 
     def tune(self, blocks_per_sm=4, sor_mode=0):
-        """sor_mode: 0 one launch per colour sweep, 1 one cooperative launch, 2 temporal blocking."""
+        """sor_mode: 0 one launch per colour sweep, 1 one cooperative launch, 2/3 temporal blocking (2/4 sweeps)."""
         self._c(N.lib().suiri_tune(self._h, int(blocks_per_sm), int(sor_mode)))
 
     def sor_phase_ms(self):

@@ -88,7 +88,7 @@ def test_rk2_advection_matches_oracle(pkg):
     eul.close()
 
 
-@pytest.mark.parametrize('sor_mode', [0, 2])
+@pytest.mark.parametrize('sor_mode', [0, 2, 3])
 def test_sor_bit_exact_with_reference_operation_order(pkg, sor_mode):
     """Given the GPU's own float32 operands, the reference's float32 SOR loop reproduces its pressure bit for
     bit, for one launch per sweep and for temporal blocking; the FP64 residual of the solve is stated."""
@@ -313,26 +313,29 @@ def _run_form(pkg, w, mode, iters, steps=3):
     return out
 
 
-@pytest.mark.parametrize('mode', [1, 2])
+@pytest.mark.parametrize('mode', [1, 2, 3])
 def test_solve_forms_equal_per_sweep_launches(pkg, mode):
-    """The cooperative whole-solve launch (1) and the temporal-blocked launches (2) relax the same colours
-    in the same order as one launch per sweep (0): identical pressures and particles, bit for bit."""
+    """The cooperative whole-solve launch (1) and the temporal-blocked launches (2: two sweeps each, 3:
+    four) relax the same colours in the same order as one launch per sweep (0): identical pressures and
+    particles, bit for bit."""
     w = pkg.workloads.obstacles_inflow(scale=4)
     for a, b in zip(_run_form(pkg, w, 0, 40), _run_form(pkg, w, mode, 40)):
         np.testing.assert_array_equal(a, b)
 
 
-@pytest.mark.parametrize('iters', [6, 7, 1])
-def test_temporal_blocking_edges(pkg, iters):
-    """Temporal blocking on a grid that is no multiple of the tile (odd x), with an odd number of launches
-    (6 iterations: 3 launches, the result copied back), a short last launch (7: 4+4+4+2 sweeps) and a
-    single launch of two sweeps (1)."""
+@pytest.mark.parametrize('mode', [2, 3])
+@pytest.mark.parametrize('iters', [6, 7, 1, 3])
+def test_temporal_blocking_edges(pkg, iters, mode):
+    """Temporal blocking on a grid that is no multiple of the tile (odd x). Four sweeps a launch: an odd
+    number of launches (6 iterations: 3 launches, the result copied back), a short last launch (7:
+    4+4+4+2 sweeps), a single launch of two sweeps (1). Two sweeps a launch: odd counts (1, 3, 7)."""
     w = pkg.workloads.random_tank(5, axes=(21, 37, 19))
-    for a, b in zip(_run_form(pkg, w, 0, iters), _run_form(pkg, w, 2, iters)):
+    for a, b in zip(_run_form(pkg, w, 0, iters), _run_form(pkg, w, mode, iters)):
         np.testing.assert_array_equal(a, b)
 
 
-def test_temporal_blocking_batch_uneven_iterations(pkg):
+@pytest.mark.parametrize('mode', [2, 3])
+def test_temporal_blocking_batch_uneven_iterations(pkg, mode):
     """In a batch the tile launches run to the largest iteration count; tanks with fewer iterations stop
     relaxing but keep being carried between the two pressure buffers: every tank equals its solo run."""
     specs = [(pkg.workloads.random_tank(s, axes=(16, 24, 40)), it) for s, it in ((11, 5), (12, 12), (13, 9))]
@@ -351,7 +354,7 @@ def test_temporal_blocking_batch_uneven_iterations(pkg):
 
     solo, batched = make(0), make(None)
     b = pkg.Batch(batched)
-    b.tune(4, 2)
+    b.tune(4, mode)
     for _ in range(4):
         for t in solo:
             t.substep(1 / 240)
