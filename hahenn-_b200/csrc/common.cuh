@@ -33,6 +33,18 @@ constexpr uint32_t kCodePartial = 1u << 13;        // some face fraction strictl
 
 enum SdfMode { kSdfAnalytic = 0, kSdfLattice = 1 };
 
+// Division by a divisor fixed per tank as a multiply-high and a shift (Granlund & Montgomery, "Division by
+// invariant integers using multiplication", 1994, round-up variant): with l = ceil(log2 d) and
+// mul = floor(2^32 (2^l − d) / d) + 1, n / d = (umulhi(n, mul) + n) >> l exactly for 0 ≤ n < 2^31.
+struct DivU {
+  uint32_t mul, shr;
+};
+inline DivU make_divu(uint32_t d) {
+  uint32_t l = 0;
+  while ((1ull << l) < d) ++l;
+  return DivU{(uint32_t)(((1ull << 32) * ((1ull << l) - d)) / d + 1), l};
+}
+
 // An obstacle (flag 1) or drain (flag 2). Doubles: obstacle geometry feeds the bit-exact face fractions.
 struct Obj {
   double pos[3];
@@ -77,6 +89,7 @@ struct TankDev {
   int sx, sxy;              // node strides (nx+1), (nx+1)(ny+1)
   int nnodes, ncells, nhalf;
   int nyl;                  // lattice covers 2*nyl+1 points vertically
+  DivU dnx, dny, dhx, dsx, dsxy;   // exact division by nx, ny, hx, sx, sxy
   double h, ox, oy, oz, rim;
   // physics
   double g, flip, friction, ppc, drift, ww_rate, dt;
@@ -152,6 +165,10 @@ __device__ __forceinline__ bool in_grid(const TankDev& T, double gx, double gy, 
 }
 
 __device__ __forceinline__ int flags_of(float w) { return (int)w; }
+
+__device__ __forceinline__ int divu(int n, DivU v) {
+  return (int)((__umulhi((unsigned)n, v.mul) + (unsigned)n) >> v.shr);
+}
 #endif  // __CUDACC__
 
 }  // namespace suiri

@@ -253,6 +253,8 @@ Tank::Tank(const TankConfig& c) : cfg(c) {
   TankDev& D = d;
   D.nx = cfg.nx; D.ny = cfg.ny; D.nz = cfg.nz; D.hx = (cfg.nx + 1) / 2;
   D.sx = cfg.nx + 1; D.sxy = (cfg.nx + 1) * (cfg.ny + 1);
+  D.dnx = make_divu(D.nx); D.dny = make_divu(D.ny); D.dhx = make_divu(D.hx);
+  D.dsx = make_divu(D.sx); D.dsxy = make_divu(D.sxy);
   D.nnodes = (cfg.nx + 1) * (cfg.ny + 1) * (cfg.nz + 1);
   D.ncells = cfg.nx * cfg.ny * cfg.nz;
   D.nhalf = D.hx * cfg.ny * cfg.nz;

@@ -6,9 +6,9 @@
 namespace suiri {
 
 __device__ __forceinline__ void node_coord(const TankDev& T, int n, int& i, int& j, int& k) {
-  k = n / T.sxy;
+  k = divu(n, T.dsxy);
   const int r = n - k * T.sxy;
-  j = r / T.sx;
+  j = divu(r, T.dsx);
   i = r - j * T.sx;
 }
 
@@ -291,7 +291,9 @@ __global__ void __launch_bounds__(kThreads) k_grid_cells(const TankDev* __restri
   const TankDev& T = tanks[t];
   const int c = (blockIdx.x - bpfx[t]) * blockDim.x + threadIdx.x;
   if (c >= T.ncells) return;
-  const int i = c % T.nx, j = (c / T.nx) % T.ny, k = c / (T.nx * T.ny);
+  const int row = divu(c, T.dnx);
+  const int k = divu(row, T.dny);
+  const int i = c - row * T.nx, j = row - k * T.ny;
   const int count = T.off[c + 1] - T.off[c];
   const bool fluid = count > 0;
   const int n = node_idx(T, i, j, k);

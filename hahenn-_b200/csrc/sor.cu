@@ -52,8 +52,8 @@ __device__ __forceinline__ void cut_coeffs(const TankDev& T, int i, int j, int k
 
 __device__ __forceinline__ void sor_cell(const TankDev& T, int color, int s) {
   const int hx = T.hx, nx = T.nx, ny = T.ny, nz = T.nz;
-  const int ti = s % hx, row = s / hx;
-  const int j = row % ny, k = row / ny;
+  const int row = divu(s, T.dhx), ti = s - row * hx;
+  const int k = divu(row, T.dny), j = row - k * ny;
   const int i = 2 * ti + ((j + k + color) & 1);
   if (i >= nx) return;
   const size_t own = (size_t)color * T.nhalf + s;
@@ -102,8 +102,8 @@ __global__ void __launch_bounds__(kSorThreads) k_sor(const TankDev* __restrict__
 #pragma unroll
   for (int u = 0; u < kSorPer; ++u) {
     const int s = (blockIdx.x - bpfx[t]) * (kSorThreads * kSorPer) + u * kSorThreads + threadIdx.x;
-    ti[u] = s % hx; row[u] = s / hx;
-    jj[u] = row[u] % ny; kk[u] = row[u] / ny;
+    row[u] = divu(s, T.dhx); ti[u] = s - row[u] * hx;
+    kk[u] = divu(row[u], T.dny); jj[u] = row[u] - kk[u] * ny;
     ii[u] = 2 * ti[u] + ((jj[u] + kk[u] + color) & 1);
     code[u] = 0; rhs[u] = 0.f;
     if (on && s < nhalf && ii[u] < nx) {
