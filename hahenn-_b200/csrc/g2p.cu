@@ -4,8 +4,8 @@
 // FLIP/PIC blend over valid faces, explicit Euler advection, obstacle collision with friction, the glass
 // walls and floor, drains, the free-flight mark of sub-grid drops, their merging with the pool (ripple
 // impulse + crown splash at K = We·Oh^-0.4) and whitewater spawning.
-// Reference: blender_addon/suiri_lab/solver.py:527-673 and src/js/31-wgsl-sim2.js:9-251. Positions,
-// weights and velocities are float64 inside the kernel, stored as float32.
+// Reference: blender_addon/suiri_lab/solver.py:527-673 and src/js/31-wgsl-sim2.js:9-251. Positions and
+// velocities are float64 inside the kernel, stored as float32; the grid-to-particle sums are float32.
 //
 // Spawning randomness is the reference WGSL's integer hash (src/js/30-wgsl-sim.js:36-37) seeded by the
 // particle's carried id and the sub-step number, so it does not depend on particle order.
@@ -65,7 +65,8 @@ __device__ __forceinline__ bool air_at(const TankDev& T, int i, int j, int k) {
 // axis both corner nodes then exist; on the other two axes the staggered lower corner is node −1 at the
 // first half cell, the only corners that can be missing. The 8 corner loads (one float2 each: projected
 // v, P2G v or NaN where the face took no weight) are issued together, then summed in the reference's
-// corner order.
+// corner order, in float32 as the reference's GPU path sums them (31-wgsl-sim2.js:9-36); the weights come
+// from the float64 position.
 __device__ __forceinline__ void transfer(const TankDev& T, double gx, double gy, double gz, int comp, double vp,
                                          double& pic, double& flip) {
   const double qx = gx - (comp == 0 ? 0.0 : 0.5), qy = gy - (comp == 1 ? 0.0 : 0.5), qz = gz - (comp == 2 ? 0.0 : 0.5);
@@ -81,18 +82,19 @@ __device__ __forceinline__ void transfer(const TankDev& T, double gx, double gy,
     const bool ok = (dx || lx) && (dy || ly) && (dz || lz);
     c[e] = ok ? __ldg(vv + dx + dy * T.sx + dz * T.sxy) : make_float2(0.f, __int_as_float(0x7fc00000));
   }
-  double sn = 0.0, so = 0.0, sw = 0.0;
+  const float wxf[2] = {(float)wx[0], (float)wx[1]}, wyf[2] = {(float)wy[0], (float)wy[1]}, wzf[2] = {(float)wz[0], (float)wz[1]};
+  float sn = 0.f, so = 0.f, sw = 0.f;
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
     if (isnan(c[e].y)) continue;
-    const double w = (wx[e >> 2] * wy[(e >> 1) & 1]) * wz[e & 1];
-    sn += w * (double)c[e].x;
-    so += w * (double)c[e].y;
+    const float w = (wxf[e >> 2] * wyf[(e >> 1) & 1]) * wzf[e & 1];
+    sn += w * c[e].x;
+    so += w * c[e].y;
     sw += w;
   }
-  if (sw >= 1e-6) {
-    pic = sn / sw;
-    flip = vp + (sn - so) / sw;
+  if (sw >= 1e-6f) {
+    pic = (double)(sn / sw);
+    flip = vp + (double)((sn - so) / sw);
   } else {
     pic = vp;
     flip = vp;
