@@ -158,9 +158,8 @@ def faucet_particles(e, dt, rng):
     return p.astype(np.float32), v.astype(np.float32)
 
 
-def cpu_port_rate(w, steps):
-    """The CPU oracle (NumPy restatement of the reference solver, single core) on `steps` sub-steps of the
-    same workload: particle-steps/s."""
+def _port_tank(w):
+    """The CPU oracle (NumPy restatement of the reference solver) set up on the workload."""
     from oracle import flip as of
     from oracle import sdf as sdfm
     prm = w['params']
@@ -174,10 +173,13 @@ def cpu_port_rate(w, steps):
             objs.append(sdfm.make_drain(it['pos'], it['r'], tuple(it['rot'])))
     t.set_objects(objs)
     t.add_particles(w['pos'].astype(np.float64))
-    rng = np.random.default_rng(1)
-    dt = prm['dt']
+    return t
+
+
+def _port_steps(t, w, steps, rng):
+    """`steps` sub-steps with the faucet's particles added on the host; returns the particle-steps."""
+    dt = w['params']['dt']
     n_ps = 0
-    t0 = time.perf_counter()
     for _ in range(steps):
         for e in w['emitters']:
             p, v = faucet_particles(e, dt, rng)
@@ -185,8 +187,70 @@ def cpu_port_rate(w, steps):
         n_ps += len(t.pos)
         t.frame += 1
         t.substep(dt)
+    return n_ps
+
+
+def cpu_port_rate(w, steps):
+    """The CPU oracle on one core for `steps` sub-steps of the workload: particle-steps/s."""
+    t = _port_tank(w)
+    rng = np.random.default_rng(1)
+    t0 = time.perf_counter()
+    n_ps = _port_steps(t, w, steps, rng)
     el = time.perf_counter() - t0
     return n_ps / el, el
+
+
+def _port_replica(steps, warm, barrier, out, k):
+    """One CPU replica (a spawned process): set up, warm up, wait for the others, time `steps` sub-steps."""
+    sys.path.insert(0, ROOT)
+    P = pkg()
+    w = P.workloads.obstacles_inflow()
+    t = _port_tank(w)
+    rng = np.random.default_rng(1 + k)
+    if warm:
+        _port_steps(t, w, warm, rng)
+    barrier.wait(timeout=900)
+    t0 = time.perf_counter()
+    n_ps = _port_steps(t, w, steps, rng)
+    out.put((n_ps, time.perf_counter() - t0))
+
+
+def cpu_replicas_count():
+    """One replica per usable core, at most 32, and at most one per 2 GB of available memory (a replica of
+    the 1.7M-particle workload peaks near 1.1 GB)."""
+    cores = len(os.sched_getaffinity(0))
+    avail_gb = 0.0
+    try:
+        with open('/proc/meminfo') as f:
+            for line in f:
+                if line.startswith('MemAvailable:'):
+                    avail_gb = int(line.split()[1]) / 1e6
+    except OSError:
+        avail_gb = 2.0
+    return max(1, min(cores, 32, int(avail_gb // 2)))
+
+
+def cpu_replicas_rate(steps, warm, procs):
+    """`procs` independent replicas of the CPU oracle, one process (one core) each, timed together from a
+    common start: all replicas' particle-steps ÷ the slowest replica's time."""
+    import multiprocessing as mp
+    ctx = mp.get_context('spawn')
+    barrier, out = ctx.Barrier(procs), ctx.Queue()
+    env = {k: os.environ.get(k) for k in ('OMP_NUM_THREADS', 'OPENBLAS_NUM_THREADS', 'MKL_NUM_THREADS')}
+    for k in env:
+        os.environ[k] = '1'
+    ps = [ctx.Process(target=_port_replica, args=(steps, warm, barrier, out, k)) for k in range(procs)]
+    for p in ps:
+        p.start()
+    res = [out.get(timeout=1800) for _ in ps]
+    for p in ps:
+        p.join(timeout=60)
+    for k, v in env.items():
+        if v is None:
+            os.environ.pop(k, None)
+        else:
+            os.environ[k] = v
+    return sum(r[0] for r in res) / max(r[1] for r in res), max(r[1] for r in res)
 
 
 def reduce_ranks(ms, particles, sor_launch_ms, device):
@@ -212,21 +276,24 @@ def reduce_e2e(rate, world, device):
 
 
 def run_reference(args, rank):
+    """The reference's CPU path (its NumPy solver, restated and pinned bit-exact against it) on this host's
+    cores: one independent replica of the workload per core, as many as the process may use. Rank 0 only;
+    other ranks exit at once."""
     if rank != 0:
         return
     w = pkg().workloads.obstacles_inflow()
-    steps, warm = max(1, min(args.steps, 6)), min(args.warmup, 1)
-    if warm:
-        cpu_port_rate(w, warm)
-    rate, el = cpu_port_rate(w, steps)
+    steps, warm = max(1, min(args.steps, 3)), min(args.warmup, 1)
+    procs = cpu_replicas_count()
+    rate, el = cpu_replicas_rate(steps, warm, procs)
     line = dict(impl='reference', metric=METRIC, value=rate, unit=METRIC, n_gpus=args.gpus, steps=steps, warmup=warm,
                 ms_per_step=1000 * el / steps, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f64',
                 data='synthetic',
                 config=dict(workload=w['name'], particles=len(w['pos']), cells=w['nx'] * w['ny'] * w['nz'],
                             sor_iters=w['params']['iters'], omega=w['params']['omega'], dt=w['params']['dt']),
-                cpu_baseline=dict(value=rate, unit=METRIC, cores=1, kind='port',
-                                  sample=f'{steps} sub-steps of the full workload (NumPy restatement of the reference '
-                                         f'solver, pinned bit-exact against it; NumPy runs on one core of {os.cpu_count()})'),
+                cpu_baseline=dict(value=rate, unit=METRIC, cores=procs, kind='port',
+                                  sample=f'{procs} replicas × {steps} sub-steps of the full workload, one process '
+                                         f'and one core each (NumPy restatement of the reference solver, pinned '
+                                         f'bit-exact against it; NumPy runs one core per process)'),
                 e2e=dict(value=rate, unit=METRIC, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line), flush=True)
 
