@@ -16,11 +16,13 @@
 // Most cells have every face either closed or fully open; their coefficients come from the 6 "open"
 // bits of the code and the float fractions are only read for cut cells next to obstacles.
 //
-// Two launch forms:
-//   k_sor          one colour of every tank per launch (2·iters launches per solve, in the sub-step graph)
+// Three launch forms, all giving the same pressures bit for bit (the tuner picks one):
+//   k_sor          one colour of every tank per launch (2·iters launches per solve, in the sub-step graph),
+//                  with programmatic dependent launch between sweeps
 //   k_sor_persist  the whole solve in one cooperative launch: all blocks resident, a grid barrier after
 //                  every colour sweep. The barrier's wait is bounded: after kSpinLimit polls it records
 //                  an error in the tank counters and every block returns.
+//   k_sor_tb<S>    S = 2 or 4 sweeps per launch on shared-memory tiles with halos (temporal blocking)
 #include "launch.cuh"
 
 namespace suiri {
