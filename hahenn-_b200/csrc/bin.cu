@@ -31,6 +31,7 @@ __global__ void k_begin_substep(const TankDev* __restrict__ tanks, int ntanks, i
         c->frame += 1;
         c->vmax_bits64 = 0ull;
         c->ww_spawned = 0;
+        c->n_act[0] = c->n_act[1] = 0;
       }
     }
     s[threadIdx.x] = v;

@@ -80,6 +80,7 @@ struct Counters {
   int err;            // device-side error flags
   unsigned next_id;   // id of the next particle emitted on the device
   int pad;
+  int n_act[2];       // active cells of each colour this sub-step (entries of TankDev::act)
   double emit_acc[8]; // fractional particles carried by the fixed emitters
 };
 
@@ -114,6 +115,7 @@ struct TankDev {
   double* flux;             // 3*nnodes cut-cell face fluxes (divergence operand)
   float* pres;              // 2*nhalf colour-split pressure
   float* pres2;             // 2*nhalf, the other buffer of the temporal-blocked solve
+  int* act;                 // 2*nhalf: per colour, the colour slots of the active cells (this sub-step)
   float* rhs;               // 2*nhalf h²·div
   uint32_t* code;           // 2*nhalf
   const Obj* objs;

@@ -289,6 +289,7 @@ Tank::Tank(const TankConfig& c) : cfg(c) {
   D.vv = (float2*)alloc(3 * nn * 8);
   D.pres = (float*)alloc(2 * nh * 4); D.rhs = (float*)alloc(2 * nh * 4); D.code = (uint32_t*)alloc(2 * nh * 4);
   D.pres2 = (float*)alloc(2 * nh * 4);
+  D.act = (int*)alloc(2 * nh * 4);
   d_objs = (Obj*)alloc(kMaxObj * sizeof(Obj));
   D.objs = d_objs;
   D.ctr = (Counters*)alloc(sizeof(Counters));
@@ -328,7 +329,7 @@ size_t tank_bytes(const TankConfig& c) {
   size_t b = cap * 16 * 6 + cap * 2 * 4;                      // A, E, B (pos, vel), ranks
   b += (nc + 1) * 4 + (nc + 2) * 4;                           // counts, offsets
   b += nn * (6 * 8 + 4 * 16 + 2 * 3 * 8 + 3 * 8);            // accumulator, vel/velold/frac/svel, fracd/flux, vv
-  b += 2 * nh * 16;                                           // pressure (two buffers), rhs, code
+  b += 2 * nh * 20;                                           // pressure (two buffers), rhs, code, active lists
   b += kMaxObj * sizeof(Obj) + sizeof(Counters) + kMaxEmitters * sizeof(EmitterDev);
   b += 2 * (size_t)std::max(1LL, c.ww_cap) * 32;
   if (c.rx > 0) {
@@ -852,6 +853,8 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
   std::vector<int> hp(n + 1, 0);
   for (int i = 0; i < n; ++i) hp[i + 1] = hp[i] + tanks[i]->d.nhalf;
   CK(cudaMalloc(&d_hpfx, (n + 1) * sizeof(int)));
+  CK(cudaMalloc(&d_apfx, 2 * (n + 1) * sizeof(int)));
+  CK(cudaMemsetAsync(d_apfx, 0, 2 * (n + 1) * sizeof(int), stream));
   CK(cudaMemcpyAsync(d_hpfx, hp.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
   CK(cudaMalloc(&d_barrier, sizeof(GridBarrier)));
   CK(cudaMemsetAsync(d_barrier, 0, sizeof(GridBarrier), stream));
@@ -859,6 +862,7 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
   sor_blocks = std::min(std::min(sor_persist_max_blocks(device), sm_count), std::max(1, (hp[n] + kThreads - 1) / kThreads));
   CK(cudaStreamSynchronize(stream));
   ctx.hpfx = d_hpfx;
+  ctx.apfx = d_apfx;
   ctx.barrier = d_barrier;
   ctx.stream = stream;
   ctx.tanks = d_tanks;
@@ -880,7 +884,7 @@ Group::~Group() {
       if (t->dep == ev_done) { cudaStreamWaitEvent(t->stream, ev_done, 0); t->dep = nullptr; }
     cudaEventDestroy(ev_done);
   }
-  cudaFree(d_hpfx); cudaFree(d_barrier);
+  cudaFree(d_hpfx); cudaFree(d_apfx); cudaFree(d_barrier);
   cudaFree(d_tanks); cudaFreeHost(h_tanks); cudaFree(d_bpfx); cudaFree(d_ppfx); cudaFree(d_bsum);
   if (own_stream) cudaStreamDestroy(stream);
 }

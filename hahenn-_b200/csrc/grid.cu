@@ -289,8 +289,9 @@ __global__ void __launch_bounds__(kThreads) k_grid_nodes(const TankDev* __restri
 __global__ void __launch_bounds__(kThreads) k_grid_cells(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx) {
   const int t = find_slot(bpfx, ntanks, blockIdx.x);
   const TankDev& T = tanks[t];
-  const int c = (blockIdx.x - bpfx[t]) * blockDim.x + threadIdx.x;
-  if (c >= T.ncells) return;
+  const int c0 = (blockIdx.x - bpfx[t]) * blockDim.x + threadIdx.x;
+  const bool valid = c0 < T.ncells;
+  const int c = valid ? c0 : T.ncells - 1;
   const int row = divu(c, T.dnx);
   const int k = divu(row, T.dny);
   const int i = c - row * T.nx, j = row - k * T.ny;
@@ -323,10 +324,53 @@ __global__ void __launch_bounds__(kThreads) k_grid_cells(const TankDev* __restri
   }
   if (fluid && den > 0.0f) code |= kCodeActive;
   const int col = (i + j + k) & 1;
-  const size_t s = (size_t)col * T.nhalf + half_idx(T, i, j, k);
-  T.rhs[s] = rhs;
-  T.code[s] = code;
-  if (!fluid) T.pres[s] = 0.f;
+  const int hs = half_idx(T, i, j, k);
+  const size_t s = (size_t)col * T.nhalf + hs;
+  if (valid) {
+    T.rhs[s] = rhs;
+    T.code[s] = code;
+    if (!fluid) T.pres[s] = 0.f;
+  }
+  // the active cells' slots, per colour, for the sweeps (one atomic per warp and colour; the order in the
+  // lists does not matter, a sweep updates each cell from the other colour only)
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int cc = 0; cc < 2; ++cc) {
+    const bool mine = valid && (code & kCodeActive) && col == cc;
+    const unsigned m = __ballot_sync(0xffffffffu, mine);
+    if (!m) continue;
+    const int leader = __ffs(m) - 1;
+    int at = 0;
+    if (lane == leader) at = atomicAdd(&T.ctr->n_act[cc], __popc(m));
+    at = __shfl_sync(0xffffffffu, at, leader);
+    if (mine) T.act[(size_t)cc * T.nhalf + at + __popc(m & ((1u << lane) - 1))] = hs;
+  }
+}
+
+// prefix over tanks of the active counts of both colours (one block), for the sweeps' item → tank map
+__global__ void k_act_prefix(const TankDev* __restrict__ tanks, int ntanks, int* __restrict__ apfx) {
+  __shared__ int s[1024];
+  for (int cc = 0; cc < 2; ++cc) {
+    int carry = 0;
+    int* pfx = apfx + cc * (ntanks + 1);
+    for (int base = 0; base < ntanks; base += blockDim.x) {
+      const int t = base + threadIdx.x;
+      const int v = t < ntanks ? tanks[t].ctr->n_act[cc] : 0;
+      s[threadIdx.x] = v;
+      __syncthreads();
+      for (int o = 1; o < blockDim.x; o <<= 1) {
+        const int a = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
+        __syncthreads();
+        s[threadIdx.x] += a;
+        __syncthreads();
+      }
+      if (t < ntanks) pfx[t] = carry + s[threadIdx.x] - v;
+      carry += s[blockDim.x - 1];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) pfx[ntanks] = carry;
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------------------------------------- projection
@@ -392,6 +436,7 @@ void launch_grid_nodes(const LaunchCtx& L) {
 }
 void launch_grid_cells(const LaunchCtx& L) {
   k_grid_cells<<<L.nblocks[kFamCells], kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.bpfx[kFamCells]);
+  k_act_prefix<<<1, 1024, 0, L.stream>>>(L.tanks, L.ntanks, L.apfx);
 }
 void launch_project(const LaunchCtx& L) {
   k_project<<<L.nblocks[kFamNodes], kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.bpfx[kFamNodes]);

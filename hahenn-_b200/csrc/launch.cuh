@@ -27,6 +27,7 @@ struct LaunchCtx {
   long long* scan_bsum;     // device: one partial sum per scan block
   int particle_blocks;      // persistent grid for particle kernels
   int* hpfx;                // device: ntanks+1 prefix of colour slots (nhalf) for the persistent SOR
+  int* apfx;                // device: 2·(ntanks+1), per colour the prefix of the active cells (this sub-step)
   GridBarrier* barrier;     // device: grid barrier of the persistent SOR
 };
 

@@ -88,58 +88,52 @@ __device__ __forceinline__ void sor_cell(const TankDev& T, int color, int s) {
 // written by kernels that completed before the first sweep, which is launched without the attribute), so
 // that part overlaps the previous sweep; after the wait, which returns once the previous sweep has
 // completed and its writes are visible, it reads the pressures, one round of loads, and writes its own.
-__global__ void __launch_bounds__(kSorThreads) k_sor(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx,
-                                                  int color, int sweep) {
+__global__ void __launch_bounds__(kSorThreads) k_sor(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ apfx,
+                                                     int color, int sweep) {
+  // thread q relaxes the q-th active cell of this colour over all tanks (the cell pass listed them);
+  // blocks past the active cells leave at once, so the blocks of consecutive sweeps fit on the GPU together
+  const int* __restrict__ pfx = apfx + color * (ntanks + 1);
+  const int q = blockIdx.x * kSorThreads + threadIdx.x;
+  if ((int)(blockIdx.x * kSorThreads) >= pfx[ntanks]) return;
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  const int t = find_slot(bpfx, ntanks, blockIdx.x);
+  const bool live = q < pfx[ntanks];
+  const int t = find_slot(pfx, ntanks, live ? q : 0);
   const TankDev& T = tanks[t];
   const int hx = T.hx, nx = T.nx, ny = T.ny, nz = T.nz, nhalf = T.nhalf;
-  const bool on = sweep < T.iters;
+  const bool on = live && sweep < T.iters;
   float* const pres = T.pres;
   const float omega = T.omega;
-  // kSorPer slots per thread, a block's slots contiguous (kSorThreads apart per thread)
-  int ti[kSorPer], row[kSorPer], jj[kSorPer], kk[kSorPer], ii[kSorPer];
-  uint32_t code[kSorPer];
-  float rhs[kSorPer], C[kSorPer][6];
-#pragma unroll
-  for (int u = 0; u < kSorPer; ++u) {
-    const int s = (blockIdx.x - bpfx[t]) * (kSorThreads * kSorPer) + u * kSorThreads + threadIdx.x;
-    row[u] = divu(s, T.dhx); ti[u] = s - row[u] * hx;
-    kk[u] = divu(row[u], T.dny); jj[u] = row[u] - kk[u] * ny;
-    ii[u] = 2 * ti[u] + ((jj[u] + kk[u] + color) & 1);
-    code[u] = 0; rhs[u] = 0.f;
-    if (on && s < nhalf && ii[u] < nx) {
-      code[u] = T.code[(size_t)color * nhalf + s];
-      rhs[u] = T.rhs[(size_t)color * nhalf + s];
-    }
+  int s = 0;
+  uint32_t code = 0;
+  float rhs = 0.f;
+  if (on) {
+    s = T.act[(size_t)color * nhalf + (q - pfx[t])];
+    code = T.code[(size_t)color * nhalf + s];
+    rhs = T.rhs[(size_t)color * nhalf + s];
   }
+  const int row = divu(s, T.dhx), ti = s - row * hx;
+  const int k = divu(row, T.dny), j = row - k * ny;
+  const int i = 2 * ti + ((j + k + color) & 1);
+  float C[6];
+  if (code & kCodePartial) {
+    cut_coeffs(T, i, j, k, C);
+  } else {
 #pragma unroll
-  for (int u = 0; u < kSorPer; ++u) {
-    if (code[u] & kCodePartial) {
-      cut_coeffs(T, ii[u], jj[u], kk[u], C[u]);
-    } else {
-#pragma unroll
-      for (int d = 0; d < 6; ++d) C[u][d] = (code[u] >> d) & 1u ? 1.0f : 0.0f;
-    }
+    for (int d = 0; d < 6; ++d) C[d] = (code >> d) & 1u ? 1.0f : 0.0f;
   }
   asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (!on) return;
   const float* __restrict__ po = pres + (size_t)(1 - color) * nhalf;
-  float nb[kSorPer][6], p[kSorPer];
-#pragma unroll
-  for (int u = 0; u < kSorPer; ++u) {
-    if (!(code[u] & kCodeActive)) continue;
-    const int i = ii[u], j = jj[u], k = kk[u], rowb = hx * row[u];
-    nb[u][0] = i > 0 ? po[((i - 1) >> 1) + rowb] : 0.f;
-    nb[u][1] = i + 1 < nx ? po[((i + 1) >> 1) + rowb] : 0.f;
-    nb[u][2] = j > 0 ? po[ti[u] + rowb - hx] : 0.f;
-    nb[u][3] = j + 1 < ny ? po[ti[u] + rowb + hx] : 0.f;
-    nb[u][4] = k > 0 ? po[ti[u] + rowb - hx * ny] : 0.f;
-    nb[u][5] = k + 1 < nz ? po[ti[u] + rowb + hx * ny] : 0.f;
-    p[u] = pres[(size_t)color * nhalf + ti[u] + rowb];
-  }
-#pragma unroll
-  for (int u = 0; u < kSorPer; ++u)
-    if (code[u] & kCodeActive) pres[(size_t)color * nhalf + ti[u] + hx * row[u]] = sor_update(C[u], nb[u], rhs[u], p[u], omega);
+  const int rowb = hx * row;
+  float nb[6];
+  nb[0] = i > 0 ? po[((i - 1) >> 1) + rowb] : 0.f;
+  nb[1] = i + 1 < nx ? po[((i + 1) >> 1) + rowb] : 0.f;
+  nb[2] = j > 0 ? po[ti + rowb - hx] : 0.f;
+  nb[3] = j + 1 < ny ? po[ti + rowb + hx] : 0.f;
+  nb[4] = k > 0 ? po[ti + rowb - hx * ny] : 0.f;
+  nb[5] = k + 1 < nz ? po[ti + rowb + hx * ny] : 0.f;
+  const float p = pres[(size_t)color * nhalf + s];
+  pres[(size_t)color * nhalf + s] = sor_update(C, nb, rhs, p, omega);
 }
 
 constexpr unsigned kSpinLimit = 1u << 22;
@@ -427,7 +421,7 @@ void launch_sor_sweep(const LaunchCtx& L, int color, int sweep) {
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = (color | sweep) ? 1 : 0;     // the first sweep waits for the grid pass in full
-  cudaLaunchKernelEx(&cfg, k_sor, L.tanks, L.ntanks, (const int*)L.bpfx[kFamSor], color, sweep);
+  cudaLaunchKernelEx(&cfg, k_sor, L.tanks, L.ntanks, (const int*)L.apfx, color, sweep);
 }
 
 int sor_persist_max_blocks(int device) {
