@@ -153,6 +153,7 @@ __global__ void __launch_bounds__(kThreads) k_p2g(const TankDev* __restrict__ ta
   }
   __syncthreads();
   const int total = s_rowp[kBrick * kBrick];
+  if (total == 0) return;                      // an empty brick adds nothing
   const int nsx = T.nx + 1, nsy = T.ny + 1, nsz = T.nz + 1;
   // Walk the brick's particles in a strided permutation q = j·P mod total (P coprime to total, about a
   // warp's share apart): consecutive lanes of a warp then take particles of cells far apart, so their
@@ -274,7 +275,10 @@ __global__ void __launch_bounds__(kThreads) k_grid_nodes(const TankDev* __restri
     fl[a] = f[a] * v[a] + (1 - f[a]) * s[a];
   }
 #pragma unroll
-  for (int a = 0; a < 6; ++a) acc[a * nn + n] = 0;
+  for (int a = 0; a < 3; ++a) {            // a node no particle reached is zero already
+    if (W[a]) acc[(3 + a) * nn + n] = 0;
+    if (M[a]) acc[a * nn + n] = 0;
+  }
   double* __restrict__ flux = T.flux;
 #pragma unroll
   for (int a = 0; a < 3; ++a) flux[a * nn + n] = fl[a];
