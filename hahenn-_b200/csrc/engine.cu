@@ -818,7 +818,7 @@ int blocks_for(int fam, const TankDev& D) {
     case kFamHalf: return (D.nhalf + kThreads - 1) / kThreads;
     case kFamBricks: return ((D.nx + kBrick - 1) / kBrick) * ((D.ny + kBrick - 1) / kBrick) * ((D.nz + kBrick - 1) / kBrick);
     case kFamScan: return (D.ncells + 1 + kScanTile - 1) / kScanTile;
-    case kFamSor: return (D.nhalf + kSorThreads * kSorPer - 1) / (kSorThreads * kSorPer);
+    case kFamSor: return (D.nhalf + kSorThreads - 1) / kSorThreads;     // one active cell per thread at most
     case kFamTiles: return ((D.nx + kTbX - 1) / kTbX) * ((D.ny + kTbY - 1) / kTbY) * ((D.nz + kTbZ - 1) / kTbZ);
   }
   return 0;

@@ -13,7 +13,6 @@ constexpr int kTbThreads = 512;
 
 // block families: blocks of one launch are laid out tank after tank; pfx[t] = first block of tank t
 constexpr int kSorThreads = 256;        // block size of a per-sweep SOR launch (128, 512, 1024 measured slower)
-constexpr int kSorPer = 1;               // colour slots per thread of a per-sweep SOR launch (2 and 4 measured slower)
 enum Family { kFamNodes = 0, kFamCells, kFamHalf, kFamBricks, kFamScan, kFamTiles, kFamSor, kFamCount };
 
 struct LaunchCtx {
