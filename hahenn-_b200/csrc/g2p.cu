@@ -9,6 +9,8 @@
 //
 // Spawning randomness is the reference WGSL's integer hash (src/js/30-wgsl-sim.js:36-37) seeded by the
 // particle's carried id and the sub-step number, so it does not depend on particle order.
+#include <algorithm>
+
 #include "launch.cuh"
 #include "sdf.cuh"
 
@@ -420,8 +422,23 @@ __global__ void k_whitewater_end(const TankDev* __restrict__ tanks, int ntanks) 
   c->ww_cur ^= 1;
 }
 
+// k_g2p's grid: at most the blocks that fit on the GPU at once (its register count allows fewer per SM
+// than the other particle kernels), so that the grid-stride loop runs in one wave
+int g2p_blocks(const LaunchCtx& L) {
+  static int resident[128] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 128 && !resident[dev]) {
+    int per_sm = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_g2p, kThreads, 0);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    resident[dev] = std::max(1, per_sm * sms);
+  }
+  return std::min(L.particle_blocks, dev >= 0 && dev < 128 ? resident[dev] : L.particle_blocks);
+}
+
 void launch_g2p(const LaunchCtx& L) {
-  k_g2p<<<L.particle_blocks, kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_sorted);
+  k_g2p<<<g2p_blocks(L), kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_sorted);
 }
 void launch_whitewater(const LaunchCtx& L, double frame_dt) {
   k_whitewater<<<L.particle_blocks, kThreads, 0, L.stream>>>(L.tanks, L.ntanks, frame_dt);
