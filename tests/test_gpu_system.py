@@ -94,6 +94,13 @@ def test_serving_budget_admission(pkg):
     big = dict(prm, nx=128, ny=128, nz=128, h=1 / 128, capacity=20_000_000)
     j = srv.submit(sc, big, em, steps=1)
     assert srv.poll(j)['state'] == 'failed'
+    # a malformed scene is refused at submission with a parse error; the server keeps serving
+    with pytest.raises(pkg.native.SuiriError) as e:
+        srv.submit('{"scene": {"tank": ', prm, em, steps=1)
+    assert e.value.code == -5
+    k = srv.submit(sc, prm, em, steps=2)
+    srv.wait(k)
+    assert srv.poll(k)['state'] == 'done'
     srv.close()
 
 
