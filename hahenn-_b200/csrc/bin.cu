@@ -232,8 +232,10 @@ void launch_begin_substep(const LaunchCtx& L) {
 void launch_begin_count(const LaunchCtx& L) {
   k_begin_substep<<<1, 1024, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_in, 0);
 }
+// binning and scatter are chains of dependent loads per particle: as many resident threads as fit
 void launch_bin(const LaunchCtx& L) {
-  k_bin<<<L.particle_blocks, kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_in);
+  static int resident[128] = {};
+  k_bin<<<resident_grid((const void*)k_bin, resident), kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_in);
 }
 void launch_scan(const LaunchCtx& L) {
   const int nb = L.nblocks[kFamScan];
@@ -241,7 +243,8 @@ void launch_scan(const LaunchCtx& L) {
   k_scan_b<<<nb, kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.bpfx[kFamScan], L.scan_bsum);
 }
 void launch_scatter(const LaunchCtx& L) {
-  k_scatter<<<L.particle_blocks, kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_in);
+  static int resident[128] = {};
+  k_scatter<<<resident_grid((const void*)k_scatter, resident), kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_in);
 }
 void launch_sorted_prefix(const LaunchCtx& L) {
   k_sorted_prefix<<<1, 1024, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_sorted);

@@ -426,15 +426,7 @@ __global__ void k_whitewater_end(const TankDev* __restrict__ tanks, int ntanks) 
 // than the other particle kernels), so that the grid-stride loop runs in one wave
 int g2p_blocks(const LaunchCtx& L) {
   static int resident[128] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 128 && !resident[dev]) {
-    int per_sm = 0, sms = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_g2p, kThreads, 0);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    resident[dev] = std::max(1, per_sm * sms);
-  }
-  return std::min(L.particle_blocks, dev >= 0 && dev < 128 ? resident[dev] : L.particle_blocks);
+  return std::min(L.particle_blocks, resident_grid((const void*)k_g2p, resident));
 }
 
 void launch_g2p(const LaunchCtx& L) {

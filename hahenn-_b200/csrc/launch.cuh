@@ -30,6 +30,21 @@ struct LaunchCtx {
   GridBarrier* barrier;     // device: grid barrier of the persistent SOR
 };
 
+// Blocks of kThreads threads of kernel k that fit on the current GPU at once (cached per device in cache[]).
+// The grid-stride particle kernels are launched with this many blocks: all resident, one wave.
+inline int resident_grid(const void* k, int* cache) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 128) return 1;
+  if (!cache[dev]) {
+    int per_sm = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, 0);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cache[dev] = per_sm * sms > 0 ? per_sm * sms : 1;
+  }
+  return cache[dev];
+}
+
 // per-kernel launchers (bin.cu, grid.cu, sor.cu, g2p.cu)
 void launch_begin_substep(const LaunchCtx& L);
 void launch_begin_count(const LaunchCtx& L);   // prefix only, for a count pass between sub-steps
