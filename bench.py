@@ -490,15 +490,17 @@ def main():
             t2.stats()
         nA = t2.stats()['count']
         h2d = d2h = 0
+        readback = int(P.native.lib().suiri_stats_readback_bytes())
         t0 = time.perf_counter()
         for _ in range(args.steps):
             for e in w['emitters']:
                 p, v = faucet_particles(e, dt, rng)
                 t2.add_particles(p, v)
-                h2d += p.nbytes + v.nbytes
+                h2d += 32 * len(p)            # staged as two float4 per particle
             t2.substep(dt)
-            t2.stats()
-            d2h += 128
+            t2.poll_stats()                   # the step's stats read, collected without waiting (pollStats)
+            d2h += readback
+        t2.sync()
         el = time.perf_counter() - t0
         nB = t2.stats()['count']
         e2e_rate = 0.5 * (nA + nB) * args.steps / el

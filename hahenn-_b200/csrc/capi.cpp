@@ -129,6 +129,31 @@ Tank* T(suiri_tank* h) {
 
 }  // namespace
 
+namespace {
+// the public stats from a copy of the device counters (alive = A without the dead flags + pending
+// emissions: A's dead are only known after binning; n_sorted counts them out once the next sub-step, or a
+// count pass, has run)
+void fill_stats(Tank& t, const Counters& c, suiri_stats* s) {
+  if (c.vmax_bits64 != 0ull) {
+    const unsigned long long b = c.vmax_bits64 - 1ull;
+    memcpy(&t.vmax, &b, 8);
+  }
+  const long long alive = (long long)c.n_live + c.n_emit;
+  memset(s, 0, sizeof(*s));
+  s->count = alive;
+  s->ww_count = std::min<long long>(c.ww_count, t.d.ww_cap);
+  s->impacts = c.impacts;
+  s->vmax = t.vmax;
+  s->time = t.time;
+  s->liters = alive * t.d.vp * 1000;
+  s->full = c.full;
+  s->frame = c.frame;
+  s->errors = c.err;
+  s->nx = t.d.nx; s->ny = t.d.ny; s->nz = t.d.nz; s->h = t.d.h;
+  s->origin[0] = t.d.ox; s->origin[1] = t.d.oy; s->origin[2] = t.d.oz;
+}
+}  // namespace
+
 extern "C" {
 
 int suiri_params_default(suiri_params* p) {
@@ -400,31 +425,22 @@ int suiri_get_stats(suiri_tank* h, suiri_stats* s) {
     Tank* t = T(h);
     if (!s) throw Error(SUIRI_ERR_INVALID, "null stats");
     t->read_counters();
-    const Counters& c = *t->h_ctr;
-    if (c.vmax_bits64 != 0ull) {
-      const unsigned long long b = c.vmax_bits64 - 1ull;
-      memcpy(&t->vmax, &b, 8);
-    }
-    long long alive = 0;
-    {
-      // alive = A without the dead flags + pending emissions: A's dead are only known after binning,
-      // n_sorted counts them out once the next sub-step (or a count pass) has run
-      alive = (long long)c.n_live + c.n_emit;
-    }
-    memset(s, 0, sizeof(*s));
-    s->count = alive;
-    s->ww_count = std::min<long long>(c.ww_count, t->d.ww_cap);
-    s->impacts = c.impacts;
-    s->vmax = t->vmax;
-    s->time = t->time;
-    s->liters = alive * t->d.vp * 1000;
-    s->full = c.full;
-    s->frame = c.frame;
-    s->errors = c.err;
-    s->nx = t->d.nx; s->ny = t->d.ny; s->nz = t->d.nz; s->h = t->d.h;
-    s->origin[0] = t->d.ox; s->origin[1] = t->d.oy; s->origin[2] = t->d.oz;
+    fill_stats(*t, *t->h_ctr, s);
   });
 }
+
+int suiri_poll_stats(suiri_tank* h, suiri_stats* s, int32_t* fresh) {
+  return guard(h ? &h->err : nullptr, [&] {
+    Tank* t = T(h);
+    if (!s) throw Error(SUIRI_ERR_INVALID, "null stats");
+    Counters c;
+    const bool f = t->poll_counters(c);
+    if (fresh) *fresh = f ? 1 : 0;
+    if (f) fill_stats(*t, c, s);
+  });
+}
+
+size_t suiri_stats_readback_bytes(void) { return sizeof(Counters); }
 
 int suiri_snapshot(suiri_tank* h, int32_t* id) {
   return guard(h ? &h->err : nullptr, [&] {

@@ -310,7 +310,12 @@ Tank::~Tank() {
   if (snap.p) { cudaFree(snap.p); cudaFree(snap.v); cudaFree(snap.wp); cudaFree(snap.wv); cudaFree(snap.pres); cudaFree(snap.ripple); }
   free_ripple(*this);
   if (h_ctr) cudaFreeHost(h_ctr);
-  if (h_stage_p) { cudaFreeHost(h_stage_p); cudaFreeHost(h_stage_v); }
+  for (int k = 0; k < 2; ++k) {
+    if (h_stage_p[k]) { cudaFreeHost(h_stage_p[k]); cudaFreeHost(h_stage_v[k]); }
+    if (stage_ev[k]) cudaEventDestroy(stage_ev[k]);
+  }
+  if (h_poll) cudaFreeHost(h_poll);
+  if (poll_ev) cudaEventDestroy(poll_ev);
   if (ev_own) cudaEventDestroy(ev_own);
   if (stream && own_stream) cudaStreamDestroy(stream);
 }
@@ -407,6 +412,31 @@ void Tank::read_counters() {
   n_upper = h_ctr->n_live + h_ctr->n_emit;
 }
 
+bool Tank::poll_counters(Counters& out) {
+  join();
+  bool fresh = false;
+  if (poll_pending) {
+    const cudaError_t q = cudaEventQuery(poll_ev);
+    if (q == cudaSuccess) {
+      out = *h_poll;
+      fresh = true;
+      poll_pending = false;
+    } else if (q != cudaErrorNotReady) {
+      CK(q);
+    }
+  }
+  if (!poll_pending) {
+    if (!h_poll) {
+      CK(cudaMallocHost(&h_poll, sizeof(Counters)));
+      CK(cudaEventCreateWithFlags(&poll_ev, cudaEventDisableTiming));
+    }
+    CK(cudaMemcpyAsync(h_poll, d.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
+    CK(cudaEventRecord(poll_ev, stream));
+    poll_pending = true;
+  }
+  return fresh;
+}
+
 void Tank::stage(const float4* p, const float4* v, long long n) {
   join();
   if (n <= 0) return;
@@ -429,24 +459,31 @@ void Tank::add_particles(const float* pos, const float* vel, const float* air, l
     room = std::min<long long>(cfg.cap - n_upper, emit_cap - n_emit_host);
   }
   long long take = std::max(0LL, std::min(n, room));
-  if ((size_t)take > stage_cap) {
-    if (h_stage_p) { CK(cudaStreamSynchronize(stream)); cudaFreeHost(h_stage_p); cudaFreeHost(h_stage_v); }
-    stage_cap = (size_t)take;
-    CK(cudaMallocHost(&h_stage_p, stage_cap * 16));
-    CK(cudaMallocHost(&h_stage_v, stage_cap * 16));
-  } else {
-    CK(cudaStreamSynchronize(stream));     // the staging buffer may still feed an earlier copy
+  // two pinned staging buffers in turn: a buffer is refilled once the copies out of it two calls ago have
+  // finished (an event, not a wait for the whole stream, so the host stays ahead of the device)
+  const int k = stage_k;
+  stage_k ^= 1;
+  if (stage_ev[k]) CK(cudaEventSynchronize(stage_ev[k]));
+  else CK(cudaEventCreateWithFlags(&stage_ev[k], cudaEventDisableTiming));
+  if ((size_t)take > stage_cap[k]) {
+    if (h_stage_p[k]) { cudaFreeHost(h_stage_p[k]); cudaFreeHost(h_stage_v[k]); }
+    stage_cap[k] = (size_t)take;
+    CK(cudaMallocHost(&h_stage_p[k], stage_cap[k] * 16));
+    CK(cudaMallocHost(&h_stage_v[k], stage_cap[k] * 16));
   }
+  float4* sp = h_stage_p[k];
+  float4* sv = h_stage_v[k];
   for (long long i = 0; i < take; ++i) {
     const float a = air ? air[i] : 0.f;
-    h_stage_p[i] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], a > 0.5f ? (float)kFlagAir : 0.f);
+    sp[i] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], a > 0.5f ? (float)kFlagAir : 0.f);
     const float vx = vel ? vel[3 * i] : 0.f, vy = vel ? vel[3 * i + 1] : 0.f, vz = vel ? vel[3 * i + 2] : 0.f;
     uint32_t id = next_id + (uint32_t)i;
     float idf;
     memcpy(&idf, &id, 4);
-    h_stage_v[i] = make_float4(vx, vy, vz, idf);
+    sv[i] = make_float4(vx, vy, vz, idf);
   }
-  stage(h_stage_p, h_stage_v, take);
+  stage(sp, sv, take);
+  CK(cudaEventRecord(stage_ev[k], stream));
   next_id += (uint32_t)take;
   if (take < n) {
     h_ctr->full = 1;

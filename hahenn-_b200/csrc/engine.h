@@ -84,8 +84,13 @@ struct Tank {
   uint32_t next_id = 0;
   long long n_emit_host = 0;      // particles staged in E for the next sub-step
   long long n_upper = 0;          // upper bound of live particles (exact after a stats read)
-  float4 *h_stage_p = nullptr, *h_stage_v = nullptr;
-  size_t stage_cap = 0;
+  float4 *h_stage_p[2] = {}, *h_stage_v[2] = {};   // pinned staging of added particles, used in turn
+  size_t stage_cap[2] = {};
+  cudaEvent_t stage_ev[2] = {};   // the copies out of each staging buffer have finished
+  int stage_k = 0;
+  Counters* h_poll = nullptr;     // pinned target of the asynchronous counter read
+  cudaEvent_t poll_ev = nullptr;
+  bool poll_pending = false;
   std::string err;
   Group* solo = nullptr;
   bool use_graphs = true;
@@ -111,6 +116,7 @@ struct Tank {
   void set_objects(const std::vector<Obj>& o);
   void set_lattice(const double* sdf, const int* oid, int lx, int ly, int lz);
   void read_counters();           // synchronous
+  bool poll_counters(Counters& out);   // non-blocking: the last finished read into out (true); starts the next
   void add_particles(const float* pos, const float* vel, const float* air, long long n, uint32_t* first);
   void stage(const float4* p, const float4* v, long long n);
   void emit_block(const double lo[3], const double hi[3], bool fill);

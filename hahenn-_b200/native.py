@@ -95,6 +95,8 @@ SIGNATURES = {
     'suiri_read_whitewater': (C.c_int, [P, P, P, C.c_int64, C.POINTER(C.c_int64)]),
     'suiri_read_grid': (C.c_int, [P, C.c_int32, P, C.c_size_t]),
     'suiri_get_stats': (C.c_int, [P, C.POINTER(Stats)]),
+    'suiri_poll_stats': (C.c_int, [P, C.POINTER(Stats), C.POINTER(C.c_int32)]),
+    'suiri_stats_readback_bytes': (C.c_size_t, []),
     'suiri_snapshot': (C.c_int, [P, C.POINTER(C.c_int32)]),
     'suiri_restore': (C.c_int, [P, C.c_int32]),
     'suiri_stream': (C.c_int, [P, C.POINTER(P)]),

@@ -250,11 +250,22 @@ class Tank:
         self._c(N.lib().suiri_read_grid(self._h, field, _ptr(out), out.nbytes))
         return out
 
+    @staticmethod
+    def _stats_dict(s):
+        return dict(count=s.count, ww_count=s.ww_count, impacts=s.impacts, vmax=s.vmax, time=s.time, liters=s.liters,
+                    full=bool(s.full), frame=s.frame, errors=s.errors, nx=s.nx, ny=s.ny, nz=s.nz, h=s.h, origin=tuple(s.origin))
+
     def stats(self):
         s = N.Stats()
         self._c(N.lib().suiri_get_stats(self._h, C.byref(s)))
-        return dict(count=s.count, ww_count=s.ww_count, impacts=s.impacts, vmax=s.vmax, time=s.time, liters=s.liters,
-                    full=bool(s.full), frame=s.frame, errors=s.errors, nx=s.nx, ny=s.ny, nz=s.nz, h=s.h, origin=tuple(s.origin))
+        return self._stats_dict(s)
+
+    def poll_stats(self):
+        """Non-blocking (FluidSim.pollStats): the stats of the read the previous call started, or None if it
+        has not finished; every call starts a new read behind the work enqueued so far."""
+        s, fresh = N.Stats(), C.c_int32(0)
+        self._c(N.lib().suiri_poll_stats(self._h, C.byref(s), C.byref(fresh)))
+        return self._stats_dict(s) if fresh.value else None
 
     @property
     def water_liters(self):

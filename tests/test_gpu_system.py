@@ -201,6 +201,48 @@ def test_empty_tank_steps_cleanly(pkg):
     t.close()
 
 
+def test_poll_stats_and_pipelined_particle_adds(pkg):
+    """Non-blocking stats (pollStats): the first call only starts a read; once the stream is idle the next
+    call returns exactly what the blocking read returns. Particles added every sub-step through the two
+    staging buffers, without waits in between, all arrive with their ids and values."""
+    w = pkg.workloads.dam_break()
+    t = pkg.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], whitewater=False, ripple=None,
+                 capacity=len(w['pos']) + 4096, iters=20)
+    t.add_particles(w['pos'])
+    assert t.poll_stats() is None
+    rng = np.random.default_rng(3)
+    added = []
+    for _ in range(12):
+        p = (np.array([0.0, 0.8, 0.0]) + rng.uniform(-0.05, 0.05, (7, 3))).astype(np.float32)
+        v = np.tile(np.float32([0.0, -1.0, 0.0]), (7, 1))
+        added.append(p)
+        t.add_particles(p, v)
+        t.substep(1 / 240)
+        t.poll_stats()
+    t.sync()
+    st = t.poll_stats()
+    ref = t.stats()
+    assert st is not None and st == ref
+    assert ref['count'] == len(w['pos']) + 12 * 7 and ref['frame'] == 12
+    pos, vel, air, ids = t.particles()
+    assert len(np.unique(ids)) == len(ids) and ids.max() == len(w['pos']) + 12 * 7 - 1
+    t.close()
+    # the same adds, staged one at a time with a sync after each, give the same particles bit for bit
+    u = pkg.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], whitewater=False, ripple=None,
+                 capacity=len(w['pos']) + 4096, iters=20)
+    u.add_particles(w['pos'])
+    for p in added:
+        u.add_particles(p, np.tile(np.float32([0.0, -1.0, 0.0]), (7, 1)))
+        u.sync()
+        u.substep(1 / 240)
+        u.sync()
+    pu, vu, au, iu = u.particles()
+    o, ou = np.argsort(ids), np.argsort(iu)
+    np.testing.assert_array_equal(pos[o], pu[ou])
+    np.testing.assert_array_equal(vel[o], vu[ou])
+    u.close()
+
+
 def test_capacity_reached_sets_full_and_caps_the_count(pkg):
     """An emitter that outruns the particle capacity: emission stops at the capacity (minus its margin),
     the full flag is raised, and the step keeps running."""
