@@ -506,6 +506,7 @@ static void tune_group(Group& g, int32_t particle_blocks_per_sm, int32_t sor_mod
   CK(cudaStreamSynchronize(g.stream));
   g.blocks_per_sm = particle_blocks_per_sm;
   g.ctx.particle_blocks = particle_blocks_per_sm * g.sm_count;
+  if (sor_mode == 2) g.ensure_tbl();
   g.sor_mode = sor_mode;
   g.drop_graph();
 }

@@ -922,8 +922,17 @@ Group::~Group() {
     cudaEventDestroy(ev_done);
   }
   cudaFree(d_hpfx); cudaFree(d_apfx); cudaFree(d_barrier);
+  if (d_tbl) cudaFree(d_tbl);
   cudaFree(d_tanks); cudaFreeHost(h_tanks); cudaFree(d_bpfx); cudaFree(d_ppfx); cudaFree(d_bsum);
   if (own_stream) cudaStreamDestroy(stream);
+}
+
+void Group::ensure_tbl() {
+  if (d_tbl) return;
+  CK(cudaSetDevice(device));
+  const int tiles = std::max(1, ctx.nblocks[kFamTiles]);
+  CK(cudaMalloc(&d_tbl, tbl_list_bytes(tiles)));
+  tbl_assign(ctx, d_tbl, tiles);
 }
 
 void Group::set_profile(bool on) {
@@ -1011,6 +1020,7 @@ void Group::enqueue_body() {
   } else if (sor_mode == 2 || sor_mode == 3) {
     // S sweeps per launch; launch l reads pres (l even) or pres2 and writes the other; an odd count ends in pres2
     const int S = sor_mode == 2 ? 2 : 4;
+    if (S == 2) launch_tbl_lists(ctx);
     const int sweeps = 2 * max_iters, nl = (sweeps + S - 1) / S;
     for (int l = 0; l < nl; ++l) launch_sor_tb(ctx, S, l * S, std::min(S, sweeps - l * S), l & 1);
     if (nl & 1) launch_sor_copy(ctx);

@@ -152,6 +152,8 @@ struct Group {
   cudaEvent_t ev_done = nullptr;  // recorded after every sub-step (tanks on other streams wait for it)
   int* d_hpfx = nullptr;          // colour-slot prefix for the persistent SOR
   int* d_apfx = nullptr;          // per colour, prefix of the active cells over the tanks
+  void* d_tbl = nullptr;          // per-tile lists of the two-sweeps-per-launch solve (allocated when tuned to it)
+  void ensure_tbl();
   GridBarrier* d_barrier = nullptr;
   int sor_mode = 0;               // 0: one launch per colour sweep, 1: one cooperative launch per solve,
                                   // 2, 3: 2 or 4 sweeps per launch (temporal blocking)

@@ -28,6 +28,9 @@ struct LaunchCtx {
   int* hpfx;                // device: ntanks+1 prefix of colour slots (nhalf) for the persistent SOR
   int* apfx;                // device: 2·(ntanks+1), per colour the prefix of the active cells (this sub-step)
   GridBarrier* barrier;     // device: grid barrier of the persistent SOR
+  uint2* tbl_list;          // device, two sweeps per launch: per tile the active-cell lists (k_tbl_lists)
+  int* tbl_cnt;             //   per tile: entries of list A, B, C
+  int2* tbl_c;              //   per tile: colour-0 cells with a constant pressure other than +0
 };
 
 // Blocks of kThreads threads of kernel k that fit on the current GPU at once (cached per device in cache[]).
@@ -62,6 +65,9 @@ int sor_persist_max_blocks(int device);                                  // co-r
 cudaError_t sor_tb_prepare();                                            // once per device, outside capture
 void launch_sor_tb(const LaunchCtx& L, int sweeps_per_launch, int sweep0, int nsweeps, int dir);  // 2 or 4; dir 0: pres→pres2
 void launch_sor_copy(const LaunchCtx& L);                                // pres ← pres2
+void launch_tbl_lists(const LaunchCtx& L);                               // per sub-step, before a 2-sweep solve
+size_t tbl_list_bytes(int tiles);                                        // device bytes of those lists
+void tbl_assign(LaunchCtx& L, void* base, int tiles);                    // point the context into them
 void launch_project(const LaunchCtx& L);
 void launch_g2p(const LaunchCtx& L);
 void launch_whitewater(const LaunchCtx& L, double frame_dt);

@@ -16,14 +16,15 @@
 // Most cells have every face either closed or fully open; their coefficients come from the 6 "open"
 // bits of the code and the float fractions are only read for cut cells next to obstacles.
 //
-// Three launch forms, all giving the same pressures bit for bit (the tuner picks one):
+// Four launch forms, all giving the same pressures bit for bit (the tuner picks one):
 //   k_sor          one colour of every tank per launch (2·iters launches per solve, in the sub-step graph),
 //                  with programmatic dependent launch between sweeps; over the listed active cells, the
 //                  grid capped at the blocks resident at once (threads loop past it)
 //   k_sor_persist  the whole solve in one cooperative launch: all blocks resident, a grid barrier after
 //                  every colour sweep. The barrier's wait is bounded: after kSpinLimit polls it records
 //                  an error in the tank counters and every block returns.
-//   k_sor_tb<S>    S = 2 or 4 sweeps per launch on shared-memory tiles with halos (temporal blocking)
+//   k_sor_tbl      two sweeps per launch over per-tile lists of active cells (temporal blocking)
+//   k_sor_tb<4>    four sweeps per launch on shared-memory tiles with halos
 #include "launch.cuh"
 
 namespace suiri {
@@ -386,6 +387,272 @@ __global__ void __launch_bounds__(kTbThreads, 2) k_sor_tb(const TankDev* __restr
   }
 }
 
+// ---------------------------------------------------------------------------- two sweeps per launch, listed
+// A launch relaxes colour 0 then colour 1 (one iteration) on 16×16×8 tiles. The first sweep relaxes the
+// active colour-0 cells of the tile and of its face ring (the cells one step outside a face: the colour-0
+// neighbours of the tile's cells); ring cells are relaxed by each tile that needs them, from the same
+// operands as by their own tile, so the values agree. The second sweep relaxes the tile's active colour-1
+// cells with those neighbours from shared memory. Before griddepcontrol.wait a block only reads constant
+// data: the tile's lists, built once per sub-step by k_tbl_lists. After it, each thread issues the
+// global loads of its (at most 3) colour-0 cells together, as a per-sweep launch does for its one cell,
+// so a launch costs about one per-sweep launch for two sweeps. Pressures ping-pong between pres and pres2
+// (a neighbouring tile may still read the values this block replaces); inactive cells are constant over
+// the solve and k_tbl_lists makes the two buffers agree on them.
+//
+// List entry (uint2): x = box coordinates (bits 0-4, 5-9, 10-13: i − x0 + 1, j − y0 + 1, k − z0 + 1), open
+// bits (14-19), cut cell (20), inside the tile (21); y = rhs bits. In shared memory bits 22-30 carry the
+// cut-table index (kTblCut: not held, read from the face fractions).
+constexpr int kTblBX = kTbX + 2, kTblBY = kTbY + 2, kTblBZ = kTbZ + 2;
+constexpr int kTblBox = kTblBX * kTblBY * kTblBZ;
+constexpr int kTblCapA = kTbX * kTbY * kTbZ / 2 + kTbY * kTbZ + kTbX * kTbZ + kTbX * kTbY;   // colour 0: tile + face ring
+constexpr int kTblCapB = kTbX * kTbY * kTbZ / 2;                                           // colour 1: tile
+constexpr int kTblThreads = 512;
+constexpr int kTblCut = 256;
+constexpr int kTblPerA = (kTblCapA + kTblThreads - 1) / kTblThreads;
+constexpr int kTblPerB = (kTblCapB + kTblThreads - 1) / kTblThreads;
+static_assert(kTblBX <= 32 && kTblBY <= 32 && kTblBZ <= 16, "box coordinates fit their bits");
+
+struct TblSmem {
+  float box[kTblBox];          // colour-0 values of the box: sweep-1 results, constants of inactive cells
+  int sa[kTblCapA];            // global slots (colour 1: + nhalf)
+  int sb[kTblCapB];
+  uint2 ea[kTblCapA];          // entries as listed, cut-table index added
+  uint2 eb[kTblCapB];
+  float cut[kTblCut * 6];
+  int ncut;
+};
+
+__device__ __forceinline__ void tbl_cell(uint32_t m, int x0, int y0, int z0, int& bidx, int& i, int& j, int& k) {
+  const int bi = m & 31, bj = (m >> 5) & 31, bk = (m >> 10) & 15;
+  bidx = bi + kTblBX * (bj + kTblBY * bk);
+  i = x0 - 1 + bi;
+  j = y0 - 1 + bj;
+  k = z0 - 1 + bk;
+}
+
+__device__ __forceinline__ void tbl_coeffs(const TankDev& T, uint32_t m, const float* cut, int i, int j, int k, float C[6]) {
+  if (m & (1u << 20)) {
+    const unsigned x = (m >> 22) & 0x1FF;
+    if (x < kTblCut) {
+#pragma unroll
+      for (int d = 0; d < 6; ++d) C[d] = cut[6 * x + d];
+    } else {
+      cut_coeffs(T, i, j, k, C);
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < 6; ++d) C[d] = (m >> (14 + d)) & 1u ? 1.0f : 0.0f;
+  }
+}
+
+__device__ __forceinline__ void tbl_tile(const TankDev& T, int lt, int& x0, int& y0, int& z0) {
+  const int tnx = (T.nx + kTbX - 1) / kTbX, tny = (T.ny + kTbY - 1) / kTbY;
+  x0 = (lt % tnx) * kTbX;
+  y0 = ((lt / tnx) % tny) * kTbY;
+  z0 = (lt / (tnx * tny)) * kTbZ;
+}
+
+// Once per sub-step, before the solve: per tile, the lists of active cells (A: colour 0 in the tile and its
+// face ring; B: colour 1 in the tile), the colour-0 cells of the box whose constant pressure is not +0 (C),
+// and pres2 = pres on the tile's inactive cells.
+__global__ void __launch_bounds__(kThreads) k_tbl_lists(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx,
+                                                        uint2* __restrict__ list, int* __restrict__ cnt, int2* __restrict__ clist) {
+  __shared__ int s_na, s_nb, s_nc;
+  const int t = find_slot(bpfx, ntanks, blockIdx.x);
+  const TankDev& T = tanks[t];
+  const int nx = T.nx, ny = T.ny, nz = T.nz, hx = T.hx;
+  const size_t nh = T.nhalf;
+  int x0, y0, z0;
+  tbl_tile(T, blockIdx.x - bpfx[t], x0, y0, z0);
+  if (threadIdx.x == 0) { s_na = 0; s_nb = 0; s_nc = 0; }
+  __syncthreads();
+  uint2* la = list + (size_t)blockIdx.x * (kTblCapA + kTblCapB);
+  uint2* lb = la + kTblCapA;
+  int2* lc = clist + (size_t)blockIdx.x * kTblCapA;
+  for (int b = threadIdx.x; b < kTblBox; b += blockDim.x) {
+    const int bi = b % kTblBX, bj = (b / kTblBX) % kTblBY, bk = b / (kTblBX * kTblBY);
+    const int i = x0 - 1 + bi, j = y0 - 1 + bj, k = z0 - 1 + bk;
+    if (i < 0 || j < 0 || k < 0 || i >= nx || j >= ny || k >= nz) continue;
+    const int nout = (bi == 0 || bi == kTblBX - 1) + (bj == 0 || bj == kTblBY - 1) + (bk == 0 || bk == kTblBZ - 1);
+    const int col = (i + j + k) & 1;
+    if (nout > 1 || (col == 1 && nout == 1)) continue;        // no neighbour of a tile cell in the other colour
+    const size_t s = (size_t)col * nh + (i >> 1) + (size_t)hx * (j + (size_t)ny * k);
+    const uint32_t code = T.code[s];
+    if (code & kCodeActive) {
+      const uint32_t m = (uint32_t)(bi | (bj << 5) | (bk << 10)) | ((code & 0x3Fu) << 14) |
+                         ((code & kCodePartial) ? 1u << 20 : 0u) | (nout == 0 ? 1u << 21 : 0u);
+      const uint2 e = make_uint2(m, __float_as_uint(T.rhs[s]));
+      if (col == 0) la[atomicAdd(&s_na, 1)] = e;
+      else lb[atomicAdd(&s_nb, 1)] = e;
+    } else {
+      const float p = T.pres[s];
+      if (col == 0 && __float_as_uint(p) != 0u) lc[atomicAdd(&s_nc, 1)] = make_int2(b, __float_as_int(p));
+      if (nout == 0) T.pres2[s] = p;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    cnt[3 * blockIdx.x] = s_na;
+    cnt[3 * blockIdx.x + 1] = s_nb;
+    cnt[3 * blockIdx.x + 2] = s_nc;
+  }
+}
+
+__global__ void __launch_bounds__(kTblThreads, 2) k_sor_tbl(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx,
+                                                           const uint2* __restrict__ list, const int* __restrict__ cnt,
+                                                           const int2* __restrict__ clist, int sweep0, int dir) {
+  extern __shared__ __align__(16) unsigned char tbl_smem[];
+  TblSmem& S = *reinterpret_cast<TblSmem*>(tbl_smem);
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  const int na = cnt[3 * blockIdx.x], nb = cnt[3 * blockIdx.x + 1], nc = cnt[3 * blockIdx.x + 2];
+  if (na + nb == 0) return;                  // no active cell: nothing to relax or carry
+  const int t = find_slot(bpfx, ntanks, blockIdx.x);
+  const TankDev& T = tanks[t];
+  const int nx = T.nx, ny = T.ny, nz = T.nz, hx = T.hx;
+  const int nh = T.nhalf;
+  int x0, y0, z0;
+  tbl_tile(T, blockIdx.x - bpfx[t], x0, y0, z0);
+  const bool on = sweep0 < 2 * T.iters;    // a batch runs to its largest count; the others are carried
+  const float omega = T.omega;
+  const uint2* __restrict__ la = list + (size_t)blockIdx.x * (kTblCapA + kTblCapB);
+  const uint2* __restrict__ lb = la + kTblCapA;
+  const int2* __restrict__ lc = clist + (size_t)blockIdx.x * kTblCapA;
+  for (int b = threadIdx.x; b < kTblBox; b += kTblThreads) S.box[b] = 0.f;
+  if (threadIdx.x == 0) S.ncut = 0;
+  __syncthreads();
+  for (int e = threadIdx.x; e < nc; e += kTblThreads) {
+    const int2 v = lc[e];
+    S.box[v.x] = __int_as_float(v.y);
+  }
+  // the lists into shared memory: all of a thread's loads first
+  {
+    uint2 ea[kTblPerA], eb[kTblPerB];
+#pragma unroll
+    for (int u = 0; u < kTblPerA; ++u) {
+      const int e = threadIdx.x + u * kTblThreads;
+      ea[u] = e < na ? la[e] : make_uint2(0u, 0u);
+    }
+#pragma unroll
+    for (int u = 0; u < kTblPerB; ++u) {
+      const int e = threadIdx.x + u * kTblThreads;
+      eb[u] = e < nb ? lb[e] : make_uint2(0u, 0u);
+    }
+#pragma unroll
+    for (int u = 0; u < kTblPerA + kTblPerB; ++u) {
+      const bool isa = u < kTblPerA;
+      const int e = threadIdx.x + (isa ? u : u - kTblPerA) * kTblThreads;
+      if (e >= (isa ? na : nb)) continue;
+      uint2 en = isa ? ea[u] : eb[u - kTblPerA];
+      int bidx, i, j, k;
+      tbl_cell(en.x, x0, y0, z0, bidx, i, j, k);
+      if (en.x & (1u << 20)) {
+        const int x = atomicAdd(&S.ncut, 1);
+        if (x < kTblCut) {
+          float C[6];
+          cut_coeffs(T, i, j, k, C);
+#pragma unroll
+          for (int d = 0; d < 6; ++d) S.cut[6 * x + d] = C[d];
+        }
+        en.x |= (uint32_t)min(x, kTblCut) << 22;
+      }
+      const int s = (isa ? 0 : nh) + (i >> 1) + hx * (j + ny * k);
+      if (isa) { S.sa[e] = s; S.ea[e] = en; }
+      else { S.sb[e] = s; S.eb[e] = en; }
+    }
+  }
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  __syncthreads();
+  const float* __restrict__ pin = dir ? T.pres2 : T.pres;
+  float* __restrict__ pout = dir ? T.pres : T.pres2;
+  // every global load of the thread: own values of its colour-1 cells, neighbours and own values of its
+  // colour-0 cells
+  float pb[kTblPerB], pa[kTblPerA], nba[kTblPerA][6];
+#pragma unroll
+  for (int u = 0; u < kTblPerB; ++u) {
+    const int e = threadIdx.x + u * kTblThreads;
+    pb[u] = e < nb ? pin[S.sb[e]] : 0.f;
+  }
+  const float* __restrict__ po = pin + nh;
+#pragma unroll
+  for (int u = 0; u < kTblPerA; ++u) {
+    const int e = threadIdx.x + u * kTblThreads;
+    pa[u] = 0.f;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) nba[u][d] = 0.f;
+    if (e < na) {
+      const int s = S.sa[e];
+      int bidx, i, j, k;
+      tbl_cell(S.ea[e].x, x0, y0, z0, bidx, i, j, k);
+      const int rowb = s - (i >> 1);
+      pa[u] = pin[s];
+      if (on) {
+        nba[u][0] = i > 0 ? po[((i - 1) >> 1) + rowb] : 0.f;
+        nba[u][1] = i + 1 < nx ? po[((i + 1) >> 1) + rowb] : 0.f;
+        nba[u][2] = j > 0 ? po[(i >> 1) + rowb - hx] : 0.f;
+        nba[u][3] = j + 1 < ny ? po[(i >> 1) + rowb + hx] : 0.f;
+        nba[u][4] = k > 0 ? po[(i >> 1) + rowb - hx * ny] : 0.f;
+        nba[u][5] = k + 1 < nz ? po[(i >> 1) + rowb + hx * ny] : 0.f;
+      }
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kTblPerA; ++u) {
+    const int e = threadIdx.x + u * kTblThreads;
+    if (e >= na) continue;
+    const uint2 en = S.ea[e];
+    int bidx, i, j, k;
+    tbl_cell(en.x, x0, y0, z0, bidx, i, j, k);
+    float v = pa[u];
+    if (on) {
+      float C[6];
+      tbl_coeffs(T, en.x, S.cut, i, j, k, C);
+      v = sor_update(C, nba[u], __uint_as_float(en.y), pa[u], omega);
+    }
+    S.box[bidx] = v;
+    if (en.x & (1u << 21)) pout[S.sa[e]] = v;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < kTblPerB; ++u) {
+    const int e = threadIdx.x + u * kTblThreads;
+    if (e >= nb) continue;
+    const uint2 en = S.eb[e];
+    int bidx, i, j, k;
+    tbl_cell(en.x, x0, y0, z0, bidx, i, j, k);
+    float v = pb[u];
+    if (on) {
+      float nbv[6];
+      nbv[0] = i > 0 ? S.box[bidx - 1] : 0.f;
+      nbv[1] = i + 1 < nx ? S.box[bidx + 1] : 0.f;
+      nbv[2] = j > 0 ? S.box[bidx - kTblBX] : 0.f;
+      nbv[3] = j + 1 < ny ? S.box[bidx + kTblBX] : 0.f;
+      nbv[4] = k > 0 ? S.box[bidx - kTblBX * kTblBY] : 0.f;
+      nbv[5] = k + 1 < nz ? S.box[bidx + kTblBX * kTblBY] : 0.f;
+      float C[6];
+      tbl_coeffs(T, en.x, S.cut, i, j, k, C);
+      v = sor_update(C, nbv, __uint_as_float(en.y), pb[u], omega);
+    }
+    pout[S.sb[e]] = v;
+  }
+}
+
+void launch_tbl_lists(const LaunchCtx& L) {
+  k_tbl_lists<<<L.nblocks[kFamTiles], kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.bpfx[kFamTiles], L.tbl_list, L.tbl_cnt, L.tbl_c);
+}
+
+size_t tbl_list_bytes(int tiles) {
+  return (size_t)tiles * ((kTblCapA + kTblCapB) * sizeof(uint2) + 3 * sizeof(int) + kTblCapA * sizeof(int2));
+}
+
+void tbl_assign(LaunchCtx& L, void* base, int tiles) {
+  char* p = static_cast<char*>(base);
+  L.tbl_list = reinterpret_cast<uint2*>(p);
+  p += (size_t)tiles * (kTblCapA + kTblCapB) * sizeof(uint2);
+  L.tbl_c = reinterpret_cast<int2*>(p);
+  p += (size_t)tiles * kTblCapA * sizeof(int2);
+  L.tbl_cnt = reinterpret_cast<int*>(p);
+}
+
 // pres ← pres2 (after an odd number of temporal-blocked launches)
 __global__ void __launch_bounds__(kThreads) k_sor_copy(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx) {
   const int t = find_slot(bpfx, ntanks, blockIdx.x);
@@ -397,7 +664,7 @@ __global__ void __launch_bounds__(kThreads) k_sor_copy(const TankDev* __restrict
 }
 
 cudaError_t sor_tb_prepare() {
-  const cudaError_t e = cudaFuncSetAttribute(k_sor_tb<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, TbShape<2>::SMEM);
+  const cudaError_t e = cudaFuncSetAttribute(k_sor_tbl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TblSmem));
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_sor_tb<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, TbShape<4>::SMEM);
 }
@@ -405,16 +672,17 @@ cudaError_t sor_tb_prepare() {
 void launch_sor_tb(const LaunchCtx& L, int sweeps_per_launch, int sweep0, int nsweeps, int dir) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(L.nblocks[kFamTiles]);
-  cfg.blockDim = dim3(kTbThreads);
-  cfg.dynamicSmemBytes = sweeps_per_launch == 2 ? TbShape<2>::SMEM : TbShape<4>::SMEM;
+  cfg.blockDim = dim3(sweeps_per_launch == 2 ? kTblThreads : kTbThreads);
+  cfg.dynamicSmemBytes = sweeps_per_launch == 2 ? sizeof(TblSmem) : TbShape<4>::SMEM;
   cfg.stream = L.stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = sweep0 > 0 ? 1 : 0;     // the first launch waits for the grid pass in full
+  cfg.numAttrs = sweep0 > 0 ? 1 : 0;     // the first launch waits for the grid pass (and the lists) in full
   if (sweeps_per_launch == 2)
-    cudaLaunchKernelEx(&cfg, k_sor_tb<2>, L.tanks, L.ntanks, (const int*)L.bpfx[kFamTiles], sweep0, nsweeps, dir);
+    cudaLaunchKernelEx(&cfg, k_sor_tbl, L.tanks, L.ntanks, (const int*)L.bpfx[kFamTiles], (const uint2*)L.tbl_list,
+                       (const int*)L.tbl_cnt, (const int2*)L.tbl_c, sweep0, dir);
   else
     cudaLaunchKernelEx(&cfg, k_sor_tb<4>, L.tanks, L.ntanks, (const int*)L.bpfx[kFamTiles], sweep0, nsweeps, dir);
 }

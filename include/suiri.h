@@ -227,8 +227,9 @@ int suiri_batch_substep(suiri_batch* b, double dt);
 int suiri_batch_sync(suiri_batch* b);
 /* tuning knobs picked by the autotuner: blocks per SM of the persistent particle kernels, and the form of
    the pressure solve, sor_mode: 0 one launch per colour sweep; 1 the whole solve in one cooperative launch
-   with a grid barrier between sweeps; 2 and 3 two and four colour sweeps per launch on shared-memory tiles
-   with halos (temporal blocking). All give the same pressures bit for bit. */
+   with a grid barrier between sweeps; 2 two colour sweeps per launch over per-tile lists of active cells
+   (allocates those lists for the tank or batch, once); 3 four sweeps per launch on shared-memory tiles with
+   halos. All give the same pressures bit for bit. */
 int suiri_batch_tune(suiri_batch* b, int32_t particle_blocks_per_sm, int32_t sor_mode);
 int suiri_tune(suiri_tank* t, int32_t particle_blocks_per_sm, int32_t sor_mode);
 int suiri_batch_stream(suiri_batch* b, void** stream);
