@@ -515,7 +515,7 @@ def main():
         achieved = alg_bytes / (sor_launch_ms * 1e-3) / 1e9
         tr = sor_traffic()
         cpu_rate, cpu_el = cpu_port_rate(w, args.cpu_steps)
-        launches_per_step = 14 + 2 * prm['iters']
+        launches_per_step = 10 + 2 * prm['iters']  # the sub-step graph; dt is constant, so it is uploaded once
         line = dict(metric=METRIC, value=value, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
                     ms_per_step=ms, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
                     data='synthetic (seeded particles, analytic obstacles)',
@@ -540,7 +540,7 @@ def main():
 
 def run_for_profiler(args, local):
     """The obstacles-and-inflow tank stepped 3 + N times and synchronised: a fixed launch sequence for ncu
-    (per sub-step: 14 kernels + 2 per SOR iteration)."""
+    (per sub-step: 10 kernels + 2 per SOR iteration)."""
     P = pkg()
     w = P.workloads.obstacles_inflow()
     t = make_tank(P, w, local)

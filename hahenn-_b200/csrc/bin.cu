@@ -181,7 +181,8 @@ __global__ void __launch_bounds__(kThreads) k_scan_b(const TankDev* __restrict__
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_scatter(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ pfx) {
+__global__ void __launch_bounds__(kThreads) k_scatter(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ pfx,
+                                                      int* __restrict__ spfx, unsigned* __restrict__ ticket) {
   const int total = pfx[ntanks];
   const int stride = gridDim.x * blockDim.x;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
@@ -197,38 +198,19 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const TankDev* __restrict_
     T.pB[dst] = p;
     T.vB[dst] = v;
   }
-}
-
-__global__ void k_sorted_prefix(const TankDev* __restrict__ tanks, int ntanks, int* __restrict__ pfx) {
-  __shared__ int s[1024];
-  int carry = 0;
-  for (int base = 0; base < ntanks; base += blockDim.x) {
-    const int t = base + threadIdx.x;
-    int v = 0;
-    if (t < ntanks) {
-      Counters* c = tanks[t].ctr;
-      v = c->n_sorted;
-      c->n_live = v;                // A will hold exactly B's particles after G2P
+  // the last block, once every block has read n_live: prefix of the sorted particles over tanks; A will
+  // hold exactly B's particles after G2P
+  if (last_block(ticket)) {
+    tank_prefix(ntanks, spfx, [&](int u) {
+      Counters* c = tanks[u].ctr;
+      const int v = __ldcg(&c->n_sorted);
+      c->n_live = v;
       c->n_emit = 0;
-    }
-    s[threadIdx.x] = v;
-    __syncthreads();
-    for (int o = 1; o < blockDim.x; o <<= 1) {
-      int a = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
-      __syncthreads();
-      s[threadIdx.x] += a;
-      __syncthreads();
-    }
-    if (t < ntanks) pfx[t] = carry + s[threadIdx.x] - v;
-    carry += s[blockDim.x - 1];
-    __syncthreads();
+      return v;
+    });
   }
-  if (threadIdx.x == 0) pfx[ntanks] = carry;
 }
 
-void launch_begin_substep(const LaunchCtx& L) {
-  k_begin_substep<<<1, 1024, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_in, 1);
-}
 void launch_begin_count(const LaunchCtx& L) {
   k_begin_substep<<<1, 1024, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_in, 0);
 }
@@ -244,10 +226,8 @@ void launch_scan(const LaunchCtx& L) {
 }
 void launch_scatter(const LaunchCtx& L) {
   static int resident[128] = {};
-  k_scatter<<<resident_grid((const void*)k_scatter, resident), kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_in);
-}
-void launch_sorted_prefix(const LaunchCtx& L) {
-  k_sorted_prefix<<<1, 1024, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_sorted);
+  k_scatter<<<resident_grid((const void*)k_scatter, resident), kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_in,
+                                                                                      L.ppfx_sorted, L.ticket + 1);
 }
 
 }  // namespace suiri

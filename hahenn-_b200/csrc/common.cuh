@@ -171,6 +171,47 @@ __device__ __forceinline__ int flags_of(float w) { return (int)w; }
 __device__ __forceinline__ int divu(int n, DivU v) {
   return (int)((__umulhi((unsigned)n, v.mul) + (unsigned)n) >> v.shr);
 }
+// Every block calls this once, with all its threads, after its last global write. It returns true in exactly
+// one block, the last to arrive, which then sees the writes of all the others (each block fences before it
+// takes its ticket; read them with __ldcg). The ticket is left at 0 for the next launch.
+__device__ __forceinline__ bool last_block(unsigned* ticket) {
+  __shared__ int s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned k = atomicAdd(ticket, 1u);
+    s_last = k == gridDim.x - 1;
+    if (s_last) *ticket = 0u;
+  }
+  __syncthreads();
+  if (s_last) __threadfence();
+  return s_last != 0;
+}
+
+// exclusive prefix over tanks of v(t) into pfx[0 … ntanks], by one block of up to 1024 threads; v is
+// called once per tank
+template <class V>
+__device__ void tank_prefix(int ntanks, int* pfx, V v) {
+  __shared__ int s[1024];
+  int carry = 0;
+  for (int base = 0; base < ntanks; base += blockDim.x) {
+    const int t = base + threadIdx.x;
+    const int x = t < ntanks ? v(t) : 0;
+    s[threadIdx.x] = x;
+    __syncthreads();
+    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+      const int a = (int)threadIdx.x >= o ? s[threadIdx.x - o] : 0;
+      __syncthreads();
+      s[threadIdx.x] += a;
+      __syncthreads();
+    }
+    if (t < ntanks) pfx[t] = carry + s[threadIdx.x] - x;
+    carry += s[blockDim.x - 1];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) pfx[ntanks] = carry;
+  __syncthreads();
+}
 #endif  // __CUDACC__
 
 }  // namespace suiri

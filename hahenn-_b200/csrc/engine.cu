@@ -115,69 +115,83 @@ __global__ void k_emit(TankDev T, const EmitRec* __restrict__ recs, int nrec, in
   T.vE[slot] = make_float4((float)v[0], (float)v[1], (float)v[2], __uint_as_float(e.first_id + (uint32_t)local));
 }
 
-// Fixed-rate emitters, one block per tank, inside the captured sub-step: a disc outlet emits as the
-// stream source of src/js/31-wgsl-sim2.js:276-288, the rain area as :307-310. Ids of device-emitted
-// particles carry the top bit so they never meet host-assigned ids.
-__global__ void k_emit_fixed(const TankDev* __restrict__ tanks) {
+// Start of a sub-step, one block per tank, inside the captured sub-step. The tank's fixed-rate emitters
+// append their particles to E: a disc outlet emits as the stream source of src/js/31-wgsl-sim2.js:276-288,
+// the rain area as :307-310. Ids of device-emitted particles carry the top bit so they never meet
+// host-assigned ids. Then the last block to finish advances every tank's sub-step counters and writes the
+// prefix over tanks of |A∪E|.
+__global__ void k_emit_begin(const TankDev* __restrict__ tanks, int ntanks, int* __restrict__ pfx, unsigned* __restrict__ ticket) {
   const TankDev& T = tanks[blockIdx.x];
-  if (T.nemit == 0) return;
-  __shared__ int s_base, s_total, s_first[kMaxEmitters + 1];
-  __shared__ unsigned s_id;
-  Counters* c = T.ctr;
-  if (threadIdx.x == 0) {
-    const int base = c->n_emit;
-    long long room = (long long)T.cap - (c->n_live + c->n_emit) - 64;
-    room = min(room, (long long)T.emit_cap - c->n_emit);
-    int total = 0;
-    for (int e = 0; e < T.nemit; ++e) {
-      const double acc = c->emit_acc[e] + T.emitters[e].per_substep;
-      const double fl = floor(acc);
-      c->emit_acc[e] = acc - fl;
-      int n = (int)fl;
-      if (n > room - total) { n = (int)max(0LL, room - total); c->full = 1; }
-      s_first[e] = total;
-      total += n;
+  if (T.nemit > 0) {
+    __shared__ int s_base, s_total, s_first[kMaxEmitters + 1];
+    __shared__ unsigned s_id;
+    Counters* c = T.ctr;
+    if (threadIdx.x == 0) {
+      const int base = c->n_emit;
+      long long room = (long long)T.cap - (c->n_live + c->n_emit) - 64;
+      room = min(room, (long long)T.emit_cap - c->n_emit);
+      int total = 0;
+      for (int e = 0; e < T.nemit; ++e) {
+        const double acc = c->emit_acc[e] + T.emitters[e].per_substep;
+        const double fl = floor(acc);
+        c->emit_acc[e] = acc - fl;
+        int n = (int)fl;
+        if (n > room - total) { n = (int)max(0LL, room - total); c->full = 1; }
+        s_first[e] = total;
+        total += n;
+      }
+      s_first[T.nemit] = total;
+      s_base = base;
+      s_total = total;
+      s_id = c->next_id;
     }
-    s_first[T.nemit] = total;
-    s_base = base;
-    s_total = total;
-    s_id = c->next_id;
-  }
-  __syncthreads();
-  const int frame = c->frame + 1;
-  for (int q = threadIdx.x; q < s_total; q += blockDim.x) {
-    int e = 0;
-    while (q >= s_first[e + 1]) ++e;
-    const EmitterDev& E = T.emitters[e];
-    const int local = q - s_first[e];
-    uint32_t s = hash32((uint32_t)local * 747796405u + hash32(T.seed * 2891336453u + (uint32_t)frame * 97u + (uint32_t)e) + 1u);
-    double p[3], v[3];
-    if (E.shape == 0) {
-      const double rr = E.radius * sqrt(rnd01(s));
-      const double th = 6.283185307179586 * rnd01(s);
-      const double ct = cos(th), st = sin(th);
-      const double along = rnd01(s) * (E.speed * T.dt);
-      const double j0 = rnd01(s) - 0.5, j1 = rnd01(s) - 0.5, j2 = rnd01(s) - 0.5;
-      for (int k = 0; k < 3; ++k) p[k] = E.pos[k] + (E.u[k] * ct + E.w[k] * st) * rr + E.dir[k] * along;
-      v[0] = E.dir[0] * E.speed + j0 * (0.02 * E.speed);
-      v[1] = E.dir[1] * E.speed + j1 * (0.02 * E.speed);
-      v[2] = E.dir[2] * E.speed + j2 * (0.02 * E.speed);
-    } else {
-      p[0] = E.pos[0] + (rnd01(s) * 2 - 1) * E.radius;
-      p[1] = E.pos[1] - rnd01(s) * (E.speed * T.dt);
-      p[2] = E.pos[2] + (rnd01(s) * 2 - 1) * E.radius_z;
-      v[0] = 0.0; v[1] = -E.speed; v[2] = 0.0;
+    __syncthreads();
+    const int frame = c->frame + 1;
+    for (int q = threadIdx.x; q < s_total; q += blockDim.x) {
+      int e = 0;
+      while (q >= s_first[e + 1]) ++e;
+      const EmitterDev& E = T.emitters[e];
+      const int local = q - s_first[e];
+      uint32_t s = hash32((uint32_t)local * 747796405u + hash32(T.seed * 2891336453u + (uint32_t)frame * 97u + (uint32_t)e) + 1u);
+      double p[3], v[3];
+      if (E.shape == 0) {
+        const double rr = E.radius * sqrt(rnd01(s));
+        const double th = 6.283185307179586 * rnd01(s);
+        const double ct = cos(th), st = sin(th);
+        const double along = rnd01(s) * (E.speed * T.dt);
+        const double j0 = rnd01(s) - 0.5, j1 = rnd01(s) - 0.5, j2 = rnd01(s) - 0.5;
+        for (int k = 0; k < 3; ++k) p[k] = E.pos[k] + (E.u[k] * ct + E.w[k] * st) * rr + E.dir[k] * along;
+        v[0] = E.dir[0] * E.speed + j0 * (0.02 * E.speed);
+        v[1] = E.dir[1] * E.speed + j1 * (0.02 * E.speed);
+        v[2] = E.dir[2] * E.speed + j2 * (0.02 * E.speed);
+      } else {
+        p[0] = E.pos[0] + (rnd01(s) * 2 - 1) * E.radius;
+        p[1] = E.pos[1] - rnd01(s) * (E.speed * T.dt);
+        p[2] = E.pos[2] + (rnd01(s) * 2 - 1) * E.radius_z;
+        v[0] = 0.0; v[1] = -E.speed; v[2] = 0.0;
+      }
+      const bool alive = !(T.has_obst && tank_sdf(T, p[0], p[1], p[2]) < 0.0);
+      const int flags = (E.airborne ? kFlagAir : 0) | (alive ? 0 : kFlagDead);
+      const int slot = s_base + q;
+      T.pE[slot] = make_float4((float)p[0], (float)p[1], (float)p[2], (float)flags);
+      T.vE[slot] = make_float4((float)v[0], (float)v[1], (float)v[2], __uint_as_float(0x80000000u | (s_id + (unsigned)q)));
     }
-    const bool alive = !(T.has_obst && tank_sdf(T, p[0], p[1], p[2]) < 0.0);
-    const int flags = (E.airborne ? kFlagAir : 0) | (alive ? 0 : kFlagDead);
-    const int slot = s_base + q;
-    T.pE[slot] = make_float4((float)p[0], (float)p[1], (float)p[2], (float)flags);
-    T.vE[slot] = make_float4((float)v[0], (float)v[1], (float)v[2], __uint_as_float(0x80000000u | (s_id + (unsigned)q)));
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      c->n_emit = s_base + s_total;
+      c->next_id = s_id + (unsigned)s_total;
+    }
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    c->n_emit = s_base + s_total;
-    c->next_id = s_id + (unsigned)s_total;
+  if (last_block(ticket)) {
+    tank_prefix(ntanks, pfx, [&](int u) {
+      Counters* c = tanks[u].ctr;
+      const int v = __ldcg(&c->n_live) + __ldcg(&c->n_emit);
+      c->frame += 1;
+      c->vmax_bits64 = 0ull;
+      c->ww_spawned = 0;
+      c->n_act[0] = c->n_act[1] = 0;
+      return v;
+    });
   }
 }
 
@@ -895,12 +909,15 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
   CK(cudaMemcpyAsync(d_hpfx, hp.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
   CK(cudaMalloc(&d_barrier, sizeof(GridBarrier)));
   CK(cudaMemsetAsync(d_barrier, 0, sizeof(GridBarrier), stream));
+  CK(cudaMalloc(&d_ticket, 4 * sizeof(unsigned)));
+  CK(cudaMemsetAsync(d_ticket, 0, 4 * sizeof(unsigned), stream));
   // one block per SM: the grid barrier's cost grows with the number of arriving blocks
   sor_blocks = std::min(std::min(sor_persist_max_blocks(device), sm_count), std::max(1, (hp[n] + kThreads - 1) / kThreads));
   CK(cudaStreamSynchronize(stream));
   ctx.hpfx = d_hpfx;
   ctx.apfx = d_apfx;
   ctx.barrier = d_barrier;
+  ctx.ticket = d_ticket;
   ctx.stream = stream;
   ctx.tanks = d_tanks;
   ctx.ntanks = n;
@@ -921,7 +938,7 @@ Group::~Group() {
       if (t->dep == ev_done) { cudaStreamWaitEvent(t->stream, ev_done, 0); t->dep = nullptr; }
     cudaEventDestroy(ev_done);
   }
-  cudaFree(d_hpfx); cudaFree(d_apfx); cudaFree(d_barrier);
+  cudaFree(d_hpfx); cudaFree(d_apfx); cudaFree(d_barrier); cudaFree(d_ticket);
   if (d_tbl) cudaFree(d_tbl);
   cudaFree(d_tanks); cudaFreeHost(h_tanks); cudaFree(d_bpfx); cudaFree(d_ppfx); cudaFree(d_bsum);
   if (own_stream) cudaStreamDestroy(stream);
@@ -972,6 +989,7 @@ void Group::ensure_uploaded() {
   }
   CK(cudaMemcpyAsync(d_tanks, h_tanks, tanks.size() * sizeof(TankDev), cudaMemcpyHostToDevice, stream));
   CK(cudaStreamSynchronize(stream));
+  dt_on_device = false;                          // the host images carry no sub-step dt
   bool em = false;
   for (Tank* t : tanks) em |= t->d.nemit > 0;
   if (mi != max_iters || em != graph_emitters) { max_iters = mi; graph_emitters = em; drop_graph(); }
@@ -992,20 +1010,19 @@ void Tank::set_emitters(const std::vector<EmitterDev>& e) {
 }
 
 void Group::set_dt(double dt) {
+  if (dt_on_device && dt == dev_dt) return;      // the device descriptors carry it already
   const int n = (int)tanks.size();
   k_set_dt<<<(n + 127) / 128, 128, 0, stream>>>(d_tanks, n, dt);
   CK(cudaGetLastError());
+  dev_dt = dt;
+  dt_on_device = true;
 }
 
 void Group::enqueue_body() {
-  bool emitters = false;
-  for (Tank* t : tanks) emitters |= t->d.nemit > 0;
-  if (emitters) k_emit_fixed<<<(int)tanks.size(), 128, 0, stream>>>(d_tanks);
-  launch_begin_substep(ctx);
+  k_emit_begin<<<(int)tanks.size(), 128, 0, stream>>>(d_tanks, (int)tanks.size(), ctx.ppfx_in, ctx.ticket + 2);
   launch_bin(ctx);
   launch_scan(ctx);
   launch_scatter(ctx);
-  launch_sorted_prefix(ctx);
   launch_p2g(ctx);
   launch_grid_nodes(ctx);
   launch_grid_cells(ctx);

@@ -153,6 +153,7 @@ struct Group {
   int* d_hpfx = nullptr;          // colour-slot prefix for the persistent SOR
   int* d_apfx = nullptr;          // per colour, prefix of the active cells over the tanks
   void* d_tbl = nullptr;          // per-tile lists of the two-sweeps-per-launch solve (allocated when tuned to it)
+  unsigned* d_ticket = nullptr;   // last-block tickets of the kernels that end in a prefix over tanks
   void ensure_tbl();
   GridBarrier* d_barrier = nullptr;
   int sor_mode = 0;               // 0: one launch per colour sweep, 1: one cooperative launch per solve,
@@ -170,6 +171,8 @@ struct Group {
   ~Group();
   void ensure_uploaded();
   void set_dt(double dt);
+  double dev_dt = 0;              // the sub-step dt the device descriptors hold, when dt_on_device
+  bool dt_on_device = false;
   void enqueue_body();            // the sub-step without GEOM
   void substep(double dt);
   void drop_graph();

@@ -290,7 +290,8 @@ __global__ void __launch_bounds__(kThreads) k_grid_nodes(const TankDev* __restri
 // divergence with the drift correction (solver.py:467-472), the float32 SOR right-hand side h²·div
 // (solver.py:487), the per-cell SOR code (open / partial faces, active = liquid with an open face:
 // solver.py:478-486) and the warm start: liquid cells keep last sub-step's pressure, others 0 (:474).
-__global__ void __launch_bounds__(kThreads) k_grid_cells(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx) {
+__global__ void __launch_bounds__(kThreads) k_grid_cells(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ bpfx,
+                                                         int* __restrict__ apfx, unsigned* __restrict__ ticket) {
   const int t = find_slot(bpfx, ntanks, blockIdx.x);
   const TankDev& T = tanks[t];
   const int c0 = (blockIdx.x - bpfx[t]) * blockDim.x + threadIdx.x;
@@ -349,31 +350,10 @@ __global__ void __launch_bounds__(kThreads) k_grid_cells(const TankDev* __restri
     at = __shfl_sync(0xffffffffu, at, leader);
     if (mine) T.act[(size_t)cc * T.nhalf + at + __popc(m & ((1u << lane) - 1))] = hs;
   }
-}
-
-// prefix over tanks of the active counts of both colours (one block), for the sweeps' item → tank map
-__global__ void k_act_prefix(const TankDev* __restrict__ tanks, int ntanks, int* __restrict__ apfx) {
-  __shared__ int s[1024];
-  for (int cc = 0; cc < 2; ++cc) {
-    int carry = 0;
-    int* pfx = apfx + cc * (ntanks + 1);
-    for (int base = 0; base < ntanks; base += blockDim.x) {
-      const int t = base + threadIdx.x;
-      const int v = t < ntanks ? tanks[t].ctr->n_act[cc] : 0;
-      s[threadIdx.x] = v;
-      __syncthreads();
-      for (int o = 1; o < blockDim.x; o <<= 1) {
-        const int a = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
-        __syncthreads();
-        s[threadIdx.x] += a;
-        __syncthreads();
-      }
-      if (t < ntanks) pfx[t] = carry + s[threadIdx.x] - v;
-      carry += s[blockDim.x - 1];
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) pfx[ntanks] = carry;
-    __syncthreads();
+  // the last block: per colour, the prefix over tanks of the active counts (the sweeps' item → tank map)
+  if (last_block(ticket)) {
+    for (int cc = 0; cc < 2; ++cc)
+      tank_prefix(ntanks, apfx + cc * (ntanks + 1), [&](int u) { return __ldcg(&tanks[u].ctr->n_act[cc]); });
   }
 }
 
@@ -439,8 +419,7 @@ void launch_grid_nodes(const LaunchCtx& L) {
   k_grid_nodes<<<L.nblocks[kFamNodes], kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.bpfx[kFamNodes]);
 }
 void launch_grid_cells(const LaunchCtx& L) {
-  k_grid_cells<<<L.nblocks[kFamCells], kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.bpfx[kFamCells]);
-  k_act_prefix<<<1, 1024, 0, L.stream>>>(L.tanks, L.ntanks, L.apfx);
+  k_grid_cells<<<L.nblocks[kFamCells], kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.bpfx[kFamCells], L.apfx, L.ticket + 0);
 }
 void launch_project(const LaunchCtx& L) {
   k_project<<<L.nblocks[kFamNodes], kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.bpfx[kFamNodes]);

@@ -28,6 +28,7 @@ struct LaunchCtx {
   int* hpfx;                // device: ntanks+1 prefix of colour slots (nhalf) for the persistent SOR
   int* apfx;                // device: 2·(ntanks+1), per colour the prefix of the active cells (this sub-step)
   GridBarrier* barrier;     // device: grid barrier of the persistent SOR
+  unsigned* ticket;         // device: last-block tickets (0 cell pass, 1 scatter, 2 sub-step start)
   uint2* tbl_list;          // device, two sweeps per launch: per tile the active-cell lists (k_tbl_lists)
   int* tbl_cnt;             //   per tile: entries of list A, B, C
   int2* tbl_c;              //   per tile: colour-0 cells with a constant pressure other than +0
@@ -49,12 +50,10 @@ inline int resident_grid(const void* k, int* cache) {
 }
 
 // per-kernel launchers (bin.cu, grid.cu, sor.cu, g2p.cu)
-void launch_begin_substep(const LaunchCtx& L);
 void launch_begin_count(const LaunchCtx& L);   // prefix only, for a count pass between sub-steps
 void launch_bin(const LaunchCtx& L);
 void launch_scan(const LaunchCtx& L);
 void launch_scatter(const LaunchCtx& L);
-void launch_sorted_prefix(const LaunchCtx& L);
 void launch_geom(const LaunchCtx& L);
 void launch_p2g(const LaunchCtx& L);
 void launch_grid_nodes(const LaunchCtx& L);

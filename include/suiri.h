@@ -200,10 +200,10 @@ int suiri_read_whitewater(suiri_tank* t, float* pos4, float* vel4, int64_t cap, 
 int suiri_read_grid(suiri_tank* t, int32_t field, void* out, size_t bytes);
 int suiri_get_stats(suiri_tank* t, suiri_stats* s);
 /* Non-blocking stats, as the reference's FluidSim.pollStats (src/js/50-sim.js:346-363) maps its staging
-   buffers asynchronously: if the read started by the previous call has finished, *s gets those stats and
-   *fresh = 1 (else *s is left as it is and *fresh = 0); then a new read of the device counters is enqueued
-   on the tank's stream behind the work enqueued so far. Values lag by the work enqueued between two calls.
-   fresh may be NULL. */
+   buffers asynchronously. One read of the device counters is in flight at a time. If it has finished, *s
+   gets those stats and *fresh = 1 (else *s is left as it is and *fresh = 0); when no read is in flight any
+   more, a new one is enqueued on the tank's stream behind the work enqueued so far. The stats returned
+   therefore date from the call that started their read. fresh may be NULL. */
 int suiri_poll_stats(suiri_tank* t, suiri_stats* s, int32_t* fresh);
 /* bytes one stats read (suiri_get_stats, suiri_poll_stats) copies from the device */
 size_t suiri_stats_readback_bytes(void);

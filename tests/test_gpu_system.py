@@ -202,8 +202,8 @@ def test_empty_tank_steps_cleanly(pkg):
 
 
 def test_poll_stats_and_pipelined_particle_adds(pkg):
-    """Non-blocking stats (pollStats): the first call only starts a read; once the stream is idle the next
-    call returns exactly what the blocking read returns. Particles added every sub-step through the two
+    """Non-blocking stats (pollStats): the first call only starts a read; a read started once the stream is
+    idle returns exactly what the blocking read returns. Particles added every sub-step through the two
     staging buffers, without waits in between, all arrive with their ids and values."""
     w = pkg.workloads.dam_break()
     t = pkg.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], whitewater=False, ripple=None,
@@ -219,6 +219,8 @@ def test_poll_stats_and_pipelined_particle_adds(pkg):
         t.add_particles(p, v)
         t.substep(1 / 240)
         t.poll_stats()
+    t.sync()
+    t.poll_stats()          # collects the read in flight (it may date from an earlier step), starts one now
     t.sync()
     st = t.poll_stats()
     ref = t.stats()
