@@ -17,36 +17,10 @@
 
 namespace suiri {
 
-__global__ void k_begin_substep(const TankDev* __restrict__ tanks, int ntanks, int* __restrict__ pfx, int advance) {
-  // one block: prefix of |A∪E| over tanks; per-tank sub-step counters (advance = 0: a count pass only)
-  __shared__ int s[1024];
-  int carry = 0;
-  for (int base = 0; base < ntanks; base += blockDim.x) {
-    const int t = base + threadIdx.x;
-    int v = 0;
-    if (t < ntanks) {
-      Counters* c = tanks[t].ctr;
-      v = c->n_live + c->n_emit;
-      if (advance) {
-        c->frame += 1;
-        c->vmax_bits64 = 0ull;
-        c->ww_spawned = 0;
-        c->n_act[0] = c->n_act[1] = 0;
-      }
-    }
-    s[threadIdx.x] = v;
-    __syncthreads();
-    for (int o = 1; o < blockDim.x; o <<= 1) {
-      int a = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
-      __syncthreads();
-      s[threadIdx.x] += a;
-      __syncthreads();
-    }
-    if (t < ntanks) pfx[t] = carry + s[threadIdx.x] - v;
-    carry += s[blockDim.x - 1];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) pfx[ntanks] = carry;
+// one block: prefix over tanks of |A∪E| for a count pass between sub-steps (the sub-step itself writes it in
+// k_emit_begin, which also advances the sub-step counters)
+__global__ void k_count_prefix(const TankDev* __restrict__ tanks, int ntanks, int* __restrict__ pfx) {
+  tank_prefix(ntanks, pfx, [&](int t) { return tanks[t].ctr->n_live + tanks[t].ctr->n_emit; });
 }
 
 __device__ __forceinline__ int particle_cell(const TankDev& T, float4 p) {
@@ -212,7 +186,7 @@ __global__ void __launch_bounds__(kThreads) k_scatter(const TankDev* __restrict_
 }
 
 void launch_begin_count(const LaunchCtx& L) {
-  k_begin_substep<<<1, 1024, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_in, 0);
+  k_count_prefix<<<1, 1024, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_in);
 }
 // binning and scatter are chains of dependent loads per particle: as many resident threads as fit
 void launch_bin(const LaunchCtx& L) {
