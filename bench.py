@@ -282,7 +282,7 @@ def run_reference(args, rank):
     if rank != 0:
         return
     w = pkg().workloads.obstacles_inflow()
-    steps, warm = max(1, min(args.steps, 3)), min(args.warmup, 1)
+    steps, warm = max(1, min(args.steps, 3)), min(args.warmup, 3)   # ≈4 s a sub-step per core
     procs = cpu_replicas_count()
     rate, el = cpu_replicas_rate(steps, warm, procs)
     line = dict(impl='reference', metric=METRIC, value=rate, unit=METRIC, n_gpus=args.gpus, steps=steps, warmup=warm,
