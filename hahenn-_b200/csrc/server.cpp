@@ -1,8 +1,10 @@
 // Serving: a request loop that admits scene solves by HBM budget and advances every resident scene with
 // shared batched launches (continuous batching). Requests arriving while others run are admitted at the
 // next sub-step boundary as memory frees up; finished ones leave at a boundary and their memory returns
-// to the budget. All device work runs on one worker thread and one stream; the state of a request stays
-// on the device from admission to completion.
+// to the budget. Resident scenes are grouped in lanes by size, one stream and one batch per lane; each lane
+// queues up to kLaneRunAhead sub-steps ahead of the device and is refilled as its sub-steps complete. All
+// device work is issued by one worker thread; the state of a request stays on the device from admission
+// to completion.
 #include "server.h"
 
 #include <algorithm>
@@ -20,9 +22,16 @@ double now_s() {
 
 Server::Server(int device, double budget_bytes, double dt_) : budget(budget_bytes), dt(dt_), dev(device) {
   CK(cudaSetDevice(device));
-  CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  for (Lane& L : lanes) CK(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
   t_start = now_s();
   worker = std::thread([this] { loop(); });
+}
+
+int Server::lane_of(const TankConfig& c) {
+  const long long cells = (long long)c.nx * c.ny * c.nz;
+  int l = 0;
+  while (l < kLanes - 1 && cells >= kLaneCells[l]) ++l;
+  return l;
 }
 
 Server::~Server() {
@@ -33,9 +42,14 @@ Server::~Server() {
   cv.notify_all();
   if (worker.joinable()) worker.join();
   cudaSetDevice(dev);
-  group.reset();
+  for (Lane& L : lanes) L.group.reset();
   for (auto& kv : reqs) kv.second->tank.reset();
-  cudaStreamDestroy(stream);
+  for (Lane& L : lanes) {
+    cudaStreamSynchronize(L.stream);
+    for (cudaEvent_t e : L.inflight) cudaEventDestroy(e);
+    for (cudaEvent_t e : L.spare) cudaEventDestroy(e);
+    cudaStreamDestroy(L.stream);
+  }
 }
 
 long long Server::submit(std::unique_ptr<Request> r) {
@@ -70,7 +84,7 @@ void Server::admit_locked(std::vector<Request*>& admitted) {
 
 void Server::start_request(Request* r) {
   try {
-    r->cfg.stream = stream;
+    r->cfg.stream = lanes[lane_of(r->cfg)].stream;
     r->cfg.device = dev;
     r->tank.reset(new Tank(r->cfg));
     Tank& t = *r->tank;
@@ -112,64 +126,103 @@ void Server::finish_request(Request* r) {
   cv.notify_all();
 }
 
+bool Server::advance(Lane& L) {
+  // sub-steps of this lane that have finished on the device free their places
+  while (!L.inflight.empty()) {
+    const cudaError_t q = cudaEventQuery(L.inflight.front());
+    if (q == cudaErrorNotReady) break;
+    CK(q);
+    L.spare.push_back(L.inflight.front());
+    L.inflight.pop_front();
+  }
+  if ((int)L.inflight.size() >= kLaneRunAhead) return false;
+  if (L.changed || !L.group) {
+    L.group.reset();
+    std::vector<Tank*> ts;
+    for (Request* r : L.active) ts.push_back(r->tank.get());
+    L.group.reset(new Group(ts, L.stream));
+    ++rebuilds;
+    L.changed = false;
+  }
+  try {
+    L.group->substep(dt);
+  } catch (const Error& e) {
+    // a failed launch ends every request of this batch with the message; the server keeps serving
+    for (Request* r : L.active) {
+      r->state = kFailed;
+      r->err = e.what();
+      r->t_done = now_s();
+      r->tank.reset();
+      std::lock_guard<std::mutex> g(m);
+      used -= (double)r->bytes;
+    }
+    L.active.clear();
+    L.group.reset();
+    return true;
+  }
+  cudaEvent_t ev;
+  if (L.spare.empty()) {
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  } else {
+    ev = L.spare.back();
+    L.spare.pop_back();
+  }
+  CK(cudaEventRecord(ev, L.stream));
+  L.inflight.push_back(ev);
+  ++substeps;
+  {
+    // work done: every resident scene of the lane advanced one sub-step (particles counted at admission)
+    double w = 0;
+    for (Request* r : L.active) w += (double)r->start_count;
+    std::lock_guard<std::mutex> g(m);
+    total_particle_steps += w;
+  }
+  std::vector<Request*> still, done;
+  for (Request* r : L.active) (++r->steps_done >= r->steps ? done : still).push_back(r);
+  if (!done.empty()) {
+    L.group.reset();                 // the batch refers to the tanks that are about to be freed
+    for (Request* r : done) finish_request(r);
+    L.changed = true;
+  }
+  L.active.swap(still);
+  return true;
+}
+
 void Server::loop() {
   cudaSetDevice(dev);
-  std::vector<Request*> active;
-  bool changed = false;
   while (true) {
     std::vector<Request*> admitted;
+    bool idle = true;
+    for (Lane& L : lanes) idle &= L.active.empty();
     {
       std::unique_lock<std::mutex> g(m);
-      if (active.empty() && queue.empty()) cv.wait_for(g, std::chrono::milliseconds(20));
+      if (idle && queue.empty()) cv.wait_for(g, std::chrono::milliseconds(20));
       if (stop) break;
       admit_locked(admitted);
     }
     for (Request* r : admitted) {
       start_request(r);
-      if (r->state == kRunning) { active.push_back(r); changed = true; }
-    }
-    if (active.empty()) continue;
-    if (changed || !group) {
-      group.reset();
-      std::vector<Tank*> ts;
-      for (Request* r : active) ts.push_back(r->tank.get());
-      group.reset(new Group(ts, stream));
-      ++rebuilds;
-      changed = false;
-    }
-    try {
-      group->substep(dt);
-    } catch (const Error& e) {
-      // a failed launch ends every request of this batch with the message; the server keeps serving
-      for (Request* r : active) {
-        r->state = kFailed;
-        r->err = e.what();
-        r->t_done = now_s();
-        r->tank.reset();
-        std::lock_guard<std::mutex> g(m);
-        used -= (double)r->bytes;
+      if (r->state == kRunning) {
+        Lane& L = lanes[lane_of(r->cfg)];
+        L.active.push_back(r);
+        L.changed = true;
       }
-      active.clear();
-      group.reset();
-      continue;
     }
-    ++substeps;
-    sum_active += (double)active.size();
-    {
-      // work done: every resident scene advanced one sub-step (particles counted at admission)
-      double w = 0;
-      for (Request* r : active) w += (double)r->start_count;
-      std::lock_guard<std::mutex> g(m);
-      total_particle_steps += w;
+    bool any = false, moved = false;
+    long long resident = 0;
+    for (Lane& L : lanes) resident += (long long)L.active.size();
+    for (Lane& L : lanes) {
+      if (L.active.empty()) continue;
+      any = true;
+      moved |= advance(L);
     }
-    std::vector<Request*> still, done;
-    for (Request* r : active) (++r->steps_done >= r->steps ? done : still).push_back(r);
-    if (!done.empty()) {
-      group.reset();                 // the batch refers to the tanks that are about to be freed
-      for (Request* r : done) finish_request(r);
-      changed = true;
+    if (!any) continue;
+    if (moved) {
+      ++rounds;
+      sum_active += (double)resident;
+    } else {
+      std::this_thread::sleep_for(std::chrono::microseconds(20));   // every lane is its run-ahead in front
     }
-    active.swap(still);
   }
 }
 
@@ -197,7 +250,7 @@ ServerStats Server::stats() {
   s.budget_bytes = budget;
   s.rebuilds = rebuilds;
   s.substeps = substeps;
-  s.mean_active = substeps ? sum_active / substeps : 0.0;
+  s.mean_active = rounds ? sum_active / rounds : 0.0;
   std::vector<double> l = lat_ms;
   std::sort(l.begin(), l.end());
   auto pct = [&](double q) { return l.empty() ? 0.0 : l[std::min(l.size() - 1, (size_t)floor(q * (l.size() - 1) + 0.5))]; };

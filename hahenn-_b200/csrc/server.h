@@ -37,18 +37,33 @@ struct ServerStats {
   double particle_steps = 0, elapsed_s = 0, used_bytes = 0, budget_bytes = 0, p50_ms = 0, p99_ms = 0, mean_active = 0;
 };
 
+// Resident scenes are batched by size class: each lane has its own stream and batched graph and advances
+// at its own pace, so a small scene's sub-steps do not wait for the largest scene's, and the lanes' kernels
+// overlap on the GPU.
+constexpr int kLanes = 3;
+constexpr long long kLaneCells[kLanes - 1] = {1LL << 16, 1LL << 19};   // lane upper bounds, in cells
+constexpr int kLaneRunAhead = 4;                                      // sub-steps queued per lane at most
+
+struct Lane {
+  cudaStream_t stream = nullptr;
+  std::vector<Request*> active;
+  std::unique_ptr<Group> group;
+  bool changed = false;
+  std::deque<cudaEvent_t> inflight;   // one per queued sub-step, oldest first
+  std::vector<cudaEvent_t> spare;
+};
+
 struct Server {
   double budget, used = 0, dt;
   int dev;
-  cudaStream_t stream = nullptr;
+  Lane lanes[kLanes];
   std::mutex m;
   std::condition_variable cv;
   std::deque<Request*> queue;
   std::map<long long, std::unique_ptr<Request>> reqs;
-  std::unique_ptr<Group> group;
   std::thread worker;
   bool stop = false;
-  long long next_id = 0, completed = 0, rebuilds = 0, substeps = 0;
+  long long next_id = 0, completed = 0, rebuilds = 0, substeps = 0, rounds = 0;
   double total_particle_steps = 0, sum_active = 0, t_start = 0;
   std::vector<double> lat_ms;
 
@@ -62,6 +77,8 @@ struct Server {
   void admit_locked(std::vector<Request*>& admitted);
   void start_request(Request* r);
   void finish_request(Request* r);
+  static int lane_of(const TankConfig& c);
+  bool advance(Lane& L);                 // queue one sub-step of the lane if it may run ahead; true if it did
   void apply(Tank& t, const Scene& sc);
 };
 

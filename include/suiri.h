@@ -250,16 +250,19 @@ typedef struct suiri_request {
 } suiri_request;
 
 typedef struct suiri_server_stats {
-  int64_t completed, queued, running, failed, rebuilds, substeps;
+  int64_t completed, queued, running, failed, rebuilds;
+  int64_t substeps;                 /* batched sub-steps issued, summed over the size lanes */
   double particle_steps;            /* work done so far: per batched sub-step, the liquid particles (counted at
-                                       admission) of every resident scene */
+                                       admission) of every scene it advanced */
   double elapsed_s, used_bytes, budget_bytes;
   double p50_ms, p99_ms;            /* request latency: submit → results ready */
-  double mean_active;               /* resident scenes per batched sub-step */
+  double mean_active;               /* resident scenes (all lanes) per round in which some lane advanced */
 } suiri_server_stats;
 
-/* a worker thread admits requests FIFO while their device memory fits the budget, advances all resident
-   scenes with one batched sub-step of length dt at a time, and retires finished ones at sub-step boundaries */
+/* a worker thread admits requests FIFO while their device memory fits the budget, and retires finished ones at
+   sub-step boundaries. Resident scenes are batched in three lanes by size (under 2^16 cells, under 2^19,
+   larger), each with its own stream: a lane advances its scenes one batched sub-step of length dt at a time,
+   keeping up to 4 sub-steps queued on the device, so small scenes do not wait for large ones */
 int suiri_server_create(int32_t device, double budget_bytes, double dt, suiri_server** out);
 int suiri_server_destroy(suiri_server* s);
 int suiri_server_submit(suiri_server* s, const suiri_request* r, int64_t* id);
