@@ -54,10 +54,12 @@ def test_set_objects_moving_obstacle_velocity(pkg):
 
 def test_serving_result_alone_equals_result_in_mix(pkg):
     """Each request gives the same particles alone and co-scheduled with others (the step is deterministic:
-    integer P2G sums, id-keyed randomness), here bit for bit."""
+    integer P2G sums, id-keyed randomness), here bit for bit; the 48³ scene runs in another size lane (its
+    own stream and batch) beside the small ones."""
     from importlib import import_module
     serve = import_module('hahenn-_b200.serve')
     reqs = [serve.scene_request(s, axes=(16, 24, 32), faucet_p=0.5 if s == 2 else 0.0) for s in (1, 2, 3)]
+    reqs.append(serve.scene_request(4, axes=(48,)))
     srv = serve.Server(budget_bytes=8e9)
     alone = []
     for sc, prm, em, _ in reqs:
@@ -68,7 +70,7 @@ def test_serving_result_alone_equals_result_in_mix(pkg):
     for i in ids:
         srv.wait(i)
     st = srv.stats()
-    assert st['mean_active'] > 1.0 and st['completed'] == 6
+    assert st['mean_active'] > 1.0 and st['completed'] == 8
     for (Pa, Va), i in zip(alone, ids):
         Pm, Vm = srv.result(i)
         ka, km = Va[:, 3].view(np.uint32), Vm[:, 3].view(np.uint32)
