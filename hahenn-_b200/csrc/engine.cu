@@ -990,9 +990,8 @@ void Group::ensure_uploaded() {
   CK(cudaMemcpyAsync(d_tanks, h_tanks, tanks.size() * sizeof(TankDev), cudaMemcpyHostToDevice, stream));
   CK(cudaStreamSynchronize(stream));
   dt_on_device = false;                          // the host images carry no sub-step dt
-  bool em = false;
-  for (Tank* t : tanks) em |= t->d.nemit > 0;
-  if (mi != max_iters || em != graph_emitters) { max_iters = mi; graph_emitters = em; drop_graph(); }
+  // the graph's shape depends only on the iteration count (the emitter kernel reads nemit on the device)
+  if (mi != max_iters) { max_iters = mi; drop_graph(); }
 }
 
 void Tank::set_emitters(const std::vector<EmitterDev>& e) {

@@ -148,7 +148,6 @@ struct Group {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int max_iters = 0;
-  bool graph_emitters = false;
   cudaEvent_t ev_done = nullptr;  // recorded after every sub-step (tanks on other streams wait for it)
   int* d_hpfx = nullptr;          // colour-slot prefix for the persistent SOR
   int* d_apfx = nullptr;          // per colour, prefix of the active cells over the tanks

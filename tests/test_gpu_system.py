@@ -247,6 +247,24 @@ def test_poll_stats_and_pipelined_particle_adds(pkg):
     u.close()
 
 
+def test_emitters_switched_on_and_off_after_capture(pkg):
+    """Fixed emitters set and cleared once the sub-step graph exists: emission follows at once (the graph
+    reads the emitter count on the device), 20 particles a sub-step, none lost in the closed tank."""
+    t = pkg.Tank(nx=16, ny=16, nz=16, h=1 / 32, whitewater=False, ripple=None, capacity=20000, iters=10)
+    for _ in range(3):
+        t.substep(1 / 240)
+    assert t.stats()['count'] == 0
+    t.set_emitters([dict(shape='disc', pos=[0.0, 0.4, 0.0], dir=[0.0, -1.0, 0.0], radius=0.05, speed=1.0, count=20)])
+    for _ in range(5):
+        t.substep(1 / 240)
+    assert t.stats()['count'] == 100
+    t.set_emitters([])
+    for _ in range(3):
+        t.substep(1 / 240)
+    assert t.stats()['count'] == 100
+    t.close()
+
+
 def test_capacity_reached_sets_full_and_caps_the_count(pkg):
     """An emitter that outruns the particle capacity: emission stops at the capacity (minus its margin),
     the full flag is raised, and the step keeps running."""
