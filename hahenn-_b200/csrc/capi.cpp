@@ -16,7 +16,7 @@ struct suiri_tank {
   std::string err;
 };
 struct suiri_batch {
-  std::unique_ptr<Group> g;
+  std::unique_ptr<Batch> b;
   std::string err;
 };
 struct suiri_server {
@@ -471,7 +471,7 @@ int suiri_batch_create(suiri_tank* const* tanks, int32_t n, suiri_batch** out) {
   const int rc = guard(nullptr, [&] {
     std::vector<Tank*> v;
     for (int i = 0; i < n; ++i) v.push_back(T(tanks[i]));
-    b->g.reset(new Group(v, nullptr));
+    b->b.reset(new Batch(v));
   });
   if (rc != SUIRI_OK) return rc;
   *out = b.release();
@@ -480,23 +480,23 @@ int suiri_batch_create(suiri_tank* const* tanks, int32_t n, suiri_batch** out) {
 
 int suiri_batch_destroy(suiri_batch* b) {
   if (!b) return SUIRI_ERR_INVALID;
-  const int rc = guard(nullptr, [&] { b->g.reset(); });
+  const int rc = guard(nullptr, [&] { b->b.reset(); });
   delete b;
   return rc;
 }
 
 int suiri_batch_substep(suiri_batch* b, double dt) {
   return guard(b ? &b->err : nullptr, [&] {
-    if (!b || !b->g) throw Error(SUIRI_ERR_INVALID, "null batch");
+    if (!b || !b->b) throw Error(SUIRI_ERR_INVALID, "null batch");
     if (!(dt > 0) || !std::isfinite(dt)) throw Error(SUIRI_ERR_INVALID, "dt must be positive");
-    b->g->substep(dt);
+    b->b->substep(dt);
   });
 }
 
 int suiri_batch_sync(suiri_batch* b) {
   return guard(b ? &b->err : nullptr, [&] {
-    if (!b || !b->g) throw Error(SUIRI_ERR_INVALID, "null batch");
-    CK(cudaStreamSynchronize(b->g->stream));
+    if (!b || !b->b) throw Error(SUIRI_ERR_INVALID, "null batch");
+    CK(cudaStreamSynchronize(b->b->stream));
   });
 }
 
@@ -513,8 +513,8 @@ static void tune_group(Group& g, int32_t particle_blocks_per_sm, int32_t sor_mod
 
 int suiri_batch_tune(suiri_batch* b, int32_t particle_blocks_per_sm, int32_t sor_mode) {
   return guard(b ? &b->err : nullptr, [&] {
-    if (!b || !b->g) throw Error(SUIRI_ERR_INVALID, "null batch");
-    tune_group(*b->g, particle_blocks_per_sm, sor_mode);
+    if (!b || !b->b) throw Error(SUIRI_ERR_INVALID, "null batch");
+    for (auto& g : b->b->lanes) tune_group(*g, particle_blocks_per_sm, sor_mode);
   });
 }
 
@@ -524,8 +524,8 @@ int suiri_tune(suiri_tank* h, int32_t particle_blocks_per_sm, int32_t sor_mode) 
 
 int suiri_batch_stream(suiri_batch* b, void** stream) {
   return guard(b ? &b->err : nullptr, [&] {
-    if (!b || !b->g || !stream) throw Error(SUIRI_ERR_INVALID, "null batch or output");
-    *stream = (void*)b->g->stream;
+    if (!b || !b->b || !stream) throw Error(SUIRI_ERR_INVALID, "null batch or output");
+    *stream = (void*)b->b->stream;
   });
 }
 
@@ -551,8 +551,8 @@ int suiri_time_substeps(suiri_tank* h, double dt, int32_t steps, double* ms) {
 
 int suiri_batch_time_substeps(suiri_batch* bt, double dt, int32_t steps, double* ms) {
   return guard(bt ? &bt->err : nullptr, [&] {
-    if (!bt || !bt->g || !ms || steps <= 0) throw Error(SUIRI_ERR_INVALID, "bad timing arguments");
-    Group& g = *bt->g;
+    if (!bt || !bt->b || !ms || steps <= 0) throw Error(SUIRI_ERR_INVALID, "bad timing arguments");
+    Batch& g = *bt->b;
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
@@ -582,15 +582,17 @@ int suiri_sor_phase_ms(suiri_tank* h, double* ms) {
 
 int suiri_batch_profile(suiri_batch* b, int32_t on) {
   return guard(b ? &b->err : nullptr, [&] {
-    if (!b || !b->g) throw Error(SUIRI_ERR_INVALID, "null batch");
-    b->g->set_profile(on != 0);
+    if (!b || !b->b) throw Error(SUIRI_ERR_INVALID, "null batch");
+    for (auto& g : b->b->lanes) g->set_profile(on != 0);
   });
 }
 
 int suiri_batch_sor_phase_ms(suiri_batch* b, double* ms) {
   return guard(b ? &b->err : nullptr, [&] {
-    if (!b || !b->g || !ms) throw Error(SUIRI_ERR_INVALID, "null batch or output");
-    *ms = b->g->sor_phase_ms();
+    if (!b || !b->b || !ms) throw Error(SUIRI_ERR_INVALID, "null batch or output");
+    double m = 0;
+    for (auto& g : b->b->lanes) m = std::max(m, g->sor_phase_ms());   // lanes overlap: the longest
+    *ms = m;
   });
 }
 

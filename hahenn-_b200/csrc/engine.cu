@@ -952,6 +952,48 @@ void Group::ensure_tbl() {
   tbl_assign(ctx, d_tbl, tiles);
 }
 
+Batch::Batch(const std::vector<Tank*>& t) {
+  if (t.empty()) throw Error(-1, "a batch needs at least one tank");
+  for (Tank* x : t)
+    if (x->cfg.device != t[0]->cfg.device) throw Error(-1, "all tanks of a batch must be on one device");
+  std::vector<Tank*> by_lane[kSizeLanes];
+  for (Tank* x : t) by_lane[size_lane((long long)x->d.nx * x->d.ny * x->d.nz)].push_back(x);
+  for (auto& v : by_lane)
+    if (!v.empty()) lanes.emplace_back(new Group(v, nullptr));
+  if (lanes.size() == 1) {
+    stream = lanes[0]->stream;
+    return;
+  }
+  CK(cudaSetDevice(t[0]->cfg.device));
+  CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  own_stream = true;
+  CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  join.resize(lanes.size());
+  for (auto& e : join) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+}
+
+Batch::~Batch() {
+  if (own_stream) cudaStreamSynchronize(stream);
+  lanes.clear();
+  if (fork) cudaEventDestroy(fork);
+  for (cudaEvent_t e : join) cudaEventDestroy(e);
+  if (own_stream) cudaStreamDestroy(stream);
+}
+
+void Batch::substep(double dt) {
+  if (lanes.size() == 1) {
+    lanes[0]->substep(dt);
+    return;
+  }
+  CK(cudaEventRecord(fork, stream));
+  for (size_t i = 0; i < lanes.size(); ++i) {
+    CK(cudaStreamWaitEvent(lanes[i]->stream, fork, 0));
+    lanes[i]->substep(dt);
+    CK(cudaEventRecord(join[i], lanes[i]->stream));
+    CK(cudaStreamWaitEvent(stream, join[i], 0));
+  }
+}
+
 void Group::set_profile(bool on) {
   if (on == profile) return;
   if (on && !ev_sor[0]) {

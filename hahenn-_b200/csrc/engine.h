@@ -2,6 +2,7 @@
 // and the sub-step / frame sequence. The C ABI (capi.cpp) is a thin layer over this.
 #pragma once
 #include <map>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -175,6 +176,26 @@ struct Group {
   void enqueue_body();            // the sub-step without GEOM
   void substep(double dt);
   void drop_graph();
+};
+
+// Size lanes: tanks under 2^16 cells, under 2^19, and larger. A batch (and the server) advances each lane
+// as its own group on its own stream, so a lane of small tanks does not wait for the largest tank's
+// kernels and the lanes' kernels overlap on the GPU.
+constexpr int kSizeLanes = 3;
+inline int size_lane(long long cells) { return cells < (1LL << 16) ? 0 : (cells < (1LL << 19) ? 1 : 2); }
+
+// A batch of tanks: one group per occupied size lane. Every sub-step forks from the batch's stream to the
+// lanes and joins back to it, so work ordered on that stream sees all of the batch's tanks.
+struct Batch {
+  std::vector<std::unique_ptr<Group>> lanes;
+  cudaStream_t stream = nullptr;  // the single lane's stream, or an own stream the lanes fork from and join
+  bool own_stream = false;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+
+  explicit Batch(const std::vector<Tank*>& t);
+  ~Batch();
+  void substep(double dt);
 };
 
 }  // namespace suiri

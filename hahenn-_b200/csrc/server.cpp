@@ -27,12 +27,7 @@ Server::Server(int device, double budget_bytes, double dt_) : budget(budget_byte
   worker = std::thread([this] { loop(); });
 }
 
-int Server::lane_of(const TankConfig& c) {
-  const long long cells = (long long)c.nx * c.ny * c.nz;
-  int l = 0;
-  while (l < kLanes - 1 && cells >= kLaneCells[l]) ++l;
-  return l;
-}
+int Server::lane_of(const TankConfig& c) { return size_lane((long long)c.nx * c.ny * c.nz); }
 
 Server::~Server() {
   {

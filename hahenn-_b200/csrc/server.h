@@ -37,11 +37,10 @@ struct ServerStats {
   double particle_steps = 0, elapsed_s = 0, used_bytes = 0, budget_bytes = 0, p50_ms = 0, p99_ms = 0, mean_active = 0;
 };
 
-// Resident scenes are batched by size class: each lane has its own stream and batched graph and advances
-// at its own pace, so a small scene's sub-steps do not wait for the largest scene's, and the lanes' kernels
-// overlap on the GPU.
-constexpr int kLanes = 3;
-constexpr long long kLaneCells[kLanes - 1] = {1LL << 16, 1LL << 19};   // lane upper bounds, in cells
+// Resident scenes are batched by size lane (size_lane, engine.h): each lane has its own stream and batched
+// graph and advances at its own pace, so a small scene's sub-steps do not wait for the largest scene's, and
+// the lanes' kernels overlap on the GPU.
+constexpr int kLanes = kSizeLanes;
 constexpr int kLaneRunAhead = 4;                                      // sub-steps queued per lane at most
 
 struct Lane {

@@ -219,8 +219,11 @@ int suiri_use_graphs(suiri_tank* t, int32_t on);
 
 /* ---------------------------------------------------------------- batching: many tanks, one set of launches */
 
-/* a batch steps existing tanks (same device) together: every kernel of the sub-step covers all of them
-   in one launch, through per-tank descriptor and block-offset tables; the sub-step is one CUDA graph */
+/* a batch steps existing tanks (same device) together: every kernel of the sub-step covers all the tanks of
+   a size lane (under 2^16 cells, under 2^19, larger) in one launch, through per-tank descriptor and
+   block-offset tables, and each lane's sub-step is one CUDA graph on the lane's own stream. A sub-step forks
+   from the batch's stream (suiri_batch_stream) to the lanes and joins back to it, so the lanes' kernels
+   overlap and small tanks do not wait for the largest one's kernels. */
 int suiri_batch_create(suiri_tank* const* tanks, int32_t n, suiri_batch** out);
 int suiri_batch_destroy(suiri_batch* b);
 int suiri_batch_substep(suiri_batch* b, double dt);
@@ -288,6 +291,7 @@ int suiri_time_sor(suiri_tank* t, int32_t iters, double* ms);
 int suiri_profile(suiri_tank* t, int32_t on);
 int suiri_sor_phase_ms(suiri_tank* t, double* ms);
 int suiri_batch_profile(suiri_batch* b, int32_t on);
+/* the longest of the lanes' pressure-solve times (the lanes run concurrently) */
 int suiri_batch_sor_phase_ms(suiri_batch* b, double* ms);
 
 #ifdef __cplusplus
