@@ -170,7 +170,8 @@ __global__ void k_emit_begin(const TankDev* __restrict__ tanks, int ntanks, int*
         p[2] = E.pos[2] + (rnd01(s) * 2 - 1) * E.radius_z;
         v[0] = 0.0; v[1] = -E.speed; v[2] = 0.0;
       }
-      const bool alive = !(T.has_obst && tank_sdf(T, p[0], p[1], p[2]) < 0.0);
+      // the bounding-sphere test first (the outlet is usually far from every obstacle): same result
+      const bool alive = !(T.has_obst && maybe_within(T, p[0], p[1], p[2], 0.0) && tank_sdf(T, p[0], p[1], p[2]) < 0.0);
       const int flags = (E.airborne ? kFlagAir : 0) | (alive ? 0 : kFlagDead);
       const int slot = s_base + q;
       T.pE[slot] = make_float4((float)p[0], (float)p[1], (float)p[2], (float)flags);
