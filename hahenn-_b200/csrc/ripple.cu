@@ -10,9 +10,10 @@
 // exact damped oscillator of ω² = (gk + σ/ρ k³) tanh(kd) and kicked by the impulse, transformed back to
 // heights and slopes, multiplied by the absorption mask (obstacle walls at the water line, dry floor)
 // and transformed forward again. The reference's square layer is Rx = Rz; here the layer may be
-// rectangular. The 2D FFTs are written here: rows, then columns, each line in shared memory, in-place
-// radix-2 decimation in time from a bit-reversed load, twiddles from a float64 table (as the reference's
-// WGSL does, 64-ripple.js:32-33, :175-178), complex64 data.
+// rectangular. The 2D FFTs are written here: rows, then columns, each line in shared memory, radix-4
+// Stockham stages (natural order, no bit-reversed load) and one radix-2 stage for odd log2 lengths,
+// twiddles from a table computed in float64 (as the reference's WGSL does, 64-ripple.js:32-33, :175-178),
+// complex64 data.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -143,27 +144,75 @@ __global__ void k_ripple_src(TankDev T, const long long* __restrict__ src, float
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 
+// Stockham autosort FFT of a power-of-two length M in shared memory (natural order in and out): radix-4
+// stages, then one radix-2 stage when log2 M is odd, ping-ponging between two buffers. A stage takes the
+// R inputs of butterfly j at stride M/R, multiplies input r by w^(r·(j mod Ns)) with w = e^(±2πi/(Ns·R))
+// (from the table tw[k] = e^(2πik/M)), transforms them, and writes them at stride Ns from
+// (j − j mod Ns)·R + j mod Ns. Unnormalised; sign −1 forward, +1 inverse.
+template <int R>
+__device__ __forceinline__ void fft_stage(const float2* __restrict__ in, float2* __restrict__ out, int M, int Ns, int j,
+                                          const float2* __restrict__ tw, float sign) {
+  float2 v[R];
+  const int k = j & (Ns - 1);
+  const int step = M / (Ns * R);
+#pragma unroll
+  for (int r = 0; r < R; ++r) v[r] = in[j + r * (M / R)];
+  // one table read per butterfly: w, then w^2 and w^3 by multiplication
+  float2 w = __ldg(tw + k * step);
+  w.y *= sign;
+  float2 wr = w;
+#pragma unroll
+  for (int r = 1; r < R; ++r) {
+    v[r] = cmul(v[r], wr);
+    if (r + 1 < R) wr = cmul(wr, w);
+  }
+  if (R == 2) {
+    const float2 a = v[0], b = v[1];
+    v[0] = make_float2(a.x + b.x, a.y + b.y);
+    v[1] = make_float2(a.x - b.x, a.y - b.y);
+  } else {
+    // y1 = b + (i·sign)·d, y3 = b − (i·sign)·d with a = x0 + x2, b = x0 − x2, c = x1 + x3, d = x1 − x3
+    const float2 a = make_float2(v[0].x + v[2].x, v[0].y + v[2].y), b = make_float2(v[0].x - v[2].x, v[0].y - v[2].y);
+    const float2 c = make_float2(v[1].x + v[3].x, v[1].y + v[3].y), d = make_float2(v[1].x - v[3].x, v[1].y - v[3].y);
+    const float2 id = make_float2(-sign * d.y, sign * d.x);
+    v[0] = make_float2(a.x + c.x, a.y + c.y);
+    v[2] = make_float2(a.x - c.x, a.y - c.y);
+    v[1] = make_float2(b.x + id.x, b.y + id.y);
+    v[3] = make_float2(b.x - id.x, b.y - id.y);
+  }
+  const int d0 = (j - k) * R + k;
+#pragma unroll
+  for (int r = 0; r < R; ++r) out[d0 + r * Ns] = v[r];
+}
+
+// the transform of C lines of length M stored line after line in buf (two buffers of C·M); returns the
+// buffer holding the result
+__device__ __forceinline__ float2* fft_lines(float2* a, float2* b, int M, int C, const float2* __restrict__ tw, float sign) {
+  int logM = 0;
+  while ((1 << logM) < M) ++logM;
+  for (int Ns = 1; Ns < M;) {
+    const int R = M / Ns >= 4 ? 4 : 2;
+    const int lper = logM - (R == 4 ? 2 : 1), per = 1 << lper;
+    for (int e = threadIdx.x; e < per * C; e += blockDim.x) {
+      const int cl = e >> lper, j = e & (per - 1);
+      if (R == 4) fft_stage<4>(a + cl * M, b + cl * M, M, Ns, j, tw, sign);
+      else fft_stage<2>(a + cl * M, b + cl * M, M, Ns, j, tw, sign);
+    }
+    __syncthreads();
+    float2* t = a; a = b; b = t;
+    Ns *= R;
+  }
+  return a;
+}
+
 // one line per block: rows of length M (stride 1) starting at data + line*M
 __global__ void k_fft_rows(float2* __restrict__ data, int M, int logM, const float2* __restrict__ tw, float sign) {
   extern __shared__ float2 s[];
   float2* row = data + (size_t)blockIdx.x * M;
-  for (int i = threadIdx.x; i < M; i += blockDim.x) s[__brev(i) >> (32 - logM)] = row[i];
+  for (int i = threadIdx.x; i < M; i += blockDim.x) s[i] = row[i];
   __syncthreads();
-  for (int half = 1; half < M; half <<= 1) {
-    const int step = M / (2 * half);
-    for (int k = threadIdx.x; k < M / 2; k += blockDim.x) {
-      const int pos = k & (half - 1);
-      const int i = ((k - pos) << 1) + pos, j = i + half;
-      float2 w = tw[pos * step];
-      w.y *= sign;
-      const float2 t = cmul(w, s[j]);
-      const float2 a = s[i];
-      s[j] = make_float2(a.x - t.x, a.y - t.y);
-      s[i] = make_float2(a.x + t.x, a.y + t.y);
-    }
-    __syncthreads();
-  }
-  for (int i = threadIdx.x; i < M; i += blockDim.x) row[i] = s[i];
+  const float2* res = fft_lines(s, s + M, M, 1, tw, sign);
+  for (int i = threadIdx.x; i < M; i += blockDim.x) row[i] = res[i];
 }
 
 // C columns per block: columns of length M with row stride `ld`
@@ -172,27 +221,13 @@ __global__ void k_fft_cols(float2* __restrict__ data, int M, int logM, int ld, i
   const int c0 = blockIdx.x * C;
   for (int e = threadIdx.x; e < M * C; e += blockDim.x) {
     const int r = e / C, cl = e % C;
-    s[cl * M + (__brev(r) >> (32 - logM))] = data[(size_t)r * ld + c0 + cl];
+    s[cl * M + r] = data[(size_t)r * ld + c0 + cl];
   }
   __syncthreads();
-  for (int half = 1; half < M; half <<= 1) {
-    const int step = M / (2 * half);
-    for (int e = threadIdx.x; e < (M / 2) * C; e += blockDim.x) {
-      const int cl = e / (M / 2), k = e % (M / 2);
-      const int pos = k & (half - 1);
-      const int i = cl * M + ((k - pos) << 1) + pos, j = i + half;
-      float2 w = tw[pos * step];
-      w.y *= sign;
-      const float2 t = cmul(w, s[j]);
-      const float2 a = s[i];
-      s[j] = make_float2(a.x - t.x, a.y - t.y);
-      s[i] = make_float2(a.x + t.x, a.y + t.y);
-    }
-    __syncthreads();
-  }
+  const float2* res = fft_lines(s, s + M * C, M, C, tw, sign);
   for (int e = threadIdx.x; e < M * C; e += blockDim.x) {
     const int r = e / C, cl = e % C;
-    data[(size_t)r * ld + c0 + cl] = s[cl * M + r];
+    data[(size_t)r * ld + c0 + cl] = res[cl * M + r];
   }
 }
 
@@ -256,11 +291,11 @@ int ilog2(int x) { int l = 0; while ((1 << l) < x) ++l; return l; }
 void fft2(Tank& t, float2* data, float sign) {
   RippleState& r = *rs(t);
   const int lx = ilog2(r.Mx), lz = ilog2(r.Mz);
-  k_fft_rows<<<r.Mz, 256, r.Mx * sizeof(float2), t.stream>>>(data, r.Mx, lx, r.twx, sign);
-  int C = 8;
-  while (C > 1 && (size_t)r.Mz * C * sizeof(float2) > 96 * 1024) C >>= 1;
+  k_fft_rows<<<r.Mz, 256, 2 * r.Mx * sizeof(float2), t.stream>>>(data, r.Mx, lx, r.twx, sign);
+  int C = 4;                        // columns per block: 32 B of each row per load, two buffers in shared memory
+  while (C > 1 && 2 * (size_t)r.Mz * C * sizeof(float2) > 96 * 1024) C >>= 1;
   while (r.Mx % C) C >>= 1;
-  k_fft_cols<<<r.Mx / C, 256, r.Mz * C * sizeof(float2), t.stream>>>(data, r.Mz, lz, r.Mx, C, r.twz, sign);
+  k_fft_cols<<<r.Mx / C, 256, 2 * r.Mz * C * sizeof(float2), t.stream>>>(data, r.Mz, lz, r.Mx, C, r.twz, sign);
   CK(cudaGetLastError());
 }
 
@@ -297,7 +332,7 @@ RippleState& ensure(Tank& t) {
   static_assert(sizeof(float2) == 8, "");
   CK(cudaFuncSetAttribute(k_fft_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(k_fft_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-  if ((size_t)r->Mx * 8 > 200 * 1024 || (size_t)r->Mz * 8 > 200 * 1024) throw Error(-1, "ripple layer too large");
+  if (2 * (size_t)r->Mx * 8 > 200 * 1024 || 2 * (size_t)r->Mz * 8 > 200 * 1024) throw Error(-1, "ripple layer too large");
   r->topkey = (unsigned*)ralloc(t, *r, (size_t)W * W * 4);
   r->hA = (double*)ralloc(t, *r, (size_t)W * W * 8);
   r->hB = (double*)ralloc(t, *r, (size_t)W * W * 8);
