@@ -355,6 +355,7 @@ size_t tank_bytes(const TankConfig& c) {
   if (c.rx > 0) {
     const size_t nv = (size_t)(c.rx + 1) * (c.rz + 1), W = (size_t)c.wmap;
     b += nv * 8 + nv * 20 + (size_t)(2 * c.rx) * (2 * c.rz) * 16 + W * W * 28 + (size_t)(2 * c.rx + 2 * c.rz) * 8;
+    if (c.ripple_depth > 0) b += (size_t)(2 * c.rx) * (2 * c.rz) * 40;   // the fixed-depth update per mode
   }
   return b + (64 << 10) * 24;                                 // allocation granularity
 }

@@ -47,6 +47,9 @@ struct RippleState {
   double* blur_w = nullptr;
   int blur_rad = 0;
   double texel[2] = {0, 0};
+  double4* coef = nullptr;      // fixed depth: per mode the exact update over coef_dt as a 2×2 matrix
+  double* kick = nullptr;       //   and the impulse kick factor
+  double coef_dt = -1.0;
   std::vector<void*> mem;
 };
 
@@ -267,6 +270,53 @@ __global__ void k_ripple_evolve(TankDev T, float2* __restrict__ S, const float2*
   S[e] = make_float2((float)Hs, (float)Vs);
 }
 
+// With a fixed depth the update of a mode over dt is the same every frame: the damped rotation above as
+// (H, V) ← [[a11, a12], [a21, a22]]·(H, V), then V −= kick·Re(hat). Computed once per dt by
+// k_ripple_coef (same formulas, rearranged: a11 = e^(−γdt)(cos + γ sin/ω_d), a12 = e^(−γdt) sin/ω_d,
+// a21 = −e^(−γdt) ω² sin/ω_d, a22 = e^(−γdt)(cos − γ sin/ω_d)) and applied by k_ripple_evolve_fixed.
+__global__ void k_ripple_coef(TankDev T, double4* __restrict__ coef, double* __restrict__ kick, int Mx, int Mz, double Lx,
+                              double Lz, double dt, double g, double sigma_rho, double rho, double depth) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= Mx * Mz) return;
+  const int i = e % Mx, j = e / Mx;
+  const int Rx = T.rx, Rz = T.rz;
+  const int mx = i < Rx ? i : i - Mx, mz = j < Rz ? j : j - Mz;
+  if ((mx == 0 && mz == 0) || mx == -Rx || mz == -Rz) {
+    coef[e] = make_double4(0.0, 0.0, 0.0, 0.0);
+    kick[e] = 0.0;
+    return;
+  }
+  const double kx = mx * M_PI / Lx, kz = mz * M_PI / Lz;
+  const double kk = sqrt(kx * kx + kz * kz);
+  const double D = fmax(depth, 0.002);
+  const double kd = fmin(kk * D, 15.0);
+  const double th = tanh(kd);
+  const double nu = 1.0e-6, film = 0.3;
+  const double w2 = (g * kk + sigma_rho * kk * kk * kk) * th;
+  const double w = sqrt(w2);
+  const double gam = 2 * nu * kk * kk + film * kk * sqrt(nu * w * 0.125) + kk * sqrt(nu * w * 0.5) / fmax(sinh(fmin(2 * kd, 30.0)), 1e-4);
+  const double wd = sqrt(fmax(w2 - gam * gam, 1e-6));
+  const double c = cos(wd * dt), sn = sin(wd * dt), ex = exp(-gam * dt);
+  coef[e] = make_double4(ex * (c + gam * sn / wd), ex * sn / wd, -ex * w2 * sn / wd, ex * (c - gam * sn / wd));
+  const double kh = 2 * M_PI / 0.12;
+  const double hp = 1 - exp(-(kk * kk) / (kh * kh));
+  const double sw = fmax(1.2 * Lx / Rx, 0.003);
+  const double spread = exp(-0.5 * kk * kk * sw * sw);
+  kick[e] = (kk * th / rho) * hp * spread;
+}
+
+__global__ void k_ripple_evolve_fixed(float2* __restrict__ S, const float2* __restrict__ hat, const double4* __restrict__ coef,
+                                      const double* __restrict__ kick, int n) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const double4 a = coef[e];
+  const float2 v = S[e];
+  const double Hs = v.x, Vs = v.y;
+  const double H2 = a.x * Hs + a.y * Vs;
+  const double V2 = a.z * Hs + a.w * Vs - kick[e] * (double)hat[e].x;
+  S[e] = make_float2((float)H2, (float)V2);
+}
+
 // field = ifft (already in S, unnormalised) → heights and slopes; masked = field · mirrored mask → A
 __global__ void k_ripple_field(TankDev T, const float2* __restrict__ S, float2* __restrict__ A, const float* __restrict__ mask,
                                float4* __restrict__ field, int Mx, int Mz, double dx, double dz) {
@@ -449,7 +499,19 @@ void ripple_frame(Tank& t, double frame_dt) {
   k_ripple_src<<<nb, 256, 0, t.stream>>>(t.d, t.d.rsrc, r.A, r.Mx, r.Mz, 1.0 / (dx * dz));
   CK(cudaMemsetAsync(t.d.rsrc, 0, (size_t)nv * 8, t.stream));
   fft2(t, r.A, -1.f);
-  k_ripple_evolve<<<nb, 256, 0, t.stream>>>(t.d, r.S, r.A, r.Mx, r.Mz, r.Lx, r.Lz, frame_dt, r.g, r.sigma_rho, r.rho, r.depth);
+  if (r.depth > 0 && frame_dt > 0) {
+    if (!r.coef) {
+      r.coef = (double4*)ralloc(t, r, (size_t)nm * sizeof(double4));
+      r.kick = (double*)ralloc(t, r, (size_t)nm * sizeof(double));
+    }
+    if (frame_dt != r.coef_dt) {
+      k_ripple_coef<<<nb, 256, 0, t.stream>>>(t.d, r.coef, r.kick, r.Mx, r.Mz, r.Lx, r.Lz, frame_dt, r.g, r.sigma_rho, r.rho, r.depth);
+      r.coef_dt = frame_dt;
+    }
+    k_ripple_evolve_fixed<<<nb, 256, 0, t.stream>>>(r.S, r.A, r.coef, r.kick, nm);
+  } else {
+    k_ripple_evolve<<<nb, 256, 0, t.stream>>>(t.d, r.S, r.A, r.Mx, r.Mz, r.Lx, r.Lz, frame_dt, r.g, r.sigma_rho, r.rho, r.depth);
+  }
   fft2(t, r.S, 1.f);
   k_ripple_field<<<nb, 256, 0, t.stream>>>(t.d, r.S, r.A, r.mask, r.field, r.Mx, r.Mz, dx, dz);
   fft2(t, r.A, -1.f);

@@ -683,8 +683,10 @@ class Tank:
         vmax = max(self.vmax, 0.4)
         return int(min(max(math.ceil(frame_dt / (1.4 * self.h / vmax)), 1), 6))
 
-    def step(self, frame_dt, ripple_layer=None):
-        """A frame: CFL sub-steps, then whitewater, top height and ripples (``solver.py:716-728``)."""
+    def step(self, frame_dt, ripple_layer=None, ripple_depth=0.0):
+        """A frame: CFL sub-steps, then whitewater, top height and ripples (``solver.py:716-728``). A
+        ripple_depth > 0 fixes the dispersion depth (the build's extension for a stated depth); otherwise it is
+        the mean liquid depth, as the reference."""
         n = self.substeps_for(frame_dt)
         dt = frame_dt / n
         for _ in range(n):
@@ -696,7 +698,7 @@ class Tank:
             from . import ripple as rp
             self.top = rp.top_height(self)
             mean_depth = min(max(len(self.pos) * self.vp / (self.nx * self.nz * self.h * self.h), 0.003), self.rim)
-            ripple_layer.frame(frame_dt, mean_depth, self.rsrc, rp.ripple_mask(self))
+            ripple_layer.frame(frame_dt, ripple_depth if ripple_depth > 0 else mean_depth, self.rsrc, rp.ripple_mask(self))
             self.rsrc[:] = 0
         return n
 

@@ -236,10 +236,13 @@ def test_frame_step_whitewater_top_height_and_ripples(pkg):
     gpu.close()
 
 
-def test_ripple_layer_spectral_update(pkg):
-    """One ripple frame with a known impulse pattern and no particles (dry floor: mask 0.75)."""
+@pytest.mark.parametrize('depth', [0.0, 0.05])
+def test_ripple_layer_spectral_update(pkg, depth):
+    """Two ripple frames with impulses from merging drops, at the mean liquid depth (0) and at a stated depth
+    (the per-mode update then computed once and reused on the second frame)."""
     R = 32
-    gpu = pkg.Tank(nx=24, ny=8, nz=16, h=0.025, iters=4, whitewater=False, ripple=(R, R), wmap=32, capacity=16384)
+    gpu = pkg.Tank(nx=24, ny=8, nz=16, h=0.025, iters=4, whitewater=False, ripple=(R, R), wmap=32, capacity=16384,
+                   ripple_depth=depth)
     # drops landing put impulses into the source grid; here: add a few airborne particles that merge
     rng = np.random.default_rng(3)
     pool = gpu.origin + (np.stack(np.meshgrid(np.arange(24), np.arange(3), np.arange(16), indexing='ij'), -1).reshape(-1, 3)
@@ -256,7 +259,7 @@ def test_ripple_layer_spectral_update(pkg):
     layer = orp.RippleLayer(R, R, 24 * 0.025, 16 * 0.025)
     for f in range(2):
         gpu.step(1 / 60)
-        ora.step(1 / 60, layer)
+        ora.step(1 / 60, layer, ripple_depth=depth)
     S = gpu.ripple_field(pkg.native.FIELD_RIPPLE_STATE, (2 * R, 2 * R, 2), np.float32)
     assert np.abs(layer.S).max() > 0
     assert_close_field(S[..., 0], layer.S.real, rtol=1e-4, what='ripple state (height)')
