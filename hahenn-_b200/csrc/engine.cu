@@ -310,8 +310,7 @@ Tank::Tank(const TankConfig& c) : cfg(c) {
   D.ctr = (Counters*)alloc(sizeof(Counters));
   D.wpos = (float4*)alloc(2 * (size_t)D.ww_cap * 16); D.wvel = (float4*)alloc(2 * (size_t)D.ww_cap * 16);
   if (D.rx > 0) D.rsrc = (long long*)alloc((size_t)(D.rx + 1) * (D.rz + 1) * 8);
-  CK(cudaMallocHost(&h_ctr, sizeof(Counters)));
-  memset(h_ctr, 0, sizeof(Counters));
+  h_ctr = new Counters();          // read back with a synchronised copy: host memory needs no pinning
   CK(cudaStreamSynchronize(stream));
   solo = new Group({this}, stream);
 }
@@ -324,7 +323,7 @@ Tank::~Tank() {
   if (stream) cudaStreamSynchronize(stream);
   if (snap.p) { cudaFree(snap.p); cudaFree(snap.v); cudaFree(snap.wp); cudaFree(snap.wv); cudaFree(snap.pres); cudaFree(snap.ripple); }
   free_ripple(*this);
-  if (h_ctr) cudaFreeHost(h_ctr);
+  delete h_ctr;
   for (int k = 0; k < 2; ++k) {
     if (h_stage_p[k]) { cudaFreeHost(h_stage_p[k]); cudaFreeHost(h_stage_v[k]); }
     if (stage_ev[k]) cudaEventDestroy(stage_ev[k]);
@@ -888,10 +887,10 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
   CK(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device));
   CK(sor_tb_prepare());
   const int n = (int)tanks.size();
-  CK(cudaMalloc(&d_tanks, n * sizeof(TankDev)));
-  CK(cudaMallocHost(&h_tanks, n * sizeof(TankDev)));
-  CK(cudaMalloc(&d_bpfx, kFamCount * (n + 1) * sizeof(int)));
-  CK(cudaMalloc(&d_ppfx, 2 * (n + 1) * sizeof(int)));
+  CK(cudaMallocAsync(&d_tanks, n * sizeof(TankDev), stream));
+  h_tanks = new TankDev[n];
+  CK(cudaMallocAsync(&d_bpfx, kFamCount * (n + 1) * sizeof(int), stream));
+  CK(cudaMallocAsync(&d_ppfx, 2 * (n + 1) * sizeof(int), stream));
   CK(cudaMemsetAsync(d_ppfx, 0, 2 * (n + 1) * sizeof(int), stream));
   std::vector<int> pf(kFamCount * (n + 1));
   for (int f = 0; f < kFamCount; ++f) {
@@ -901,17 +900,17 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
     ctx.nblocks[f] = acc;
     ctx.bpfx[f] = d_bpfx + f * (n + 1);
   }
-  CK(cudaMalloc(&d_bsum, std::max(1, ctx.nblocks[kFamScan]) * sizeof(long long)));
+  CK(cudaMallocAsync(&d_bsum, std::max(1, ctx.nblocks[kFamScan]) * sizeof(long long), stream));
   CK(cudaMemcpyAsync(d_bpfx, pf.data(), pf.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
   std::vector<int> hp(n + 1, 0);
   for (int i = 0; i < n; ++i) hp[i + 1] = hp[i] + tanks[i]->d.nhalf;
-  CK(cudaMalloc(&d_hpfx, (n + 1) * sizeof(int)));
-  CK(cudaMalloc(&d_apfx, 2 * (n + 1) * sizeof(int)));
+  CK(cudaMallocAsync(&d_hpfx, (n + 1) * sizeof(int), stream));
+  CK(cudaMallocAsync(&d_apfx, 2 * (n + 1) * sizeof(int), stream));
   CK(cudaMemsetAsync(d_apfx, 0, 2 * (n + 1) * sizeof(int), stream));
   CK(cudaMemcpyAsync(d_hpfx, hp.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
-  CK(cudaMalloc(&d_barrier, sizeof(GridBarrier)));
+  CK(cudaMallocAsync(&d_barrier, sizeof(GridBarrier), stream));
   CK(cudaMemsetAsync(d_barrier, 0, sizeof(GridBarrier), stream));
-  CK(cudaMalloc(&d_ticket, 4 * sizeof(unsigned)));
+  CK(cudaMallocAsync(&d_ticket, 4 * sizeof(unsigned), stream));
   CK(cudaMemsetAsync(d_ticket, 0, 4 * sizeof(unsigned), stream));
   // one block per SM: the grid barrier's cost grows with the number of arriving blocks
   sor_blocks = std::min(std::min(sor_persist_max_blocks(device), sm_count), std::max(1, (hp[n] + kThreads - 1) / kThreads));
@@ -940,9 +939,11 @@ Group::~Group() {
       if (t->dep == ev_done) { cudaStreamWaitEvent(t->stream, ev_done, 0); t->dep = nullptr; }
     cudaEventDestroy(ev_done);
   }
-  cudaFree(d_hpfx); cudaFree(d_apfx); cudaFree(d_barrier); cudaFree(d_ticket);
-  if (d_tbl) cudaFree(d_tbl);
-  cudaFree(d_tanks); cudaFreeHost(h_tanks); cudaFree(d_bpfx); cudaFree(d_ppfx); cudaFree(d_bsum);
+  // stream-ordered frees: no device-wide synchronisation (other batches keep running)
+  for (void* p : {(void*)d_hpfx, (void*)d_apfx, (void*)d_barrier, (void*)d_ticket, d_tbl, (void*)d_tanks, (void*)d_bpfx,
+                  (void*)d_ppfx, (void*)d_bsum})
+    if (p) cudaFreeAsync(p, stream);
+  delete[] h_tanks;
   if (own_stream) cudaStreamDestroy(stream);
 }
 
@@ -950,7 +951,8 @@ void Group::ensure_tbl() {
   if (d_tbl) return;
   CK(cudaSetDevice(device));
   const int tiles = std::max(1, ctx.nblocks[kFamTiles]);
-  CK(cudaMalloc(&d_tbl, tbl_list_bytes(tiles)));
+  CK(cudaMallocAsync(&d_tbl, tbl_list_bytes(tiles), stream));
+  CK(cudaStreamSynchronize(stream));
   tbl_assign(ctx, d_tbl, tiles);
 }
 

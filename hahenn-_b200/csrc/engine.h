@@ -69,7 +69,7 @@ struct Snapshot {
 struct Tank {
   TankConfig cfg;
   TankDev d{};                    // host image of the device descriptor
-  Counters* h_ctr = nullptr;      // pinned mirror for reads
+  Counters* h_ctr = nullptr;      // host mirror for reads
   cudaStream_t stream = nullptr;
   std::vector<void*> dmem;        // device allocations owned by the tank
   Obj* d_objs = nullptr;
@@ -140,7 +140,7 @@ struct Group {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   TankDev* d_tanks = nullptr;
-  TankDev* h_tanks = nullptr;     // pinned
+  TankDev* h_tanks = nullptr;     // host images, uploaded by ensure_uploaded
   int* d_bpfx = nullptr;
   int* d_ppfx = nullptr;          // [0, n+1) in, [n+1, 2n+2) sorted
   long long* d_bsum = nullptr;
