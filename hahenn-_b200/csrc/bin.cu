@@ -64,6 +64,30 @@ __global__ void __launch_bounds__(kThreads) k_bin(const TankDev* __restrict__ ta
   }
 }
 
+// the cell counts alone, for a count pass between sub-steps (no ranks: the next sub-step bins again)
+__global__ void __launch_bounds__(kThreads) k_bin_count(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ pfx) {
+  const int total = pfx[ntanks];
+  const int lane = threadIdx.x & 31;
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < total; base += stride) {
+    const int idx = base + lane;
+    int cell = -1, t = 0;
+    const TankDev* T = nullptr;
+    if (idx < total) {
+      t = find_slot(pfx, ntanks, idx);
+      T = tanks + t;
+      const int local = idx - pfx[t];
+      const int n_live = T->ctr->n_live;
+      cell = particle_cell(*T, load_in(*T, local, n_live, T->pA, T->pE));
+    }
+    const unsigned act = __ballot_sync(0xffffffffu, cell >= 0);
+    if (cell >= 0) {
+      const unsigned peers = __match_any_sync(act, ((unsigned long long)(unsigned)t << 32) | (unsigned)cell);
+      if (lane == __ffs(peers) - 1) atomicAdd(T->cnt + cell, __popc(peers));   // result unused: a reduction
+    }
+  }
+}
+
 // --- scan: tiles of kScanTile cells; bsum[block] = tile sum; then per tile: prefix of earlier tiles of the
 // same tank + in-tile exclusive scan
 __device__ __forceinline__ int block_sum(int v, int* red) {
@@ -192,6 +216,10 @@ void launch_begin_count(const LaunchCtx& L) {
 void launch_bin(const LaunchCtx& L) {
   static int resident[128] = {};
   k_bin<<<resident_grid((const void*)k_bin, resident), kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_in);
+}
+void launch_bin_count(const LaunchCtx& L) {
+  static int resident[128] = {};
+  k_bin_count<<<resident_grid((const void*)k_bin_count, resident), kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_in);
 }
 void launch_scan(const LaunchCtx& L) {
   const int nb = L.nblocks[kFamScan];

@@ -542,7 +542,7 @@ void Tank::count_pass() {
   join();
   solo->ensure_uploaded();
   launch_begin_count(solo->ctx);
-  launch_bin(solo->ctx);
+  launch_bin_count(solo->ctx);
   launch_scan(solo->ctx);
   CK(cudaGetLastError());
 }

@@ -52,6 +52,7 @@ inline int resident_grid(const void* k, int* cache) {
 // per-kernel launchers (bin.cu, grid.cu, sor.cu, g2p.cu)
 void launch_begin_count(const LaunchCtx& L);   // prefix only, for a count pass between sub-steps
 void launch_bin(const LaunchCtx& L);
+void launch_bin_count(const LaunchCtx& L);     // cell counts only, for a count pass
 void launch_scan(const LaunchCtx& L);
 void launch_scatter(const LaunchCtx& L);
 void launch_geom(const LaunchCtx& L);
