@@ -289,9 +289,15 @@ def test_sor_bit_exact_when_the_sweep_grid_is_capped(pkg):
     gpu.close()
 
 
-def test_batch_equals_solo_bit_for_bit(pkg):
-    """Tanks of uneven sizes stepped in one batch give exactly the particles they give alone."""
-    specs = [pkg.workloads.random_tank(s, axes=(16, 24, 32)) for s in (1, 2, 3)]
+@pytest.mark.parametrize('axes,seeds', [((16, 24, 32), (1, 2, 3)), ((16, 48), (1, 2, 16))])
+def test_batch_equals_solo_bit_for_bit(pkg, axes, seeds):
+    """Tanks of uneven sizes stepped in one batch give exactly the particles they give alone; with the 48³
+    tank (seed 16) the batch spans two size lanes (its own stream and graph each, forked and joined every
+    sub-step)."""
+    specs = [pkg.workloads.random_tank(s, axes=axes) for s in seeds]
+    if axes == (16, 48):
+        sizes = [w['nx'] * w['ny'] * w['nz'] for w in specs]
+        assert min(sizes) < 1 << 16 <= max(sizes), sizes
 
     def make():
         out = []
