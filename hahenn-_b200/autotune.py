@@ -3,8 +3,9 @@
 Knobs (``suiri_tune`` / ``suiri_batch_tune``):
   * blocks per SM of the persistent particle kernels (binning, scatter, G2P);
   * the form of the pressure solve (sor_mode): 0 one launch per colour sweep inside the sub-step graph,
-    1 the whole solve as one cooperative launch with a grid barrier between sweeps, 2 and 3 two and four
-    colour sweeps per launch on shared-memory tiles with halos (temporal blocking).
+    1 the whole solve as one cooperative launch with a grid barrier between sweeps, 2 two colour sweeps
+    per launch over per-tile lists of active cells, 3 four sweeps per launch on shared-memory tiles with
+    halos (temporal blocking).
 
 Each candidate is timed on the device (events on the tank's or batch's stream) over a few sub-steps of the
 real state, after one sub-step that captures its graph. Tuning advances the simulation by those

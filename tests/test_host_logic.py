@@ -1,0 +1,56 @@
+"""Host-side logic that needs no GPU: the autotuner's choice (with a stand-in for a tank or batch) and the
+synthetic workloads' shapes and seeding."""
+import importlib
+
+import numpy as np
+import pytest
+
+autotune = importlib.import_module('hahenn-_b200.autotune')
+workloads = importlib.import_module('hahenn-_b200.workloads')
+
+
+class FakeTarget:
+    """Times each (blocks per SM, sor_mode) from a table; a None entry cannot be launched."""
+
+    def __init__(self, table):
+        self.table, self.current, self.applied = table, None, []
+
+    def tune(self, bps, mode):
+        self.current = (bps, mode)
+        self.applied.append(self.current)
+
+    def time_substeps(self, dt, steps):
+        ms = self.table[self.current]
+        if ms is None:
+            raise RuntimeError(f'{self.current} cannot be launched')
+        return ms * steps
+
+
+def test_autotune_keeps_the_fastest_and_skips_shapes_that_fail():
+    table = {c: 5.0 for c in autotune.CANDIDATES}
+    table[(8, 0)] = 3.0
+    table[(4, 1)] = None
+    t = FakeTarget(table)
+    best, timings = autotune.autotune(t, 1 / 240)
+    assert best == (8, 0) and t.current == (8, 0)
+    assert timings[(4, 1)] == float('inf') and timings[(8, 0)] == pytest.approx(3.0)
+    assert set(timings) == set(autotune.CANDIDATES)
+
+
+def test_autotune_raises_when_nothing_launches():
+    t = FakeTarget({c: None for c in autotune.CANDIDATES})
+    with pytest.raises(RuntimeError):
+        autotune.autotune(t, 1 / 240)
+
+
+def test_workloads_shapes_and_seeds():
+    w = workloads.obstacles_inflow()
+    assert (w['nx'], w['ny'], w['nz']) == (128, 64, 64)
+    assert 1.69e6 < len(w['pos']) < 1.71e6 and w['pos'].dtype == np.float32
+    lo, hi = w['origin'], w['origin'] + w['h'] * np.array([w['nx'], w['ny'], w['nz']])
+    assert np.all(w['pos'] >= lo) and np.all(w['pos'] <= hi)    # float32 may round onto the upper wall
+    np.testing.assert_array_equal(workloads.obstacles_inflow()['pos'], w['pos'])          # seeded
+    specs = workloads.batch_tanks(64)
+    assert len(specs) == 64
+    assert all(a in workloads.AXES_BATCH for s in specs for a in (s['nx'], s['ny'], s['nz']))
+    assert len({(s['nx'], s['ny'], s['nz']) for s in specs}) > 10                        # uneven sizes
