@@ -1,16 +1,24 @@
 #!/usr/bin/env python
-"""Benchmark: particle-steps/s of the FLIP sub-step on the obstacles-and-inflow workload.
+"""Benchmark: particle-steps/s of the FLIP sub-step, batched against plain, on one GPU per rank.
 
-Workload (one GPU): 128×64(up)×64 cells at h = 1/64 m, ≈1.70M particles (bottom 26 layers at 8 per cell),
-a sphere, a turned box and a cylinder (face fractions from analytic SDFs), a 2 cm faucet at 1.5 m/s
-emitting 10 particles per sub-step, one floor drain, 100 SOR iterations at ω = 1.8, FLIP 0.95,
-dt = 1/240 s. A step is one sub-step of the liquid: binning, P2G, forces and divergence, the pressure
-solve, projection, G2P with collisions, drains and drop/whitewater logic. Synthetic seeded data.
+Default workload (`--workload batch`): 64 independent tanks of uneven sizes, each grid axis drawn from
+{16, 24, 32, 48, 64} cells, h = 1 m / (vertical cells), a bottom block filled to U[0.2, 0.6] at 8 particles
+per cell, 0-3 random obstacles (sphere, box or cylinder; face fractions from analytic SDFs), 80 SOR
+iterations at ω = 1.7, FLIP 0.95, dt = 1/240 s (11.7M particles, 3.7M cells; seed = tank index). A step is
+one sub-step of all 64 tanks: binning, P2G, forces and divergence, the pressure solve, projection, G2P with
+collisions and drop/whitewater logic, advanced together by the batched, graph-captured launches with the
+form of the pressure solve picked by the autotuner. `value` is the batch's particle-steps/s; the same 64
+scenes stepped one by one on the plain path give `plain_sequential`. Synthetic seeded data.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl suiri|reference]
+Other workloads: `obstacles_inflow` (one 128×64×64 tank with obstacles, a faucet and a drain),
+`full_scene` (256×128×128 with rain and the 1024×512 ripple layer), `serve` (Poisson scene requests).
 
-Under torchrun each rank advances its own replica of the workload (tanks do not interact: no collective
-in the data path); the time is the max over ranks and the value counts every rank's particles.
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl suiri|reference] [--workload ...]
+
+Under torchrun each rank advances its own replica of the workload (tanks do not interact: no collective in
+the data path); the time is the max over ranks and the value counts every rank's particles. `--impl
+reference` times the reference's CPU solver (its NumPy restatement, pinned bit-exact against it) on the
+same workload on this host's cores.
 """
 import argparse
 import importlib
@@ -28,6 +36,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 METRIC = 'particle-steps/s'
 L2_FLUSH_BYTES = 256 << 20          # larger than the 126 MB L2; written between timed steps
+DT = 1 / 240
 
 
 def pkg():
@@ -43,10 +52,10 @@ def peaks():
         return 6650.0, 'fallback'
 
 
-def sor_traffic():
-    """DRAM bytes per SOR sweep launch from the committed ncu summary (null if none)."""
+def profile_figure(name):
+    """A figure from a committed ncu summary under profiles/ (None if absent)."""
     try:
-        with open(os.path.join(ROOT, 'profiles', 'sor_sweep_traffic.json')) as f:
+        with open(os.path.join(ROOT, 'profiles', name)) as f:
             return json.load(f)
     except Exception:
         return None
@@ -131,7 +140,9 @@ class Clocks:
                     reasons=reasons, samples=len(sm), source='nvml' if self.nv else 'nvidia-smi')
 
 
+# ------------------------------------------------------------------ workloads
 def make_tank(P, w, device, host_inflow=False):
+    """The single-tank workload (obstacles and inflow) on the plain path."""
     prm = w['params']
     t = P.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=prm['flip'], omega=prm['omega'], iters=prm['iters'],
                gravity=prm['g'], whitewater=True, ripple=None, capacity=int(len(w['pos']) * 1.25) + 100000,
@@ -158,13 +169,63 @@ def faucet_particles(e, dt, rng):
     return p.astype(np.float32), v.astype(np.float32)
 
 
-def _port_tank(w):
-    """The CPU oracle (NumPy restatement of the reference solver) set up on the workload."""
+def batch_specs(n):
+    return pkg().workloads.batch_tanks(n)
+
+
+def batch_config(specs):
+    """The batching workload's config, identical in both arms."""
+    return dict(workload=f'batch_{len(specs)}_tanks', tanks=len(specs),
+                particles=int(sum(len(w['pos']) for w in specs)),
+                cells=int(sum(w['nx'] * w['ny'] * w['nz'] for w in specs)),
+                axes=[16, 24, 32, 48, 64], sor_iters=80, omega=1.7, flip=0.95, dt=DT, sdf_mode='analytic',
+                whitewater=True, seed='tank index')
+
+
+def plain_config(w):
+    prm = w['params']
+    return dict(workload=w['name'], particles=int(len(w['pos'])), cells=w['nx'] * w['ny'] * w['nz'],
+                sor_iters=prm['iters'], omega=prm['omega'], flip=prm['flip'], dt=prm['dt'], sdf_mode='analytic',
+                inflow_per_step=w['emitters'][0]['count'], whitewater=True)
+
+
+def make_batch_tanks(P, specs, device, add=True):
+    ts = []
+    for w in specs:
+        prm = w['params']
+        t = P.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=prm['flip'], omega=prm['omega'],
+                   iters=prm['iters'], gravity=prm['g'], whitewater=True, ripple=None,
+                   capacity=int(len(w['pos']) * 1.2) + 1000, ww_capacity=20000, device=device, sdf_mode='analytic')
+        t.set_objects(w['objects'])
+        if add:
+            t.add_particles(w['pos'])
+        ts.append(t)
+    return ts
+
+
+def size_lanes(specs):
+    """Each tank's size lane as the library forms them (under 2^16 cells, under 2^19, larger; occupied lanes
+    in that order) and the number of lanes."""
+    raw = [0 if c < 1 << 16 else (1 if c < 1 << 19 else 2) for c in (w['nx'] * w['ny'] * w['nz'] for w in specs)]
+    occ = sorted(set(raw))
+    return [occ.index(r) for r in raw], len(occ)
+
+
+def launches_per_substep(sor_mode, iters, residual=False):
+    """Kernels of one sub-step graph of a group (bin, scan ×2, scatter and the rest: 10) plus the solve's."""
+    sor = {0: 2 * iters, 1: 1, 2: 1 + iters + (iters & 1), 3: -(-2 * iters // 4) + (-(-2 * iters // 4) & 1), 4: 1}[sor_mode]
+    return 10 + (sor if iters > 0 else 0) + (2 if residual else 0)
+
+
+# ------------------------------------------------------------------ the CPU oracle (reference arm, cpu_baseline)
+def _port_tank(w, ww_cap=140000):
+    """The CPU oracle (NumPy restatement of the reference solver) set up on a workload tank, obstacles as the
+    web version's analytic shapes, as the GPU arm uses them."""
     from oracle import flip as of
     from oracle import sdf as sdfm
     prm = w['params']
     t = of.Tank(w['nx'], w['ny'], w['nz'], w['h'], origin=w['origin'], flip=prm['flip'], omega=prm['omega'],
-                iters=prm['iters'], g=prm['g'], whitewater=True, rng_mode='hash', sdf_mode='lattice')
+                iters=prm['iters'], g=prm['g'], whitewater=True, rng_mode='hash', sdf_mode='analytic', ww_cap=ww_cap)
     objs = []
     for it in w['objects']:
         if it['kind'] == 'obstacle':
@@ -176,48 +237,45 @@ def _port_tank(w):
     return t
 
 
-def _port_steps(t, w, steps, rng):
-    """`steps` sub-steps with the faucet's particles added on the host; returns the particle-steps."""
-    dt = w['params']['dt']
+def _port_steps(tanks, specs, steps, rng):
+    """`steps` sub-steps of every oracle tank (faucet particles added on the host); returns particle-steps."""
     n_ps = 0
     for _ in range(steps):
-        for e in w['emitters']:
-            p, v = faucet_particles(e, dt, rng)
-            t.add_particles(p.astype(np.float64), v.astype(np.float64))
-        n_ps += len(t.pos)
-        t.frame += 1
-        t.substep(dt)
+        for t, w in zip(tanks, specs):
+            for e in w['emitters']:
+                p, v = faucet_particles(e, w['params']['dt'], rng)
+                t.add_particles(p.astype(np.float64), v.astype(np.float64))
+            n_ps += len(t.pos)
+            t.frame += 1
+            t.substep(w['params']['dt'])
     return n_ps
 
 
-def cpu_port_rate(w, steps):
-    """The CPU oracle on one core for `steps` sub-steps of the workload: particle-steps/s."""
-    t = _port_tank(w)
-    rng = np.random.default_rng(1)
-    t0 = time.perf_counter()
-    n_ps = _port_steps(t, w, steps, rng)
-    el = time.perf_counter() - t0
-    return n_ps / el, el
-
-
-def _port_replica(steps, warm, barrier, out, k):
-    """One CPU replica (a spawned process): set up, warm up, wait for the others, time `steps` sub-steps."""
-    sys.path.insert(0, ROOT)
+def _workload_specs(workload, n_tanks):
     P = pkg()
-    w = P.workloads.obstacles_inflow()
-    t = _port_tank(w)
+    if workload == 'batch':
+        return P.workloads.batch_tanks(n_tanks)
+    return [P.workloads.obstacles_inflow()]
+
+
+def _port_worker(workload, n_tanks, idx, steps, warm, barrier, out, k):
+    """One CPU process (spawned): its share of the workload's tanks, warmed up, then `steps` timed sub-steps
+    of all of them from a common start."""
+    sys.path.insert(0, ROOT)
+    specs = [_workload_specs(workload, n_tanks)[i] for i in idx]
+    ww = 20000 if workload == 'batch' else 140000
+    tanks = [_port_tank(w, ww) for w in specs]
     rng = np.random.default_rng(1 + k)
     if warm:
-        _port_steps(t, w, warm, rng)
+        _port_steps(tanks, specs, warm, rng)
     barrier.wait(timeout=900)
     t0 = time.perf_counter()
-    n_ps = _port_steps(t, w, steps, rng)
+    n_ps = _port_steps(tanks, specs, steps, rng)
     out.put((n_ps, time.perf_counter() - t0))
 
 
-def cpu_replicas_count():
-    """One replica per usable core, at most 32, and at most one per 2 GB of available memory (a replica of
-    the 1.7M-particle workload peaks near 1.1 GB)."""
+def cpu_processes():
+    """One process per usable core, at most 32, and at most one per 2 GB of available memory."""
     cores = len(os.sched_getaffinity(0))
     avail_gb = 0.0
     try:
@@ -230,19 +288,36 @@ def cpu_replicas_count():
     return max(1, min(cores, 32, int(avail_gb // 2)))
 
 
-def cpu_replicas_rate(steps, warm, procs):
-    """`procs` independent replicas of the CPU oracle, one process (one core) each, timed together from a
-    common start: all replicas' particle-steps ÷ the slowest replica's time."""
+def partition(sizes, parts):
+    """Indices split into `parts` groups of near-equal total size (largest first onto the lightest group)."""
+    groups, load = [[] for _ in range(parts)], [0] * parts
+    for i in sorted(range(len(sizes)), key=lambda i: -sizes[i]):
+        g = load.index(min(load))
+        groups[g].append(i)
+        load[g] += sizes[i]
+    return [g for g in groups if g]
+
+
+def cpu_parallel_rate(workload, n_tanks, steps, warm, procs):
+    """The workload on `procs` processes of one core each, timed together from a common start: all processes'
+    particle-steps ÷ the slowest process's time. The batch's tanks are partitioned over the processes; the
+    single-tank workload runs one replica per process."""
     import multiprocessing as mp
+    specs = _workload_specs(workload, n_tanks)
+    if workload == 'batch':
+        groups = partition([len(w['pos']) for w in specs], procs)
+    else:
+        groups = [[0] for _ in range(procs)]
     ctx = mp.get_context('spawn')
-    barrier, out = ctx.Barrier(procs), ctx.Queue()
+    barrier, out = ctx.Barrier(len(groups)), ctx.Queue()
     env = {k: os.environ.get(k) for k in ('OMP_NUM_THREADS', 'OPENBLAS_NUM_THREADS', 'MKL_NUM_THREADS')}
     for k in env:
         os.environ[k] = '1'
-    ps = [ctx.Process(target=_port_replica, args=(steps, warm, barrier, out, k)) for k in range(procs)]
+    ps = [ctx.Process(target=_port_worker, args=(workload, n_tanks, g, steps, warm, barrier, out, k))
+          for k, g in enumerate(groups)]
     for p in ps:
         p.start()
-    res = [out.get(timeout=1800) for _ in ps]
+    res = [out.get(timeout=3600) for _ in ps]
     for p in ps:
         p.join(timeout=60)
     for k, v in env.items():
@@ -250,9 +325,52 @@ def cpu_replicas_rate(steps, warm, procs):
             os.environ.pop(k, None)
         else:
             os.environ[k] = v
-    return sum(r[0] for r in res) / max(r[1] for r in res), max(r[1] for r in res)
+    el = max(r[1] for r in res)
+    return sum(r[0] for r in res) / el, el, len(groups)
 
 
+def cpu_sample_rate(specs, steps=1, every=4):
+    """The oracle on one core over a bounded sample of the workload: every `every`-th tank, `steps`
+    sub-steps (setup untimed). Returns particle-steps/s, seconds and the sample's description."""
+    sub = specs[::every]
+    tanks = [_port_tank(w, 20000 if len(specs) > 1 else 140000) for w in sub]
+    rng = np.random.default_rng(1)
+    t0 = time.perf_counter()
+    n_ps = _port_steps(tanks, sub, steps, rng)
+    el = time.perf_counter() - t0
+    what = (f'{len(sub)} of the {len(specs)} tanks (every {every}th, {sum(len(w["pos"]) for w in sub)} particles)'
+            if len(specs) > 1 else 'the tank')
+    return n_ps / el, el, f'{what} × {steps} sub-step(s) on the host, 1 core of {os.cpu_count()} (NumPy ' \
+                          f'restatement of the reference solver, {el:.1f} s)'
+
+
+def run_reference(args, rank):
+    """The reference's CPU path (its NumPy solver, restated and pinned bit-exact against it) on the same
+    workload, on this host's cores: rank 0 only; other ranks exit at once."""
+    if rank != 0:
+        return
+    workload = 'batch' if args.workload == 'batch' else 'obstacles_inflow'
+    specs = _workload_specs(workload, args.tanks)
+    cfg = batch_config(specs) if workload == 'batch' else plain_config(specs[0])
+    steps, warm = max(1, args.steps), max(0, args.warmup)
+    procs = cpu_processes()
+    rate, el, used = cpu_parallel_rate(workload, args.tanks, steps, warm, procs)
+    if workload == 'batch':
+        sample = (f'all {len(specs)} tanks partitioned over {used} processes (one core each, balanced by particle '
+                  f'count), each stepping all of its tanks {steps} timed sub-steps after {warm} warm-up')
+    else:
+        sample = f'{used} replicas of the tank, one process and one core each, {steps} timed sub-steps after {warm}'
+    line = dict(impl='reference', metric=METRIC, value=rate, unit=METRIC, n_gpus=args.gpus, steps=steps, warmup=warm,
+                ms_per_step=1000 * el / steps, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f64',
+                data='synthetic (seeded particles, analytic obstacles)', config=cfg,
+                cpu_baseline=dict(value=rate, unit=METRIC, cores=used, kind='port',
+                                  sample=sample + ' (NumPy restatement of the reference solver, pinned bit-exact '
+                                                  'against it; NumPy runs one core per process)'),
+                e2e=dict(value=rate, unit=METRIC, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ multi-rank bookkeeping
 def reduce_ranks(ms, particles, sor_launch_ms, device):
     """Whole-job figures of the replicas: the slowest rank's step and SOR-launch times (max over ranks) and
     the particles of all ranks (sum), so value = all ranks' particle-steps ÷ the slowest rank's time."""
@@ -275,78 +393,275 @@ def reduce_e2e(rate, world, device):
     return float(x[0]) * world
 
 
-def run_reference(args, rank):
-    """The reference's CPU path (its NumPy solver, restated and pinned bit-exact against it) on this host's
-    cores: one independent replica of the workload per core, as many as the process may use. Rank 0 only;
-    other ranks exit at once."""
-    if rank != 0:
-        return
-    w = pkg().workloads.obstacles_inflow()
-    steps, warm = max(1, min(args.steps, 3)), min(args.warmup, 3)   # ≈4 s a sub-step per core
-    procs = cpu_replicas_count()
-    rate, el = cpu_replicas_rate(steps, warm, procs)
-    line = dict(impl='reference', metric=METRIC, value=rate, unit=METRIC, n_gpus=args.gpus, steps=steps, warmup=warm,
-                ms_per_step=1000 * el / steps, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f64',
-                data='synthetic',
-                config=dict(workload=w['name'], particles=len(w['pos']), cells=w['nx'] * w['ny'] * w['nz'],
-                            sor_iters=w['params']['iters'], omega=w['params']['omega'], dt=w['params']['dt']),
-                cpu_baseline=dict(value=rate, unit=METRIC, cores=procs, kind='port',
-                                  sample=f'{procs} replicas × {steps} sub-steps of the full workload, one process '
-                                         f'and one core each (NumPy restatement of the reference solver, pinned '
-                                         f'bit-exact against it; NumPy runs one core per process)'),
-                e2e=dict(value=rate, unit=METRIC, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
-    print(json.dumps(line), flush=True)
-
-
-def run_batch(args, local):
-    """Batching workload: 64 tanks of uneven sizes (axes from {16,24,32,48,64}, h = 1/ny, fill U[0.2,0.6],
-    0-3 obstacles, 80 SOR iterations at ω = 1.7) advanced together in one set of batched, graph-captured
-    launches, against the same 64 scenes run one by one on the plain path. Both paths compute identical
-    results (the batch is bit-for-bit the plain path), so the divergence residual is equal by construction."""
+def init_ranks(world, local):
     import torch
-    from importlib import import_module
-    P = pkg()
-    autotune = import_module('hahenn-_b200.autotune').autotune
-    specs = P.workloads.batch_tanks(args.tanks)
-    dt = 1 / 240
+    import torch.distributed as dist
+    if world > 1:
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
 
-    def make():
-        ts = []
-        for w in specs:
-            t = P.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=0.95, omega=1.7, iters=80, whitewater=True,
-                       ripple=None, capacity=int(len(w['pos']) * 1.2) + 1000, ww_capacity=20000, device=local)
-            t.set_objects(w['objects'])
-            t.add_particles(w['pos'])
-            ts.append(t)
-        return ts
-    particles = sum(len(w['pos']) for w in specs)
-    cells = sum(w['nx'] * w['ny'] * w['nz'] for w in specs)
-    plain = make()
-    for t in plain:
-        t.substep(dt)
-    torch.cuda.synchronize()
-    ms_plain = 0.0
-    for t in plain:
-        ms_plain += t.time_substeps(dt, args.steps) / args.steps
-    for t in plain:
-        t.close()
-    tanks = make()
+
+# ------------------------------------------------------------------ the batching workload (default)
+def e2e_batch(P, specs, device, best, steps):
+    """The job end to end through the public API with host buffers: every scene's particles added from host
+    arrays (staged through pinned memory into the device), `steps` batched sub-steps with each scene's stats
+    read back every sub-step (pollStats), and every scene's particles read back into host arrays at the end.
+    Wall clock around all of it, after an untimed run of the same job (graph capture, staging buffers)."""
+    tanks = make_batch_tanks(P, specs, device, add=False)
     b = P.Batch(tanks)
-    best, timings = autotune(b, dt)
-    for _ in range(args.warmup):
-        b.substep(dt)
-    ms_batch = b.time_substeps(dt, args.steps) / args.steps
-    rate_b, rate_p = particles * 1000 / ms_batch, particles * 1000 / ms_plain
-    line = dict(metric=METRIC, value=rate_b, unit=METRIC, n_gpus=1, steps=args.steps, warmup=args.warmup, ms_per_step=ms_batch,
-                higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32', data='synthetic',
-                config=dict(workload=f'batch_{len(specs)}_tanks', tanks=len(specs), particles=particles, cells=cells,
-                            sor_iters=80, omega=1.7, dt=dt, tuned=dict(blocks_per_sm=best[0], sor_mode=best[1]),
-                            tuning_ms={f'{k[0]}x{k[1]}': v for k, v in timings.items()}),
-                plain_sequential=dict(value=rate_p, ms_per_step=ms_plain), batched_over_plain=rate_b / rate_p)
-    print(json.dumps(line), flush=True)
+    b.tune(best[0], best[1])
+    if len(best) > 2 and best[2]:
+        b.tune_piece(best[2])
+    host = [np.ascontiguousarray(w['pos'], np.float32) for w in specs]
+    readback = int(P.native.lib().suiri_stats_readback_bytes())
+
+    def job(n_steps):
+        h2d = d2h = 0
+        for t, pos in zip(tanks, host):
+            t.add_particles(pos)
+            h2d += 32 * len(pos)                      # staged as two float4 per particle
+        for _ in range(n_steps):
+            b.substep(DT)
+            for t in tanks:
+                t.poll_stats()
+                d2h += readback
+        n_end = 0
+        for t in tanks:
+            pos, vel, air, ids = t.particles()
+            n_end += len(ids)
+            d2h += 32 * len(ids)
+        return h2d, d2h, n_end
+
+    job(3)
+    for t in tanks:
+        t.clear_water()
+    b.sync()
+    t0 = time.perf_counter()
+    h2d, d2h, n_end = job(steps)
+    el = time.perf_counter() - t0
+    n0 = sum(len(p) for p in host)
     b.close()
     for t in tanks:
         t.close()
+    return dict(value=0.5 * (n0 + n_end) * steps / el, unit=METRIC, h2d_bytes_per_step=h2d // steps,
+                d2h_bytes_per_step=d2h // steps, wall_s=el,
+                job=f'{len(specs)} scenes uploaded from host arrays, {steps} batched sub-steps with every scene\'s '
+                    f'stats read back each sub-step, every scene\'s particles read back at the end')
+
+
+def run_batch(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    init_ranks(world, local)
+    P = pkg()
+    autotune = importlib.import_module('hahenn-_b200.autotune').autotune
+    specs = batch_specs(args.tanks)
+    cfg = batch_config(specs)
+    lane_of, nlanes = size_lanes(specs)
+    dev = f'cuda:{local}'
+
+    # the same scenes one by one on the plain path (each tank's own sub-step graph and stream)
+    plain = make_batch_tanks(P, specs, local)
+    for t in plain:
+        t.substep(DT)                                # GEOM and graph capture, untimed
+    steps_plain = max(3, min(args.steps, 20))
+    ms_plain = sum(t.time_substeps(DT, steps_plain) / steps_plain for t in plain)
+    for t in plain:
+        t.close()
+
+    tanks = make_batch_tanks(P, specs, local)
+    b = P.Batch(tanks)
+    best, timings = autotune(b, DT)
+    b.profile(True)
+    stream = torch.cuda.ExternalStream(b.stream())
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    for _ in range(max(args.warmup, 3)):
+        b.substep(DT)
+    b.sync()
+    n0 = sum(t.stats()['count'] for t in tanks)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    phases = []
+    clocks = Clocks(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()                          # L2 flush, outside the timed interval
+        ev[k][0].record(stream)
+        b.substep(DT)
+        ev[k][1].record(stream)
+        phases.append([b.phase_ms(l) for l in range(nlanes)])
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if world > 1:
+        dist.barrier()
+    step_ms = [a.elapsed_time(c) for a, c in ev]
+    st = [t.stats() for t in tanks]
+    n1 = sum(s['count'] for s in st)
+    ms = float(np.mean(step_ms))
+    particles = 0.5 * (n0 + n1)
+    sor_lane = [float(np.mean([ph[l]['pressure_solve'] for ph in phases])) for l in range(nlanes)]
+    sor_ms = max(sor_lane)
+    if world > 1:
+        ms, particles, sor_ms = reduce_ranks(ms, particles, sor_ms, dev)
+    value = particles * 1000.0 / ms
+    b.profile(False)
+    b.close()
+    for t in tanks:
+        t.close()
+    e2e = e2e_batch(P, specs, local, best, args.steps)
+    if world > 1:
+        e2e['value'] = reduce_e2e(e2e['value'], world, dev)
+    if rank == 0:
+        peak, kind = peaks()
+        iters = cfg['sor_iters']
+        mode = best[1]
+        lanes = []
+        for l in range(nlanes):
+            idx = [i for i in range(len(specs)) if lane_of[i] == l]
+            parts = sum(st[i]['count'] for i in idx)
+            nodes = sum((specs[i]['nx'] + 1) * (specs[i]['ny'] + 1) * (specs[i]['nz'] + 1) for i in idx)
+            active = sum(st[i]['active_cells'] for i in idx)
+            ph = {k: float(np.mean([p[l][k] for p in phases])) for k in P.native.PHASES}
+            fig = {}
+            for name, alg in (('p2g', 32.0 * parts + 48.0 * nodes), ('g2p', 64.0 * parts + 24.0 * nodes),
+                              ('pressure_solve', 20.0 * active * iters)):
+                gbs = alg / (ph[name] * 1e-3) / 1e9
+                fig[name] = dict(alg_bytes=alg, ms=ph[name], achieved_gbs=gbs, frac=gbs / peak)
+            lanes.append(dict(tanks=len(idx), particles=parts, nodes=nodes, active_cells=active, phases_ms=ph,
+                              kernels=fig))
+        dom = max(range(nlanes), key=lambda l: lanes[l]['phases_ms']['pressure_solve'])
+        sol = lanes[dom]['kernels']['pressure_solve']
+        per_launch = 1 if mode in (1, 4) else 2 * iters
+        tr = profile_figure('sor_cluster_batch_traffic.json' if mode == 4 else 'sor_sweep_traffic.json')
+        roofline = dict(bound='hbm', kernel='k_sor_cluster (whole solve, one launch per lane)' if mode == 4 else
+                        f'sor mode {mode}', achieved=sol['achieved_gbs'], peak=peak, unit='GB/s',
+                        frac=sol['achieved_gbs'] / peak, peak_kind=kind,
+                        traffic=None if tr is None else tr.get('dram_bytes_per_launch'),
+                        alg_bytes_per_launch=sol['alg_bytes'] / per_launch, launch_ms=sol['ms'] / per_launch,
+                        lane=dom, active_cells=lanes[dom]['active_cells'], iters=iters,
+                        unit_bytes='20 B per active cell per colour sweep',
+                        note='the solve\'s operands stay on chip (shared memory) or in L2, so the algorithmic '
+                             'rate may exceed the HBM copy rate; traffic is the DRAM bytes ncu measured per launch')
+        cpu_rate, cpu_el, cpu_what = cpu_sample_rate(specs)
+        launches = args.steps * sum(launches_per_substep(mode, iters) for _ in range(nlanes))
+        line = dict(metric=METRIC, value=value, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
+                    ms_per_step=ms, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
+                    data='synthetic (seeded particles, analytic obstacles)', config=cfg,
+                    l2='flushed (256 MiB write) between timed steps', parallelism=f'replicas{world}',
+                    tuned=dict(blocks_per_sm=best[0], sor_mode=best[1], piece_kb=best[2] if len(best) > 2 else 0),
+                    tuning_ms={'x'.join(str(v) for v in k): v for k, v in timings.items()},
+                    plain_sequential=dict(value=particles / world * 1000.0 / ms_plain, ms_per_step=ms_plain,
+                                          note='the same scenes one by one, device time summed'),
+                    batched_over_plain=ms_plain / ms if world == 1 else None,
+                    roofline=roofline, kernels=dict(peak_gbs=peak, lanes=lanes),
+                    cpu_baseline=dict(value=cpu_rate, unit=METRIC, cores=1, kind='port', sample=cpu_what),
+                    e2e=e2e, gpu_launches=launches, clocks=clk)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------ the single-tank workload
+def run_plain(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    init_ranks(world, local)
+    P = pkg()
+    w = P.workloads.obstacles_inflow()
+    prm = w['params']
+    dt = prm['dt']
+    tank = make_tank(P, w, local)
+    tank.profile(True)
+    stream = torch.cuda.ExternalStream(tank.stream())
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f'cuda:{local}')
+    for _ in range(max(args.warmup, 3)):
+        tank.substep(dt)
+    tank.sync()
+    n0 = tank.stats()['count']
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    phases = []
+    clocks = Clocks(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ev[k][0].record(stream)
+        tank.substep(dt)
+        ev[k][1].record(stream)
+        phases.append(tank.phase_ms())
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if world > 1:
+        dist.barrier()
+    st = tank.stats()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    particles = 0.5 * (n0 + st['count'])
+    ph = {k: float(np.mean([p[k] for p in phases])) for k in P.native.PHASES}
+    sor_launch_ms = ph['pressure_solve'] / (2 * prm['iters'])
+    if world > 1:
+        ms, particles, sor_launch_ms = reduce_ranks(ms, particles, sor_launch_ms, f'cuda:{local}')
+    value = particles * 1000.0 / ms
+
+    # end-to-end through the C ABI: host inflow particles (pinned) up, stats back, every step
+    t2 = make_tank(P, w, local, host_inflow=True)
+    rng = np.random.default_rng(7)
+    for _ in range(3):
+        for e in w['emitters']:
+            p, v = faucet_particles(e, dt, rng)
+            t2.add_particles(p, v)
+        t2.substep(dt)
+        t2.stats()
+    nA = t2.stats()['count']
+    h2d = d2h = 0
+    readback = int(P.native.lib().suiri_stats_readback_bytes())
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for e in w['emitters']:
+            p, v = faucet_particles(e, dt, rng)
+            t2.add_particles(p, v)
+            h2d += 32 * len(p)
+        t2.substep(dt)
+        t2.poll_stats()
+        d2h += readback
+    t2.sync()
+    el = time.perf_counter() - t0
+    nB = t2.stats()['count']
+    e2e_rate = 0.5 * (nA + nB) * args.steps / el
+    if world > 1:
+        e2e_rate = reduce_e2e(e2e_rate, world, f'cuda:{local}')
+    e2e = dict(value=e2e_rate, unit=METRIC, h2d_bytes_per_step=h2d // args.steps, d2h_bytes_per_step=d2h // args.steps)
+    t2.close()
+
+    if rank == 0:
+        peak, kind = peaks()
+        active = st['active_cells']
+        alg = 20.0 * active / 2                      # one colour sweep: read p 4 + fractions 12 + rhs 2 + write 2 per cell
+        achieved = alg / (sor_launch_ms * 1e-3) / 1e9
+        tr = profile_figure('sor_sweep_traffic.json')
+        cpu_rate, cpu_el, cpu_what = cpu_sample_rate([w], steps=args.cpu_steps)
+        line = dict(metric=METRIC, value=value, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
+                    ms_per_step=ms, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
+                    data='synthetic (seeded particles, analytic obstacles)', config=plain_config(w),
+                    l2='flushed (256 MiB write) between timed steps', parallelism=f'replicas{world}',
+                    roofline=dict(bound='hbm', kernel='k_sor (one colour sweep)', achieved=achieved, peak=peak,
+                                  unit='GB/s', frac=achieved / peak, peak_kind=kind,
+                                  traffic=None if tr is None else tr.get('dram_bytes_per_launch'),
+                                  alg_bytes_per_launch=alg, launch_ms=sor_launch_ms, active_cells=active,
+                                  unit_bytes='20 B per active cell per colour sweep'),
+                    phases_ms=ph,
+                    cpu_baseline=dict(value=cpu_rate, unit=METRIC, cores=1, kind='port', sample=cpu_what),
+                    e2e=e2e, gpu_launches=launches_per_substep(0, prm['iters']) * args.steps, clocks=clk)
+        print(json.dumps(line), flush=True)
+    tank.close()
+    if world > 1:
+        dist.destroy_process_group()
 
 
 def run_full_scene(args, local):
@@ -360,7 +675,8 @@ def run_full_scene(args, local):
     prm = w['params']
     t = P.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=prm['flip'], omega=prm['omega'], iters=prm['iters'],
                whitewater=True, ripple=w['ripple'], wmap=512, capacity=int(len(w['pos']) * 1.1) + 200000,
-               ww_capacity=400000, ripple_sigma=prm['sigma'], ripple_rho=prm['rho'], ripple_depth=prm['depth'], device=local)
+               ww_capacity=400000, ripple_sigma=prm['sigma'], ripple_rho=prm['rho'], ripple_depth=prm['depth'], device=local,
+               drop_d=prm['drop_d'])
     t.add_particles(w['pos'])
     t.set_emitters(w['emitters'])
     stream = torch.cuda.ExternalStream(t.stream())
@@ -383,7 +699,8 @@ def run_full_scene(args, local):
                 dtype='f32', data='synthetic',
                 config=dict(workload=w['name'], particles=int(particles), cells=w['nx'] * w['ny'] * w['nz'],
                             ripple=list(w['ripple']), substeps=subs, impacts=st['impacts'], whitewater=st['ww_count'],
-                            sor_iters=prm['iters'], dt=prm['dt']))
+                            sor_iters=prm['iters'], dt=prm['dt'], drop_d_median=prm['drop_d'][0],
+                            drop_d_sigma_log=prm['drop_d'][1]))
     print(json.dumps(line), flush=True)
     t.close()
 
@@ -404,151 +721,63 @@ def run_serve(args, local):
     print(json.dumps(line), flush=True)
 
 
+def run_for_profiler(args, local):
+    """A fixed launch sequence for ncu: the workload set up (the batch tuned to --sor-mode), stepped 3 + N
+    sub-steps and synchronised; no timing, no JSON line."""
+    P = pkg()
+    if args.workload == 'batch':
+        specs = batch_specs(args.tanks)
+        tanks = make_batch_tanks(P, specs, local)
+        b = P.Batch(tanks)
+        b.tune(args.bps, args.sor_mode)
+        for _ in range(3 + args.ncu_steps):
+            b.substep(DT)
+        b.sync()
+        print('sub-steps', 3 + args.ncu_steps, 'particles', sum(t.stats()['count'] for t in tanks))
+        b.close()
+        for t in tanks:
+            t.close()
+        return
+    w = P.workloads.obstacles_inflow()
+    t = make_tank(P, w, local)
+    t.tune(args.bps, args.sor_mode)
+    for _ in range(3 + args.ncu_steps):
+        t.substep(w['params']['dt'])
+    t.sync()
+    print('sub-steps', 3 + args.ncu_steps, 'particles', t.stats()['count'])
+    t.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=200)
+    ap.add_argument('--steps', type=int, default=20)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='suiri', choices=['suiri', 'reference'])
-    ap.add_argument('--workload', default='obstacles_inflow', choices=['obstacles_inflow', 'batch', 'serve', 'full_scene'])
-    ap.add_argument('--cpu-steps', type=int, default=2, help='sub-steps of the CPU baseline sample')
+    ap.add_argument('--workload', default='batch', choices=['batch', 'obstacles_inflow', 'serve', 'full_scene'])
+    ap.add_argument('--cpu-steps', type=int, default=2, help='sub-steps of the single-tank CPU baseline sample')
     ap.add_argument('--tanks', type=int, default=64)
     ap.add_argument('--rate', type=float, default=200.0)
     ap.add_argument('--duration', type=float, default=60.0)
     ap.add_argument('--req-steps', type=int, default=120)
     ap.add_argument('--ncu-steps', type=int, default=0,
                     help='profiler run: 3 warm-up and N more sub-steps of the workload, no timing, no JSON line')
+    ap.add_argument('--bps', type=int, default=2, help='profiler run: particle blocks per SM')
+    ap.add_argument('--sor-mode', type=int, default=4, help='profiler run: form of the pressure solve')
     args = ap.parse_args()
     rank, world = int(os.environ.get('RANK', 0)), int(os.environ.get('WORLD_SIZE', 1))
     local = int(os.environ.get('LOCAL_RANK', 0))
     if args.impl == 'reference':
         return run_reference(args, rank)
+    if args.ncu_steps:
+        return run_for_profiler(args, local)
     if args.workload == 'batch':
-        return run_batch(args, local)
+        return run_batch(args, rank, world, local)
     if args.workload == 'serve':
         return run_serve(args, local)
     if args.workload == 'full_scene':
         return run_full_scene(args, local)
-    if args.ncu_steps:
-        return run_for_profiler(args, local)
-    import torch
-    import torch.distributed as dist
-    if world > 1:
-        import datetime
-        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
-    torch.cuda.set_device(local)
-    P = pkg()
-    w = P.workloads.obstacles_inflow()
-    prm = w['params']
-    dt = prm['dt']
-    ncell = w['nx'] * w['ny'] * w['nz']
-    tank = make_tank(P, w, local)
-    tank.profile(True)
-    stream = torch.cuda.ExternalStream(tank.stream())
-    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f'cuda:{local}')
-    for _ in range(max(args.warmup, 3)):
-        tank.substep(dt)
-    tank.sync()
-    n0 = tank.stats()['count']
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    step_ms, sor_ms = [], []
-    clocks = Clocks(local)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    for k in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()                          # L2 flush, outside the timed interval
-        ev[k][0].record(stream)
-        tank.substep(dt)
-        ev[k][1].record(stream)
-        sor_ms.append(tank.sor_phase_ms())
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    if world > 1:
-        dist.barrier()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    n1 = tank.stats()['count']
-    ms = float(np.mean(step_ms))
-    particles = 0.5 * (n0 + n1)
-    sor_launch_ms = float(np.mean(sor_ms)) / (2 * prm['iters'])
-    if world > 1:
-        ms, particles, sor_launch_ms = reduce_ranks(ms, particles, sor_launch_ms, f'cuda:{local}')
-    value = particles * 1000.0 / ms
-
-    # end-to-end through the C ABI: host inflow particles (pinned) up, stats back, every step
-    e2e = None
-    if rank == 0 or world > 1:
-        t2 = make_tank(P, w, local, host_inflow=True)
-        rng = np.random.default_rng(7)
-        for _ in range(3):
-            for e in w['emitters']:
-                p, v = faucet_particles(e, dt, rng)
-                t2.add_particles(p, v)
-            t2.substep(dt)
-            t2.stats()
-        nA = t2.stats()['count']
-        h2d = d2h = 0
-        readback = int(P.native.lib().suiri_stats_readback_bytes())
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            for e in w['emitters']:
-                p, v = faucet_particles(e, dt, rng)
-                t2.add_particles(p, v)
-                h2d += 32 * len(p)            # staged as two float4 per particle
-            t2.substep(dt)
-            t2.poll_stats()                   # the step's stats read, collected without waiting (pollStats)
-            d2h += readback
-        t2.sync()
-        el = time.perf_counter() - t0
-        nB = t2.stats()['count']
-        e2e_rate = 0.5 * (nA + nB) * args.steps / el
-        if world > 1:
-            e2e_rate = reduce_e2e(e2e_rate, world, f'cuda:{local}')
-        e2e = dict(value=e2e_rate, unit=METRIC, h2d_bytes_per_step=h2d // args.steps, d2h_bytes_per_step=d2h // args.steps)
-        t2.close()
-
-    if rank == 0:
-        peak, kind = peaks()
-        alg_bytes = 20.0 * ncell                 # one colour sweep: read p 4 + 3 fractions 12 + rhs 2 + write p 2 per cell
-        achieved = alg_bytes / (sor_launch_ms * 1e-3) / 1e9
-        tr = sor_traffic()
-        cpu_rate, cpu_el = cpu_port_rate(w, args.cpu_steps)
-        launches_per_step = 10 + 2 * prm['iters']  # the sub-step graph; dt is constant, so it is uploaded once
-        line = dict(metric=METRIC, value=value, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
-                    ms_per_step=ms, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
-                    data='synthetic (seeded particles, analytic obstacles)',
-                    config=dict(workload=w['name'], particles=int(particles / world), cells=ncell,
-                                sor_iters=prm['iters'], omega=prm['omega'], flip=prm['flip'], dt=dt,
-                                inflow_per_step=w['emitters'][0]['count'], l2='flushed (256 MiB write) between timed steps',
-                                parallelism=f'replicas{world}'),
-                    roofline=dict(bound='hbm', kernel='k_sor (one colour sweep)', achieved=achieved, peak=peak,
-                                  unit='GB/s', frac=achieved / peak, peak_kind=kind,
-                                  traffic=None if tr is None else tr.get('dram_bytes_per_launch'),
-                                  alg_bytes_per_launch=alg_bytes, launch_ms=sor_launch_ms,
-                                  sor_share=float(np.mean(sor_ms)) / ms),
-                    cpu_baseline=dict(value=cpu_rate, unit=METRIC, cores=1, kind='port',
-                                      sample=f'{args.cpu_steps} sub-steps of the same workload on the host (NumPy '
-                                             f'restatement of the reference solver, {cpu_el:.1f} s, 1 core of {os.cpu_count()})'),
-                    e2e=e2e, gpu_launches=launches_per_step * args.steps, clocks=clk)
-        print(json.dumps(line), flush=True)
-    tank.close()
-    if world > 1:
-        dist.destroy_process_group()
-
-
-def run_for_profiler(args, local):
-    """The obstacles-and-inflow tank stepped 3 + N times and synchronised: a fixed launch sequence for ncu
-    (per sub-step: 10 kernels + 2 per SOR iteration)."""
-    P = pkg()
-    w = P.workloads.obstacles_inflow()
-    t = make_tank(P, w, local)
-    for _ in range(3 + args.ncu_steps):
-        t.substep(w['params']['dt'])
-    t.sync()
-    print('sub-steps', 3 + args.ncu_steps, 'particles', t.stats()['count'])
-    t.close()
+    return run_plain(args, rank, world, local)
 
 
 if __name__ == '__main__':

@@ -151,6 +151,13 @@ void fill_stats(Tank& t, const Counters& c, suiri_stats* s) {
   s->errors = c.err;
   s->nx = t.d.nx; s->ny = t.d.ny; s->nz = t.d.nz; s->h = t.d.h;
   s->origin[0] = t.d.ox; s->origin[1] = t.d.oy; s->origin[2] = t.d.oz;
+  s->active_cells = (long long)c.n_act[0] + c.n_act[1];
+  double rmax, hmax;
+  memcpy(&rmax, &c.res_max_bits, 8);
+  memcpy(&hmax, &c.rhs_max_bits, 8);
+  s->residual_max = rmax;
+  s->rhs_max = hmax;
+  s->residual_rms = s->active_cells > 0 ? sqrt(c.res_sum2 / (double)s->active_cells) : 0.0;
 }
 }  // namespace
 
@@ -167,6 +174,7 @@ int suiri_params_default(suiri_params* p) {
   p->capacity = 0; p->ww_capacity = 0; p->ripple_rx = 0; p->ripple_rz = 0; p->wmap = 0;
   p->sdf_mode = 0; p->device = 0; p->seed = 1;
   p->ripple_sigma = 0.0728; p->ripple_rho = 998.0; p->ripple_depth = 0.0;
+  p->sor_mode = 0; p->watchdog_polls = kWatchdogPolls;
   return SUIRI_OK;
 }
 
@@ -233,6 +241,13 @@ TankConfig make_config(const suiri_params& p, const char* scene_json, Scene& sc)
     c.ripple_sigma = p.ripple_sigma; c.ripple_rho = p.ripple_rho; c.ripple_depth = p.ripple_depth;
     if (p.advect != 0 && p.advect != 1) throw Error(SUIRI_ERR_INVALID, "advect is 0 (Euler) or 1 (RK2)");
     c.advect = p.advect;
+    if (!(p.drop_d_median >= 0) || !(p.drop_d_sigma_log >= 0) || p.drop_d_median > 0.02)
+      throw Error(SUIRI_ERR_INVALID, "drop_d_median in [0, 0.02] m, drop_d_sigma_log >= 0");
+    c.drop_d_median = p.drop_d_median; c.drop_d_sigma = p.drop_d_sigma_log;
+    if (p.sor_mode < -1 || p.sor_mode > 4) throw Error(SUIRI_ERR_INVALID, "sor_mode is -1 (auto) or 0..4");
+    if (p.watchdog_polls < 0 || p.watchdog_polls > 0xFFFFFFFFLL) throw Error(SUIRI_ERR_INVALID, "watchdog_polls in [0, 2^32)");
+    c.sor_mode = p.sor_mode;
+    c.watchdog_polls = p.watchdog_polls;
     if (!(c.omega > 0 && c.omega < 2)) throw Error(SUIRI_ERR_INVALID, "omega must be in (0, 2)");
     if (c.cap > (1LL << 30)) throw Error(SUIRI_ERR_INVALID, "capacity above 2^30 particles");
     return c;
@@ -318,6 +333,20 @@ int suiri_eval_sdf_static(suiri_tank* h, const double* pts, int64_t n, double* o
   return guard(h ? &h->err : nullptr, [&] {
     if (n < 0 || (n > 0 && (!pts || !out))) throw Error(SUIRI_ERR_INVALID, "bad point arrays");
     T(h)->eval_sdf_static(pts, n, out);
+  });
+}
+
+int suiri_scene_validate(const char* scene_json, int32_t clamp_tank, char* out, size_t cap, size_t* len) {
+  return guard(nullptr, [&] {
+    if (!scene_json || !len) throw Error(SUIRI_ERR_INVALID, "null scene or length");
+    Scene sc;
+    std::string err;
+    if (!parse_scene(scene_json, clamp_tank != 0, sc, err)) throw Error(SUIRI_ERR_PARSE, err);
+    const std::string txt = scene_json_text(sc);
+    *len = txt.size();
+    if (!out) return;
+    if (cap <= txt.size()) throw Error(SUIRI_ERR_INVALID, "output buffer too small (" + std::to_string(txt.size() + 1) + " bytes needed)");
+    memcpy(out, txt.c_str(), txt.size() + 1);
   });
 }
 
@@ -413,6 +442,10 @@ int suiri_read_whitewater(suiri_tank* h, float* pos4, float* vel4, int64_t cap, 
   });
 }
 
+int suiri_add_whitewater(suiri_tank* h, const float* pos4, const float* vel4, int64_t n) {
+  return guard(h ? &h->err : nullptr, [&] { T(h)->add_whitewater(pos4, vel4, n); });
+}
+
 int suiri_read_grid(suiri_tank* h, int32_t field, void* out, size_t bytes) {
   return guard(h ? &h->err : nullptr, [&] {
     if (!out) throw Error(SUIRI_ERR_INVALID, "null output");
@@ -502,13 +535,59 @@ int suiri_batch_sync(suiri_batch* b) {
 
 static void tune_group(Group& g, int32_t particle_blocks_per_sm, int32_t sor_mode) {
   if (particle_blocks_per_sm < 1 || particle_blocks_per_sm > 32) throw Error(SUIRI_ERR_INVALID, "blocks per SM in 1..32");
-  if (sor_mode < 0 || sor_mode > 3) throw Error(SUIRI_ERR_INVALID, "sor_mode is 0, 1, 2 or 3");
+  if (sor_mode < 0 || sor_mode > 4) throw Error(SUIRI_ERR_INVALID, "sor_mode is 0, 1, 2, 3 or 4");
   CK(cudaStreamSynchronize(g.stream));
+  if (sor_mode == 4) g.plan_cluster();     // throws (and changes nothing else) when a tank does not fit
   g.blocks_per_sm = particle_blocks_per_sm;
   g.ctx.particle_blocks = particle_blocks_per_sm * g.sm_count;
   if (sor_mode == 2) g.ensure_tbl();
   g.sor_mode = sor_mode;
   g.drop_graph();
+}
+
+static void tune_piece(Group& g, int32_t piece_kb) {
+  if (piece_kb < 0) throw Error(SUIRI_ERR_INVALID, "piece_kb must be >= 0");
+  CK(cudaStreamSynchronize(g.stream));
+  const int old = g.cl_piece_kb;
+  g.cl_piece_kb = piece_kb;
+  if (g.sor_mode == 4) {
+    try {
+      g.plan_cluster();
+    } catch (...) {
+      g.cl_piece_kb = old;
+      throw;
+    }
+    g.drop_graph();
+  }
+}
+
+static void set_residual(Group& g, bool on) {
+  if (on == g.residual) return;
+  CK(cudaStreamSynchronize(g.stream));
+  g.residual = on;
+  g.drop_graph();
+}
+
+int suiri_tune_piece(suiri_tank* h, int32_t piece_kb) {
+  return guard(h ? &h->err : nullptr, [&] { tune_piece(*T(h)->solo, piece_kb); });
+}
+
+int suiri_batch_tune_piece(suiri_batch* b, int32_t piece_kb) {
+  return guard(b ? &b->err : nullptr, [&] {
+    if (!b || !b->b) throw Error(SUIRI_ERR_INVALID, "null batch");
+    for (auto& g : b->b->lanes) tune_piece(*g, piece_kb);
+  });
+}
+
+int suiri_residual(suiri_tank* h, int32_t on) {
+  return guard(h ? &h->err : nullptr, [&] { set_residual(*T(h)->solo, on != 0); });
+}
+
+int suiri_batch_residual(suiri_batch* b, int32_t on) {
+  return guard(b ? &b->err : nullptr, [&] {
+    if (!b || !b->b) throw Error(SUIRI_ERR_INVALID, "null batch");
+    for (auto& g : b->b->lanes) set_residual(*g, on != 0);
+  });
 }
 
 int suiri_batch_tune(suiri_batch* b, int32_t particle_blocks_per_sm, int32_t sor_mode) {
@@ -593,6 +672,28 @@ int suiri_batch_sor_phase_ms(suiri_batch* b, double* ms) {
     double m = 0;
     for (auto& g : b->b->lanes) m = std::max(m, g->sor_phase_ms());   // lanes overlap: the longest
     *ms = m;
+  });
+}
+
+int suiri_phase_ms(suiri_tank* h, double* ms) {
+  return guard(h ? &h->err : nullptr, [&] {
+    if (!ms) throw Error(SUIRI_ERR_INVALID, "null output");
+    for (int k = 0; k < Group::kPhases; ++k) ms[k] = T(h)->solo->phase_ms(k);
+  });
+}
+
+int suiri_batch_lanes(suiri_batch* b, int32_t* n) {
+  return guard(b ? &b->err : nullptr, [&] {
+    if (!b || !b->b || !n) throw Error(SUIRI_ERR_INVALID, "null batch or output");
+    *n = (int32_t)b->b->lanes.size();
+  });
+}
+
+int suiri_batch_phase_ms(suiri_batch* b, int32_t lane, double* ms) {
+  return guard(b ? &b->err : nullptr, [&] {
+    if (!b || !b->b || !ms) throw Error(SUIRI_ERR_INVALID, "null batch or output");
+    if (lane < 0 || lane >= (int32_t)b->b->lanes.size()) throw Error(SUIRI_ERR_INVALID, "lane out of range");
+    for (int k = 0; k < Group::kPhases; ++k) ms[k] = b->b->lanes[lane]->phase_ms(k);
   });
 }
 

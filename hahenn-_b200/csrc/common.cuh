@@ -82,6 +82,10 @@ struct Counters {
   int pad;
   int n_act[2];       // active cells of each colour this sub-step (entries of TankDev::act)
   double emit_acc[8]; // fractional particles carried by the fixed emitters
+  // FP64 residual of the last solve (when enabled): max |r| and max |rhs| as float64 bits (non-negative
+  // doubles order like their bits), and Σ r², over the active cells
+  unsigned long long res_max_bits, rhs_max_bits;
+  double res_sum2;
 };
 
 struct TankDev {
@@ -98,6 +102,7 @@ struct TankDev {
   float omega;
   int iters, whitewater, nobj, sdf_mode, has_obst, moving;
   int advect;               // 0 explicit Euler, 1 RK2 midpoint through the grid velocity
+  double drop_d_median, drop_d_sigma;   // > 0: sub-grid drops have lognormal diameters from their ids
   int cap, emit_cap, ww_cap;
   int rx, rz;               // ripple vertices (rx+1)×(rz+1); 0 = no ripple layer
   // particles: A live, E emitted, B sorted; pos.w = flags (bit0 airborne, bit1 dead), vel.w = id bits

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "../../include/suiri.h"
 #include "sdf.cuh"
 
 namespace suiri {
@@ -191,6 +192,8 @@ __global__ void k_emit_begin(const TankDev* __restrict__ tanks, int ntanks, int*
       c->vmax_bits64 = 0ull;
       c->ww_spawned = 0;
       c->n_act[0] = c->n_act[1] = 0;
+      c->res_max_bits = c->rhs_max_bits = 0ull;
+      c->res_sum2 = 0.0;
       return v;
     });
   }
@@ -212,14 +215,19 @@ std::mutex g_static_mu;
 double* g_static_ptr[128] = {};
 
 // Device address of g_sdf_static on `dev` (host code cannot use the symbol itself: its host-side name is a
-// stand-in, not a device address). Looked up once per device, with that device current.
+// stand-in, not a device address). Looked up once per device, with that device current; the calling
+// thread's current device is put back afterwards.
 double* sdf_static_scratch(int dev) {
-  if (dev < 0 || dev >= 128) throw Error(-1, "device ordinal out of range");
+  if (dev < 0 || dev >= 128) throw Error(SUIRI_ERR_INVALID, "device ordinal out of range");
   std::lock_guard<std::mutex> g(g_static_mu);
   if (!g_static_ptr[dev]) {
+    int prev = 0;
+    CK(cudaGetDevice(&prev));
     CK(cudaSetDevice(dev));
     void* p = nullptr;
-    CK(cudaGetSymbolAddress(&p, g_sdf_static));
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_sdf_static);
+    CK(cudaSetDevice(prev));
+    CK(e);
     g_static_ptr[dev] = (double*)p;
   }
   return g_static_ptr[dev];
@@ -228,7 +236,7 @@ double* sdf_static_scratch(int dev) {
 
 void Tank::eval_sdf_static(const double* pts, long long n, double* out) {
   if (n > kSdfStaticMax)
-    throw Error(-1, "suiri_eval_sdf_static: " + std::to_string(n) + " points, at most " + std::to_string(kSdfStaticMax) +
+    throw Error(SUIRI_ERR_INVALID, "suiri_eval_sdf_static: " + std::to_string(n) + " points, at most " + std::to_string(kSdfStaticMax) +
                         " per call (the static staging array is fixed)");
   join();
   if (n <= 0) return;
@@ -285,6 +293,7 @@ Tank::Tank(const TankConfig& c) : cfg(c) {
   D.sdf_mode = cfg.sdf_mode;
   D.seed = cfg.seed;
   D.advect = cfg.advect;
+  D.drop_d_median = cfg.drop_d_median; D.drop_d_sigma = cfg.drop_d_sigma;
   D.cap = (int)cfg.cap;
   emit_cap = cfg.cap;
   D.emit_cap = (int)emit_cap;
@@ -762,6 +771,23 @@ long long Tank::read_whitewater(float* pos4, float* vel4, long long cap) {
   return n;
 }
 
+void Tank::add_whitewater(const float* pos4, const float* vel4, long long n) {
+  if (n < 0 || (n > 0 && (!pos4 || !vel4))) throw Error(-1, "add_whitewater: bad arrays");
+  read_counters();
+  const long long cur = std::min<long long>(h_ctr->ww_count, d.ww_cap);
+  const long long take = std::min<long long>(n, d.ww_cap - cur);
+  const size_t half = (h_ctr->ww_cur & 1) ? (size_t)d.ww_cap : 0;
+  if (take > 0) {
+    CK(cudaMemcpyAsync(d.wpos + half + cur, pos4, take * 16, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(d.wvel + half + cur, vel4, take * 16, cudaMemcpyHostToDevice, stream));
+    const int count = (int)(cur + take);
+    CK(cudaMemcpyAsync(&d.ctr->ww_count, &count, sizeof(int), cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+    h_ctr->ww_count = count;
+  }
+  if (take < n) throw Error(-4, "whitewater capacity reached: " + std::to_string(take) + " of " + std::to_string(n) + " added");
+}
+
 void Tank::read_grid(int field, void* out, size_t bytes) {
   join();
   const size_t nn = d.nnodes, nc = d.ncells;
@@ -927,13 +953,29 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
   ctx.scan_bsum = d_bsum;
   ctx.particle_blocks = blocks_per_sm * sm_count;
   uploaded.assign(n, 0);
+  for (Tank* x : tanks) watchdog_polls = std::min<unsigned>(watchdog_polls, (unsigned)x->cfg.watchdog_polls);
+  // the solve form the first tank asks for; -1: cluster-resident where every tank fits, else per sweep
+  const int want = tanks[0]->cfg.sor_mode;
+  if (want == 4 || want == -1) {
+    try {
+      plan_cluster();
+      sor_mode = 4;
+    } catch (const Error&) {
+      if (want == 4) throw;
+      sor_mode = 0;
+    }
+  } else {
+    if (want == 2) ensure_tbl();
+    sor_mode = want;
+  }
 }
 
 Group::~Group() {
   cudaSetDevice(device);
   cudaStreamSynchronize(stream);
   drop_graph();
-  if (ev_sor[0]) { cudaEventDestroy(ev_sor[0]); cudaEventDestroy(ev_sor[1]); }
+  for (cudaEvent_t e : ev_ph)
+    if (e) cudaEventDestroy(e);
   if (ev_done) {
     for (Tank* t : tanks)
       if (t->dep == ev_done) { cudaStreamWaitEvent(t->stream, ev_done, 0); t->dep = nullptr; }
@@ -941,7 +983,7 @@ Group::~Group() {
   }
   // stream-ordered frees: no device-wide synchronisation (other batches keep running)
   for (void* p : {(void*)d_hpfx, (void*)d_apfx, (void*)d_barrier, (void*)d_ticket, d_tbl, (void*)d_tanks, (void*)d_bpfx,
-                  (void*)d_ppfx, (void*)d_bsum})
+                  (void*)d_ppfx, (void*)d_bsum, (void*)d_pieces})
     if (p) cudaFreeAsync(p, stream);
   delete[] h_tanks;
   if (own_stream) cudaStreamDestroy(stream);
@@ -954,6 +996,62 @@ void Group::ensure_tbl() {
   CK(cudaMallocAsync(&d_tbl, tbl_list_bytes(tiles), stream));
   CK(cudaStreamSynchronize(stream));
   tbl_assign(ctx, d_tbl, tiles);
+}
+
+// The CTA plan of the cluster-resident solve. Each tank is cut into m pieces of np whole z planes, as few
+// as fit the shared memory a CTA may take (cl_piece_kb, or the device's opt-in maximum); the cluster size K
+// is the largest m, and the tanks are packed into clusters of K CTAs first-fit by decreasing m (a tank's
+// pieces on consecutive ranks; unused ranks idle). Throws if a tank needs more than kClusterMax pieces or the
+// device cannot hold one such cluster.
+void Group::plan_cluster() {
+  CK(cudaSetDevice(device));
+  int optin = 0;
+  CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  const int budget = cl_piece_kb > 0 ? std::min(optin, cl_piece_kb * 1024) : optin;
+  const int n = (int)tanks.size();
+  std::vector<int> m(n), np(n);
+  int K = 1, smem = 16;
+  for (int i = 0; i < n; ++i) {
+    const TankDev& D = tanks[i]->d;
+    const int npm = budget / cluster_plane_bytes(D);
+    if (npm < 1) throw Error(-1, "cluster solve: one z plane of a tank does not fit a CTA's shared memory");
+    int mi = (D.nz + npm - 1) / npm;
+    np[i] = (D.nz + mi - 1) / mi;
+    m[i] = (D.nz + np[i] - 1) / np[i];
+    if (m[i] > kClusterMax) throw Error(-1, "cluster solve: a tank needs more than 16 CTAs");
+    K = std::max(K, m[i]);
+    smem = std::max(smem, cluster_smem_bytes(D, np[i]));
+  }
+  CK(sor_cluster_prepare(optin, kClusterMax));
+  if (sor_cluster_max_active(smem, K) < 1) throw Error(-1, "cluster solve: the device cannot hold one cluster of this size");
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return m[a] > m[b]; });
+  std::vector<std::vector<int>> bins;
+  std::vector<int> fill;
+  for (int i : order) {
+    size_t b = 0;
+    while (b < bins.size() && fill[b] + m[i] > K) ++b;
+    if (b == bins.size()) { bins.emplace_back(); fill.push_back(0); }
+    bins[b].push_back(i);
+    fill[b] += m[i];
+  }
+  std::vector<ClusterPiece> pcs;
+  for (const auto& bin : bins) {
+    for (int i : bin)
+      for (int p = 0; p < m[i]; ++p) {
+        const int k0 = p * np[i];
+        pcs.push_back(ClusterPiece{i, k0, std::min(np[i], tanks[i]->d.nz - k0), np[i]});
+      }
+    while (pcs.size() % K) pcs.push_back(ClusterPiece{-1, 0, 0, 0});
+  }
+  if (d_pieces) CK(cudaFreeAsync(d_pieces, stream));
+  CK(cudaMallocAsync((void**)&d_pieces, pcs.size() * sizeof(ClusterPiece), stream));
+  CK(cudaMemcpyAsync(d_pieces, pcs.data(), pcs.size() * sizeof(ClusterPiece), cudaMemcpyHostToDevice, stream));
+  CK(cudaStreamSynchronize(stream));
+  cl_blocks = (int)pcs.size();
+  cl_size = K;
+  cl_smem = smem;
 }
 
 Batch::Batch(const std::vector<Tank*>& t) {
@@ -1000,22 +1098,23 @@ void Batch::substep(double dt) {
 
 void Group::set_profile(bool on) {
   if (on == profile) return;
-  if (on && !ev_sor[0]) {
-    CK(cudaEventCreate(&ev_sor[0]));
-    CK(cudaEventCreate(&ev_sor[1]));
-  }
+  if (on && !ev_ph[0])
+    for (cudaEvent_t& e : ev_ph) CK(cudaEventCreate(&e));
   profile = on;
   CK(cudaStreamSynchronize(stream));
   drop_graph();
 }
 
-double Group::sor_phase_ms() {
+double Group::phase_ms(int k) {
   if (!profile) throw Error(-6, "profiling is off");
-  CK(cudaEventSynchronize(ev_sor[1]));
+  if (k < 0 || k >= kPhases) throw Error(-1, "phase index out of range");
+  CK(cudaEventSynchronize(ev_ph[kPhases]));
   float f = 0;
-  CK(cudaEventElapsedTime(&f, ev_sor[0], ev_sor[1]));
+  CK(cudaEventElapsedTime(&f, ev_ph[k], ev_ph[k + 1]));
   return f;
 }
+
+double Group::sor_phase_ms() { return phase_ms(3); }
 
 void Group::drop_graph() {
   if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
@@ -1064,20 +1163,26 @@ void Group::set_dt(double dt) {
 }
 
 void Group::enqueue_body() {
-  k_emit_begin<<<(int)tanks.size(), 128, 0, stream>>>(d_tanks, (int)tanks.size(), ctx.ppfx_in, ctx.ticket + 2);
-  launch_bin(ctx);
-  launch_scan(ctx);
-  launch_scatter(ctx);
-  launch_p2g(ctx);
-  launch_grid_nodes(ctx);
-  launch_grid_cells(ctx);
   // inside a capture an event record must be an external event node to be replayed with the graph
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   if (profile) CK(cudaStreamIsCapturing(stream, &cap));
   const unsigned evflags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
-  if (profile) CK(cudaEventRecordWithFlags(ev_sor[0], stream, evflags));
+  auto mark = [&](int k) {
+    if (profile) CK(cudaEventRecordWithFlags(ev_ph[k], stream, evflags));
+  };
+  mark(0);
+  k_emit_begin<<<(int)tanks.size(), 128, 0, stream>>>(d_tanks, (int)tanks.size(), ctx.ppfx_in, ctx.ticket + 2);
+  launch_bin(ctx);
+  launch_scan(ctx);
+  launch_scatter(ctx);
+  mark(1);
+  launch_p2g(ctx);
+  mark(2);
+  launch_grid_nodes(ctx);
+  launch_grid_cells(ctx);
+  mark(3);
   if (sor_mode == 1 && max_iters > 0) {
-    launch_sor_persist(ctx, max_iters, sor_blocks);
+    launch_sor_persist(ctx, max_iters, sor_blocks, watchdog_polls);
     CK(cudaGetLastError());
   } else if (sor_mode == 2 || sor_mode == 3) {
     // S sweeps per launch; launch l reads pres (l even) or pres2 and writes the other; an odd count ends in pres2
@@ -1087,6 +1192,9 @@ void Group::enqueue_body() {
     for (int l = 0; l < nl; ++l) launch_sor_tb(ctx, S, l * S, std::min(S, sweeps - l * S), l & 1);
     if (nl & 1) launch_sor_copy(ctx);
     CK(cudaGetLastError());
+  } else if (sor_mode == 4) {
+    if (max_iters > 0) launch_sor_cluster(ctx, d_pieces, cl_blocks, cl_smem, cl_size, max_iters);
+    CK(cudaGetLastError());
   } else {
     for (int it = 0; it < max_iters; ++it) {
       launch_sor_sweep(ctx, 0, it);
@@ -1094,9 +1202,15 @@ void Group::enqueue_body() {
     }
     CK(cudaGetLastError());
   }
-  if (profile) CK(cudaEventRecordWithFlags(ev_sor[1], stream, evflags));
+  mark(4);
+  if (residual) {
+    launch_sor_residual(ctx);
+    CK(cudaGetLastError());
+  }
   launch_project(ctx);
+  mark(5);
   launch_g2p(ctx);
+  mark(6);
 }
 
 void Group::substep(double dt) {

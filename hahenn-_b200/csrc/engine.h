@@ -44,6 +44,9 @@ struct TankConfig {
   uint32_t seed = 1;
   double ripple_sigma = 0.0728, ripple_rho = 998.0, ripple_depth = 0.0;
   int advect = 0;                 // 0 explicit Euler (the reference), 1 RK2 midpoint through the grid velocity
+  double drop_d_median = 0, drop_d_sigma = 0;   // lognormal sub-grid drop diameters (0: the particle mass)
+  int sor_mode = 0;               // form of the pressure solve of the tank's own group (-1: cluster-resident where it fits)
+  long long watchdog_polls = kWatchdogPolls;    // polls of a bounded device wait before it gives up
   cudaStream_t stream = nullptr;  // use this stream instead of creating one (not owned)
 };
 
@@ -129,6 +132,7 @@ struct Tank {
   void source_emits(double dt);
   long long read_particles(float* pos4, float* vel4, long long cap);
   long long read_whitewater(float* pos4, float* vel4, long long cap);
+  void add_whitewater(const float* pos4, const float* vel4, long long n);
   void read_grid(int field, void* out, size_t bytes);
   int snapshot();
   void restore(int id);
@@ -157,10 +161,19 @@ struct Group {
   void ensure_tbl();
   GridBarrier* d_barrier = nullptr;
   int sor_mode = 0;               // 0: one launch per colour sweep, 1: one cooperative launch per solve,
-                                  // 2, 3: 2 or 4 sweeps per launch (temporal blocking)
+                                  // 2, 3: 2 or 4 sweeps per launch (temporal blocking), 4: cluster-resident
   int sor_blocks = 0;
-  bool profile = false;           // record events around the SOR phase (inside the graph too)
-  cudaEvent_t ev_sor[2] = {nullptr, nullptr};
+  unsigned watchdog_polls = kWatchdogPolls;   // polls of a bounded device wait before it gives up (tanks' min)
+  // cluster-resident solve (sor_mode 4): the CTA plan, planned by plan_cluster when tuned to it
+  ClusterPiece* d_pieces = nullptr;
+  int cl_blocks = 0, cl_size = 1, cl_smem = 0;
+  int cl_piece_kb = 0;            // shared memory per CTA at most (tile knob; 0: the device maximum)
+  void plan_cluster();            // throws if a tank cannot be held by one cluster
+  bool residual = false;          // FP64 residual of every solve into the tank counters
+  bool profile = false;           // record events between the phases of the sub-step (inside the graph too)
+  static constexpr int kPhases = 6;   // binning+sort, P2G, node+cell passes, pressure solve, projection, G2P
+  cudaEvent_t ev_ph[kPhases + 1] = {};
+  double phase_ms(int k);         // phase k of the last sub-step (waits for it)
   int blocks_per_sm = 4;
   void set_profile(bool on);
   double sor_phase_ms();          // SOR phase of the last sub-step (waits for it)

@@ -121,6 +121,18 @@ __device__ inline void ww_write(const TankDev& T, int k, double px, double py, d
   wv[k] = make_float4((float)vx, (float)vy, (float)vz, 0.f);
 }
 
+// Diameter of a sub-grid drop when the tank gives drops their own sizes (no reference counterpart: there
+// every merging drop has the particle mass). Lognormal with median drop_d_median and log-standard-deviation
+// drop_d_sigma, drawn from the drop's carried id so that a drop keeps its size from emission to impact:
+// z = sqrt(−2 ln u1)·cos(2π u2) (Box–Muller) from two draws of the id's hash stream, |z| clamped to 4.
+__device__ inline double drop_diameter(const TankDev& T, uint32_t id) {
+  uint32_t s = hash_u32(id * 0x9E3779B1u + 0x632BE5ABu);
+  const double u1 = rnd(s) + 0.5 / 16777216.0;
+  const double u2 = rnd(s);
+  const double z = fmin(fmax(sqrt(-2.0 * log(u1)) * cos(2.0 * M_PI * u2), -4.0), 4.0);
+  return T.drop_d_median * exp(T.drop_d_sigma * z);
+}
+
 // crown splash of a drop of mass m at speed U (solver.py:632-657, 31-wgsl-sim2.js:119-148)
 __device__ inline void crown(const TankDev& T, double cx, double cy, double cz, double U, double m, uint32_t id, int frame) {
   if (!T.whitewater) return;
@@ -158,17 +170,30 @@ __global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ ta
   const int lane = threadIdx.x & 31;
   // warp-uniform loop: the speed maximum is reduced over the warp before its one atomic (one global
   // address per tank would otherwise take an atomic from every particle)
-  for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < total; base += stride) {
-    const int idx = base + lane;
+  // The particle of the next iteration is loaded at the top of this one (its tank lookup, descriptor and
+  // the two float4 streamed from HBM), so that its load latency overlaps this particle's work.
+  int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+  int nt = -1, nlocal = 0;
+  float4 nP = make_float4(0.f, 0.f, 0.f, 0.f), nV = nP;
+  auto fetch = [&](int q) {
+    nt = -1;
+    if (q < total) {
+      nt = find_slot(pfx, ntanks, q);
+      nlocal = q - pfx[nt];
+      nP = __ldcs(tanks[nt].pB + nlocal);
+      nV = __ldcs(tanks[nt].vB + nlocal);
+    }
+  };
+  fetch(base + lane);
+  for (; base < total; base += stride) {
+    const int t = nt, local = nlocal;
+    const float4 P = nP, V = nV;
+    fetch(base + stride + lane);
     unsigned long long vbits = 0ull;
     int tt = -1;
-    if (idx < total) {
-    const int t = find_slot(pfx, ntanks, idx);
+    if (t >= 0) {
     tt = t;
     const TankDev& T = tanks[t];
-    const int local = idx - pfx[t];
-    const float4 P = T.pB[local];
-    const float4 V = T.vB[local];
     const int flags = flags_of(P.w);
     const uint32_t id = __float_as_uint(V.w);
     const double dt = T.dt, h = T.h;
@@ -271,7 +296,11 @@ __global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ ta
           v[0] = vl[0]; v[1] = vl[1]; v[2] = vl[2];
           air = false;
           atomicAdd(&T.ctr->impacts, 1);
-          const double m = T.drop_mass;
+          double m = T.drop_mass;
+          if (T.drop_d_median > 0) {
+            const double D = drop_diameter(T, id);
+            m = 998.0 * (M_PI / 6.0) * D * D * D;
+          }
           ripple_deposit(T, x[0], x[2], 2.0 * m * fmin(dv, 8.0), 2e-3);
           const double level = T.oy + (c1[1] + fmin(cnt1 / T.ppc, 1.0)) * h;
           crown(T, x[0], level + 0.25 * h, x[2], -vold[1], m, id, frame);

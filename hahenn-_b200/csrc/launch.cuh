@@ -34,6 +34,14 @@ struct LaunchCtx {
   int2* tbl_c;              //   per tile: colour-0 cells with a constant pressure other than +0
 };
 
+// One CTA of the cluster-resident solve: planes [k0, k0+nk) of tank `tank` (index into the launch's
+// descriptors; -1: an idle CTA that only takes part in its cluster's barriers). np = planes per piece of
+// that tank, the same for all its pieces (the last may hold fewer); a tank's pieces sit on consecutive
+// cluster ranks, first plane first.
+struct ClusterPiece {
+  int tank, k0, nk, np;
+};
+
 // Blocks of kThreads threads of kernel k that fit on the current GPU at once (cached per device in cache[]).
 // The grid-stride particle kernels are launched with this many blocks: all resident, one wave.
 inline int resident_grid(const void* k, int* cache) {
@@ -60,7 +68,9 @@ void launch_p2g(const LaunchCtx& L);
 void launch_grid_nodes(const LaunchCtx& L);
 void launch_grid_cells(const LaunchCtx& L);
 void launch_sor_sweep(const LaunchCtx& L, int color, int sweep);
-void launch_sor_persist(const LaunchCtx& L, int max_iters, int blocks);   // whole solve, one cooperative launch
+// whole solve, one cooperative launch; a barrier wait gives up after `limit` polls (error bit in the counters)
+void launch_sor_persist(const LaunchCtx& L, int max_iters, int blocks, unsigned limit);
+constexpr unsigned kWatchdogPolls = 1u << 22;                            // default poll limit of a bounded wait
 int sor_persist_max_blocks(int device);                                  // co-resident blocks of k_sor_persist
 cudaError_t sor_tb_prepare();                                            // once per device, outside capture
 void launch_sor_tb(const LaunchCtx& L, int sweeps_per_launch, int sweep0, int nsweeps, int dir);  // 2 or 4; dir 0: pres→pres2
@@ -68,6 +78,16 @@ void launch_sor_copy(const LaunchCtx& L);                                // pres
 void launch_tbl_lists(const LaunchCtx& L);                               // per sub-step, before a 2-sweep solve
 size_t tbl_list_bytes(int tiles);                                        // device bytes of those lists
 void tbl_assign(LaunchCtx& L, void* base, int tiles);                    // point the context into them
+// cluster-resident solve (one launch per solve; each tank's field held in one cluster's shared memory)
+constexpr int kClusterMax = 16;                                          // CTAs per cluster (non-portable above 8)
+int cluster_smem_bytes(const TankDev& D, int np);                        // shared bytes of a piece of np planes
+int cluster_plane_bytes(const TankDev& D);                               // shared bytes of one z plane
+cudaError_t sor_cluster_prepare(int smem_bytes, int cluster);            // once per device, outside capture
+int sor_cluster_max_active(int smem_bytes, int cluster);                 // co-resident clusters (0: cannot launch)
+void launch_sor_cluster(const LaunchCtx& L, const ClusterPiece* pieces, int nblocks, int smem_bytes, int cluster,
+                        int max_iters);
+// FP64 residual of the solve just finished, max |r| and Σ r² over the active cells into the tank counters
+void launch_sor_residual(const LaunchCtx& L);
 void launch_project(const LaunchCtx& L);
 void launch_g2p(const LaunchCtx& L);
 void launch_whitewater(const LaunchCtx& L, double frame_dt);

@@ -1,7 +1,9 @@
 // Minimal JSON reader and the scene model (see scene.h).
 #include "scene.h"
 
+#include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
@@ -229,16 +231,75 @@ double bound_radius(int t, const double d[4]) {
   return 0.1;
 }
 
+namespace {
+
+// JSON text of the validated scene (the reference's validScene result, src/js/80-ui.js:430-459)
+std::string jnum(double v) {
+  char b[40];
+  snprintf(b, sizeof b, "%.15g", v);
+  if (strtod(b, nullptr) != v) snprintf(b, sizeof b, "%.17g", v);
+  return b;
+}
+std::string jstr(const std::string& v) {
+  std::string o = "\"";
+  for (const char c : v) {
+    if (c == '"' || c == '\\') { o += '\\'; o += c; }
+    else if ((unsigned char)c < 0x20) { char b[8]; snprintf(b, sizeof b, "\\u%04x", (unsigned)(unsigned char)c); o += b; }
+    else o += c;
+  }
+  return o + "\"";
+}
+std::string jvec(const double v[3]) { return "[" + jnum(v[0]) + "," + jnum(v[1]) + "," + jnum(v[2]) + "]"; }
+
+// a string field: the item's if it is a non-empty string, else the fresh item's
+std::string str_or(const JVal* v, const char* d) { return v && v->kind == JVal::Str && !v->s.empty() ? v->s : std::string(d); }
+bool bool_or(const JVal* v, bool d) { return v && v->kind == JVal::Bool ? v->b : d; }
+
+// names, colours and materials of fresh items (src/js/10-scene.js:5-15, :56-86)
+const char* shape_label(const std::string& s) {
+  static const char* const L[][2] = {{"box", "箱"}, {"plate", "板"}, {"sphere", "球"}, {"cylinder", "円柱"}, {"cone", "円錐"},
+                                     {"torus", "ドーナツ"}, {"cup", "コップ"}, {"container", "容器"}, {"gutter", "樋（とい）"}};
+  for (const auto& x : L)
+    if (s == x[0]) return x[1];
+  return "箱";
+}
+bool is_material(const std::string& m) { return m == "ceramic" || m == "plastic" || m == "metal" || m == "stone"; }
+
+}  // namespace
+
 bool parse_items(const JVal& items, Scene& sc, std::string& err) {
   if (items.kind != JVal::Arr) { err = "scene JSON: items must be an array"; return false; }
-  int next_id = 1;
+  // ids as validScene assigns them: a positive integer not seen before is kept; the others get max + 1, +2, …
+  // in item order
+  std::vector<const JVal*> kept;
+  std::vector<long long> ids;
+  std::vector<long long> seen;
   for (const JVal& it : items.arr) {
     if (it.kind != JVal::Obj) continue;
     const JVal* kind = it.get("kind");
     if (!kind || kind->kind != JVal::Str) continue;
+    if (kind->s != "obstacle" && kind->s != "drain" && kind->s != "block" && kind->s != "source") continue;
     const JVal* idv = it.get("id");
-    const int id = (idv && idv->is_num() && idv->num > 0 && idv->num == floor(idv->num)) ? (int)idv->num : 1000000 + next_id++;
-    if (kind->s == "obstacle" || kind->s == "drain") {
+    long long id = -1;
+    if (idv && idv->is_num() && idv->num > 0 && idv->num == floor(idv->num) && idv->num < 2147483647.0 &&
+        std::find(seen.begin(), seen.end(), (long long)idv->num) == seen.end()) {
+      id = (long long)idv->num;
+      seen.push_back(id);
+    }
+    kept.push_back(&it);
+    ids.push_back(id);
+  }
+  long long next = 1;
+  for (long long v : seen) next = std::max(next, v + 1);
+  for (long long& v : ids)
+    if (v < 0) v = next++;
+  std::string out = "[";
+  for (size_t n = 0; n < kept.size(); ++n) {
+    const JVal& it = *kept[n];
+    const std::string kind = it.get("kind")->s;
+    const int id = (int)ids[n];
+    std::string js = "{\"id\":" + std::to_string(id) + ",\"kind\":" + jstr(kind);
+    if (kind == "obstacle" || kind == "drain") {
       SceneItem si;
       si.id = id;
       Obj& o = si.obj;
@@ -248,14 +309,27 @@ bool parse_items(const JVal& items, Scene& sc, std::string& err) {
       vec_or(it.get("rot"), rot, zero);
       euler_deg(rot[0], rot[1], rot[2], si.R);
       memcpy(o.rot, si.R, sizeof(si.R));
-      if (kind->s == "obstacle") {
+      if (kind == "obstacle") {
         const double p0[3] = {0, 0.05, 0};
         vec_or(it.get("pos"), o.pos, p0);
         const JVal* sh = it.get("shape");
-        std::string shape = (sh && sh->kind == JVal::Str && find_shape(sh->s)) ? sh->s : "box";
+        const std::string shape = (sh && sh->kind == JVal::Str && find_shape(sh->s)) ? sh->s : "box";
         shape_params(shape, it.get("dims"), o.type, o.dims);
         o.bound = bound_radius(o.type, o.dims) + 0.002;
         o.flag = 1;
+        const ShapeDef* sd = find_shape(shape);
+        const JVal* dims = it.get("dims");
+        std::string dj = "{";
+        for (int k = 0; k < 4 && sd->keys[k]; ++k)
+          dj += std::string(k ? "," : "") + jstr(sd->keys[k]) + ":" + jnum(dim(sd, dims, sd->keys[k]));
+        dj += "}";
+        const char* color = shape == "cup" ? "#e9e4da" : shape == "gutter" ? "#8a8f94" : "#c9c2b4";
+        const char* mat = shape == "gutter" ? "metal" : (shape == "sphere" || shape == "cone") ? "stone" : "ceramic";
+        std::string m = str_or(it.get("material"), mat);
+        if (!is_material(m)) m = mat;
+        js += ",\"shape\":" + jstr(shape) + ",\"name\":" + jstr(str_or(it.get("name"), shape_label(shape))) +
+              ",\"pos\":" + jvec(o.pos) + ",\"rot\":" + jvec(rot) + ",\"dims\":" + dj +
+              ",\"color\":" + jstr(str_or(it.get("color"), color)) + ",\"material\":" + jstr(m);
       } else {
         vec_or(it.get("pos"), o.pos, zero);
         o.type = 9;
@@ -263,9 +337,11 @@ bool parse_items(const JVal& items, Scene& sc, std::string& err) {
         o.dims[1] = 0.012;
         o.bound = o.dims[0] + 0.02;
         o.flag = 2;
+        js += ",\"name\":" + jstr(str_or(it.get("name"), "排水口")) + ",\"pos\":" + jvec(o.pos) + ",\"rot\":" + jvec(rot) +
+              ",\"r\":" + jnum(o.dims[0]);
       }
       sc.solids.push_back(si);
-    } else if (kind->s == "block") {
+    } else if (kind == "block") {
       const double p0[3] = {0, 0.05, 0};
       double pos[3];
       vec_or(it.get("pos"), pos, p0);
@@ -276,14 +352,15 @@ bool parse_items(const JVal& items, Scene& sc, std::string& err) {
       b.lo[0] = pos[0] - w / 2; b.lo[1] = pos[1] - h / 2; b.lo[2] = pos[2] - d / 2;
       b.hi[0] = pos[0] + w / 2; b.hi[1] = pos[1] + h / 2; b.hi[2] = pos[2] + d / 2;
       sc.blocks.push_back(b);
-    } else if (kind->s == "source") {
+      js += ",\"name\":" + jstr(str_or(it.get("name"), "水の塊")) + ",\"pos\":" + jvec(pos) +
+            ",\"dims\":{\"w\":" + jnum(w) + ",\"h\":" + jnum(h) + ",\"d\":" + jnum(d) + "}";
+    } else {
       SourceItem s;
       s.id = id;
       const JVal* m = it.get("mode");
       if (m && m->kind == JVal::Str && (m->s == "stream" || m->s == "drops" || m->s == "shower" || m->s == "burst" || m->s == "rain"))
         s.mode = m->s;
-      const JVal* en = it.get("enabled");
-      if (en && en->kind == JVal::Bool) s.enabled = en->b;
+      s.enabled = bool_or(it.get("enabled"), true);
       const double p0[3] = {0, 0.4, 0};
       vec_or(it.get("pos"), s.pos, p0);
       s.pitch = num_or(it.get("pitch"), -90); s.yaw = num_or(it.get("yaw"), 0);
@@ -293,8 +370,16 @@ bool parse_items(const JVal& items, Scene& sc, std::string& err) {
       s.burst_every = num_or(it.get("burstEvery"), 0); s.rain_rate = num_or(it.get("rainRate"), 60);
       s.rain_size = num_or(it.get("rainSize"), 0.3); s.total = num_or(it.get("total"), 0);
       sc.sources.push_back(s);
+      js += ",\"name\":" + jstr(str_or(it.get("name"), "水源")) + ",\"pos\":" + jvec(s.pos) + ",\"pitch\":" + jnum(s.pitch) +
+            ",\"yaw\":" + jnum(s.yaw) + ",\"mode\":" + jstr(s.mode) + ",\"enabled\":" + (s.enabled ? "true" : "false") +
+            ",\"flow\":" + jnum(s.flow) + ",\"speed\":" + jnum(s.speed) + ",\"dropD\":" + jnum(s.drop_d) +
+            ",\"dropRate\":" + jnum(s.drop_rate) + ",\"spread\":" + jnum(s.spread) + ",\"burst\":" + jnum(s.burst) +
+            ",\"burstEvery\":" + jnum(s.burst_every) + ",\"rainRate\":" + jnum(s.rain_rate) +
+            ",\"rainSize\":" + jnum(s.rain_size) + ",\"total\":" + jnum(s.total);
     }
+    out += (n ? "," : "") + js + "}";
   }
+  sc.items_json = out + "]";
   return true;
 }
 
@@ -324,6 +409,11 @@ bool parse_scene(const std::string& text, bool clamp_tank, Scene& sc, std::strin
     sc.tank[2] = std::min(std::max(sc.tank[2], 0.15), 1.0);
   }
   return parse_items(*items, sc, err);
+}
+
+std::string scene_json_text(const Scene& sc) {
+  return "{\"tank\":{\"w\":" + jnum(sc.tank[0]) + ",\"h\":" + jnum(sc.tank[1]) + ",\"d\":" + jnum(sc.tank[2]) +
+         "},\"items\":" + sc.items_json + "}";
 }
 
 }  // namespace suiri

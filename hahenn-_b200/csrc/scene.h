@@ -49,12 +49,16 @@ struct Scene {
   std::vector<SceneItem> solids;          // obstacles (flag 1) and drains (flag 2)
   std::vector<WaterBlock> blocks;
   std::vector<SourceItem> sources;
+  std::string items_json;                 // the validated items as JSON (every field filled, ids assigned)
 };
 
 // items only (for set_objects); returns false with err on malformed JSON
 bool parse_items(const JVal& items, Scene& sc, std::string& err);
 // a whole scene file; clamp_tank applies the editor's tank limits (w∈[0.2,1.2], h∈[0.1,0.6], d∈[0.15,1])
 bool parse_scene(const std::string& text, bool clamp_tank, Scene& sc, std::string& err);
+
+// the validated scene {tank, items} as JSON text (what the reference's validScene returns)
+std::string scene_json_text(const Scene& sc);
 
 void euler_deg(double rx, double ry, double rz, double R[9]);
 // (type, d0..d3) of an obstacle shape (src/js/10-scene.js:143-157); false for an unknown shape

@@ -104,6 +104,18 @@ void Server::finish_request(Request* r) {
   Tank& t = *r->tank;
   t.read_counters();
   r->final_count = t.h_ctr->n_live;
+  if (const int bits = t.h_ctr->err) {
+    // a bounded device wait of this scene's solves gave up: its results are not those of the full solve
+    r->tank.reset();
+    const double tdone = now_s();
+    std::lock_guard<std::mutex> g(m);
+    used -= (double)r->bytes;
+    r->err = "device error bits " + std::to_string(bits) + " (1: a grid-barrier wait of the pressure solve gave up)";
+    r->t_done = tdone;
+    r->state = kFailed;
+    cv.notify_all();
+    return;
+  }
   if (r->keep_result) {
     const long long n = t.read_particles(nullptr, nullptr, 0);
     r->res_pos.resize(4 * n);

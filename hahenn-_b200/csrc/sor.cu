@@ -149,10 +149,9 @@ __global__ void __launch_bounds__(kSorThreads) k_sor(const TankDev* __restrict__
   }
 }
 
-constexpr unsigned kSpinLimit = 1u << 22;
-
-// sense-free generation barrier over all blocks of a cooperative launch; false if the wait gave up
-__device__ __forceinline__ bool grid_barrier(GridBarrier* b, unsigned nblocks) {
+// sense-free generation barrier over all blocks of a cooperative launch; false if the wait gave up after
+// `limit` polls (or another block's did)
+__device__ __forceinline__ bool grid_barrier(GridBarrier* b, unsigned nblocks, unsigned limit) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -166,7 +165,7 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* b, unsigned nblocks) {
     } else {
       unsigned spins = 0;
       while (*(volatile unsigned*)&b->gen == g) {
-        if (++spins > kSpinLimit || *(volatile int*)&b->err) { ok = 0; break; }
+        if (++spins > limit || *(volatile int*)&b->err) { ok = 0; break; }
         __nanosleep(32);
       }
     }
@@ -179,7 +178,7 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* b, unsigned nblocks) {
 }
 
 __global__ void __launch_bounds__(kThreads) k_sor_persist(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ hpfx,
-                                                          int max_iters, GridBarrier* bar) {
+                                                          int max_iters, GridBarrier* bar, unsigned limit) {
   const int total = hpfx[ntanks];
   const int stride = gridDim.x * blockDim.x;
   for (int sweep = 0; sweep < 2 * max_iters; ++sweep) {
@@ -189,7 +188,7 @@ __global__ void __launch_bounds__(kThreads) k_sor_persist(const TankDev* __restr
       const TankDev& T = tanks[t];
       if (it < T.iters) sor_cell(T, color, q - hpfx[t]);
     }
-    if (sweep + 1 < 2 * max_iters && !grid_barrier(bar, gridDim.x)) {
+    if (sweep + 1 < 2 * max_iters && !grid_barrier(bar, gridDim.x, limit)) {
       if (threadIdx.x == 0 && blockIdx.x == 0)
         for (int t = 0; t < ntanks; ++t) atomicOr(&tanks[t].ctr->err, kErrBarrier);
       return;
@@ -691,6 +690,155 @@ void launch_sor_copy(const LaunchCtx& L) {
   k_sor_copy<<<L.nblocks[kFamHalf], kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.bpfx[kFamHalf]);
 }
 
+// ---------------------------------------------------------------------------- cluster-resident solve
+// The whole solve in one launch, each tank held on chip by one thread-block cluster: the tank is cut into
+// pieces of whole z planes, one piece per CTA, and each CTA keeps its planes' pressure (both colours),
+// right-hand side and a one-byte cell code in shared memory for all 2·iters colour sweeps. A sweep relaxes
+// the CTA's cells of one colour from the other colour's values; the z neighbours of a piece's first and last
+// plane sit in the neighbouring CTAs of the cluster and are read through distributed shared memory
+// (mapa + ld.shared::cluster). The hardware cluster barrier (barrier.cluster arrive.release / wait.acquire)
+// separates the sweeps: no global memory and no launch between them. Small tanks share a cluster (each
+// piece only reads the pieces of its own tank), and every CTA takes part in every barrier of its cluster.
+// The update is sor_update in the same colour order, so the pressures equal one launch per sweep bit for
+// bit. Shared layout per CTA, S = hx·ny·np slots per colour (np = the tank's planes per piece, so every
+// piece of a tank has the same offsets): pressure [2][S] f32, rhs [2][S] f32, code [2][S] u8 (bits 0-5 open
+// faces, 6 cut cell, 7 active).
+constexpr int kClusterThreads = 1024;
+constexpr int kClusterBytesPerSlot = 9;
+
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ unsigned cluster_ctarank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+// the float at the same shared-memory offset as `local` in the CTA of cluster rank `rank`
+__device__ __forceinline__ float ld_cluster(const float* local, unsigned rank) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(local);
+  unsigned ra;
+  float v;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(a), "r"(rank));
+  asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(ra) : "memory");
+  return v;
+}
+
+__global__ void __launch_bounds__(kClusterThreads, 1) k_sor_cluster(const TankDev* __restrict__ tanks,
+                                                                    const ClusterPiece* __restrict__ pieces, int max_iters) {
+  extern __shared__ __align__(16) unsigned char cl_smem[];
+  const ClusterPiece pc = pieces[blockIdx.x];
+  const bool on = pc.tank >= 0;
+  const TankDev& T = tanks[on ? pc.tank : 0];
+  const int hx = T.hx, nx = T.nx, ny = T.ny, nz = T.nz;
+  const int plane = hx * ny;
+  const int S = plane * pc.np, U = on ? plane * pc.nk : 0;
+  const size_t g0 = (size_t)plane * pc.k0;      // first slot of the piece in each colour's global array
+  const size_t nh = T.nhalf;
+  float* sp = reinterpret_cast<float*>(cl_smem);
+  float* sr = sp + 2 * S;
+  uint8_t* sc = reinterpret_cast<uint8_t*>(sr + 2 * S);
+  const unsigned rank = cluster_ctarank();
+  for (int q = threadIdx.x; q < 2 * U; q += kClusterThreads) {
+    const int c = q >= U, l = q - c * U;
+    const size_t g = c * nh + g0 + l;
+    const uint32_t cd = T.code[g];
+    sp[c * S + l] = T.pres[g];
+    sr[c * S + l] = T.rhs[g];
+    sc[c * S + l] = (uint8_t)((cd & 0x3Fu) | ((cd & kCodePartial) ? 0x40u : 0u) | ((cd & kCodeActive) ? 0x80u : 0u));
+  }
+  cluster_barrier();                      // every piece is loaded before any neighbour reads it
+  const int iters = on ? T.iters : 0;
+  const float omega = T.omega;
+  for (int it = 0; it < max_iters; ++it) {
+#pragma unroll 1
+    for (int c = 0; c < 2; ++c) {
+      if (it < iters) {
+        const float* po = sp + (1 - c) * S;
+        float* pw = sp + c * S;
+        const float* rw = sr + c * S;
+        const uint8_t* cw = sc + c * S;
+        for (int l = threadIdx.x; l < U; l += kClusterThreads) {
+          const uint32_t cd = cw[l];
+          if (!(cd & 0x80u)) continue;
+          const int row = divu(l, T.dhx), ti = l - row * hx;
+          const int kl = divu(row, T.dny), j = row - kl * ny, k = pc.k0 + kl;
+          const int i = 2 * ti + ((j + k + c) & 1);
+          const int rowb = l - ti;
+          float nb[6];
+          nb[0] = i > 0 ? po[((i - 1) >> 1) + rowb] : 0.f;
+          nb[1] = i + 1 < nx ? po[((i + 1) >> 1) + rowb] : 0.f;
+          nb[2] = j > 0 ? po[l - hx] : 0.f;
+          nb[3] = j + 1 < ny ? po[l + hx] : 0.f;
+          nb[4] = k == 0 ? 0.f : (kl > 0 ? po[l - plane] : ld_cluster(po + l + plane * (pc.np - 1), rank - 1));
+          nb[5] = k + 1 >= nz ? 0.f : (kl + 1 < pc.nk ? po[l + plane] : ld_cluster(po + (l - plane * kl), rank + 1));
+          float C[6];
+          if (cd & 0x40u) {
+            cut_coeffs(T, i, j, k, C);
+          } else {
+#pragma unroll
+            for (int d = 0; d < 6; ++d) C[d] = (cd >> d) & 1u ? 1.0f : 0.0f;
+          }
+          pw[l] = sor_update(C, nb, rw[l], pw[l], omega);
+        }
+      }
+      cluster_barrier();                  // this colour is complete in every piece before the next reads it
+    }
+  }
+  for (int q = threadIdx.x; q < 2 * U; q += kClusterThreads) {
+    const int c = q >= U, l = q - c * U;
+    T.pres[c * nh + g0 + l] = sp[c * S + l];
+  }
+}
+
+int cluster_plane_bytes(const TankDev& D) { return kClusterBytesPerSlot * 2 * D.hx * D.ny; }
+
+int cluster_smem_bytes(const TankDev& D, int np) { return (cluster_plane_bytes(D) * np + 15) & ~15; }
+
+cudaError_t sor_cluster_prepare(int smem_bytes, int cluster) {
+  cudaError_t e = cudaFuncSetAttribute(k_sor_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  if (e != cudaSuccess) return e;
+  if (cluster > 8) e = cudaFuncSetAttribute(k_sor_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  return e;
+}
+
+static void cluster_config(cudaLaunchConfig_t& cfg, cudaLaunchAttribute* attr, int nblocks, int smem_bytes, int cluster,
+                           cudaStream_t stream) {
+  cfg = {};
+  cfg.gridDim = dim3(nblocks);
+  cfg.blockDim = dim3(kClusterThreads);
+  cfg.dynamicSmemBytes = smem_bytes;
+  cfg.stream = stream;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+}
+
+int sor_cluster_max_active(int smem_bytes, int cluster) {
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute attr[1];
+  cluster_config(cfg, attr, cluster, smem_bytes, cluster, nullptr);
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k_sor_cluster, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+void launch_sor_cluster(const LaunchCtx& L, const ClusterPiece* pieces, int nblocks, int smem_bytes, int cluster,
+                        int max_iters) {
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute attr[1];
+  cluster_config(cfg, attr, nblocks, smem_bytes, cluster, L.stream);
+  cudaLaunchKernelEx(&cfg, k_sor_cluster, L.tanks, pieces, max_iters);
+}
+
 void launch_sor_sweep(const LaunchCtx& L, int color, int sweep) {
   cudaLaunchConfig_t cfg = {};
   // A grid larger than what is resident at once is capped there and loops: the next sweep's blocks then
@@ -710,6 +858,80 @@ void launch_sor_sweep(const LaunchCtx& L, int color, int sweep) {
   else cudaLaunchKernelEx(&cfg, k_sor<false>, L.tanks, L.ntanks, (const int*)L.apfx, color, sweep);
 }
 
+// FP64 residual of the solve just finished, per active cell of `color`: r = Σ C_d·p_nb − rhs − (Σ C_d)·p,
+// evaluated in float64 from the float32 coefficients, right-hand side and pressures (outside the grid p = 0).
+// It is the residual of the linear system the float32 sweeps approximate; max |r|, max |rhs| and Σ r² go to
+// the tank counters, one atomic per warp where the warp's cells belong to one tank.
+__global__ void __launch_bounds__(kThreads) k_sor_residual(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ apfx,
+                                                           int color) {
+  const int* __restrict__ pfx = apfx + color * (ntanks + 1);
+  const int total = pfx[ntanks];
+  if ((int)(blockIdx.x * blockDim.x) >= total) return;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = q < total;
+  const int t = find_slot(pfx, ntanks, live ? q : total - 1);
+  double ra = 0.0, rh = 0.0, r2 = 0.0;
+  if (live) {
+    const TankDev& T = tanks[t];
+    const int hx = T.hx, nx = T.nx, ny = T.ny, nz = T.nz;
+    const int s = T.act[(size_t)color * T.nhalf + (q - pfx[t])];
+    const int row = divu(s, T.dhx), ti = s - row * hx;
+    const int k = divu(row, T.dny), j = row - k * ny;
+    const int i = 2 * ti + ((j + k + color) & 1);
+    const size_t own = (size_t)color * T.nhalf + s;
+    const uint32_t code = T.code[own];
+    const float* __restrict__ po = T.pres + (size_t)(1 - color) * T.nhalf;
+    const int rowb = hx * row;
+    float nb[6];
+    nb[0] = i > 0 ? po[((i - 1) >> 1) + rowb] : 0.f;
+    nb[1] = i + 1 < nx ? po[((i + 1) >> 1) + rowb] : 0.f;
+    nb[2] = j > 0 ? po[ti + rowb - hx] : 0.f;
+    nb[3] = j + 1 < ny ? po[ti + rowb + hx] : 0.f;
+    nb[4] = k > 0 ? po[ti + rowb - hx * ny] : 0.f;
+    nb[5] = k + 1 < nz ? po[ti + rowb + hx * ny] : 0.f;
+    float C[6];
+    if (code & kCodePartial) {
+      cut_coeffs(T, i, j, k, C);
+    } else {
+#pragma unroll
+      for (int d = 0; d < 6; ++d) C[d] = (code >> d) & 1u ? 1.0f : 0.0f;
+    }
+    double num = 0.0, den = 0.0;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) {
+      num = __dadd_rn(num, __dmul_rn((double)C[d], (double)nb[d]));
+      den = __dadd_rn(den, (double)C[d]);
+    }
+    const double rhs = (double)T.rhs[own];
+    const double r = __dsub_rn(__dsub_rn(num, rhs), __dmul_rn(den, (double)T.pres[own]));
+    ra = fabs(r);
+    rh = fabs(rhs);
+    r2 = __dmul_rn(r, r);
+  }
+  const unsigned lanes = __ballot_sync(0xffffffffu, true);
+  const int t0 = __shfl_sync(lanes, t, 0);
+  if (__all_sync(lanes, t == t0)) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ra = fmax(ra, __shfl_xor_sync(lanes, ra, o));
+      rh = fmax(rh, __shfl_xor_sync(lanes, rh, o));
+      r2 = __dadd_rn(r2, __shfl_xor_sync(lanes, r2, o));
+    }
+    if ((threadIdx.x & 31) != 0) return;
+  } else if (!live) {
+    return;
+  }
+  Counters* c = tanks[t].ctr;
+  atomicMax(&c->res_max_bits, (unsigned long long)__double_as_longlong(ra));
+  atomicMax(&c->rhs_max_bits, (unsigned long long)__double_as_longlong(rh));
+  atomicAdd(&c->res_sum2, r2);
+}
+
+void launch_sor_residual(const LaunchCtx& L) {
+  for (int c = 0; c < 2; ++c)
+    k_sor_residual<<<L.nblocks[kFamSor], kThreads, 0, L.stream>>>(L.tanks, L.ntanks, (const int*)L.apfx, c);
+}
+
 int sor_persist_max_blocks(int device) {
   int per_sm = 0, sms = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sor_persist, kThreads, 0);
@@ -717,7 +939,9 @@ int sor_persist_max_blocks(int device) {
   return per_sm * sms;
 }
 
-void launch_sor_persist(const LaunchCtx& L, int max_iters, int blocks) {
+void launch_sor_persist(const LaunchCtx& L, int max_iters, int blocks, unsigned limit) {
+  // the barrier starts every solve cleared: a solve whose wait gave up leaves its counts behind
+  cudaMemsetAsync(L.barrier, 0, sizeof(GridBarrier), L.stream);
   // cooperative launch: the runtime refuses it unless every block can be resident at once
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
@@ -728,7 +952,7 @@ void launch_sor_persist(const LaunchCtx& L, int max_iters, int blocks) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k_sor_persist, L.tanks, L.ntanks, (const int*)L.hpfx, max_iters, L.barrier);
+  cudaLaunchKernelEx(&cfg, k_sor_persist, L.tanks, L.ntanks, (const int*)L.hpfx, max_iters, L.barrier, limit);
 }
 
 }  // namespace suiri

@@ -25,14 +25,19 @@ class Params(C.Structure):
                 ('whitewater', C.c_int32), ('capacity', C.c_int64), ('ww_capacity', C.c_int64),
                 ('ripple_rx', C.c_int32), ('ripple_rz', C.c_int32), ('wmap', C.c_int32), ('sdf_mode', C.c_int32),
                 ('device', C.c_int32), ('seed', C.c_uint32), ('ripple_sigma', C.c_double), ('ripple_rho', C.c_double),
-                ('ripple_depth', C.c_double), ('advect', C.c_int32)]
+                ('ripple_depth', C.c_double), ('advect', C.c_int32), ('drop_d_median', C.c_double),
+                ('drop_d_sigma_log', C.c_double), ('sor_mode', C.c_int32), ('watchdog_polls', C.c_int64)]
 
 
 class Stats(C.Structure):
     _fields_ = [('count', C.c_int64), ('ww_count', C.c_int64), ('impacts', C.c_int64), ('vmax', C.c_double),
                 ('time', C.c_double), ('liters', C.c_double), ('full', C.c_int32), ('frame', C.c_int32),
                 ('errors', C.c_int32), ('pad', C.c_int32), ('nx', C.c_int32), ('ny', C.c_int32), ('nz', C.c_int32), ('h', C.c_double),
-                ('origin', C.c_double * 3)]
+                ('origin', C.c_double * 3), ('active_cells', C.c_int64), ('residual_max', C.c_double),
+                ('residual_rms', C.c_double), ('rhs_max', C.c_double)]
+
+
+PHASES = ('bin_sort', 'p2g', 'grid_passes', 'pressure_solve', 'projection', 'g2p')
 
 
 class Object(C.Structure):
@@ -110,6 +115,15 @@ SIGNATURES = {
     'suiri_time_substeps': (C.c_int, [P, C.c_double, C.c_int32, C.POINTER(C.c_double)]),
     'suiri_batch_time_substeps': (C.c_int, [P, C.c_double, C.c_int32, C.POINTER(C.c_double)]),
     'suiri_time_sor': (C.c_int, [P, C.c_int32, C.POINTER(C.c_double)]),
+    'suiri_add_whitewater': (C.c_int, [P, P, P, C.c_int64]),
+    'suiri_scene_validate': (C.c_int, [C.c_char_p, C.c_int32, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    'suiri_tune_piece': (C.c_int, [P, C.c_int32]),
+    'suiri_batch_tune_piece': (C.c_int, [P, C.c_int32]),
+    'suiri_residual': (C.c_int, [P, C.c_int32]),
+    'suiri_batch_residual': (C.c_int, [P, C.c_int32]),
+    'suiri_phase_ms': (C.c_int, [P, C.POINTER(C.c_double)]),
+    'suiri_batch_lanes': (C.c_int, [P, C.POINTER(C.c_int32)]),
+    'suiri_batch_phase_ms': (C.c_int, [P, C.c_int32, C.POINTER(C.c_double)]),
 }
 
 _lib = None
@@ -133,6 +147,18 @@ def lib():
             f.restype, f.argtypes = res, args
         _lib = L
     return _lib
+
+
+def validate_scene(scene, clamp_tank=True):
+    """The scene (JSON text or a dict) as the library reads it (suiri_scene_validate): a dict {tank, items}."""
+    import json
+    js = (scene if isinstance(scene, (str, bytes)) else json.dumps(scene))
+    js = js.encode() if isinstance(js, str) else js
+    n = C.c_size_t()
+    check(lib().suiri_scene_validate(js, 1 if clamp_tank else 0, None, 0, C.byref(n)))
+    buf = C.create_string_buffer(n.value + 1)
+    check(lib().suiri_scene_validate(js, 1 if clamp_tank else 0, buf, n.value + 1, C.byref(n)))
+    return json.loads(buf.value.decode())
 
 
 def check(rc, handle=None):

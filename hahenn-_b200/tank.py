@@ -25,7 +25,8 @@ class Tank:
     def __init__(self, scene=None, *, nx=0, ny=0, nz=0, h=0.0, quality='standard', clamp_tank=True,
                  extra_height=0.0, flip=0.96, omega=1.6, iters=0, gravity=9.81, friction=0.03, ppc=8.0, drift=6.0,
                  ww_rate=7.0, whitewater=True, capacity=0, ww_capacity=0, ripple=(0, 0), wmap=0, sdf_mode='analytic',
-                 device=0, seed=1, ripple_sigma=0.0728, ripple_rho=998.0, ripple_depth=0.0, advect='euler'):
+                 device=0, seed=1, ripple_sigma=0.0728, ripple_rho=998.0, ripple_depth=0.0, advect='euler',
+                 drop_d=None, sor_mode=0, watchdog_polls=None):
         L = N.lib()
         p = N.Params()
         N.check(L.suiri_params_default(C.byref(p)))
@@ -46,6 +47,11 @@ class Tank:
         p.device, p.seed = int(device), int(seed)
         p.ripple_sigma, p.ripple_rho, p.ripple_depth = float(ripple_sigma), float(ripple_rho), float(ripple_depth)
         p.advect = {'euler': 0, 'rk2': 1}[advect]
+        if drop_d is not None:          # (median [m], sigma_log): lognormal sub-grid drop diameters
+            p.drop_d_median, p.drop_d_sigma_log = float(drop_d[0]), float(drop_d[1])
+        p.sor_mode = int(sor_mode)
+        if watchdog_polls is not None:
+            p.watchdog_polls = int(watchdog_polls)
         if scene is not None and not isinstance(scene, (str, bytes)):
             scene = json.dumps(scene)
         h_ = C.c_void_p()
@@ -149,6 +155,14 @@ class Tank:
         self._c(N.lib().suiri_snapshot(self._h, C.byref(i)))
         return i.value
 
+    def save_state(self):
+        """The tank's state in its one water-copy slot (for rolling back, e.g. after tuning)."""
+        return self.save_water()
+
+    def restore_state(self, copy_id):
+        if not self.restore_water(copy_id):
+            raise RuntimeError('the saved state was already restored or replaced')
+
     def restore_water(self, copy_id):
         try:
             self._c(N.lib().suiri_restore(self._h, int(copy_id)))
@@ -192,13 +206,28 @@ class Tank:
         self._c(N.lib().suiri_profile(self._h, 1 if on else 0))
 
     def tune(self, blocks_per_sm=4, sor_mode=0):
-        """sor_mode: 0 one launch per colour sweep, 1 one cooperative launch, 2/3 temporal blocking (2/4 sweeps)."""
+        """sor_mode: 0 one launch per colour sweep, 1 one cooperative launch, 2/3 temporal blocking (2/4 sweeps),
+        4 the whole solve held in one thread-block cluster's shared memory."""
         self._c(N.lib().suiri_tune(self._h, int(blocks_per_sm), int(sor_mode)))
+
+    def tune_piece(self, piece_kb=0):
+        """Shared memory per CTA of the cluster-resident solve, KiB (0: the device maximum)."""
+        self._c(N.lib().suiri_tune_piece(self._h, int(piece_kb)))
+
+    def residual(self, on=True):
+        """Evaluate every solve's FP64 residual on the device (stats: residual_max, residual_rms, rhs_max)."""
+        self._c(N.lib().suiri_residual(self._h, 1 if on else 0))
 
     def sor_phase_ms(self):
         ms = C.c_double()
         self._c(N.lib().suiri_sor_phase_ms(self._h, C.byref(ms)))
         return ms.value
+
+    def phase_ms(self):
+        """Device ms of each phase of the last sub-step (profiling on), keyed by native.PHASES."""
+        ms = (C.c_double * len(N.PHASES))()
+        self._c(N.lib().suiri_phase_ms(self._h, ms))
+        return dict(zip(N.PHASES, list(ms)))
 
     # ------------------------------------------------------------------ read-back
     def particles(self):
@@ -230,6 +259,15 @@ class Tank:
         self._c(N.lib().suiri_read_whitewater(self._h, _ptr(P), _ptr(V), n.value, C.byref(n)))
         return P, V
 
+    def add_whitewater(self, pos, vel, life, kind):
+        """Append whitewater particles: pos, vel (N,3), life, kind (N,) (0 spray, 1 foam, 2 bubble)."""
+        pos = np.asarray(pos, np.float32).reshape(-1, 3)
+        P = np.empty((len(pos), 4), np.float32)
+        V = np.empty((len(pos), 4), np.float32)
+        P[:, :3], P[:, 3] = pos, np.asarray(life, np.float32).reshape(-1)
+        V[:, :3], V[:, 3] = np.asarray(vel, np.float32).reshape(-1, 3), np.asarray(kind, np.float32).reshape(-1)
+        self._c(N.lib().suiri_add_whitewater(self._h, _ptr(P), _ptr(V), len(P)))
+
     def grid(self, field):
         """A grid field as the oracle indexes it: faces (3, nx+1, ny+1, nz+1), cells (nx, ny, nz)."""
         nx, ny, nz = self.nx, self.ny, self.nz
@@ -253,7 +291,9 @@ class Tank:
     @staticmethod
     def _stats_dict(s):
         return dict(count=s.count, ww_count=s.ww_count, impacts=s.impacts, vmax=s.vmax, time=s.time, liters=s.liters,
-                    full=bool(s.full), frame=s.frame, errors=s.errors, nx=s.nx, ny=s.ny, nz=s.nz, h=s.h, origin=tuple(s.origin))
+                    full=bool(s.full), frame=s.frame, errors=s.errors, nx=s.nx, ny=s.ny, nz=s.nz, h=s.h, origin=tuple(s.origin),
+                    active_cells=s.active_cells, residual_max=s.residual_max, residual_rms=s.residual_rms,
+                    rhs_max=s.rhs_max)
 
     def stats(self):
         s = N.Stats()
@@ -298,11 +338,37 @@ class Batch:
     def substep(self, dt):
         N.check(N.lib().suiri_batch_substep(self._h, float(dt)))
 
+    def save_state(self):
+        """Every tank's state in its water-copy slot."""
+        self.sync()
+        return [t.save_water() for t in self.tanks]
+
+    def restore_state(self, ids):
+        self.sync()
+        for t, i in zip(self.tanks, ids):
+            t.restore_state(i)
+
     def sync(self):
         N.check(N.lib().suiri_batch_sync(self._h))
 
     def tune(self, blocks_per_sm=4, sor_mode=0):
         N.check(N.lib().suiri_batch_tune(self._h, int(blocks_per_sm), int(sor_mode)))
+
+    def tune_piece(self, piece_kb=0):
+        N.check(N.lib().suiri_batch_tune_piece(self._h, int(piece_kb)))
+
+    def residual(self, on=True):
+        N.check(N.lib().suiri_batch_residual(self._h, 1 if on else 0))
+
+    def lanes(self):
+        n = C.c_int32()
+        N.check(N.lib().suiri_batch_lanes(self._h, C.byref(n)))
+        return n.value
+
+    def phase_ms(self, lane):
+        ms = (C.c_double * len(N.PHASES))()
+        N.check(N.lib().suiri_batch_phase_ms(self._h, int(lane), ms))
+        return dict(zip(N.PHASES, list(ms)))
 
     def profile(self, on=True):
         N.check(N.lib().suiri_batch_profile(self._h, 1 if on else 0))

@@ -86,12 +86,14 @@ def full_scene(seed=0, scale=1):
     cells = block_cells(nx, ny, nz, lambda i, j, k: j < 32 // scale)
     pos = fill_cells(cells, h, o, 8, seed)
     W, H, D = nx * h, ny * h, nz * h
-    # every sub-grid drop is one particle carrying the free-flight mark; its crown uses the particle mass
-    # 998·(h/2)³ as the reference does (31-wgsl-sim2.js:224)
+    # every sub-grid drop is one particle carrying the free-flight mark; its impulse and crown use the drop's
+    # own diameter, lognormal with median 2 mm and σ_log 0.4 (drop_d; the reference's rule, the particle mass
+    # 998·(h/2)³ of 31-wgsl-sim2.js:224, is drop_d=None)
     rain = dict(shape='rain', pos=[0.0, 0.98 * H, 0.0], radius=W / 2, radius_z=D / 2, speed=4.0,
                 count=2000.0 / 240.0, airborne=True)
     return dict(name=f'full_scene_{nx}x{ny}x{nz}', nx=nx, ny=ny, nz=nz, h=h, origin=o, pos=pos,
-                params=dict(flip=0.95, omega=1.8, iters=100, g=9.81, dt=1 / 240, sigma=0.072, rho=1000.0, depth=0.1),
+                params=dict(flip=0.95, omega=1.8, iters=100, g=9.81, dt=1 / 240, sigma=0.072, rho=1000.0, depth=0.1,
+                            drop_d=(0.002, 0.4)),
                 objects=[], emitters=[rain], ripple=(1024 // scale, 512 // scale), steps=300)
 
 

@@ -71,6 +71,18 @@ typedef struct suiri_params {
      (solver.py:545-550, 31-wgsl-sim2.js:168); 1 second-order midpoint (RK2) through the interpolated grid
      velocity u for in-grid particles, x0 + u(x0 + u(x0)·dt/2)·dt (not in the reference) */
   int32_t advect;
+  /* sub-grid drop diameters (not in the reference, whose merging drops all carry the particle mass
+     998·(h/2)³, src/js/31-wgsl-sim2.js:224, solver.py:596): drop_d_median > 0 gives every drop its own
+     diameter, lognormal with this median [m] and log-standard-deviation drop_d_sigma_log, drawn from the
+     drop's carried id; its impulse and crown then use the drop's mass 998·π/6·D³ */
+  double drop_d_median;
+  double drop_d_sigma_log;
+  /* form of the pressure solve of the tank's own sub-steps, and of a batch or serving lane whose first tank
+     it is (sor_mode of suiri_tune; -1: cluster-resident where the lane's tanks fit, else one launch per sweep) */
+  int32_t sor_mode;
+  /* polls of a bounded device wait (the cooperative solve's grid barrier) before it gives up, records error
+     bit 1 in the tank's stats and returns (default 2^22; a batch or lane takes its tanks' smallest) */
+  int64_t watchdog_polls;
 } suiri_params;
 
 typedef struct suiri_stats {
@@ -87,6 +99,13 @@ typedef struct suiri_stats {
   int32_t nx, ny, nz;
   double h;
   double origin[3];
+  int64_t active_cells;    /* liquid cells with an open face, relaxed by the last solve (both colours) */
+  /* FP64 residual of the last pressure solve, r = Σ C·p_nb − h²·div − (Σ C)·p over the active cells, in
+     float64 from the float32 operands (the check solver.py:473-509's operands allow); 0 unless switched on
+     with suiri_residual / suiri_batch_residual */
+  double residual_max;     /* max |r| */
+  double residual_rms;     /* sqrt(Σ r² / active_cells) */
+  double rhs_max;          /* max |h²·div| over the same cells (the scale of r) */
 } suiri_stats;
 
 /* An obstacle or drain in binary form (instead of scene JSON items). */
@@ -153,10 +172,20 @@ int suiri_eval_sdf(suiri_tank* t, const double* pts, int64_t n, double* out);
    points and distances in memory it allocates per call; this one stages them in one fixed array inside
    the library, at most 65536 points per call (more: SUIRI_ERR_INVALID). The array (2 MiB) exists on every
    GPU that loads the library, until the process exits. The first call on a device looks up the array's
-   address there; make that first call before any stream capture. All calls share the one array: calls
-   that overlap on the GPU (two threads, two tanks on different streams) race on it, so serialise them.
-   Every call writes all the staging it reads, so nothing is left over from the previous call. */
+   address there; make that first call before any stream capture. Like every call on a tank, it leaves the
+   tank's device current for the calling thread. All calls share the one array: calls that overlap on the
+   GPU (two threads, two tanks on different streams) race on it, so serialise them. Every call writes all
+   the staging it reads, so nothing is left over from the previous call. */
 int suiri_eval_sdf_static(suiri_tank* t, const double* pts, int64_t n, double* out);
+/* validScene (src/js/80-ui.js:430-459) without creating a tank (needs no GPU): the scene as the library reads
+   it, as JSON {"tank":{w,h,d},"items":[…]}, the tank clamped to the editor's limits when clamp_tank is 1,
+   items of an unknown kind dropped, every field missing or unusable taken from a fresh item of the same kind
+   (src/js/10-scene.js:56-86; an unknown shape is a box, an unknown material or source mode the fresh item's),
+   ids kept when positive, integral and not seen before, the others numbered on from the largest.
+   *len = the text's length without its terminating NUL; it is written to out (NUL-terminated) when cap is
+   larger than that, else nothing is written and SUIRI_ERR_INVALID returned (out may be NULL to query the
+   length). SUIRI_ERR_PARSE for malformed JSON or a tank without positive w, h, d. */
+int suiri_scene_validate(const char* scene_json, int32_t clamp_tank, char* out, size_t cap, size_t* len);
 /* device bytes a tank of these parameters and scene would take (admission planning) */
 int suiri_estimate_bytes(const char* scene_json, const suiri_params* params, double* bytes);
 
@@ -196,6 +225,11 @@ int suiri_sync(suiri_tank* t);
 int suiri_read_particles(suiri_tank* t, float* pos4, float* vel4, int64_t cap, int64_t* n);
 /* whitewater: pos4 = (x, y, z, life), vel4 = (vx, vy, vz, kind) */
 int suiri_read_whitewater(suiri_tank* t, float* pos4, float* vel4, int64_t cap, int64_t* n);
+/* whitewater particles appended from host memory, in the layout suiri_read_whitewater gives (life in pos4.w,
+   kind in vel4.w: 0 spray, 1 foam, 2 bubble), e.g. a state saved by a host (the Blender add-on keeps its
+   wpos/wvel/wlife/wkind arrays, solver.py:86-89). SUIRI_ERR_CAPACITY if they do not all fit (those that fit
+   are kept). */
+int suiri_add_whitewater(suiri_tank* t, const float* pos4, const float* vel4, int64_t n);
 /* a grid field (enum suiri_field) into out (bytes long) */
 int suiri_read_grid(suiri_tank* t, int32_t field, void* out, size_t bytes);
 int suiri_get_stats(suiri_tank* t, suiri_stats* s);
@@ -232,9 +266,22 @@ int suiri_batch_sync(suiri_batch* b);
    the pressure solve, sor_mode: 0 one launch per colour sweep; 1 the whole solve in one cooperative launch
    with a grid barrier between sweeps; 2 two colour sweeps per launch over per-tile lists of active cells
    (allocates those lists for the tank or batch, once); 3 four sweeps per launch on shared-memory tiles with
-   halos. All give the same pressures bit for bit. */
+   halos; 4 the whole solve in one launch with each tank held in the shared memory of one thread-block
+   cluster (distributed shared memory between its CTAs, the hardware cluster barrier between sweeps); it
+   fails with SUIRI_ERR_INVALID when a tank needs more than 16 CTAs of shared memory (then keep another
+   form). The tile of mode 4 is the shared memory a CTA takes, set by suiri_tune_piece. All five forms give
+   the same pressures bit for bit. */
 int suiri_batch_tune(suiri_batch* b, int32_t particle_blocks_per_sm, int32_t sor_mode);
 int suiri_tune(suiri_tank* t, int32_t particle_blocks_per_sm, int32_t sor_mode);
+/* tile knob of the cluster-resident solve: at most piece_kb KiB of shared memory per CTA (0: the device's
+   maximum), i.e. fewer z planes per CTA and more CTAs per tank; applies now if tuned to sor_mode 4, else at
+   the next suiri_tune with it */
+int suiri_tune_piece(suiri_tank* t, int32_t piece_kb);
+int suiri_batch_tune_piece(suiri_batch* b, int32_t piece_kb);
+/* 1: after every pressure solve, evaluate its FP64 residual on the device (two extra launches); read it
+   with suiri_get_stats (residual_max, residual_rms, rhs_max) */
+int suiri_residual(suiri_tank* t, int32_t on);
+int suiri_batch_residual(suiri_batch* b, int32_t on);
 int suiri_batch_stream(suiri_batch* b, void** stream);
 
 /* ---------------------------------------------------------------- serving: continuous batching under an HBM budget */
@@ -293,6 +340,14 @@ int suiri_sor_phase_ms(suiri_tank* t, double* ms);
 int suiri_batch_profile(suiri_batch* b, int32_t on);
 /* the longest of the lanes' pressure-solve times (the lanes run concurrently) */
 int suiri_batch_sor_phase_ms(suiri_batch* b, double* ms);
+/* with profiling on, the device time of each phase of the last sub-step, ms[6]: binning and sort, P2G, node and
+   cell passes, pressure solve, projection (with the residual when on), G2P */
+#define SUIRI_PHASES 6
+int suiri_phase_ms(suiri_tank* t, double* ms);
+/* the same for one size lane of a batch (lane in [0, suiri_batch_lanes)); occupied lanes in order of size
+   (under 2^16 cells, under 2^19, larger) */
+int suiri_batch_lanes(suiri_batch* b, int32_t* n);
+int suiri_batch_phase_ms(suiri_batch* b, int32_t lane, double* ms);
 
 #ifdef __cplusplus
 }

@@ -31,7 +31,8 @@ OFF = (np.array([0.0, 0.5, 0.5]), np.array([0.5, 0.0, 0.5]), np.array([0.5, 0.5,
 class Tank:
     def __init__(self, nx, ny, nz, h, *, origin=None, extra_height=0.0, flip=0.96, omega=1.6, iters=40,
                  g=9.81, ppc=8.0, drift=6.0, friction=0.03, ww_rate=7.0, whitewater=True, ww_cap=140000,
-                 ripple=(128, 128), wmap=256, seed=1, rng_mode='numpy', sdf_mode='lattice', advect='euler'):
+                 ripple=(128, 128), wmap=256, seed=1, rng_mode='numpy', sdf_mode='lattice', advect='euler',
+                 drop_d=None):
         self.nx, self.ny, self.nz, self.h = int(nx), int(ny), int(nz), float(h)
         h = self.h
         self.origin = np.array([-self.nx * h / 2, 0.0, -self.nz * h / 2]) if origin is None else np.array(origin, float)
@@ -48,6 +49,9 @@ class Tank:
         if advect not in ('euler', 'rk2'):
             raise ValueError('advect is euler or rk2')
         self.advect = advect
+        # (median, sigma_log): sub-grid drops get their own lognormal diameters (hashrng.drop_diameter);
+        # None: every drop has the particle mass, as the reference
+        self.drop_d = drop_d
         self.time, self.frame, self.vmax, self.impacts = 0.0, 0, 1.0, 0
         self.pos = np.zeros((0, 3)); self.vel = np.zeros((0, 3)); self.air = np.zeros(0)
         self.pid = np.zeros(0, np.int64)
@@ -536,13 +540,16 @@ class Tank:
                     air[ids] = 0.0
                     self.impacts += len(ids)
                     self.merged = self.pid[ids].copy()
-                    m = RHO * (0.5 * h) ** 3
+                    m = np.full(len(ids), RHO * (0.5 * h) ** 3)
+                    if self.drop_d is not None:
+                        D = hashrng.drop_diameter(self.pid[ids], *self.drop_d)
+                        m = RHO * (math.pi / 6.0) * D * D * D
                     self.ripple_deposit(x[ids], 2.0 * m * np.minimum(dv, 8.0), 2e-3)
                     cnt = self.count_at(c1[ids])
                     level = self.origin[1] + (c1[ids, 1] + np.minimum(cnt / self.PPC, 1.0)) * h
                     for k in range(len(ids)):
-                        self.crown(np.array([x[ids[k], 0], level[k] + 0.25 * h, x[ids[k], 2]]), -self.vel[ids[k], 1], m,
-                                   int(self.pid[ids[k]]))
+                        self.crown(np.array([x[ids[k], 0], level[k] + 0.25 * h, x[ids[k], 2]]), -self.vel[ids[k], 1],
+                                   float(m[k]), int(self.pid[ids[k]]))
         if ing.any():
             sp = np.linalg.norm(v[ing], axis=1)
             self.vmax = float(min(sp.max(), 60.0)) if len(sp) else 0.0

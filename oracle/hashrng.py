@@ -40,6 +40,18 @@ def seed_ww(pid, frame):
     return hash_u32((pid * 9781 + np.uint64(frame) * 6271 + 17) & M32)
 
 
+def drop_diameter(pid, median, sigma):
+    """Lognormal diameter of sub-grid drop `pid` (the build's own rule; the reference gives every drop the
+    particle mass): Box-Muller z = sqrt(-2 ln u1)·cos(2π u2) from the first two draws of the stream seeded
+    hash(pid·0x9E3779B1 + 0x632BE5AB), u1 shifted by half a step off zero, |z| clamped to 4."""
+    pid = np.asarray(pid, dtype=np.uint64)
+    st = Stream(hash_u32((pid * 0x9E3779B1 + 0x632BE5AB) & M32))
+    u1 = st.rnd() + 0.5 / 16777216.0
+    u2 = st.rnd()
+    z = np.clip(np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2), -4.0, 4.0)
+    return median * np.exp(sigma * z)
+
+
 def seed_crown(pid, frame):
     """Seed for the crown splash of particle `pid` (cf. ``31-wgsl-sim2.js:128``)."""
     pid = np.asarray(pid, dtype=np.uint64)

@@ -5,8 +5,8 @@ numpy) on seeded inputs and stores inputs and outputs as small ``.npz`` files in
 (``oracle/``) is pinned against these files by ``tests/test_oracle_golden.py``; the CUDA path is compared
 with the oracle and, where shapes allow, with these files directly.
 
-Usage (in a checkout that has the reference at REF, default /root/reference):
-    python tests/golden/make_golden.py [REF]
+Usage, with REF the root of a checkout of the reference (given as the argument or in SUIRI_REFERENCE):
+    python tests/golden/make_golden.py REF
 
 Obstacle lattices are the analytic shapes of ``oracle/sdf.py`` sampled at the solver's lattice points
 (``solver.py:106-110``) — the role the Blender host's mesh distance queries play (``bake.py:83-119``).
@@ -216,7 +216,9 @@ def scenario_dam32(S):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('SUIRI_REFERENCE')
+    if not ref:
+        sys.exit('usage: make_golden.py REF (the reference checkout; or set SUIRI_REFERENCE)')
     for name, fn in (('dam16', scenario_dam), ('obstacles', scenario_obstacles), ('drops', scenario_drops),
                      ('frame', scenario_frame), ('ripple', scenario_ripple), ('dam32', scenario_dam32)):
         S = load_solver(ref)

@@ -72,6 +72,20 @@ def sync_oracle_particles(gpu, ora):
     ora.pos, ora.vel, ora.air, ora.pid = gp[o].astype(np.float64), gv[o].astype(np.float64), ga[o].astype(np.float64), gi[o].astype(np.int64)
 
 
+def gpu_max_divergence(pkg, gpu):
+    """Post-projection max |div| over the GPU's liquid cells, from its own face velocities and fractions, as
+    the oracle's max_divergence forms it (static solids: the solid velocity is zero)."""
+    N = pkg.native
+    nx, ny, nz, h = gpu.nx, gpu.ny, gpu.nz, gpu.h
+    vel = gpu.grid(N.FIELD_VEL).astype(np.float64)
+    frac = gpu.grid(N.FIELD_FRAC).astype(np.float64)
+    cnt = gpu.grid(N.FIELD_CELL_COUNT)
+    F = [frac[a] * vel[a] for a in range(3)]
+    div = (F[0][1:nx + 1, :ny, :nz] - F[0][:nx, :ny, :nz] + F[1][:nx, 1:ny + 1, :nz] - F[1][:nx, :ny, :nz]
+           + F[2][:nx, :ny, 1:nz + 1] - F[2][:nx, :ny, :nz]) / h
+    return float(np.abs(div[cnt > 0]).max()) if (cnt > 0).any() else 0.0
+
+
 def obstacle_items():
     """Scene items (JSON form) with the oracle objects made from them."""
     items = [dict(kind='obstacle', shape='sphere', pos=[0.15, 0.18, 0.0], rot=[0, 0, 0], dims=dict(r=0.09)),

@@ -88,14 +88,16 @@ def test_rk2_advection_matches_oracle(pkg):
     eul.close()
 
 
-@pytest.mark.parametrize('sor_mode', [0, 2, 3])
+@pytest.mark.parametrize('sor_mode', [0, 2, 3, 4])
 def test_sor_bit_exact_with_reference_operation_order(pkg, sor_mode):
     """Given the GPU's own float32 operands, the reference's float32 SOR loop reproduces its pressure bit for
-    bit, for one launch per sweep and for temporal blocking; the FP64 residual of the solve is stated."""
+    bit, for one launch per sweep, temporal blocking and the cluster-resident solve. The device's FP64
+    residual of the solve equals the host's FP64 residual of the same operands, and is stated."""
     d = load('dam16')
     nx, ny, nz, h = int(d['nx']), int(d['ny']), int(d['nz']), float(d['h'])
     gpu = gpu_from(pkg, nx, ny, nz, h, flip=0.95, omega=1.7, iters=30)
     gpu.tune(4, sor_mode)
+    gpu.residual(True)
     gpu.add_particles(f32(d['pos0']), f32(d['vel0']))
     gpu.substep(1 / 240)
     g = grid_fields(pkg, gpu)
@@ -107,6 +109,13 @@ def test_sor_bit_exact_with_reference_operation_order(pkg, sor_mode):
     r30 = of.residual_f64(C, rhs, fluid, p)
     r0 = of.residual_f64(C, rhs, fluid, np.zeros_like(p))
     assert r30 < r0
+    st = gpu.stats()
+    act = fluid & (sum(C) > 0)
+    assert st['active_cells'] == int(act.sum())
+    assert abs(st['residual_max'] - r30) <= 1e-12 * r30, (st['residual_max'], r30)
+    assert st['rhs_max'] == float(np.abs(rhs.astype(np.float64)[act]).max())
+    print(f"FP64 residual after 30 iterations: max {st['residual_max']:.3e} (rms {st['residual_rms']:.3e}), "
+          f"{st['residual_max'] / st['rhs_max']:.3e} of max |h²·div|; before the solve {r0:.3e}")
     gpu.close()
 
 
@@ -328,11 +337,13 @@ def test_batch_equals_solo_bit_for_bit(pkg, axes, seeds):
         t.close()
 
 
-def _run_form(pkg, w, mode, iters, steps=3):
+def _run_form(pkg, w, mode, iters, steps=3, piece_kb=0):
     t = pkg.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=0.95, omega=1.8, iters=iters, whitewater=True,
                  ripple=None, capacity=len(w['pos']) * 2)
     t.set_objects(w['objects'])
     t.add_particles(w['pos'])
+    if piece_kb:
+        t.tune_piece(piece_kb)
     t.tune(4, mode)
     for _ in range(steps):
         t.substep(1 / 240)
@@ -344,17 +355,28 @@ def _run_form(pkg, w, mode, iters, steps=3):
     return out
 
 
-@pytest.mark.parametrize('mode', [1, 2, 3])
+@pytest.mark.parametrize('mode', [1, 2, 3, 4])
 def test_solve_forms_equal_per_sweep_launches(pkg, mode):
-    """The cooperative whole-solve launch (1) and the temporal-blocked launches (2: two sweeps each, 3:
-    four) relax the same colours in the same order as one launch per sweep (0): identical pressures and
-    particles, bit for bit."""
+    """The cooperative whole-solve launch (1), the temporal-blocked launches (2: two sweeps each, 3:
+    four) and the cluster-resident solve (4) relax the same colours in the same order as one launch per
+    sweep (0): identical pressures and particles, bit for bit."""
     w = pkg.workloads.obstacles_inflow(scale=4)
     for a, b in zip(_run_form(pkg, w, 0, 40), _run_form(pkg, w, mode, 40)):
         np.testing.assert_array_equal(a, b)
 
 
-@pytest.mark.parametrize('mode', [2, 3])
+@pytest.mark.parametrize('piece_kb', [8, 16, 40])
+def test_cluster_solve_pieces_across_ctas(pkg, piece_kb):
+    """The cluster-resident solve with less shared memory per CTA, so the 32×16×16 tank is cut into
+    pieces of 1 z plane (16 CTAs, every z neighbour read from another CTA's shared memory), 3 planes (six
+    pieces, the last of one plane) and 8 planes (two): bit for bit the per-sweep launches."""
+    w = pkg.workloads.obstacles_inflow(scale=4)
+    assert (w['nx'], w['ny'], w['nz']) == (32, 16, 16)
+    for a, b in zip(_run_form(pkg, w, 0, 40), _run_form(pkg, w, 4, 40, piece_kb=piece_kb)):
+        np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize('mode', [2, 3, 4])
 @pytest.mark.parametrize('iters', [6, 7, 1, 3])
 def test_temporal_blocking_edges(pkg, iters, mode):
     """Temporal blocking on a grid that is no multiple of the tile (odd x). Four sweeps a launch: an odd
@@ -365,10 +387,12 @@ def test_temporal_blocking_edges(pkg, iters, mode):
         np.testing.assert_array_equal(a, b)
 
 
-@pytest.mark.parametrize('mode', [2, 3])
+@pytest.mark.parametrize('mode', [2, 3, 4])
 def test_temporal_blocking_batch_uneven_iterations(pkg, mode):
-    """In a batch the tile launches run to the largest iteration count; tanks with fewer iterations stop
-    relaxing but keep being carried between the two pressure buffers: every tank equals its solo run."""
+    """In a batch the tile launches (and the cluster solve's sweeps) run to the largest iteration count;
+    tanks with fewer iterations stop relaxing but keep their pressures (carried between the two buffers by
+    the tile forms; held in shared memory by the cluster form, where small tanks share a cluster): every
+    tank equals its solo run."""
     specs = [(pkg.workloads.random_tank(s, axes=(16, 24, 40)), it) for s, it in ((11, 5), (12, 12), (13, 9))]
 
     def make(mode):
@@ -421,3 +445,148 @@ def test_snapshot_restore(pkg):
         np.testing.assert_array_equal(a, b)
     assert not t.restore_water(sid)      # one copy, restored once
     t.close()
+
+
+def _match_sets(a, b, tol):
+    """Pair the rows of a and b (N, k) one to one by nearest position (first 3 columns); the order of
+    whitewater particles follows atomics, so they are compared as sets."""
+    from scipy.spatial import cKDTree
+    assert len(a) == len(b), f'{len(a)} against {len(b)}'
+    if not len(a):
+        return np.zeros(0, np.int64)
+    d, j = cKDTree(b[:, :3]).query(a[:, :3])
+    assert np.all(d <= tol), f'unpaired rows, worst distance {d.max():.3e}'
+    assert len(np.unique(j)) == len(j), 'two rows paired with one'
+    return j
+
+
+def test_whitewater_advance_two_frames(pkg):
+    """Spray, foam and bubbles seeded from the frame fixture's whitewater state (wpos0, wvel0, wlife0, wkind0,
+    arrays of the reference's own solver) advance over two frames with the liquid: the GPU's whitewater equals
+    the oracle's after each frame (spawns by the hash stream in both, landing spray into ripple impulses):
+    same count, positions and life within the particle tolerance, velocities within 1e-4, same kind."""
+    d = load('frame')
+    nx, ny, nz, h = int(d['nx']), int(d['ny']), int(d['nz']), float(d['h'])
+    R, W = int(d['ripple']), int(d['wmap'])
+    kw = dict(flip=float(d['flip']), omega=float(d['omega']), iters=int(d['iters']), whitewater=True)
+    gpu = gpu_from(pkg, nx, ny, nz, h, ripple=(R, R), wmap=W, ww_capacity=4000, sdf_mode='lattice', **kw)
+    ora = oracle_from(nx, ny, nz, h, d['origin'], ripple=(R, R), wmap=W, ww_cap=4000, rng_mode='hash', sdf_mode='lattice', **kw)
+    from oracle import sdf as sdfm
+    ora.set_objects([sdfm.make_obstacle('cylinder', [0.1, 0.15, -0.1], r=0.08, h=0.3),
+                     sdfm.make_obstacle('torus', [-0.2, 0.15, 0.15], R=0.1, r=0.03)])
+    gpu.set_objects([dict(kind='obstacle', shape='cylinder', pos=[0.1, 0.15, -0.1], rot=[0, 0, 0], dims=dict(r=0.08, h=0.3)),
+                     dict(kind='obstacle', shape='torus', pos=[-0.2, 0.15, 0.15], rot=[0, 0, 0], dims=dict(R=0.1, r=0.03))])
+    gpu.set_lattice(d['lattice'])
+    pos, vel, air = f32(d['pos0']), f32(d['vel0']), d['air0']
+    gpu.add_particles(pos, vel, air)
+    ora.add_particles(pos, vel, air)
+    wp, wv, wl, wk = f32(d['wpos0']), f32(d['wvel0']), f32(d['wlife0']), d['wkind0'].astype(np.float64)
+    gpu.add_whitewater(wp, wv, wl, wk)
+    ora.wpos, ora.wvel, ora.wlife, ora.wkind = wp.copy(), wv.copy(), wl.copy(), wk.copy()
+    P0, V0 = gpu.whitewater()
+    np.testing.assert_array_equal(P0[:, :3], wp.astype(np.float32))
+    layer = orp.RippleLayer(R, R, nx * h, nz * h)
+    for f in (1, 2):
+        n_gpu = gpu.step(float(d['frame_dt']))
+        n_ora = ora.step(float(d['frame_dt']), layer)
+        assert n_gpu == n_ora
+        assert_particles(gpu, ora, f'frame {f}')
+        P, V = gpu.whitewater()
+        assert len(P) == len(ora.wpos) > 0, (len(P), len(ora.wpos))
+        ref = np.concatenate([ora.wpos, ora.wlife[:, None]], 1)
+        j = _match_sets(P.astype(np.float64), ref, 1e-5)
+        err = np.abs(P[:, :3] - ora.wpos[j])
+        assert np.all(err <= 1e-6 + 1e-6 * np.abs(ora.wpos[j])), f'frame {f}: whitewater position err {err.max():.3e}'
+        np.testing.assert_allclose(P[:, 3], ora.wlife[j], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(V[:, :3], ora.wvel[j], rtol=1e-4, atol=1e-5)
+        np.testing.assert_array_equal(V[:, 3], ora.wkind[j])
+        src = gpu.ripple_field(pkg.native.FIELD_RIPPLE_STATE, (2 * R, 2 * R, 2), np.float32)
+        assert_close_field(src[..., 0], layer.S.real, rtol=1e-4, what=f'frame {f}: ripple state')
+        sync_oracle_particles(gpu, ora)       # the next frame starts from the GPU's float32 liquid
+    gpu.close()
+
+
+def test_rectangular_ripple_layer_full_scene_quarter(pkg):
+    """The full scene's shape at a quarter of each axis: 64×32×32 cells, bottom 8 layers of liquid, a
+    rectangular ripple layer of 256×128 cells (mirrored FFT 512×256: an odd power-of-two exponent on x, so
+    the radix-4 passes end with one radix-2 pass on that axis only), σ = 0.072 N/m, ρ = 1000 kg/m³ at the
+    stated depth 0.1 m, and rain: sub-grid drops of lognormal diameter (median 2 mm, σ_log 0.4) added on
+    the host at 4 m/s. Over two frames: particles, impacts, top height, ripple mask, spectral state and
+    field against the oracle."""
+    w = pkg.workloads.full_scene(scale=4)
+    nx, ny, nz, h = w['nx'], w['ny'], w['nz'], w['h']
+    Rx, Rz = w['ripple']
+    assert (nx, ny, nz, Rx, Rz) == (64, 32, 32, 256, 128)
+    prm = w['params']
+    kw = dict(flip=prm['flip'], omega=prm['omega'], iters=40, whitewater=True)
+    gpu = pkg.Tank(nx=nx, ny=ny, nz=nz, h=h, ripple=(Rx, Rz), wmap=128, capacity=len(w['pos']) + 20000,
+                   ww_capacity=20000, ripple_sigma=prm['sigma'], ripple_rho=prm['rho'], ripple_depth=prm['depth'],
+                   drop_d=prm['drop_d'], **kw)
+    ora = oracle_from(nx, ny, nz, h, w['origin'], ripple=(Rx, Rz), wmap=128, ww_cap=20000, rng_mode='hash', **kw)
+    ora.drop_d = prm['drop_d']
+    layer = orp.RippleLayer(Rx, Rz, nx * h, nz * h, sigma_rho=prm['sigma'] / prm['rho'], rho=prm['rho'])
+    gpu.add_particles(w['pos'])
+    ora.add_particles(f32(w['pos']))
+    rng = np.random.default_rng(11)
+    W_, D_ = nx * h, nz * h
+    impacts = 0
+    for f in (1, 2):
+        n = 60                                 # a burst of rain per frame, so that drops land in both frames
+        drops = np.stack([rng.uniform(-0.45 * W_, 0.45 * W_, n), rng.uniform(0.3, 0.45, n) * ny * h,
+                          rng.uniform(-0.45 * D_, 0.45 * D_, n)], 1)
+        dv = np.zeros((n, 3)); dv[:, 1] = -4.0
+        gpu.add_particles(f32(drops), f32(dv), np.ones(n))
+        ora.add_particles(f32(drops), f32(dv), np.ones(n))
+        for _ in range(6):                    # the drops fall to the pool, then one frame is compared
+            n_gpu = gpu.step(1 / 60)
+            n_ora = ora.step(1 / 60, layer, ripple_depth=prm['depth'])
+            assert n_gpu == n_ora
+            assert_particles(gpu, ora, f'burst {f}')
+            sync_oracle_particles(gpu, ora)
+        st = gpu.stats()
+        assert st['impacts'] == ora.impacts
+        assert ora.impacts > impacts, 'no drop merged in this burst'
+        impacts = ora.impacts
+        top = gpu.ripple_field(pkg.native.FIELD_TOP, (128, 128), np.float32)
+        assert_close_field(top, ora.top, what=f'burst {f}: top height')
+        S = gpu.ripple_field(pkg.native.FIELD_RIPPLE_STATE, (2 * Rz, 2 * Rx, 2), np.float32)
+        assert np.abs(layer.S).max() > 0
+        assert_close_field(S[..., 0], layer.S.real, rtol=1e-4, what=f'burst {f}: ripple state (height)')
+        assert_close_field(S[..., 1], layer.S.imag, rtol=1e-4, what=f'burst {f}: ripple state (velocity)')
+        fld = gpu.ripple_field(pkg.native.FIELD_RIPPLE, (Rz + 1, Rx + 1, 3), np.float32)
+        for c in range(3):
+            assert_close_field(fld[..., c], layer.field[..., c], rtol=1e-4, atol=1e-12, what=f'burst {f}: field {c}')
+    gpu.close()
+
+
+def test_full_size_obstacles_inflow_substeps(pkg):
+    """Two sub-steps of the obstacles-and-inflow workload at its full size: 128×64×64 cells at h = 1/64 m,
+    1.70M particles, the sphere, the turned box and the cylinder (analytic shapes), the floor drain, and the
+    faucet's particles of each sub-step generated on the host and added to both; 100 SOR iterations at
+    ω = 1.8. Cell counts and valid-face masks bit-exact; P2G velocity, pressure, projected velocity and
+    particles within the parity tolerances; the post-projection divergence equal to the oracle's."""
+    import bench
+    from parity import gpu_max_divergence, objs_from_items
+    w = pkg.workloads.obstacles_inflow()
+    prm = w['params']
+    nx, ny, nz, h = w['nx'], w['ny'], w['nz'], w['h']
+    kw = dict(flip=prm['flip'], omega=prm['omega'], iters=prm['iters'], whitewater=True)
+    gpu = gpu_from(pkg, nx, ny, nz, h, capacity=int(len(w['pos']) * 1.1), **kw)
+    gpu.set_objects(w['objects'])
+    ora = oracle_from(nx, ny, nz, h, w['origin'], **kw)
+    ora.set_objects(objs_from_items(w['objects']))
+    gpu.add_particles(w['pos'])
+    ora.add_particles(f32(w['pos']))
+    rng = np.random.default_rng(5)
+    for s in (1, 2):
+        p, v = bench.faucet_particles(w['emitters'][0], prm['dt'], rng)
+        gpu.add_particles(p, v)
+        ora.add_particles(f32(p), f32(v))
+        gpu.substep(prm['dt'])
+        ora.frame = s
+        ora.substep(prm['dt'])
+        compare_substep(pkg, gpu, ora, f'full-size sub-step {s}')
+        dg, do = gpu_max_divergence(pkg, gpu), ora.max_divergence()
+        assert abs(dg - do) <= 1e-3 * do, (dg, do)
+        sync_oracle_particles(gpu, ora)
+    gpu.close()

@@ -6,7 +6,8 @@ import numpy as np
 import pytest
 
 from oracle import flip as of
-from parity import assert_close_field, assert_particles, f32, objs_from_items, oracle_from, sync_oracle_particles
+from parity import (assert_close_field, assert_particles, f32, gpu_max_divergence, objs_from_items, oracle_from,
+                    sync_oracle_particles)
 
 pytestmark = pytest.mark.gpu
 
@@ -106,6 +107,39 @@ def test_serving_budget_admission(pkg):
     srv.close()
 
 
+def test_bounded_wait_gives_up_reports_and_serving_fails_the_request(pkg):
+    """The cooperative solve (sor_mode 1) with a poll limit of 0: the grid barrier's waits give up at once.
+    The sub-step returns, the tank's stats carry error bit 1, and with the per-sweep form the next sub-steps
+    run cleanly. In the server a request whose solve gave up is reported failed with the reason, and the
+    next request completes."""
+    from importlib import import_module
+    serve = import_module('hahenn-_b200.serve')
+    w = pkg.workloads.dam_break(16)
+    t = pkg.Tank(nx=16, ny=16, nz=16, h=w['h'], iters=20, whitewater=False, ripple=None, capacity=len(w['pos']) * 2,
+                 sor_mode=1, watchdog_polls=0)
+    t.add_particles(w['pos'])
+    t.substep(1 / 240)
+    assert t.stats()['errors'] & 1
+    t.tune(4, 0)
+    for _ in range(2):
+        t.substep(1 / 240)
+    st = t.stats()
+    assert st['count'] == len(w['pos']) and np.isfinite(t.grid(pkg.native.FIELD_PRES)).all()
+    t.close()
+    sc, prm, em, _ = serve.scene_request(6, axes=(16, 24))
+    srv = serve.Server(budget_bytes=4e9)
+    bad = srv.submit(sc, dict(prm, sor_mode=1, watchdog_polls=0), em, steps=3)
+    with pytest.raises(pkg.native.SuiriError, match='grid-barrier wait'):
+        srv.wait(bad)
+    assert srv.poll(bad)['state'] == 'failed'
+    good = srv.submit(sc, prm, em, steps=3)
+    srv.wait(good)
+    assert srv.poll(good)['state'] == 'done'
+    st = srv.stats()
+    assert st['failed'] == 1 and st['completed'] == 1
+    srv.close()
+
+
 def test_dam_break_long_run(pkg):
     """The 32³ dam break: 200 sub-steps. Step-wise parity with the oracle for the first 10 sub-steps (oracle
     continued from the GPU state after each), then the free-running run compared on volume, kinetic energy
@@ -122,6 +156,9 @@ def test_dam_break_long_run(pkg):
         ora.frame = s
         ora.substep(prm['dt'])
         assert_particles(gpu, ora, f'dam break sub-step {s}')
+        # same state: the post-projection divergence equals the oracle's (velocities agree to 1e-5 relative)
+        dg, do = gpu_max_divergence(pkg, gpu), ora.max_divergence()
+        assert abs(dg - do) <= 1e-3 * do, (s, dg, do)
         sync_oracle_particles(gpu, ora)
     free = oracle_from(32, 32, 32, w['h'], w['origin'], flip=prm['flip'], omega=prm['omega'], iters=prm['iters'])
     free.pos, free.vel, free.air, free.pid = ora.pos.copy(), ora.vel.copy(), ora.air.copy(), ora.pid.copy()
@@ -139,17 +176,10 @@ def test_dam_break_long_run(pkg):
     assert st['count'] == len(w['pos']) == len(free.pos)           # closed tank: volume conserved exactly
     ke_g, ke_o = np.array(ke_g), np.array(ke_o)
     assert np.all(np.abs(ke_g - ke_o) <= 0.1 * ke_o + 1e-6), (ke_g, ke_o)
-    # post-projection divergence of the GPU's own face velocities over liquid cells
-    N = pkg.native
-    vel = gpu.grid(N.FIELD_VEL).astype(np.float64)
-    frac = gpu.grid(N.FIELD_FRAC).astype(np.float64)
-    cnt = gpu.grid(N.FIELD_CELL_COUNT)
-    h = w['h']
-    F = [frac[a] * vel[a] for a in range(3)]
-    div = (F[0][1:, :32, :32] - F[0][:32, :32, :32] + F[1][:32, 1:, :32] - F[1][:32, :32, :32]
-           + F[2][:32, :32, 1:] - F[2][:32, :32, :32]) / h
-    dmax = float(np.abs(div[cnt > 0]).max())
-    assert dmax < 0.5 * free.max_divergence() + 50.0     # same order as the CPU solver's own
+    # after 190 free-running sub-steps the two flows have drifted apart (chaotic), so their post-projection
+    # divergences are compared as figures of the same solve: within a factor of 2 of each other
+    dg, do = gpu_max_divergence(pkg, gpu), free.max_divergence()
+    assert 0.5 * do <= dg <= 2.0 * do, (dg, do)
     gpu.close()
 
 

@@ -10,31 +10,48 @@ workloads = importlib.import_module('hahenn-_b200.workloads')
 
 
 class FakeTarget:
-    """Times each (blocks per SM, sor_mode) from a table; a None entry cannot be launched."""
+    """Times each (blocks per SM, sor_mode, piece_kb) from a table; a None entry cannot be launched. Its
+    "state" is a counter of the sub-steps run, saved and restored like the tanks' water copies."""
 
     def __init__(self, table):
         self.table, self.current, self.applied = table, None, []
+        self.piece, self.substeps, self.saves = 0, 0, []
 
     def tune(self, bps, mode):
-        self.current = (bps, mode)
+        self.current = (bps, mode, self.piece)
         self.applied.append(self.current)
 
+    def tune_piece(self, kb):
+        self.piece = kb
+
     def time_substeps(self, dt, steps):
+        self.substeps += steps
         ms = self.table[self.current]
         if ms is None:
             raise RuntimeError(f'{self.current} cannot be launched')
         return ms * steps
 
+    def save_state(self):
+        self.saves.append(self.substeps)
+        return len(self.saves) - 1
+
+    def restore_state(self, k):
+        self.substeps = self.saves[k]
+
 
 def test_autotune_keeps_the_fastest_and_skips_shapes_that_fail():
     table = {c: 5.0 for c in autotune.CANDIDATES}
-    table[(8, 0)] = 3.0
-    table[(4, 1)] = None
+    table[(2, 4, 112)] = 3.0
+    table[(4, 1, 0)] = None
     t = FakeTarget(table)
+    t.substeps = 7
     best, timings = autotune.autotune(t, 1 / 240)
-    assert best == (8, 0) and t.current == (8, 0)
-    assert timings[(4, 1)] == float('inf') and timings[(8, 0)] == pytest.approx(3.0)
+    assert best == (2, 4, 112) and t.current == (2, 4, 112)
+    assert timings[(4, 1, 0)] == float('inf') and timings[(2, 4, 112)] == pytest.approx(3.0)
     assert set(timings) == set(autotune.CANDIDATES)
+    assert t.substeps == 7              # the tuning sub-steps were rolled back
+    assert {c[1] for c in autotune.CANDIDATES} >= {0, 1, 2, 3, 4}
+    assert len({c[2] for c in autotune.CANDIDATES if c[1] == 4}) >= 3     # tile sizes of the cluster solve
 
 
 def test_autotune_raises_when_nothing_launches():
