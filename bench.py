@@ -403,35 +403,37 @@ def init_ranks(world, local):
 
 
 # ------------------------------------------------------------------ the batching workload (default)
-def e2e_batch(P, specs, device, best, steps):
+def e2e_batch(P, specs, device, best, steps, workers=8):
     """The job end to end through the public API with host buffers: every scene's particles added from host
     arrays (staged through pinned memory into the device), `steps` batched sub-steps with each scene's stats
-    read back every sub-step (pollStats), and every scene's particles read back into host arrays at the end.
+    read back every sub-step (pollStats), and every scene's particles read back into host arrays (the ABI's
+    pos4/vel4 layout) at the end. The scenes are uploaded and read back from `workers` host threads, one
+    scene per thread at a time (handles are per thread; the ctypes calls release the interpreter lock).
     Wall clock around all of it, after an untimed run of the same job (graph capture, staging buffers)."""
+    from concurrent.futures import ThreadPoolExecutor
     tanks = make_batch_tanks(P, specs, device, add=False)
     b = P.Batch(tanks)
+    b.tune_piece(best[2])
     b.tune(best[0], best[1])
-    if len(best) > 2 and best[2]:
-        b.tune_piece(best[2])
+    b.tune_g2p(best[3])
     host = [np.ascontiguousarray(w['pos'], np.float32) for w in specs]
+    outs = [(np.empty((len(p) + 64, 4), np.float32), np.empty((len(p) + 64, 4), np.float32)) for p in host]
     readback = int(P.native.lib().suiri_stats_readback_bytes())
+    pool = ThreadPoolExecutor(max_workers=workers)
 
     def job(n_steps):
-        h2d = d2h = 0
-        for t, pos in zip(tanks, host):
-            t.add_particles(pos)
-            h2d += 32 * len(pos)                      # staged as two float4 per particle
+        list(pool.map(lambda tp: tp[0].add_particles(tp[1]), zip(tanks, host)))
+        h2d = sum(32 * len(p) for p in host)          # staged as two float4 per particle
+        d2h = 0
         for _ in range(n_steps):
             b.substep(DT)
             for t in tanks:
                 t.poll_stats()
                 d2h += readback
-        n_end = 0
-        for t in tanks:
-            pos, vel, air, ids = t.particles()
-            n_end += len(ids)
-            d2h += 32 * len(ids)
-        return h2d, d2h, n_end
+        b.sync()
+        res = list(pool.map(lambda to: to[0].particles4(to[1]), zip(tanks, outs)))
+        n_end = sum(len(r[0]) for r in res)
+        return h2d, d2h + 32 * n_end, n_end
 
     job(3)
     for t in tanks:
@@ -440,12 +442,13 @@ def e2e_batch(P, specs, device, best, steps):
     t0 = time.perf_counter()
     h2d, d2h, n_end = job(steps)
     el = time.perf_counter() - t0
+    pool.shutdown()
     n0 = sum(len(p) for p in host)
     b.close()
     for t in tanks:
         t.close()
     return dict(value=0.5 * (n0 + n_end) * steps / el, unit=METRIC, h2d_bytes_per_step=h2d // steps,
-                d2h_bytes_per_step=d2h // steps, wall_s=el,
+                d2h_bytes_per_step=d2h // steps, wall_s=el, host_threads=workers,
                 job=f'{len(specs)} scenes uploaded from host arrays, {steps} batched sub-steps with every scene\'s '
                     f'stats read back each sub-step, every scene\'s particles read back at the end')
 
@@ -552,7 +555,7 @@ def run_batch(args, rank, world, local):
                     ms_per_step=ms, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
                     data='synthetic (seeded particles, analytic obstacles)', config=cfg,
                     l2='flushed (256 MiB write) between timed steps', parallelism=f'replicas{world}',
-                    tuned=dict(blocks_per_sm=best[0], sor_mode=best[1], piece_kb=best[2] if len(best) > 2 else 0),
+                    tuned=dict(blocks_per_sm=best[0], sor_mode=best[1], piece_kb=best[2], g2p_form=best[3]),
                     tuning_ms={'x'.join(str(v) for v in k): v for k, v in timings.items()},
                     plain_sequential=dict(value=particles / world * 1000.0 / ms_plain, ms_per_step=ms_plain,
                                           note='the same scenes one by one, device time summed'),
@@ -575,6 +578,8 @@ def run_plain(args, rank, world, local):
     prm = w['params']
     dt = prm['dt']
     tank = make_tank(P, w, local)
+    autotune = importlib.import_module('hahenn-_b200.autotune').autotune
+    best, timings = autotune(tank, dt)
     tank.profile(True)
     stream = torch.cuda.ExternalStream(tank.stream())
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f'cuda:{local}')
@@ -611,6 +616,9 @@ def run_plain(args, rank, world, local):
 
     # end-to-end through the C ABI: host inflow particles (pinned) up, stats back, every step
     t2 = make_tank(P, w, local, host_inflow=True)
+    t2.tune_piece(best[2])
+    t2.tune(best[0], best[1])
+    t2.tune_g2p(best[3])
     rng = np.random.default_rng(7)
     for _ in range(3):
         for e in w['emitters']:
@@ -655,9 +663,9 @@ def run_plain(args, rank, world, local):
                                   traffic=None if tr is None else tr.get('dram_bytes_per_launch'),
                                   alg_bytes_per_launch=alg, launch_ms=sor_launch_ms, active_cells=active,
                                   unit_bytes='20 B per active cell per colour sweep'),
-                    phases_ms=ph,
+                    phases_ms=ph, tuned=dict(blocks_per_sm=best[0], sor_mode=best[1], piece_kb=best[2], g2p_form=best[3]),
                     cpu_baseline=dict(value=cpu_rate, unit=METRIC, cores=1, kind='port', sample=cpu_what),
-                    e2e=e2e, gpu_launches=launches_per_substep(0, prm['iters']) * args.steps, clocks=clk)
+                    e2e=e2e, gpu_launches=launches_per_substep(best[1], prm['iters']) * args.steps, clocks=clk)
         print(json.dumps(line), flush=True)
     tank.close()
     if world > 1:
@@ -730,6 +738,7 @@ def run_for_profiler(args, local):
         tanks = make_batch_tanks(P, specs, local)
         b = P.Batch(tanks)
         b.tune(args.bps, args.sor_mode)
+        b.tune_g2p(args.g2p_form)
         for _ in range(3 + args.ncu_steps):
             b.substep(DT)
         b.sync()
@@ -740,7 +749,8 @@ def run_for_profiler(args, local):
         return
     w = P.workloads.obstacles_inflow()
     t = make_tank(P, w, local)
-    t.tune(args.bps, args.sor_mode)
+    t.tune(args.bps, args.sor_mode if args.sor_mode != 4 else 0)
+    t.tune_g2p(args.g2p_form)
     for _ in range(3 + args.ncu_steps):
         t.substep(w['params']['dt'])
     t.sync()
@@ -763,6 +773,7 @@ def main():
     ap.add_argument('--ncu-steps', type=int, default=0,
                     help='profiler run: 3 warm-up and N more sub-steps of the workload, no timing, no JSON line')
     ap.add_argument('--bps', type=int, default=2, help='profiler run: particle blocks per SM')
+    ap.add_argument('--g2p-form', type=int, default=0, help='profiler run: form of the grid-to-particle pass')
     ap.add_argument('--sor-mode', type=int, default=4, help='profiler run: form of the pressure solve')
     args = ap.parse_args()
     rank, world = int(os.environ.get('RANK', 0)), int(os.environ.get('WORLD_SIZE', 1))

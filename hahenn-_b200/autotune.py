@@ -8,7 +8,9 @@ Knobs (``suiri_tune`` / ``suiri_batch_tune``, ``suiri_tune_piece`` / ``suiri_bat
     halos (temporal blocking), 4 the whole solve in one launch with each tank held in one thread-block
     cluster's shared memory;
   * the tile of sor_mode 4: the shared memory one CTA takes (piece_kb; 0 = the device's maximum), which
-    sets the z planes per CTA and so the CTAs per tank and the cluster size.
+    sets the z planes per CTA and so the CTAs per tank and the cluster size;
+  * the form of the grid-to-particle pass (``suiri_tune_g2p``): a grid-stride walk, or one block per brick
+    with the brick's faces staged in shared memory; tried with the best of the other knobs.
 
 Each candidate is timed on the device (events on the tank's or batch's stream) over a few sub-steps of the
 real state, after one sub-step that captures its graph. Targets that can save and restore their state
@@ -20,29 +22,54 @@ CANDIDATES = ((2, 0, 0), (4, 0, 0), (8, 0, 0), (4, 2, 0), (4, 3, 0), (4, 1, 0),
               (2, 4, 0), (2, 4, 160), (2, 4, 112), (2, 4, 80), (4, 4, 0))
 
 
-def autotune(target, dt, candidates=CANDIDATES, steps=3):
-    """Return ((blocks_per_sm, sor_mode, piece_kb), {candidate: ms per sub-step}) and leave the best set."""
+G2P_FORMS = (0, 1)
+
+
+def _time(target, dt, steps):
+    target.time_substeps(dt, 1)                  # captures the graph of the new shape
+    return target.time_substeps(dt, steps) / steps
+
+
+def autotune(target, dt, candidates=CANDIDATES, steps=3, g2p_forms=G2P_FORMS):
+    """Return ((blocks_per_sm, sor_mode, piece_kb, g2p_form), {candidate: ms per sub-step}) and leave the best
+    set. The candidates (blocks per SM, solve form, tile) are timed with the first G2P form; the other G2P
+    forms are then timed with the best of them."""
     timings = {}
     last = None
     saved = target.save_state() if hasattr(target, 'save_state') else None
+    has_g2p = hasattr(target, 'tune_g2p')
     try:
+        if has_g2p:
+            target.tune_g2p(g2p_forms[0])
         for cand in candidates:
-            bps, mode = cand[0], cand[1]
-            piece = cand[2] if len(cand) > 2 else 0
+            key = (cand[0], cand[1], cand[2] if len(cand) > 2 else 0, g2p_forms[0])
             try:
-                target.tune_piece(piece)
-                target.tune(bps, mode)
-                target.time_substeps(dt, 1)
-                timings[cand] = target.time_substeps(dt, steps) / steps
+                target.tune_piece(key[2])
+                target.tune(key[0], key[1])
+                timings[key] = _time(target, dt, steps)
             except Exception as e:      # a shape the device cannot launch (too large to be co-resident, …)
-                timings[cand] = float('inf')
+                timings[key] = float('inf')
                 last = e
+        best = min(timings, key=timings.get)
+        if timings[best] == float('inf'):
+            raise last
+        if has_g2p:
+            target.tune_piece(best[2])
+            target.tune(best[0], best[1])
+            for form in g2p_forms[1:]:
+                key = best[:3] + (form,)
+                try:
+                    target.tune_g2p(form)
+                    timings[key] = _time(target, dt, steps)
+                except Exception as e:
+                    timings[key] = float('inf')
+                    last = e
+            best = min((k for k in timings if k[:3] == best[:3]), key=timings.get)
     finally:
         if saved is not None:
             target.restore_state(saved)
-    best = min(timings, key=timings.get)
-    if timings[best] == float('inf'):
-        raise last
-    target.tune_piece(best[2] if len(best) > 2 else 0)
+    target.tune_piece(best[2])
     target.tune(best[0], best[1])
+    if has_g2p:
+        target.tune_g2p(best[3])
     return best, timings

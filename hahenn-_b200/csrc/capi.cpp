@@ -561,6 +561,25 @@ static void tune_piece(Group& g, int32_t piece_kb) {
   }
 }
 
+static void tune_g2p(Group& g, int32_t form) {
+  if (form != 0 && form != 1) throw Error(SUIRI_ERR_INVALID, "g2p form is 0 or 1");
+  if (form == g.g2p_form) return;
+  CK(cudaStreamSynchronize(g.stream));
+  g.g2p_form = form;
+  g.drop_graph();
+}
+
+int suiri_tune_g2p(suiri_tank* h, int32_t form) {
+  return guard(h ? &h->err : nullptr, [&] { tune_g2p(*T(h)->solo, form); });
+}
+
+int suiri_batch_tune_g2p(suiri_batch* b, int32_t form) {
+  return guard(b ? &b->err : nullptr, [&] {
+    if (!b || !b->b) throw Error(SUIRI_ERR_INVALID, "null batch");
+    for (auto& g : b->b->lanes) tune_g2p(*g, form);
+  });
+}
+
 static void set_residual(Group& g, bool on) {
   if (on == g.residual) return;
   CK(cudaStreamSynchronize(g.stream));

@@ -338,6 +338,7 @@ Tank::~Tank() {
     if (stage_ev[k]) cudaEventDestroy(stage_ev[k]);
   }
   if (h_poll) cudaFreeHost(h_poll);
+  if (h_read_p) { cudaFreeHost(h_read_p); cudaFreeHost(h_read_v); }
   if (poll_ev) cudaEventDestroy(poll_ev);
   if (ev_own) cudaEventDestroy(ev_own);
   if (stream && own_stream) cudaStreamDestroy(stream);
@@ -732,17 +733,28 @@ int Tank::step(double frame_dt) {
   return n;
 }
 
+// Particles of A then E (the previous sub-step's output and the pending emissions), dead ones skipped. The
+// device copies land in pinned buffers kept by the tank (one copy each of what is needed: positions only for a
+// count), then one pass converts them into the caller's arrays.
 long long Tank::read_particles(float* pos4, float* vel4, long long cap) {
   read_counters();
   const long long nl = h_ctr->n_live, ne = h_ctr->n_emit, tot = nl + ne;
-  std::vector<float4> P(tot), V(tot);
+  if ((size_t)tot > read_cap) {
+    if (h_read_p) { cudaFreeHost(h_read_p); cudaFreeHost(h_read_v); h_read_p = h_read_v = nullptr; read_cap = 0; }
+    CK(cudaMallocHost(&h_read_p, std::max<size_t>(tot, 1) * 16));
+    CK(cudaMallocHost(&h_read_v, std::max<size_t>(tot, 1) * 16));
+    read_cap = std::max<size_t>(tot, 1);
+  }
+  float4* P = h_read_p;
+  float4* V = h_read_v;
+  const bool want_v = vel4 != nullptr && cap > 0;
   if (nl) {
-    CK(cudaMemcpyAsync(P.data(), d.pA, nl * 16, cudaMemcpyDeviceToHost, stream));
-    CK(cudaMemcpyAsync(V.data(), d.vA, nl * 16, cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(P, d.pA, nl * 16, cudaMemcpyDeviceToHost, stream));
+    if (want_v) CK(cudaMemcpyAsync(V, d.vA, nl * 16, cudaMemcpyDeviceToHost, stream));
   }
   if (ne) {
-    CK(cudaMemcpyAsync(P.data() + nl, d.pE, ne * 16, cudaMemcpyDeviceToHost, stream));
-    CK(cudaMemcpyAsync(V.data() + nl, d.vE, ne * 16, cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(P + nl, d.pE, ne * 16, cudaMemcpyDeviceToHost, stream));
+    if (want_v) CK(cudaMemcpyAsync(V + nl, d.vE, ne * 16, cudaMemcpyDeviceToHost, stream));
   }
   CK(cudaStreamSynchronize(stream));
   long long k = 0;
@@ -750,8 +762,11 @@ long long Tank::read_particles(float* pos4, float* vel4, long long cap) {
     const int fl = (int)P[i].w;
     if (fl & kFlagDead) continue;
     if (k < cap) {
-      if (pos4) { pos4[4 * k] = P[i].x; pos4[4 * k + 1] = P[i].y; pos4[4 * k + 2] = P[i].z; pos4[4 * k + 3] = (fl & kFlagAir) ? 1.f : 0.f; }
-      if (vel4) { vel4[4 * k] = V[i].x; vel4[4 * k + 1] = V[i].y; vel4[4 * k + 2] = V[i].z; vel4[4 * k + 3] = V[i].w; }
+      if (pos4) {
+        float* o = pos4 + 4 * k;
+        o[0] = P[i].x; o[1] = P[i].y; o[2] = P[i].z; o[3] = (fl & kFlagAir) ? 1.f : 0.f;
+      }
+      if (want_v) memcpy(vel4 + 4 * k, &V[i], 16);
     }
     ++k;
   }
@@ -898,6 +913,7 @@ int blocks_for(int fam, const TankDev& D) {
     case kFamScan: return (D.ncells + 1 + kScanTile - 1) / kScanTile;
     case kFamSor: return (D.nhalf + kSorThreads - 1) / kSorThreads;     // one active cell per thread at most
     case kFamTiles: return ((D.nx + kTbX - 1) / kTbX) * ((D.ny + kTbY - 1) / kTbY) * ((D.nz + kTbZ - 1) / kTbZ);
+    case kFamG2P: return blocks_for(kFamBricks, D) + 1;       // the bricks and the particles outside the grid
   }
   return 0;
 }
@@ -1209,7 +1225,7 @@ void Group::enqueue_body() {
   }
   launch_project(ctx);
   mark(5);
-  launch_g2p(ctx);
+  launch_g2p(ctx, g2p_form);
   mark(6);
 }
 

@@ -93,6 +93,8 @@ struct Tank {
   cudaEvent_t stage_ev[2] = {};   // the copies out of each staging buffer have finished
   int stage_k = 0;
   Counters* h_poll = nullptr;     // pinned target of the asynchronous counter read
+  float4 *h_read_p = nullptr, *h_read_v = nullptr;   // pinned landing buffers of particle read-back
+  size_t read_cap = 0;
   cudaEvent_t poll_ev = nullptr;
   bool poll_pending = false;
   std::string err;
@@ -170,6 +172,7 @@ struct Group {
   int cl_piece_kb = 0;            // shared memory per CTA at most (tile knob; 0: the device maximum)
   void plan_cluster();            // throws if a tank cannot be held by one cluster
   bool residual = false;          // FP64 residual of every solve into the tank counters
+  int g2p_form = 0;               // 0 grid-stride walk, 1 per-brick with the faces in shared memory (tuner knob)
   bool profile = false;           // record events between the phases of the sub-step (inside the graph too)
   static constexpr int kPhases = 6;   // binning+sort, P2G, node+cell passes, pressure solve, projection, G2P
   cudaEvent_t ev_ph[kPhases + 1] = {};

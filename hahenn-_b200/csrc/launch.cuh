@@ -13,7 +13,7 @@ constexpr int kTbThreads = 512;
 
 // block families: blocks of one launch are laid out tank after tank; pfx[t] = first block of tank t
 constexpr int kSorThreads = 256;        // block size of a per-sweep SOR launch (128, 512, 1024 measured slower)
-enum Family { kFamNodes = 0, kFamCells, kFamHalf, kFamBricks, kFamScan, kFamTiles, kFamSor, kFamCount };
+enum Family { kFamNodes = 0, kFamCells, kFamHalf, kFamBricks, kFamScan, kFamTiles, kFamSor, kFamG2P, kFamCount };
 
 struct LaunchCtx {
   cudaStream_t stream;
@@ -89,7 +89,8 @@ void launch_sor_cluster(const LaunchCtx& L, const ClusterPiece* pieces, int nblo
 // FP64 residual of the solve just finished, max |r| and Σ r² over the active cells into the tank counters
 void launch_sor_residual(const LaunchCtx& L);
 void launch_project(const LaunchCtx& L);
-void launch_g2p(const LaunchCtx& L);
+// form 0: grid-stride walk over the sorted particles; 1: one block per brick with its faces in shared memory
+void launch_g2p(const LaunchCtx& L, int form);
 void launch_whitewater(const LaunchCtx& L, double frame_dt);
 
 }  // namespace suiri

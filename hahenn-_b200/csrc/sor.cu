@@ -46,6 +46,33 @@ __device__ __forceinline__ float sor_update(const float C[6], const float nb[6],
   return __fadd_rn(p, r);
 }
 
+// the same update with inv = 1/(C0+…+C5) given (computed in that order and correctly rounded by the caller)
+__device__ __forceinline__ float sor_update_inv(const float C[6], const float nb[6], float rhs, float p, float omega,
+                                                float inv) {
+  float num = __fmul_rn(C[0], nb[0]);
+#pragma unroll
+  for (int d = 1; d < 6; ++d) num = __fadd_rn(num, __fmul_rn(C[d], nb[d]));
+  float r = __fsub_rn(num, rhs);
+  r = __fmul_rn(r, inv);
+  r = __fsub_rn(r, p);
+  r = __fmul_rn(r, omega);
+  return __fadd_rn(p, r);
+}
+
+// 1/(C0+…+C5) as sor_update forms it: for a cell without cut faces the coefficients are 0 or 1, their float
+// sum is the number of open faces exactly, and its correctly rounded reciprocal comes from a table
+__device__ __forceinline__ float coeff_inv(bool cut, unsigned open6, const float C[6]) {
+  if (cut) {
+    float den = C[0];
+#pragma unroll
+    for (int d = 1; d < 6; ++d) den = __fadd_rn(den, C[d]);
+    return __frcp_rn(den);
+  }
+  const int n = __popc(open6 & 0x3Fu);
+  return n == 1 ? 1.f : n == 2 ? 0.5f : n == 3 ? 0x1.555556p-2f : n == 4 ? 0.25f : n == 5 ? 0x1.99999ap-3f
+       : n == 6 ? 0x1.555556p-3f : __frcp_rn(0.f);
+}
+
 // the six face coefficients of a cut cell: its own x, y, z face fractions and those of the +x, +y, +z
 // neighbours' faces
 __device__ __forceinline__ void cut_coeffs(const TankDev& T, int i, int j, int k, float C[6]) {
@@ -126,6 +153,7 @@ __global__ void __launch_bounds__(kSorThreads) k_sor(const TankDev* __restrict__
 #pragma unroll
     for (int d = 0; d < 6; ++d) C[d] = (code >> d) & 1u ? 1.0f : 0.0f;
   }
+  const float inv = coeff_inv(code & kCodePartial, code, C);
   asm volatile("griddepcontrol.wait;" ::: "memory");
   if (on) {
     const float* __restrict__ po = pres + (size_t)(1 - color) * nhalf;
@@ -138,7 +166,7 @@ __global__ void __launch_bounds__(kSorThreads) k_sor(const TankDev* __restrict__
     nb[4] = k > 0 ? po[ti + rowb - hx * ny] : 0.f;
     nb[5] = k + 1 < nz ? po[ti + rowb + hx * ny] : 0.f;
     const float p = pres[(size_t)color * nhalf + s];
-    pres[(size_t)color * nhalf + s] = sor_update(C, nb, rhs, p, omega);
+    pres[(size_t)color * nhalf + s] = sor_update_inv(C, nb, rhs, p, omega, inv);
   }
   if (kLoop) {
     for (int r = q + (int)gridDim.x * kSorThreads; r < pfx[ntanks]; r += (int)gridDim.x * kSorThreads) {
@@ -721,8 +749,9 @@ __device__ __forceinline__ float ld_cluster(const float* local, unsigned rank) {
   const unsigned a = (unsigned)__cvta_generic_to_shared(local);
   unsigned ra;
   float v;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(a), "r"(rank));
-  asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(ra) : "memory");
+  asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(a), "r"(rank));
+  // volatile keeps the load between the cluster barriers around it (those carry the memory clobber)
+  asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(ra));
   return v;
 }
 
@@ -752,6 +781,41 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_sor_cluster(const TankDe
   cluster_barrier();                      // every piece is loaded before any neighbour reads it
   const int iters = on ? T.iters : 0;
   const float omega = T.omega;
+  const DivU dhx = T.dhx, dny = T.dny;
+  const int k0 = pc.k0, nk = pc.nk, np_ = pc.np;
+  struct Cell {
+    float nb[6], C[6], inv, rhs, p;
+    int l;
+    bool on;
+  };
+  // everything one update reads, loaded before any update of the pair is stored
+  auto prep = [&](const float* po, const float* pw, const float* rw, const uint8_t* cw, int c, int l, Cell& x) {
+    x.on = false;
+    x.l = l;
+    if (l >= U) return;
+    const uint32_t cd = cw[l];
+    if (!(cd & 0x80u)) return;
+    x.on = true;
+    const int row = divu(l, dhx), ti = l - row * hx;
+    const int kl = divu(row, dny), j = row - kl * ny, k = k0 + kl;
+    const int i = 2 * ti + ((j + k + c) & 1);
+    const int rowb = l - ti;
+    x.nb[0] = i > 0 ? po[((i - 1) >> 1) + rowb] : 0.f;
+    x.nb[1] = i + 1 < nx ? po[((i + 1) >> 1) + rowb] : 0.f;
+    x.nb[2] = j > 0 ? po[l - hx] : 0.f;
+    x.nb[3] = j + 1 < ny ? po[l + hx] : 0.f;
+    x.nb[4] = k == 0 ? 0.f : (kl > 0 ? po[l - plane] : ld_cluster(po + l + plane * (np_ - 1), rank - 1));
+    x.nb[5] = k + 1 >= nz ? 0.f : (kl + 1 < nk ? po[l + plane] : ld_cluster(po + (l - plane * kl), rank + 1));
+    x.rhs = rw[l];
+    x.p = pw[l];
+    if (cd & 0x40u) {
+      cut_coeffs(T, i, j, k, x.C);
+    } else {
+#pragma unroll
+      for (int d = 0; d < 6; ++d) x.C[d] = (cd >> d) & 1u ? 1.0f : 0.0f;
+    }
+    x.inv = coeff_inv(cd & 0x40u, cd, x.C);
+  };
   for (int it = 0; it < max_iters; ++it) {
 #pragma unroll 1
     for (int c = 0; c < 2; ++c) {
@@ -760,28 +824,13 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_sor_cluster(const TankDe
         float* pw = sp + c * S;
         const float* rw = sr + c * S;
         const uint8_t* cw = sc + c * S;
-        for (int l = threadIdx.x; l < U; l += kClusterThreads) {
-          const uint32_t cd = cw[l];
-          if (!(cd & 0x80u)) continue;
-          const int row = divu(l, T.dhx), ti = l - row * hx;
-          const int kl = divu(row, T.dny), j = row - kl * ny, k = pc.k0 + kl;
-          const int i = 2 * ti + ((j + k + c) & 1);
-          const int rowb = l - ti;
-          float nb[6];
-          nb[0] = i > 0 ? po[((i - 1) >> 1) + rowb] : 0.f;
-          nb[1] = i + 1 < nx ? po[((i + 1) >> 1) + rowb] : 0.f;
-          nb[2] = j > 0 ? po[l - hx] : 0.f;
-          nb[3] = j + 1 < ny ? po[l + hx] : 0.f;
-          nb[4] = k == 0 ? 0.f : (kl > 0 ? po[l - plane] : ld_cluster(po + l + plane * (pc.np - 1), rank - 1));
-          nb[5] = k + 1 >= nz ? 0.f : (kl + 1 < pc.nk ? po[l + plane] : ld_cluster(po + (l - plane * kl), rank + 1));
-          float C[6];
-          if (cd & 0x40u) {
-            cut_coeffs(T, i, j, k, C);
-          } else {
-#pragma unroll
-            for (int d = 0; d < 6; ++d) C[d] = (cd >> d) & 1u ? 1.0f : 0.0f;
-          }
-          pw[l] = sor_update(C, nb, rw[l], pw[l], omega);
+#pragma unroll 1
+        for (int l = threadIdx.x; l < U; l += 2 * kClusterThreads) {
+          Cell a, b;
+          prep(po, pw, rw, cw, c, l, a);
+          prep(po, pw, rw, cw, c, l + kClusterThreads, b);
+          if (a.on) pw[a.l] = sor_update_inv(a.C, a.nb, a.rhs, a.p, omega, a.inv);
+          if (b.on) pw[b.l] = sor_update_inv(b.C, b.nb, b.rhs, b.p, omega, b.inv);
         }
       }
       cluster_barrier();                  // this colour is complete in every piece before the next reads it

@@ -118,6 +118,8 @@ SIGNATURES = {
     'suiri_add_whitewater': (C.c_int, [P, P, P, C.c_int64]),
     'suiri_scene_validate': (C.c_int, [C.c_char_p, C.c_int32, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     'suiri_tune_piece': (C.c_int, [P, C.c_int32]),
+    'suiri_tune_g2p': (C.c_int, [P, C.c_int32]),
+    'suiri_batch_tune_g2p': (C.c_int, [P, C.c_int32]),
     'suiri_batch_tune_piece': (C.c_int, [P, C.c_int32]),
     'suiri_residual': (C.c_int, [P, C.c_int32]),
     'suiri_batch_residual': (C.c_int, [P, C.c_int32]),

@@ -214,6 +214,10 @@ class Tank:
         """Shared memory per CTA of the cluster-resident solve, KiB (0: the device maximum)."""
         self._c(N.lib().suiri_tune_piece(self._h, int(piece_kb)))
 
+    def tune_g2p(self, form=0):
+        """Grid-to-particle pass: 0 grid-stride walk, 1 per brick with its faces in shared memory."""
+        self._c(N.lib().suiri_tune_g2p(self._h, int(form)))
+
     def residual(self, on=True):
         """Evaluate every solve's FP64 residual on the device (stats: residual_max, residual_rms, rhs_max)."""
         self._c(N.lib().suiri_residual(self._h, 1 if on else 0))
@@ -230,13 +234,23 @@ class Tank:
         return dict(zip(N.PHASES, list(ms)))
 
     # ------------------------------------------------------------------ read-back
+    def particles4(self, out=None):
+        """Liquid particles as the C ABI gives them: (pos4 (N,4) x, y, z, airborne; vel4 (N,4) vx, vy, vz, id
+        bits). One read: the arrays are sized from the stats' upper bound (or `out`, a pair of (M,4) float32
+        arrays to fill), then trimmed to the particles alive."""
+        if out is None:
+            m = self.stats()['count']
+            out = (np.empty((m, 4), np.float32), np.empty((m, 4), np.float32))
+        P, V = out
+        n = C.c_int64()
+        self._c(N.lib().suiri_read_particles(self._h, _ptr(P), _ptr(V), len(P), C.byref(n)))
+        if n.value > len(P):               # more than the bound allows cannot happen; read again to be safe
+            return self.particles4((np.empty((n.value, 4), np.float32), np.empty((n.value, 4), np.float32)))
+        return P[:n.value], V[:n.value]
+
     def particles(self):
         """(pos (N,3), vel (N,3), air (N,), id (N,) uint32) of the liquid particles."""
-        n = C.c_int64()
-        self._c(N.lib().suiri_read_particles(self._h, None, None, 0, C.byref(n)))
-        P = np.empty((n.value, 4), np.float32)
-        V = np.empty((n.value, 4), np.float32)
-        self._c(N.lib().suiri_read_particles(self._h, _ptr(P), _ptr(V), n.value, C.byref(n)))
+        P, V = self.particles4()
         return P[:, :3].copy(), V[:, :3].copy(), P[:, 3].copy(), V[:, 3].copy().view(np.uint32)
 
     @property
@@ -356,6 +370,9 @@ class Batch:
 
     def tune_piece(self, piece_kb=0):
         N.check(N.lib().suiri_batch_tune_piece(self._h, int(piece_kb)))
+
+    def tune_g2p(self, form=0):
+        N.check(N.lib().suiri_batch_tune_g2p(self._h, int(form)))
 
     def residual(self, on=True):
         N.check(N.lib().suiri_batch_residual(self._h, 1 if on else 0))

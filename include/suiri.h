@@ -278,6 +278,11 @@ int suiri_tune(suiri_tank* t, int32_t particle_blocks_per_sm, int32_t sor_mode);
    the next suiri_tune with it */
 int suiri_tune_piece(suiri_tank* t, int32_t piece_kb);
 int suiri_batch_tune_piece(suiri_batch* b, int32_t piece_kb);
+/* form of the grid-to-particle pass: 0 a grid-stride walk over the sorted particles (corner loads from the
+   node arrays), 1 one block per 8×8×8-cell brick with the brick's face nodes copied to shared memory first.
+   Both give the same particles bit for bit. */
+int suiri_tune_g2p(suiri_tank* t, int32_t form);
+int suiri_batch_tune_g2p(suiri_batch* b, int32_t form);
 /* 1: after every pressure solve, evaluate its FP64 residual on the device (two extra launches); read it
    with suiri_get_stats (residual_max, residual_rms, rhs_max) */
 int suiri_residual(suiri_tank* t, int32_t on);

@@ -53,7 +53,7 @@ def by_id(pos, vel, air, ids):
     return pos[o], vel[o], air[o], ids[o]
 
 
-def assert_particles(gpu, ora, what=''):
+def assert_particles(gpu, ora, what='', vel_rtol=RTOL):
     gp, gv, ga, gi = gpu.particles()
     gp, gv, ga, gi = by_id(gp, gv, ga, gi.astype(np.int64))
     op, ov, oa, oi = by_id(ora.pos, ora.vel, ora.air, ora.pid)
@@ -62,7 +62,7 @@ def assert_particles(gpu, ora, what=''):
     np.testing.assert_array_equal(ga, oa, err_msg=f'{what}: airborne marks')
     err = np.abs(gp - op)
     assert np.all(err <= 1e-6 + 1e-6 * np.abs(op)), f'{what}: position err {err.max():.3e}'
-    assert_close_field(gv, ov, what=f'{what}: velocity')
+    assert_close_field(gv, ov, rtol=vel_rtol, what=f'{what}: velocity')
 
 
 def sync_oracle_particles(gpu, ora):

@@ -501,7 +501,8 @@ def test_whitewater_advance_two_frames(pkg):
         np.testing.assert_allclose(V[:, :3], ora.wvel[j], rtol=1e-4, atol=1e-5)
         np.testing.assert_array_equal(V[:, 3], ora.wkind[j])
         src = gpu.ripple_field(pkg.native.FIELD_RIPPLE_STATE, (2 * R, 2 * R, 2), np.float32)
-        assert_close_field(src[..., 0], layer.S.real, rtol=1e-4, what=f'frame {f}: ripple state')
+        # near zero here (no drop lands): compared down to the float32 FFT's round-off floor, as the field is
+        assert_close_field(src[..., 0], layer.S.real, rtol=1e-4, atol=1e-11, what=f'frame {f}: ripple state')
         sync_oracle_particles(gpu, ora)       # the next frame starts from the GPU's float32 liquid
     gpu.close()
 
@@ -541,12 +542,20 @@ def test_rectangular_ripple_layer_full_scene_quarter(pkg):
             n_gpu = gpu.step(1 / 60)
             n_ora = ora.step(1 / 60, layer, ripple_depth=prm['depth'])
             assert n_gpu == n_ora
-            assert_particles(gpu, ora, f'burst {f}')
+            # velocities within 1e-4: around landing drops the corner sums of faces with little total weight
+            # lose digits in float32 (the reference GPU path's own arithmetic), against float64 in the oracle
+            assert_particles(gpu, ora, f'burst {f}', vel_rtol=1e-4)
             sync_oracle_particles(gpu, ora)
         st = gpu.stats()
         assert st['impacts'] == ora.impacts
         assert ora.impacts > impacts, 'no drop merged in this burst'
         impacts = ora.impacts
+        # crowns of the drops' own diameters (and spray of fast particles): the same whitewater
+        P, V = gpu.whitewater()
+        assert st['ww_count'] == len(ora.wpos) > 0
+        j = _match_sets(P.astype(np.float64), np.concatenate([ora.wpos, ora.wlife[:, None]], 1), 1e-4)
+        np.testing.assert_allclose(P[:, 3], ora.wlife[j], rtol=1e-4, atol=1e-5)
+        np.testing.assert_allclose(V[:, :3], ora.wvel[j], rtol=1e-3, atol=1e-4)
         top = gpu.ripple_field(pkg.native.FIELD_TOP, (128, 128), np.float32)
         assert_close_field(top, ora.top, what=f'burst {f}: top height')
         S = gpu.ripple_field(pkg.native.FIELD_RIPPLE_STATE, (2 * Rz, 2 * Rx, 2), np.float32)
@@ -590,3 +599,40 @@ def test_full_size_obstacles_inflow_substeps(pkg):
         assert abs(dg - do) <= 1e-3 * do, (dg, do)
         sync_oracle_particles(gpu, ora)
     gpu.close()
+
+
+@pytest.mark.parametrize('advect', ['euler', 'rk2'])
+def test_g2p_brick_form_equals_the_walk(pkg, advect):
+    """The per-brick grid-to-particle form (faces staged in shared memory, one block per 8×8×8 brick and one
+    for the particles outside the grid) gives the particles of the grid-stride walk bit for bit: a tank with
+    obstacles and an odd size, a pool with airborne drops falling into it, and particles above the rim
+    (outside the grid), with Euler and RK2 advection; whitewater counts and the speed maximum agree."""
+    w = pkg.workloads.random_tank(5, axes=(21, 37, 19))
+    rng = np.random.default_rng(4)
+    hi = np.array([w['nx'], w['ny'], w['nz']]) * w['h'] + w['origin']
+    n_air = 300
+    drops = w['origin'] + rng.random((n_air, 3)) * (hi - w['origin'])
+    drops[:, 1] = rng.uniform(0.7, 1.3, n_air) * hi[1]              # some above the rim, outside the grid
+    pos = np.concatenate([w['pos'], drops.astype(np.float32)])
+    vel = np.zeros_like(pos); vel[len(w['pos']):, 1] = -3.0
+    air = np.zeros(len(pos)); air[len(w['pos']):] = 1
+
+    def run(form):
+        t = pkg.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=0.95, omega=1.7, iters=20, whitewater=True,
+                     ripple=(16, 16), capacity=len(pos) * 2, advect=advect)
+        t.set_objects(w['objects'])
+        t.add_particles(pos, vel, air)
+        t.tune_g2p(form)
+        for _ in range(5):
+            t.substep(1 / 240)
+        st = t.stats()
+        p, v, a, ids = t.particles()
+        o = np.argsort(ids)
+        out = (p[o], v[o], a[o], ids[o], st['ww_count'], st['vmax'], st['impacts'])
+        t.close()
+        return out
+
+    walk, brick = run(0), run(1)
+    for x, y in zip(walk[:4], brick[:4]):
+        np.testing.assert_array_equal(x, y)
+    assert walk[4:] == brick[4:]

@@ -15,18 +15,24 @@ class FakeTarget:
 
     def __init__(self, table):
         self.table, self.current, self.applied = table, None, []
-        self.piece, self.substeps, self.saves = 0, 0, []
+        self.piece, self.substeps, self.saves, self.g2p = 0, 0, [], 0
 
     def tune(self, bps, mode):
         self.current = (bps, mode, self.piece)
         self.applied.append(self.current)
 
+    def key(self):
+        return self.current + (self.g2p,)
+
     def tune_piece(self, kb):
         self.piece = kb
 
+    def tune_g2p(self, form):
+        self.g2p = form
+
     def time_substeps(self, dt, steps):
         self.substeps += steps
-        ms = self.table[self.current]
+        ms = self.table[self.key()]
         if ms is None:
             raise RuntimeError(f'{self.current} cannot be launched')
         return ms * steps
@@ -40,22 +46,24 @@ class FakeTarget:
 
 
 def test_autotune_keeps_the_fastest_and_skips_shapes_that_fail():
-    table = {c: 5.0 for c in autotune.CANDIDATES}
-    table[(2, 4, 112)] = 3.0
-    table[(4, 1, 0)] = None
+    table = {c + (f,): 5.0 for c in autotune.CANDIDATES for f in autotune.G2P_FORMS}
+    table[(2, 4, 112, 0)] = 3.0
+    table[(2, 4, 112, 1)] = 2.5          # the brick G2P form is faster with the best solve shape
+    table[(4, 0, 0, 1)] = 1.0            # never timed: G2P forms are tried with the best shape only
+    table[(4, 1, 0, 0)] = None
     t = FakeTarget(table)
     t.substeps = 7
     best, timings = autotune.autotune(t, 1 / 240)
-    assert best == (2, 4, 112) and t.current == (2, 4, 112)
-    assert timings[(4, 1, 0)] == float('inf') and timings[(2, 4, 112)] == pytest.approx(3.0)
-    assert set(timings) == set(autotune.CANDIDATES)
+    assert best == (2, 4, 112, 1) and t.key() == (2, 4, 112, 1)
+    assert timings[(4, 1, 0, 0)] == float('inf') and timings[(2, 4, 112, 0)] == pytest.approx(3.0)
+    assert set(timings) == {c + (0,) for c in autotune.CANDIDATES} | {(2, 4, 112, 1)}
     assert t.substeps == 7              # the tuning sub-steps were rolled back
     assert {c[1] for c in autotune.CANDIDATES} >= {0, 1, 2, 3, 4}
     assert len({c[2] for c in autotune.CANDIDATES if c[1] == 4}) >= 3     # tile sizes of the cluster solve
 
 
 def test_autotune_raises_when_nothing_launches():
-    t = FakeTarget({c: None for c in autotune.CANDIDATES})
+    t = FakeTarget({c + (f,): None for c in autotune.CANDIDATES for f in autotune.G2P_FORMS})
     with pytest.raises(RuntimeError):
         autotune.autotune(t, 1 / 240)
 

@@ -152,3 +152,19 @@ def test_sor_residual_checker_decreases():
         p = t.sor(fluid, p_init=np.zeros_like(t.pres), iters=it)
         r.append(of.residual_f64(C, rhs, fluid, p))
     assert r[0] > r[1] > r[2]
+
+
+def test_drop_diameters_are_lognormal_and_fixed_by_the_id():
+    """The build's sub-grid drop sizes (the reference gives every drop the particle mass): median 2 mm and
+    log-standard-deviation 0.4 over many ids, a pure function of the id, |z| clamped to 4."""
+    from oracle import hashrng
+    ids = np.arange(400000)
+    D = hashrng.drop_diameter(ids, 0.002, 0.4)
+    z = np.log(D / 0.002) / 0.4
+    assert abs(np.median(D) / 0.002 - 1) < 0.01
+    assert abs(z.std() - 1) < 0.01 and abs(z.mean()) < 0.01
+    assert np.abs(z).max() <= 4 + 1e-12
+    np.testing.assert_array_equal(hashrng.drop_diameter(ids[::-1], 0.002, 0.4), D[::-1])
+    # the particle-mass rule is the default
+    t = of.Tank(8, 8, 8, 1 / 16, rng_mode='hash')
+    assert t.drop_d is None
