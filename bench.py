@@ -413,9 +413,8 @@ def e2e_batch(P, specs, device, best, steps, workers=8):
     from concurrent.futures import ThreadPoolExecutor
     tanks = make_batch_tanks(P, specs, device, add=False)
     b = P.Batch(tanks)
-    b.tune_piece(best[2])
-    b.tune(best[0], best[1])
-    b.tune_g2p(best[3])
+    for k, knobs in enumerate(best):
+        b.tune_lane(k, *knobs)
     host = [np.ascontiguousarray(w['pos'], np.float32) for w in specs]
     outs = [(np.empty((len(p) + 64, 4), np.float32), np.empty((len(p) + 64, 4), np.float32)) for p in host]
     readback = int(P.native.lib().suiri_stats_readback_bytes())
@@ -458,7 +457,7 @@ def run_batch(args, rank, world, local):
     import torch.distributed as dist
     init_ranks(world, local)
     P = pkg()
-    autotune = importlib.import_module('hahenn-_b200.autotune').autotune
+    autotune_batch = importlib.import_module('hahenn-_b200.autotune').autotune_batch
     specs = batch_specs(args.tanks)
     cfg = batch_config(specs)
     lane_of, nlanes = size_lanes(specs)
@@ -475,7 +474,7 @@ def run_batch(args, rank, world, local):
 
     tanks = make_batch_tanks(P, specs, local)
     b = P.Batch(tanks)
-    best, timings = autotune(b, DT)
+    best, timings = autotune_batch(b, DT)          # per lane: (blocks per SM, solve form, tile, G2P form)
     b.profile(True)
     stream = torch.cuda.ExternalStream(b.stream())
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
@@ -521,7 +520,6 @@ def run_batch(args, rank, world, local):
     if rank == 0:
         peak, kind = peaks()
         iters = cfg['sor_iters']
-        mode = best[1]
         lanes = []
         for l in range(nlanes):
             idx = [i for i in range(len(specs)) if lane_of[i] == l]
@@ -535,9 +533,11 @@ def run_batch(args, rank, world, local):
                 gbs = alg / (ph[name] * 1e-3) / 1e9
                 fig[name] = dict(alg_bytes=alg, ms=ph[name], achieved_gbs=gbs, frac=gbs / peak)
             lanes.append(dict(tanks=len(idx), particles=parts, nodes=nodes, active_cells=active, phases_ms=ph,
-                              kernels=fig))
+                              kernels=fig, tuned=dict(zip(('blocks_per_sm', 'sor_mode', 'piece_kb', 'g2p_form'),
+                                                          best[l]))))
         dom = max(range(nlanes), key=lambda l: lanes[l]['phases_ms']['pressure_solve'])
         sol = lanes[dom]['kernels']['pressure_solve']
+        mode = best[dom][1]
         per_launch = 1 if mode in (1, 4) else 2 * iters
         tr = profile_figure('sor_cluster_batch_traffic.json' if mode == 4 else 'sor_sweep_traffic.json')
         roofline = dict(bound='hbm', kernel='k_sor_cluster (whole solve, one launch per lane)' if mode == 4 else
@@ -550,13 +550,14 @@ def run_batch(args, rank, world, local):
                         note='the solve\'s operands stay on chip (shared memory) or in L2, so the algorithmic '
                              'rate may exceed the HBM copy rate; traffic is the DRAM bytes ncu measured per launch')
         cpu_rate, cpu_el, cpu_what = cpu_sample_rate(specs)
-        launches = args.steps * sum(launches_per_substep(mode, iters) for _ in range(nlanes))
+        launches = args.steps * sum(launches_per_substep(best[l][1], iters) for l in range(nlanes))
         line = dict(metric=METRIC, value=value, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
                     ms_per_step=ms, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
                     data='synthetic (seeded particles, analytic obstacles)', config=cfg,
                     l2='flushed (256 MiB write) between timed steps', parallelism=f'replicas{world}',
-                    tuned=dict(blocks_per_sm=best[0], sor_mode=best[1], piece_kb=best[2], g2p_form=best[3]),
-                    tuning_ms={'x'.join(str(v) for v in k): v for k, v in timings.items()},
+                    tuned=[dict(zip(('blocks_per_sm', 'sor_mode', 'piece_kb', 'g2p_form'), b)) for b in best],
+                    tuning_ms={f'lane{l}': {'x'.join(str(v) for v in k): v for k, v in t.items()}
+                               for l, t in timings.items()},
                     plain_sequential=dict(value=particles / world * 1000.0 / ms_plain, ms_per_step=ms_plain,
                                           note='the same scenes one by one, device time summed'),
                     batched_over_plain=ms_plain / ms if world == 1 else None,

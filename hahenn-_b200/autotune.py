@@ -12,6 +12,9 @@ Knobs (``suiri_tune`` / ``suiri_batch_tune``, ``suiri_tune_piece`` / ``suiri_bat
   * the form of the grid-to-particle pass (``suiri_tune_g2p``): a grid-stride walk, or one block per brick
     with the brick's faces staged in shared memory; tried with the best of the other knobs.
 
+A batch is tuned lane by lane (``autotune_batch``): its size lanes run concurrently, and small tanks may
+prefer another form than large ones.
+
 Each candidate is timed on the device (events on the tank's or batch's stream) over a few sub-steps of the
 real state, after one sub-step that captures its graph. Targets that can save and restore their state
 (``save_state`` / ``restore_state``: the tanks' water copies) are put back afterwards, so tuning leaves the
@@ -72,4 +75,24 @@ def autotune(target, dt, candidates=CANDIDATES, steps=3, g2p_forms=G2P_FORMS):
     target.tune(best[0], best[1])
     if has_g2p:
         target.tune_g2p(best[3])
+    return best, timings
+
+
+def autotune_batch(batch, dt, candidates=CANDIDATES, steps=3, g2p_forms=G2P_FORMS):
+    """Tune each size lane of a batch in turn (the others keep their settings) on the batch's sub-step time,
+    with the batch's state rolled back afterwards. Returns ([best per lane], {lane: timings})."""
+    saved = batch.save_state()
+    best, timings = [], {}
+    try:
+        n = batch.lanes()
+        for k in range(n):
+            batch.tune_lane(k, *CANDIDATES[0][:2], 0, g2p_forms[0])
+        for k in range(n):
+            b, t = autotune(batch.lane(k), dt, candidates, steps, g2p_forms)
+            best.append(b)
+            timings[k] = t
+    finally:
+        batch.restore_state(saved)
+    for k, b in enumerate(best):
+        batch.tune_lane(k, *b)
     return best, timings

@@ -580,6 +580,18 @@ int suiri_batch_tune_g2p(suiri_batch* b, int32_t form) {
   });
 }
 
+int suiri_batch_tune_lane(suiri_batch* b, int32_t lane, int32_t particle_blocks_per_sm, int32_t sor_mode,
+                          int32_t piece_kb, int32_t g2p_form) {
+  return guard(b ? &b->err : nullptr, [&] {
+    if (!b || !b->b) throw Error(SUIRI_ERR_INVALID, "null batch");
+    if (lane < 0 || lane >= (int32_t)b->b->lanes.size()) throw Error(SUIRI_ERR_INVALID, "lane out of range");
+    Group& g = *b->b->lanes[lane];
+    tune_piece(g, piece_kb);
+    tune_group(g, particle_blocks_per_sm, sor_mode);
+    tune_g2p(g, g2p_form);
+  });
+}
+
 static void set_residual(Group& g, bool on) {
   if (on == g.residual) return;
   CK(cudaStreamSynchronize(g.stream));

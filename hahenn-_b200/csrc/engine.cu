@@ -1029,7 +1029,7 @@ void Group::plan_cluster() {
   int K = 1, smem = 16;
   for (int i = 0; i < n; ++i) {
     const TankDev& D = tanks[i]->d;
-    const int npm = budget / cluster_plane_bytes(D);
+    const int npm = (budget - 32) / cluster_plane_bytes(D);     // the field and the work counters
     if (npm < 1) throw Error(-1, "cluster solve: one z plane of a tank does not fit a CTA's shared memory");
     int mi = (D.nz + npm - 1) / npm;
     np[i] = (D.nz + mi - 1) / mi;

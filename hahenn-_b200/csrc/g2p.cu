@@ -284,9 +284,10 @@ __device__ __forceinline__ unsigned long long g2p_particle(const TankDev& T, int
   }
   // merging with the pool (solver.py:584-606)
   const int frame = T.ctr->frame;
-  double g1[3];
-  grid_pos(T, x[0], x[1], x[2], g1[0], g1[1], g1[2]);
-  if (air && vold[1] < -0.3 && in_grid(T, g1[0], g1[1], g1[2])) {
+  double g1[3] = {-1.0, -1.0, -1.0};
+  const bool falling = air && vold[1] < -0.3;
+  if (falling) grid_pos(T, x[0], x[1], x[2], g1[0], g1[1], g1[2]);     // only a falling drop may merge
+  if (falling && in_grid(T, g1[0], g1[1], g1[2])) {
     const int c1[3] = {(int)floor(g1[0]), (int)floor(g1[1]), (int)floor(g1[2])};
     const int same = (c1[0] == c0[0] && c1[1] == c0[1] && c1[2] == c0[2]) ? 1 : 0;
     const int cnt1 = count_at(T, c1[0], c1[1], c1[2]);

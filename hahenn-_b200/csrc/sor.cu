@@ -737,6 +737,8 @@ constexpr int kClusterBytesPerSlot = 9;
 __device__ __forceinline__ void cluster_barrier() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ unsigned cluster_ctarank() {
   unsigned r;
@@ -769,7 +771,10 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_sor_cluster(const TankDe
   float* sp = reinterpret_cast<float*>(cl_smem);
   float* sr = sp + 2 * S;
   uint8_t* sc = reinterpret_cast<uint8_t*>(sr + 2 * S);
+  // work counters of the sweeps (two sets, used by alternate sweeps): behind the field, see cluster_smem_bytes
+  int* s_cnt = reinterpret_cast<int*>(cl_smem + ((18 * S + 15) & ~15));
   const unsigned rank = cluster_ctarank();
+  if (threadIdx.x < 6) s_cnt[threadIdx.x] = 0;
   for (int q = threadIdx.x; q < 2 * U; q += kClusterThreads) {
     const int c = q >= U, l = q - c * U;
     const size_t g = c * nh + g0 + l;
@@ -778,7 +783,6 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_sor_cluster(const TankDe
     sr[c * S + l] = T.rhs[g];
     sc[c * S + l] = (uint8_t)((cd & 0x3Fu) | ((cd & kCodePartial) ? 0x40u : 0u) | ((cd & kCodeActive) ? 0x80u : 0u));
   }
-  cluster_barrier();                      // every piece is loaded before any neighbour reads it
   const int iters = on ? T.iters : 0;
   const float omega = T.omega;
   const DivU dhx = T.dhx, dny = T.dny;
@@ -788,11 +792,11 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_sor_cluster(const TankDe
     int l;
     bool on;
   };
-  // everything one update reads, loaded before any update of the pair is stored
-  auto prep = [&](const float* po, const float* pw, const float* rw, const uint8_t* cw, int c, int l, Cell& x) {
+  // everything one update reads
+  auto prep = [&](const float* po, const float* pw, const float* rw, const uint8_t* cw, int c, int l, int lend, Cell& x) {
     x.on = false;
     x.l = l;
-    if (l >= U) return;
+    if (l >= lend) return;
     const uint32_t cd = cw[l];
     if (!(cd & 0x80u)) return;
     x.on = true;
@@ -816,26 +820,52 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_sor_cluster(const TankDe
     }
     x.inv = coeff_inv(cd & 0x40u, cd, x.C);
   };
+  // The planes whose z neighbours sit in another CTA (the first plane unless the piece starts the tank, the
+  // last unless it ends it) are relaxed first, between the cluster barrier's wait (the neighbours' planes of
+  // the previous sweep are complete) and its arrive (this piece's are); the interior planes read only this
+  // CTA's shared memory and are relaxed after the arrive, so the barrier's latency overlaps them, and a CTA
+  // barrier makes them visible to the next sweep. A neighbour reads this piece's boundary planes only before
+  // its own arrive, so they are not overwritten while it reads them.
+  const int lo_b = (on && k0 > 0) ? plane : 0;                         // [0, lo_b): first plane, remote below
+  const int hi_b = (on && k0 + nk < nz && !(lo_b && nk == 1)) ? U - plane : U;   // [hi_b, U): last plane, remote above
+  // Warps take 32-slot chunks of a range from a shared counter until it runs out, so that warps whose chunks
+  // hold few liquid cells (the upper rows of a plane) take more of them and the barrier waits for no one.
+  const int lane = threadIdx.x & 31;
+  auto relax = [&](const float* po, float* pw, const float* rw, const uint8_t* cw, int c, int l0, int l1, int* ctr) {
+    const int nch = (l1 - l0 + 31) >> 5;
+#pragma unroll 1
+    while (true) {
+      int ch = 0;
+      if (lane == 0) ch = atomicAdd(ctr, 1);
+      ch = __shfl_sync(0xffffffffu, ch, 0);
+      if (ch >= nch) break;
+      Cell a;
+      prep(po, pw, rw, cw, c, l0 + (ch << 5) + lane, l1, a);
+      if (a.on) pw[a.l] = sor_update_inv(a.C, a.nb, a.rhs, a.p, omega, a.inv);
+    }
+  };
+  cluster_arrive();                       // this piece is loaded
   for (int it = 0; it < max_iters; ++it) {
 #pragma unroll 1
     for (int c = 0; c < 2; ++c) {
-      if (it < iters) {
-        const float* po = sp + (1 - c) * S;
-        float* pw = sp + c * S;
-        const float* rw = sr + c * S;
-        const uint8_t* cw = sc + c * S;
-#pragma unroll 1
-        for (int l = threadIdx.x; l < U; l += 2 * kClusterThreads) {
-          Cell a, b;
-          prep(po, pw, rw, cw, c, l, a);
-          prep(po, pw, rw, cw, c, l + kClusterThreads, b);
-          if (a.on) pw[a.l] = sor_update_inv(a.C, a.nb, a.rhs, a.p, omega, a.inv);
-          if (b.on) pw[b.l] = sor_update_inv(b.C, b.nb, b.rhs, b.p, omega, b.inv);
-        }
+      const bool go = it < iters;
+      const float* po = sp + (1 - c) * S;
+      float* pw = sp + c * S;
+      const float* rw = sr + c * S;
+      const uint8_t* cw = sc + c * S;
+      int* ctr = s_cnt + 3 * c;           // this sweep's counters; the other set is zeroed for the next sweep
+      if (threadIdx.x < 3) s_cnt[3 * (1 - c) + threadIdx.x] = 0;
+      cluster_wait();
+      if (go) {
+        relax(po, pw, rw, cw, c, 0, lo_b, ctr);
+        relax(po, pw, rw, cw, c, hi_b, U, ctr + 1);
       }
-      cluster_barrier();                  // this colour is complete in every piece before the next reads it
+      cluster_arrive();
+      if (go) relax(po, pw, rw, cw, c, lo_b, hi_b, ctr + 2);
+      __syncthreads();
     }
   }
+  cluster_wait();                         // no neighbour reads this piece's shared memory any more
   for (int q = threadIdx.x; q < 2 * U; q += kClusterThreads) {
     const int c = q >= U, l = q - c * U;
     T.pres[c * nh + g0 + l] = sp[c * S + l];
@@ -844,7 +874,8 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_sor_cluster(const TankDe
 
 int cluster_plane_bytes(const TankDev& D) { return kClusterBytesPerSlot * 2 * D.hx * D.ny; }
 
-int cluster_smem_bytes(const TankDev& D, int np) { return (cluster_plane_bytes(D) * np + 15) & ~15; }
+// the field of np planes (9 B per slot of both colours) and the sweeps' six work counters
+int cluster_smem_bytes(const TankDev& D, int np) { return ((cluster_plane_bytes(D) * np + 15) & ~15) + 32; }
 
 cudaError_t sor_cluster_prepare(int smem_bytes, int cluster) {
   cudaError_t e = cudaFuncSetAttribute(k_sor_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);

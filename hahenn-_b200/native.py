@@ -120,6 +120,7 @@ SIGNATURES = {
     'suiri_tune_piece': (C.c_int, [P, C.c_int32]),
     'suiri_tune_g2p': (C.c_int, [P, C.c_int32]),
     'suiri_batch_tune_g2p': (C.c_int, [P, C.c_int32]),
+    'suiri_batch_tune_lane': (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     'suiri_batch_tune_piece': (C.c_int, [P, C.c_int32]),
     'suiri_residual': (C.c_int, [P, C.c_int32]),
     'suiri_batch_residual': (C.c_int, [P, C.c_int32]),

@@ -374,6 +374,14 @@ class Batch:
     def tune_g2p(self, form=0):
         N.check(N.lib().suiri_batch_tune_g2p(self._h, int(form)))
 
+    def tune_lane(self, lane, blocks_per_sm=4, sor_mode=0, piece_kb=0, g2p_form=0):
+        N.check(N.lib().suiri_batch_tune_lane(self._h, int(lane), int(blocks_per_sm), int(sor_mode), int(piece_kb),
+                                              int(g2p_form)))
+
+    def lane(self, k):
+        """A tuning target for lane k alone (the autotuner's interface); timing covers the whole batch."""
+        return _LaneTarget(self, k)
+
     def residual(self, on=True):
         N.check(N.lib().suiri_batch_residual(self._h, 1 if on else 0))
 
@@ -404,3 +412,29 @@ class Batch:
         s = C.c_void_p()
         N.check(N.lib().suiri_batch_stream(self._h, C.byref(s)))
         return s.value
+
+
+class _LaneTarget:
+    """One size lane of a batch as an autotuner target: its knobs are set through suiri_batch_tune_lane, the
+    other lanes keep theirs; sub-steps and saved states are the whole batch's."""
+
+    def __init__(self, batch, lane, knobs=(4, 0, 0, 0)):
+        self.batch, self.k = batch, int(lane)
+        self.knobs = list(knobs)
+
+    def _apply(self):
+        self.batch.tune_lane(self.k, *self.knobs)
+
+    def tune(self, blocks_per_sm=4, sor_mode=0):
+        self.knobs[0], self.knobs[1] = int(blocks_per_sm), int(sor_mode)
+        self._apply()
+
+    def tune_piece(self, piece_kb=0):
+        self.knobs[2] = int(piece_kb)
+
+    def tune_g2p(self, form=0):
+        self.knobs[3] = int(form)
+        self._apply()
+
+    def time_substeps(self, dt, steps):
+        return self.batch.time_substeps(dt, steps)

@@ -283,6 +283,10 @@ int suiri_batch_tune_piece(suiri_batch* b, int32_t piece_kb);
    Both give the same particles bit for bit. */
 int suiri_tune_g2p(suiri_tank* t, int32_t form);
 int suiri_batch_tune_g2p(suiri_batch* b, int32_t form);
+/* all knobs of one size lane of a batch (lane in [0, suiri_batch_lanes)): the lanes run concurrently and may
+   each prefer another form (small tanks the cluster-resident solve, large ones one launch per sweep) */
+int suiri_batch_tune_lane(suiri_batch* b, int32_t lane, int32_t particle_blocks_per_sm, int32_t sor_mode,
+                          int32_t piece_kb, int32_t g2p_form);
 /* 1: after every pressure solve, evaluate its FP64 residual on the device (two extra launches); read it
    with suiri_get_stats (residual_max, residual_rms, rhs_max) */
 int suiri_residual(suiri_tank* t, int32_t on);

@@ -543,8 +543,9 @@ def test_rectangular_ripple_layer_full_scene_quarter(pkg):
             n_ora = ora.step(1 / 60, layer, ripple_depth=prm['depth'])
             assert n_gpu == n_ora
             # velocities within 1e-4: around landing drops the corner sums of faces with little total weight
-            # lose digits in float32 (the reference GPU path's own arithmetic), against float64 in the oracle
-            assert_particles(gpu, ora, f'burst {f}', vel_rtol=1e-4)
+            # lose digits in float32 (the reference GPU path's own arithmetic), against float64 in the oracle;
+            # the vertical velocity of particles on the floor clamp is a tie (see assert_particles)
+            assert_particles(gpu, ora, f'burst {f}', vel_rtol=1e-4, floor_y=float(np.float32(0.32 * h)))
             sync_oracle_particles(gpu, ora)
         st = gpu.stats()
         assert st['impacts'] == ora.impacts

@@ -79,3 +79,41 @@ def test_workloads_shapes_and_seeds():
     assert len(specs) == 64
     assert all(a in workloads.AXES_BATCH for s in specs for a in (s['nx'], s['ny'], s['nz']))
     assert len({(s['nx'], s['ny'], s['nz']) for s in specs}) > 10                        # uneven sizes
+
+
+class FakeBatch:
+    """Two size lanes whose sub-step time is the slower lane's; lane 0 is fastest with the cluster-resident
+    solve, lane 1 with one launch per sweep. State: a sub-step counter, saved and restored."""
+
+    def __init__(self):
+        self.knobs = [None, None]
+        self.substeps, self.saves = 0, []
+
+    def lanes(self):
+        return 2
+
+    def tune_lane(self, k, bps, mode, piece, g2p):
+        self.knobs[k] = (bps, mode, piece, g2p)
+
+    def lane(self, k):
+        from importlib import import_module
+        return import_module('hahenn-_b200.tank')._LaneTarget(self, k)
+
+    def time_substeps(self, dt, steps):
+        self.substeps += steps
+        cost = [{4: 1.0}.get(self.knobs[0][1], 2.0), {0: 1.5}.get(self.knobs[1][1], 3.0)]
+        return max(cost) * steps
+
+    def save_state(self):
+        self.saves.append(self.substeps)
+        return len(self.saves) - 1
+
+    def restore_state(self, k):
+        self.substeps = self.saves[k]
+
+
+def test_batch_tuned_lane_by_lane():
+    b = FakeBatch()
+    best, timings = autotune.autotune_batch(b, 1 / 240)
+    assert [k[1] for k in best] == [4, 0] and b.knobs[0][1] == 4 and b.knobs[1][1] == 0
+    assert b.substeps == 0 and set(timings) == {0, 1}
