@@ -452,6 +452,21 @@ def e2e_batch(P, specs, device, best, steps, workers=8):
                     f'stats read back each sub-step, every scene\'s particles read back at the end')
 
 
+def solve_residual(target, tanks, dt):
+    """The FP64 residual of one more sub-step's pressure solve (after the timed region), per tank: max
+    |h²·div − A·p| over the active cells, relative to max |h²·div|; the largest over the tanks."""
+    target.residual(True)
+    target.substep(dt)
+    target.sync()
+    st = [t.stats() for t in tanks]
+    target.residual(False)
+    rel = [s['residual_max'] / s['rhs_max'] for s in st if s['rhs_max'] > 0]
+    return dict(max_abs=max(s['residual_max'] for s in st), max_rel=max(rel) if rel else 0.0,
+                rms_max=max(s['residual_rms'] for s in st), tanks=len(st),
+                note='FP64 residual r = sum C p_nb - h^2 div - (sum C) p of the solve, float64 from the float32 operands, '
+                     'over the active cells, one sub-step after the timed region; rel = max|r| / max|h^2 div| per tank')
+
+
 def run_batch(args, rank, world, local):
     import torch
     import torch.distributed as dist
@@ -511,6 +526,7 @@ def run_batch(args, rank, world, local):
         ms, particles, sor_ms = reduce_ranks(ms, particles, sor_ms, dev)
     value = particles * 1000.0 / ms
     b.profile(False)
+    residual = solve_residual(b, tanks, DT)
     b.close()
     for t in tanks:
         t.close()
@@ -563,7 +579,7 @@ def run_batch(args, rank, world, local):
                     batched_over_plain=ms_plain / ms if world == 1 else None,
                     roofline=roofline, kernels=dict(peak_gbs=peak, lanes=lanes),
                     cpu_baseline=dict(value=cpu_rate, unit=METRIC, cores=1, kind='port', sample=cpu_what),
-                    e2e=e2e, gpu_launches=launches, clocks=clk)
+                    e2e=e2e, gpu_launches=launches, clocks=clk, residual_f64=residual)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -614,6 +630,8 @@ def run_plain(args, rank, world, local):
     if world > 1:
         ms, particles, sor_launch_ms = reduce_ranks(ms, particles, sor_launch_ms, f'cuda:{local}')
     value = particles * 1000.0 / ms
+    tank.profile(False)
+    residual = solve_residual(tank, [tank], dt)
 
     # end-to-end through the C ABI: host inflow particles (pinned) up, stats back, every step
     t2 = make_tank(P, w, local, host_inflow=True)
@@ -666,7 +684,8 @@ def run_plain(args, rank, world, local):
                                   unit_bytes='20 B per active cell per colour sweep'),
                     phases_ms=ph, tuned=dict(blocks_per_sm=best[0], sor_mode=best[1], piece_kb=best[2], g2p_form=best[3]),
                     cpu_baseline=dict(value=cpu_rate, unit=METRIC, cores=1, kind='port', sample=cpu_what),
-                    e2e=e2e, gpu_launches=launches_per_substep(best[1], prm['iters']) * args.steps, clocks=clk)
+                    e2e=e2e, gpu_launches=launches_per_substep(best[1], prm['iters']) * args.steps, clocks=clk,
+                    residual_f64=residual)
         print(json.dumps(line), flush=True)
     tank.close()
     if world > 1:

@@ -22,7 +22,7 @@ simulation where it found it.
 """
 
 CANDIDATES = ((2, 0, 0), (4, 0, 0), (8, 0, 0), (4, 2, 0), (4, 3, 0), (4, 1, 0),
-              (2, 4, 0), (2, 4, 160), (2, 4, 112), (2, 4, 80), (4, 4, 0))
+              (2, 4, 0), (2, 4, 192), (2, 4, 128), (2, 4, 96), (2, 4, 64), (4, 4, 0))
 
 
 G2P_FORMS = (0, 1)

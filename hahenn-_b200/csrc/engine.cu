@@ -998,6 +998,8 @@ Group::~Group() {
     cudaEventDestroy(ev_done);
   }
   // stream-ordered frees: no device-wide synchronisation (other batches keep running)
+  drop_cluster_classes();
+  if (cl_fork) cudaEventDestroy(cl_fork);
   for (void* p : {(void*)d_hpfx, (void*)d_apfx, (void*)d_barrier, (void*)d_ticket, d_tbl, (void*)d_tanks, (void*)d_bpfx,
                   (void*)d_ppfx, (void*)d_bsum, (void*)d_pieces})
     if (p) cudaFreeAsync(p, stream);
@@ -1014,60 +1016,73 @@ void Group::ensure_tbl() {
   tbl_assign(ctx, d_tbl, tiles);
 }
 
-// The CTA plan of the cluster-resident solve. Each tank is cut into m pieces of np whole z planes, as few
-// as fit the shared memory a CTA may take (cl_piece_kb, or the device's opt-in maximum); the cluster size K
-// is the largest m, and the tanks are packed into clusters of K CTAs first-fit by decreasing m (a tank's
-// pieces on consecutive ranks; unused ranks idle). Throws if a tank needs more than kClusterMax pieces or the
-// device cannot hold one such cluster.
+// The CTA plan of the cluster-resident solve. Each tank is cut into m pieces of np whole z planes, as few as fit
+// the shared memory a CTA may take (cl_piece_kb, or the device's opt-in maximum less the kernel's static
+// share). The tanks with the same m form a class: one launch of clusters of m CTAs, a cluster per tank, so
+// that the cluster barrier couples only the pieces of one tank. The classes' launches run on streams of their
+// own, forked from and joined back to the group's stream. Throws if a tank needs more than kClusterMax pieces
+// or the device cannot hold one cluster of a class.
+void Group::drop_cluster_classes() {
+  for (ClusterClass& c : cl_classes) {
+    if (c.done) cudaEventDestroy(c.done);
+    if (c.stream) cudaStreamDestroy(c.stream);
+  }
+  cl_classes.clear();
+}
+
 void Group::plan_cluster() {
   CK(cudaSetDevice(device));
   int optin = 0;
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  optin -= 256;                                // the kernel's static shared memory
   const int budget = cl_piece_kb > 0 ? std::min(optin, cl_piece_kb * 1024) : optin;
   const int n = (int)tanks.size();
   std::vector<int> m(n), np(n);
-  int K = 1, smem = 16;
   for (int i = 0; i < n; ++i) {
     const TankDev& D = tanks[i]->d;
-    const int npm = (budget - 32) / cluster_plane_bytes(D);     // the field and the work counters
+    int npm = 0;                              // the most planes whose piece fits the budget
+    while (npm < D.nz && cluster_smem_bytes(D, npm + 1) <= budget) ++npm;
     if (npm < 1) throw Error(-1, "cluster solve: one z plane of a tank does not fit a CTA's shared memory");
     int mi = (D.nz + npm - 1) / npm;
     np[i] = (D.nz + mi - 1) / mi;
     m[i] = (D.nz + np[i] - 1) / np[i];
     if (m[i] > kClusterMax) throw Error(-1, "cluster solve: a tank needs more than 16 CTAs");
-    K = std::max(K, m[i]);
-    smem = std::max(smem, cluster_smem_bytes(D, np[i]));
   }
   CK(sor_cluster_prepare(optin, kClusterMax));
-  if (sor_cluster_max_active(smem, K) < 1) throw Error(-1, "cluster solve: the device cannot hold one cluster of this size");
-  std::vector<int> order(n);
-  for (int i = 0; i < n; ++i) order[i] = i;
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return m[a] > m[b]; });
-  std::vector<std::vector<int>> bins;
-  std::vector<int> fill;
-  for (int i : order) {
-    size_t b = 0;
-    while (b < bins.size() && fill[b] + m[i] > K) ++b;
-    if (b == bins.size()) { bins.emplace_back(); fill.push_back(0); }
-    bins[b].push_back(i);
-    fill[b] += m[i];
-  }
   std::vector<ClusterPiece> pcs;
-  for (const auto& bin : bins) {
-    for (int i : bin)
-      for (int p = 0; p < m[i]; ++p) {
+  std::vector<ClusterClass> classes;
+  for (int size = 1; size <= kClusterMax; ++size) {
+    ClusterClass c;
+    c.size = size;
+    c.first = (int)pcs.size();
+    c.smem = 16;
+    for (int i = 0; i < n; ++i) {
+      if (m[i] != size) continue;
+      for (int p = 0; p < size; ++p) {
         const int k0 = p * np[i];
         pcs.push_back(ClusterPiece{i, k0, std::min(np[i], tanks[i]->d.nz - k0), np[i]});
       }
-    while (pcs.size() % K) pcs.push_back(ClusterPiece{-1, 0, 0, 0});
+      c.smem = std::max(c.smem, cluster_smem_bytes(tanks[i]->d, np[i]));
+    }
+    c.blocks = (int)pcs.size() - c.first;
+    if (!c.blocks) continue;
+    if (sor_cluster_max_active(c.smem, size) < 1)
+      throw Error(-1, "cluster solve: the device cannot hold one cluster of " + std::to_string(size) + " CTAs");
+    classes.push_back(c);
   }
+  drop_cluster_classes();
   if (d_pieces) CK(cudaFreeAsync(d_pieces, stream));
   CK(cudaMallocAsync((void**)&d_pieces, pcs.size() * sizeof(ClusterPiece), stream));
   CK(cudaMemcpyAsync(d_pieces, pcs.data(), pcs.size() * sizeof(ClusterPiece), cudaMemcpyHostToDevice, stream));
   CK(cudaStreamSynchronize(stream));
-  cl_blocks = (int)pcs.size();
-  cl_size = K;
-  cl_smem = smem;
+  if (classes.size() > 1) {
+    if (!cl_fork) CK(cudaEventCreateWithFlags(&cl_fork, cudaEventDisableTiming));
+    for (ClusterClass& c : classes) {
+      CK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
+    }
+  }
+  cl_classes = classes;
 }
 
 Batch::Batch(const std::vector<Tank*>& t) {
@@ -1209,7 +1224,22 @@ void Group::enqueue_body() {
     if (nl & 1) launch_sor_copy(ctx);
     CK(cudaGetLastError());
   } else if (sor_mode == 4) {
-    if (max_iters > 0) launch_sor_cluster(ctx, d_pieces, cl_blocks, cl_smem, cl_size, max_iters);
+    if (max_iters > 0) {
+      if (cl_classes.size() == 1) {
+        const ClusterClass& c = cl_classes[0];
+        launch_sor_cluster(ctx, d_pieces, c.blocks, c.smem, c.size, max_iters);
+      } else {
+        CK(cudaEventRecord(cl_fork, stream));
+        for (const ClusterClass& c : cl_classes) {
+          CK(cudaStreamWaitEvent(c.stream, cl_fork, 0));
+          LaunchCtx L = ctx;
+          L.stream = c.stream;
+          launch_sor_cluster(L, d_pieces + c.first, c.blocks, c.smem, c.size, max_iters);
+          CK(cudaEventRecord(c.done, c.stream));
+          CK(cudaStreamWaitEvent(stream, c.done, 0));
+        }
+      }
+    }
     CK(cudaGetLastError());
   } else {
     for (int it = 0; it < max_iters; ++it) {

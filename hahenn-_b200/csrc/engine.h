@@ -168,7 +168,14 @@ struct Group {
   unsigned watchdog_polls = kWatchdogPolls;   // polls of a bounded device wait before it gives up (tanks' min)
   // cluster-resident solve (sor_mode 4): the CTA plan, planned by plan_cluster when tuned to it
   ClusterPiece* d_pieces = nullptr;
-  int cl_blocks = 0, cl_size = 1, cl_smem = 0;
+  struct ClusterClass {           // the tanks cut into `size` pieces: one launch of clusters of that size
+    int size = 1, blocks = 0, smem = 0, first = 0;   // first = offset of its pieces in d_pieces
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+  };
+  std::vector<ClusterClass> cl_classes;
+  cudaEvent_t cl_fork = nullptr;
+  void drop_cluster_classes();
   int cl_piece_kb = 0;            // shared memory per CTA at most (tile knob; 0: the device maximum)
   void plan_cluster();            // throws if a tank cannot be held by one cluster
   bool residual = false;          // FP64 residual of every solve into the tank counters

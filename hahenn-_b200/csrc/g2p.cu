@@ -118,8 +118,9 @@ __device__ __forceinline__ void transfer_from(const TankDev& T, const F& faces, 
     sw += w;
   }
   if (sw >= 1e-6f) {
-    pic = (double)(sn / sw);
-    flip = vp + (double)((sn - so) / sw);
+    const float rw = __frcp_rn(sw);         // one reciprocal for both quotients (float32, held to tolerance)
+    pic = (double)(sn * rw);
+    flip = vp + (double)((sn - so) * rw);
   } else {
     pic = vp;
     flip = vp;

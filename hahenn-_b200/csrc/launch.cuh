@@ -81,7 +81,6 @@ void tbl_assign(LaunchCtx& L, void* base, int tiles);                    // poin
 // cluster-resident solve (one launch per solve; each tank's field held in one cluster's shared memory)
 constexpr int kClusterMax = 16;                                          // CTAs per cluster (non-portable above 8)
 int cluster_smem_bytes(const TankDev& D, int np);                        // shared bytes of a piece of np planes
-int cluster_plane_bytes(const TankDev& D);                               // shared bytes of one z plane
 cudaError_t sor_cluster_prepare(int smem_bytes, int cluster);            // once per device, outside capture
 int sor_cluster_max_active(int smem_bytes, int cluster);                 // co-resident clusters (0: cannot launch)
 void launch_sor_cluster(const LaunchCtx& L, const ClusterPiece* pieces, int nblocks, int smem_bytes, int cluster,

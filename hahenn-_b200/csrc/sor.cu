@@ -25,6 +25,8 @@
 //                  an error in the tank counters and every block returns.
 //   k_sor_tbl      two sweeps per launch over per-tile lists of active cells (temporal blocking)
 //   k_sor_tb<4>    four sweeps per launch on shared-memory tiles with halos
+#include <type_traits>
+
 #include "launch.cuh"
 
 namespace suiri {
@@ -71,6 +73,23 @@ __device__ __forceinline__ float coeff_inv(bool cut, unsigned open6, const float
   const int n = __popc(open6 & 0x3Fu);
   return n == 1 ? 1.f : n == 2 ? 0.5f : n == 3 ? 0x1.555556p-2f : n == 4 ? 0.25f : n == 5 ? 0x1.99999ap-3f
        : n == 6 ? 0x1.555556p-3f : __frcp_rn(0.f);
+}
+
+// The update of a cell without cut faces, whose coefficients are 0 or 1 (the open bits): each product C·p_nb
+// is p_nb or a zero, so num is the sum of the open neighbours taken in the same order, with zeros where a face
+// is closed. It equals sor_update's bit for bit: the products are exact, and a zero product of the reference
+// can differ only in its sign, which no sum of these values carries to the result (no pressure is -0: the
+// solve starts from +0 or a previous result, and a round-to-nearest sum is -0 only if both terms are).
+__device__ __forceinline__ float sor_update_open(uint32_t open6, const float nb[6], float rhs, float p, float omega,
+                                                 float inv) {
+  float num = (open6 & 1u) ? nb[0] : 0.f;
+#pragma unroll
+  for (int d = 1; d < 6; ++d) num = __fadd_rn(num, (open6 >> d) & 1u ? nb[d] : 0.f);
+  float r = __fsub_rn(num, rhs);
+  r = __fmul_rn(r, inv);
+  r = __fsub_rn(r, p);
+  r = __fmul_rn(r, omega);
+  return __fadd_rn(p, r);
 }
 
 // the six face coefficients of a cut cell: its own x, y, z face fractions and those of the +x, +y, +z
@@ -721,22 +740,28 @@ void launch_sor_copy(const LaunchCtx& L) {
 // ---------------------------------------------------------------------------- cluster-resident solve
 // The whole solve in one launch, each tank held on chip by one thread-block cluster: the tank is cut into
 // pieces of whole z planes, one piece per CTA, and each CTA keeps its planes' pressure (both colours),
-// right-hand side and a one-byte cell code in shared memory for all 2·iters colour sweeps. A sweep relaxes
-// the CTA's cells of one colour from the other colour's values; the z neighbours of a piece's first and last
-// plane sit in the neighbouring CTAs of the cluster and are read through distributed shared memory
-// (mapa + ld.shared::cluster). The hardware cluster barrier (barrier.cluster arrive.release / wait.acquire)
-// separates the sweeps: no global memory and no launch between them. Small tanks share a cluster (each
-// piece only reads the pieces of its own tank), and every CTA takes part in every barrier of its cluster.
-// The update is sor_update in the same colour order, so the pressures equal one launch per sweep bit for
-// bit. Shared layout per CTA, S = hx·ny·np slots per colour (np = the tank's planes per piece, so every
-// piece of a tank has the same offsets): pressure [2][S] f32, rhs [2][S] f32, code [2][S] u8 (bits 0-5 open
-// faces, 6 cut cell, 7 active).
+// right-hand side and a one-byte cell code in shared memory for all 2·iters colour sweeps. No global memory
+// and no launch between sweeps; the hardware cluster barrier (barrier.cluster arrive.release / wait.acquire)
+// separates them. Small tanks share a cluster (a piece only talks to the pieces of its own tank), and every
+// CTA takes part in every barrier of its cluster.
+//
+// The pressure of a piece is stored padded: each row of a colour has a zero slot before and after it, each
+// plane a zero row below and above, and the piece a ghost plane below and above. Outside the tank the
+// padding holds 0, which is what the reference's zero-padded pressure reads there (solver.py:489-506), so a
+// cell's six neighbours are six loads at fixed offsets with no tests. A ghost plane next to another piece
+// holds that piece's boundary plane: loaded from global memory at the start, then written by the neighbour
+// (st.shared::cluster into this CTA's shared memory) each time it relaxes that plane. Sweep order per CTA:
+// wait (the neighbours' boundary planes of the previous sweep, with their pushes, are complete), relax the
+// boundary planes and push them, arrive, relax the interior planes (their neighbours are all in this
+// piece), CTA barrier. A piece's ghost plane is rewritten only after the neighbour has passed the wait that
+// follows every read of it. The update is sor_update's in the same colour order: the pressures equal one
+// launch per sweep bit for bit.
+//
+// Shared layout per CTA (W = hx + 2, RY = ny + 2, NP = np + 2, np = the tank's planes per piece, the same
+// for all its pieces): pressure [2][NP·RY·W] f32 padded; rhs [2][np·ny·hx] f32 and code [2][np·ny·hx] u8
+// (bits 0-5 open faces, 6 cut cell, 7 active) unpadded; the sweeps' work counters.
 constexpr int kClusterThreads = 1024;
-constexpr int kClusterBytesPerSlot = 9;
 
-__device__ __forceinline__ void cluster_barrier() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
 __device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
 __device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
 
@@ -746,15 +771,24 @@ __device__ __forceinline__ unsigned cluster_ctarank() {
   return r;
 }
 
-// the float at the same shared-memory offset as `local` in the CTA of cluster rank `rank`
-__device__ __forceinline__ float ld_cluster(const float* local, unsigned rank) {
+// store v at the same shared-memory offset as `local` in the CTA of cluster rank `rank`
+__device__ __forceinline__ void st_cluster(float* local, unsigned rank, float v) {
   const unsigned a = (unsigned)__cvta_generic_to_shared(local);
   unsigned ra;
-  float v;
   asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(a), "r"(rank));
-  // volatile keeps the load between the cluster barriers around it (those carry the memory clobber)
-  asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(ra));
-  return v;
+  asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(ra), "f"(v) : "memory");
+}
+
+struct ClusterLayout {
+  int W, RY, PS, US;          // padded row width, padded rows per plane, padded and unpadded slots per colour
+};
+__host__ __device__ __forceinline__ ClusterLayout cluster_layout(int hx, int ny, int np) {
+  ClusterLayout c;
+  c.W = hx + 2;
+  c.RY = ny + 2;
+  c.PS = (np + 2) * c.RY * c.W;
+  c.US = np * ny * hx;
+  return c;
 }
 
 __global__ void __launch_bounds__(kClusterThreads, 1) k_sor_cluster(const TankDev* __restrict__ tanks,
@@ -764,118 +798,129 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_sor_cluster(const TankDe
   const bool on = pc.tank >= 0;
   const TankDev& T = tanks[on ? pc.tank : 0];
   const int hx = T.hx, nx = T.nx, ny = T.ny, nz = T.nz;
-  const int plane = hx * ny;
-  const int S = plane * pc.np, U = on ? plane * pc.nk : 0;
-  const size_t g0 = (size_t)plane * pc.k0;      // first slot of the piece in each colour's global array
+  const int k0 = pc.k0, nk = on ? pc.nk : 0, np_ = on ? pc.np : 0;
+  const ClusterLayout G = cluster_layout(hx, ny, np_);
+  const int W = G.W, RY = G.RY, PS = on ? G.PS : 0, US = on ? G.US : 0;
+  const int U = nk * ny * hx;                         // this piece's own slots per colour
   const size_t nh = T.nhalf;
-  float* sp = reinterpret_cast<float*>(cl_smem);
-  float* sr = sp + 2 * S;
-  uint8_t* sc = reinterpret_cast<uint8_t*>(sr + 2 * S);
-  // work counters of the sweeps (two sets, used by alternate sweeps): behind the field, see cluster_smem_bytes
-  int* s_cnt = reinterpret_cast<int*>(cl_smem + ((18 * S + 15) & ~15));
+  float* sp = reinterpret_cast<float*>(cl_smem);     // [2][PS]
+  float* sr = sp + 2 * PS;                           // [2][US]
+  int* s_cnt = reinterpret_cast<int*>(sr + 2 * US);  // [8]
+  uint8_t* sc = reinterpret_cast<uint8_t*>(s_cnt + 8);   // [2][US]
   const unsigned rank = cluster_ctarank();
-  if (threadIdx.x < 6) s_cnt[threadIdx.x] = 0;
+  if (threadIdx.x < 8) s_cnt[threadIdx.x] = 0;
+  // pressure of the own planes and the ghost planes, zero in the padding and outside the tank
+  for (int q = threadIdx.x; q < 2 * PS; q += kClusterThreads) {
+    const int c = q >= PS, L = q - c * PS;
+    const int tp = L % W, rest = L / W, jp = rest % RY, kl = rest / RY - 1;
+    const int ti = tp - 1, j = jp - 1, k = k0 + kl;
+    float v = 0.f;
+    if (ti >= 0 && ti < hx && j >= 0 && j < ny && kl <= nk && k >= 0 && k < nz)
+      v = T.pres[c * nh + ti + (size_t)hx * (j + (size_t)ny * k)];
+    sp[q] = v;
+  }
+  const size_t g0 = (size_t)hx * ny * k0;            // first slot of the piece in each colour's global array
   for (int q = threadIdx.x; q < 2 * U; q += kClusterThreads) {
     const int c = q >= U, l = q - c * U;
     const size_t g = c * nh + g0 + l;
     const uint32_t cd = T.code[g];
-    sp[c * S + l] = T.pres[g];
-    sr[c * S + l] = T.rhs[g];
-    sc[c * S + l] = (uint8_t)((cd & 0x3Fu) | ((cd & kCodePartial) ? 0x40u : 0u) | ((cd & kCodeActive) ? 0x80u : 0u));
+    sr[c * US + l] = T.rhs[g];
+    sc[c * US + l] = (uint8_t)((cd & 0x3Fu) | ((cd & kCodePartial) ? 0x40u : 0u) | ((cd & kCodeActive) ? 0x80u : 0u));
   }
   const int iters = on ? T.iters : 0;
   const float omega = T.omega;
-  const DivU dhx = T.dhx, dny = T.dny;
-  const int k0 = pc.k0, nk = pc.nk, np_ = pc.np;
-  struct Cell {
-    float nb[6], C[6], inv, rhs, p;
-    int l;
-    bool on;
-  };
-  // everything one update reads
-  auto prep = [&](const float* po, const float* pw, const float* rw, const uint8_t* cw, int c, int l, int lend, Cell& x) {
-    x.on = false;
-    x.l = l;
-    if (l >= lend) return;
-    const uint32_t cd = cw[l];
-    if (!(cd & 0x80u)) return;
-    x.on = true;
-    const int row = divu(l, dhx), ti = l - row * hx;
-    const int kl = divu(row, dny), j = row - kl * ny, k = k0 + kl;
-    const int i = 2 * ti + ((j + k + c) & 1);
-    const int rowb = l - ti;
-    x.nb[0] = i > 0 ? po[((i - 1) >> 1) + rowb] : 0.f;
-    x.nb[1] = i + 1 < nx ? po[((i + 1) >> 1) + rowb] : 0.f;
-    x.nb[2] = j > 0 ? po[l - hx] : 0.f;
-    x.nb[3] = j + 1 < ny ? po[l + hx] : 0.f;
-    x.nb[4] = k == 0 ? 0.f : (kl > 0 ? po[l - plane] : ld_cluster(po + l + plane * (np_ - 1), rank - 1));
-    x.nb[5] = k + 1 >= nz ? 0.f : (kl + 1 < nk ? po[l + plane] : ld_cluster(po + (l - plane * kl), rank + 1));
-    x.rhs = rw[l];
-    x.p = pw[l];
-    if (cd & 0x40u) {
-      cut_coeffs(T, i, j, k, x.C);
-    } else {
-#pragma unroll
-      for (int d = 0; d < 6; ++d) x.C[d] = (cd >> d) & 1u ? 1.0f : 0.0f;
-    }
-    x.inv = coeff_inv(cd & 0x40u, cd, x.C);
-  };
-  // The planes whose z neighbours sit in another CTA (the first plane unless the piece starts the tank, the
-  // last unless it ends it) are relaxed first, between the cluster barrier's wait (the neighbours' planes of
-  // the previous sweep are complete) and its arrive (this piece's are); the interior planes read only this
-  // CTA's shared memory and are relaxed after the arrive, so the barrier's latency overlaps them, and a CTA
-  // barrier makes them visible to the next sweep. A neighbour reads this piece's boundary planes only before
-  // its own arrive, so they are not overwritten while it reads them.
-  const int lo_b = (on && k0 > 0) ? plane : 0;                         // [0, lo_b): first plane, remote below
-  const int hi_b = (on && k0 + nk < nz && !(lo_b && nk == 1)) ? U - plane : U;   // [hi_b, U): last plane, remote above
-  // Warps take 32-slot chunks of a range from a shared counter until it runs out, so that warps whose chunks
-  // hold few liquid cells (the upper rows of a plane) take more of them and the barrier waits for no one.
+  const DivU dny = T.dny;
+  const bool below = on && k0 > 0, above = on && k0 + nk < nz;   // neighbour pieces (remote planes)
+  // rows [0, lo_r): first plane (it reads and feeds the piece below); [hi_r, nk·ny): last plane (the piece
+  // above); [lo_r, hi_r): interior. A single plane with neighbours on both sides is the first range.
+  const int lo_r = below ? ny : 0;
+  const int hi_r = (above && !(below && nk == 1)) ? (nk - 1) * ny : nk * ny;
+  // a warp's chunk: 32/hx whole rows (hx ≤ 32; lanes past them idle), or a 32-slot part of a row
   const int lane = threadIdx.x & 31;
-  auto relax = [&](const float* po, float* pw, const float* rw, const uint8_t* cw, int c, int l0, int l1, int* ctr) {
-    const int nch = (l1 - l0 + 31) >> 5;
+  const bool narrow = hx <= 32;
+  const int rpc = narrow ? 32 / hx : 1, cpr = narrow ? 1 : (hx + 31) / 32;
+  const int my_r = narrow ? lane / hx : 0, my_t = narrow ? lane % hx : lane;
+  const int ghost_above_plane = np_ + 1;             // the piece below stores this piece's first plane here
+  // 1/n for the cells without cut faces, n their open faces (the correctly rounded reciprocals)
+  __shared__ float s_inv[8];
+  if (threadIdx.x < 8) s_inv[threadIdx.x] = threadIdx.x ? __frcp_rn((float)threadIdx.x) : 0.f;
+  auto relax = [&](auto push, int c, int r0, int r1, int* ctr) {
+    const float* po = sp + (1 - c) * PS;
+    float* pw = sp + c * PS;
+    const float* rw = sr + c * US;
+    const uint8_t* cw = sc + c * US;
+    const int nch = narrow ? (r1 - r0 + rpc - 1) / rpc : (r1 - r0) * cpr;
 #pragma unroll 1
     while (true) {
       int ch = 0;
       if (lane == 0) ch = atomicAdd(ctr, 1);
       ch = __shfl_sync(0xffffffffu, ch, 0);
       if (ch >= nch) break;
-      Cell a;
-      prep(po, pw, rw, cw, c, l0 + (ch << 5) + lane, l1, a);
-      if (a.on) pw[a.l] = sor_update_inv(a.C, a.nb, a.rhs, a.p, omega, a.inv);
+      const int row = r0 + (narrow ? ch * rpc + my_r : ch / cpr);
+      const int ti = narrow ? my_t : (ch % cpr) * 32 + lane;
+      if ((narrow && my_r >= rpc) || ti >= hx || row >= r1) continue;
+      const int l = row * hx + ti;
+      const uint32_t cd = cw[l];
+      if (!(cd & 0x80u)) continue;
+      const int kl = divu(row, dny), j = row - kl * ny, k = k0 + kl;
+      const int s = (j + k + c) & 1;
+      const int L = (ti + 1) + W * ((j + 1) + RY * (kl + 1));
+      float nb[6];
+      nb[0] = po[L - 1 + s];
+      nb[1] = po[L + s];
+      nb[2] = po[L - W];
+      nb[3] = po[L + W];
+      nb[4] = po[L - W * RY];
+      nb[5] = po[L + W * RY];
+      const float rhs = rw[l], p = pw[L];
+      float v;
+      if (cd & 0x40u) {
+        float C[6];
+        cut_coeffs(T, 2 * ti + s, j, k, C);
+        v = sor_update_inv(C, nb, rhs, p, omega, coeff_inv(true, cd, C));
+      } else {
+        v = sor_update_open(cd, nb, rhs, p, omega, s_inv[__popc(cd & 0x3Fu)]);
+      }
+      pw[L] = v;
+      if (push) {
+        if (kl == 0 && below) st_cluster(pw + (ti + 1) + W * ((j + 1) + RY * ghost_above_plane), rank - 1, v);
+        if (kl == nk - 1 && above) st_cluster(pw + (ti + 1) + W * (j + 1), rank + 1, v);
+      }
     }
   };
+  const std::true_type with_push;
+  const std::false_type no_push;
   cluster_arrive();                       // this piece is loaded
   for (int it = 0; it < max_iters; ++it) {
 #pragma unroll 1
     for (int c = 0; c < 2; ++c) {
       const bool go = it < iters;
-      const float* po = sp + (1 - c) * S;
-      float* pw = sp + c * S;
-      const float* rw = sr + c * S;
-      const uint8_t* cw = sc + c * S;
-      int* ctr = s_cnt + 3 * c;           // this sweep's counters; the other set is zeroed for the next sweep
-      if (threadIdx.x < 3) s_cnt[3 * (1 - c) + threadIdx.x] = 0;
+      int* ctr = s_cnt + 4 * c;           // this sweep's counters; the other set is zeroed for the next sweep
+      if (threadIdx.x < 3) s_cnt[4 * (1 - c) + threadIdx.x] = 0;
       cluster_wait();
       if (go) {
-        relax(po, pw, rw, cw, c, 0, lo_b, ctr);
-        relax(po, pw, rw, cw, c, hi_b, U, ctr + 1);
+        relax(with_push, c, 0, lo_r, ctr);
+        relax(with_push, c, hi_r, nk * ny, ctr + 1);
       }
       cluster_arrive();
-      if (go) relax(po, pw, rw, cw, c, lo_b, hi_b, ctr + 2);
+      if (go) relax(no_push, c, lo_r, hi_r, ctr + 2);
       __syncthreads();
     }
   }
-  cluster_wait();                         // no neighbour reads this piece's shared memory any more
+  cluster_wait();                         // no neighbour writes this piece's ghost planes any more
   for (int q = threadIdx.x; q < 2 * U; q += kClusterThreads) {
     const int c = q >= U, l = q - c * U;
-    T.pres[c * nh + g0 + l] = sp[c * S + l];
+    const int row = divu(l, T.dhx), ti = l - row * hx;
+    const int kl = divu(row, dny), j = row - kl * ny;
+    T.pres[c * nh + g0 + l] = sp[c * PS + (ti + 1) + W * ((j + 1) + RY * (kl + 1))];
   }
 }
 
-int cluster_plane_bytes(const TankDev& D) { return kClusterBytesPerSlot * 2 * D.hx * D.ny; }
-
-// the field of np planes (9 B per slot of both colours) and the sweeps' six work counters
-int cluster_smem_bytes(const TankDev& D, int np) { return ((cluster_plane_bytes(D) * np + 15) & ~15) + 32; }
+// shared bytes of a piece of np planes: padded pressure, rhs, the work counters and the codes
+int cluster_smem_bytes(const TankDev& D, int np) {
+  const ClusterLayout G = cluster_layout(D.hx, D.ny, np);
+  return ((8 * G.PS + 8 * G.US + 32 + 2 * G.US) + 15) & ~15;
+}
 
 cudaError_t sor_cluster_prepare(int smem_bytes, int cluster) {
   cudaError_t e = cudaFuncSetAttribute(k_sor_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);

@@ -365,10 +365,10 @@ def test_solve_forms_equal_per_sweep_launches(pkg, mode):
         np.testing.assert_array_equal(a, b)
 
 
-@pytest.mark.parametrize('piece_kb', [8, 16, 40])
+@pytest.mark.parametrize('piece_kb', [11, 21, 46])
 def test_cluster_solve_pieces_across_ctas(pkg, piece_kb):
-    """The cluster-resident solve with less shared memory per CTA, so the 32×16×16 tank is cut into
-    pieces of 1 z plane (16 CTAs, every z neighbour read from another CTA's shared memory), 3 planes (six
+    """The cluster-resident solve with less shared memory per CTA, so the 32×16×16 tank is cut into pieces
+    of 1 z plane (16 CTAs: every plane's z neighbours are ghost planes pushed by the next CTAs), 3 planes (six
     pieces, the last of one plane) and 8 planes (two): bit for bit the per-sweep launches."""
     w = pkg.workloads.obstacles_inflow(scale=4)
     assert (w['nx'], w['ny'], w['nz']) == (32, 16, 16)
@@ -563,9 +563,11 @@ def test_rectangular_ripple_layer_full_scene_quarter(pkg):
         assert np.abs(layer.S).max() > 0
         assert_close_field(S[..., 0], layer.S.real, rtol=1e-4, what=f'burst {f}: ripple state (height)')
         assert_close_field(S[..., 1], layer.S.imag, rtol=1e-4, what=f'burst {f}: ripple state (velocity)')
+        # the field is the inverse FFT of the state: errors at 1e-4 of the state's largest mode add up over the
+        # 512×256 modes to a few 1e-4 of the field's largest value at single vertices
         fld = gpu.ripple_field(pkg.native.FIELD_RIPPLE, (Rz + 1, Rx + 1, 3), np.float32)
         for c in range(3):
-            assert_close_field(fld[..., c], layer.field[..., c], rtol=1e-4, atol=1e-12, what=f'burst {f}: field {c}')
+            assert_close_field(fld[..., c], layer.field[..., c], rtol=1e-3, atol=1e-12, what=f'burst {f}: field {c}')
     gpu.close()
 
 
@@ -637,3 +639,37 @@ def test_g2p_brick_form_equals_the_walk(pkg, advect):
     for x, y in zip(walk[:4], brick[:4]):
         np.testing.assert_array_equal(x, y)
     assert walk[4:] == brick[4:]
+
+
+def test_moving_obstacles_solid_velocity_and_collisions(pkg):
+    """A sphere moving at 0.4 m/s along x and a turned box spinning at 3 rad/s about the vertical axis (the
+    solid velocity that setObjects gives moving obstacles, src/js/30-wgsl-sim.js:96-106, solver.py:153-165),
+    analytic shapes, in a pool stirred at random: face fractions bit-exact; P2G velocity, the projected
+    velocity (closed faces take the nearest obstacle's velocity, and the cut faces' fluxes carry it into the
+    divergence), pressure and particles (collisions rebound relative to the moving surface) within the parity
+    tolerances, over two sub-steps."""
+    from oracle import sdf as sdfm
+    nx, ny, nz, h = 32, 16, 24, 1 / 32
+    objs = [sdfm.make_obstacle('sphere', [0.1, 0.2, 0.0], lin=(0.4, 0.0, 0.0), r=0.08),
+            sdfm.make_obstacle('box', [-0.22, 0.12, 0.1], (0, 20, 0), ang=(0.0, 3.0, 0.0), w=0.12, h=0.1, d=0.08)]
+    gpu = gpu_from(pkg, nx, ny, nz, h, flip=0.95, omega=1.7, iters=30)
+    gpu.set_obstacles([dict(type=o['type'], flag=1, pos=o['pos'], rot=o['rot'], dims=o['dims'], lin=o['lin'],
+                            ang=o['ang']) for o in objs])
+    ora = oracle_from(nx, ny, nz, h, gpu.origin, flip=0.95, omega=1.7, iters=30)
+    ora.set_objects(objs)
+    cells = pkg.workloads.block_cells(nx, ny, nz, lambda i, j, k: j < 10)
+    pos = pkg.workloads.fill_cells(cells, h, gpu.origin, 8, 3)
+    pos = pos[ora.sdf_at(pos.astype(np.float64)) > 0.3 * h]          # particles outside the obstacles
+    vel = (np.random.default_rng(8).random(pos.shape) - 0.5).astype(np.float32)
+    gpu.add_particles(pos, vel)
+    ora.add_particles(f32(pos), f32(vel))
+    for s in (1, 2):
+        gpu.substep(1 / 240)
+        ora.frame = s
+        ora.substep(1 / 240)
+        g = compare_substep(pkg, gpu, ora, f'moving obstacles, sub-step {s}')
+        np.testing.assert_array_equal(g['frac'], ora.frac.astype(np.float32))
+        closed = ora.frac <= 0
+        assert np.abs(ora.svel[closed]).max() > 0.1                  # the solids' velocity reaches the faces
+        sync_oracle_particles(gpu, ora)
+    gpu.close()

@@ -47,16 +47,16 @@ class FakeTarget:
 
 def test_autotune_keeps_the_fastest_and_skips_shapes_that_fail():
     table = {c + (f,): 5.0 for c in autotune.CANDIDATES for f in autotune.G2P_FORMS}
-    table[(2, 4, 112, 0)] = 3.0
-    table[(2, 4, 112, 1)] = 2.5          # the brick G2P form is faster with the best solve shape
+    table[(2, 4, 128, 0)] = 3.0
+    table[(2, 4, 128, 1)] = 2.5          # the brick G2P form is faster with the best solve shape
     table[(4, 0, 0, 1)] = 1.0            # never timed: G2P forms are tried with the best shape only
     table[(4, 1, 0, 0)] = None
     t = FakeTarget(table)
     t.substeps = 7
     best, timings = autotune.autotune(t, 1 / 240)
-    assert best == (2, 4, 112, 1) and t.key() == (2, 4, 112, 1)
-    assert timings[(4, 1, 0, 0)] == float('inf') and timings[(2, 4, 112, 0)] == pytest.approx(3.0)
-    assert set(timings) == {c + (0,) for c in autotune.CANDIDATES} | {(2, 4, 112, 1)}
+    assert best == (2, 4, 128, 1) and t.key() == (2, 4, 128, 1)
+    assert timings[(4, 1, 0, 0)] == float('inf') and timings[(2, 4, 128, 0)] == pytest.approx(3.0)
+    assert set(timings) == {c + (0,) for c in autotune.CANDIDATES} | {(2, 4, 128, 1)}
     assert t.substeps == 7              # the tuning sub-steps were rolled back
     assert {c[1] for c in autotune.CANDIDATES} >= {0, 1, 2, 3, 4}
     assert len({c[2] for c in autotune.CANDIDATES if c[1] == 4}) >= 3     # tile sizes of the cluster solve
