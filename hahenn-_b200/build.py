@@ -4,7 +4,7 @@
 
 Objects go to hahenn-_b200/_build/, the library to hahenn-_b200/libsuiri_cuda.so. The files whose results
 are compared bit for bit (binning, obstacle geometry and face fractions, the cell pass and the pressure
-solve, the emitters and the distance queries) are built without FMA contraction (-fmad=false), so that their
+solve, the emitters, the distance queries and the surface mesh) are built without FMA contraction (-fmad=false), so that their
 float64 geometry and float32 pressure arithmetic round exactly as written; the grid-to-particle pass and the
 ripple layer, held to tolerances, let the compiler contract.
 """
@@ -20,7 +20,8 @@ BUILD = os.path.join(HERE, '_build')
 NVCC = os.environ.get('NVCC', 'nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 FLAGS = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC,-O3', '--expt-relaxed-constexpr']
-SOURCES = ['bin.cu', 'grid.cu', 'sor.cu', 'g2p.cu', 'ripple.cu', 'engine.cu', 'scene.cpp', 'server.cpp', 'capi.cpp']
+SOURCES = ['bin.cu', 'grid.cu', 'sor.cu', 'g2p.cu', 'ripple.cu', 'mesh.cu', 'engine.cu', 'scene.cpp', 'server.cpp',
+           'capi.cpp']
 CONTRACTED = {'g2p.cu', 'ripple.cu'}      # tolerance-checked results: FMA contraction allowed
 
 

@@ -158,6 +158,8 @@ void fill_stats(Tank& t, const Counters& c, suiri_stats* s) {
   s->residual_max = rmax;
   s->rhs_max = hmax;
   s->residual_rms = s->active_cells > 0 ? sqrt(c.res_sum2 / (double)s->active_cells) : 0.0;
+  s->ripple_rx = std::max(t.d.rx, 0); s->ripple_rz = std::max(t.d.rz, 0);
+  s->wmap = t.cfg.wmap;
 }
 }  // namespace
 
@@ -233,6 +235,7 @@ TankConfig make_config(const suiri_params& p, const char* scene_json, Scene& sc)
     else if (p.ripple_rx == 0 && p.ripple_rz == 0) { c.rx = c.rz = q.ripple; }
     else { c.rx = p.ripple_rx; c.rz = p.ripple_rz; }
     c.wmap = p.wmap > 0 ? p.wmap : q.wmap;
+    if (c.wmap > 8192) throw Error(SUIRI_ERR_INVALID, "wmap at most 8192 texels a side");
     c.sdf_mode = p.sdf_mode;
     c.device = p.device;
     c.seed = p.seed;
@@ -424,6 +427,13 @@ int suiri_step(suiri_tank* h, double frame_dt, int32_t* substeps) {
   });
 }
 
+int suiri_frame_end(suiri_tank* h, double frame_dt) {
+  return guard(h ? &h->err : nullptr, [&] {
+    if (!(frame_dt > 0) || !std::isfinite(frame_dt)) throw Error(SUIRI_ERR_INVALID, "frame_dt must be positive");
+    T(h)->frame_end(frame_dt);
+  });
+}
+
 int suiri_sync(suiri_tank* h) {
   return guard(h ? &h->err : nullptr, [&] { CK(cudaStreamSynchronize(T(h)->stream)); });
 }
@@ -450,6 +460,35 @@ int suiri_read_grid(suiri_tank* h, int32_t field, void* out, size_t bytes) {
   return guard(h ? &h->err : nullptr, [&] {
     if (!out) throw Error(SUIRI_ERR_INVALID, "null output");
     T(h)->read_grid(field, out, bytes);
+  });
+}
+
+int suiri_frame_maps(suiri_tank* h, const double sun_dir[3], float* out, size_t bytes) {
+  return guard(h ? &h->err : nullptr, [&] {
+    if (!sun_dir || !out) throw Error(SUIRI_ERR_INVALID, "null sun direction or output");
+    frame_maps(*T(h), sun_dir, out, bytes);
+  });
+}
+
+int suiri_surface_mesh(suiri_tank* h, double smooth, suiri_mesh_info* info) {
+  return guard(h ? &h->err : nullptr, [&] {
+    if (!info) throw Error(SUIRI_ERR_INVALID, "null mesh info");
+    if (!(smooth > 0) || smooth > 6.0) throw Error(SUIRI_ERR_INVALID, "smooth (blur sigma in lattice nodes) in (0, 6]");
+    const MeshInfo m = build_surface_mesh(*T(h), smooth);
+    memset(info, 0, sizeof(*info));
+    info->verts = m.verts; info->quads = m.quads; info->tris = m.tris;
+    info->body_verts = m.body_verts; info->lone = m.lone;
+    for (int a = 0; a < 3; ++a) { info->lattice[a] = m.lattice[a]; info->lo[a] = m.lo[a]; }
+    info->taps = m.taps;
+    info->spacing = m.spacing; info->smooth = m.smooth;
+    for (int k = 0; k < m.taps && k < 33; ++k) info->weights[k] = m.weights[k];
+  });
+}
+
+int suiri_surface_mesh_read(suiri_tank* h, float* verts, float* vel, int32_t* quads, int32_t* tris, int64_t max_verts,
+                            int64_t max_quads, int64_t max_tris) {
+  return guard(h ? &h->err : nullptr, [&] {
+    read_surface_mesh(*T(h), verts, vel, quads, tris, max_verts, max_quads, max_tris);
   });
 }
 

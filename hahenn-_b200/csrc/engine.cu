@@ -332,6 +332,7 @@ Tank::~Tank() {
   if (stream) cudaStreamSynchronize(stream);
   if (snap.p) { cudaFree(snap.p); cudaFree(snap.v); cudaFree(snap.wp); cudaFree(snap.wv); cudaFree(snap.pres); cudaFree(snap.ripple); }
   free_ripple(*this);
+  free_mesh(*this);
   delete h_ctr;
   for (int k = 0; k < 2; ++k) {
     if (h_stage_p[k]) { cudaFreeHost(h_stage_p[k]); cudaFreeHost(h_stage_v[k]); }
@@ -726,11 +727,18 @@ int Tank::step(double frame_dt) {
     source_emits(dt);
     substep(dt);
   }
+  frame_end(frame_dt);
+  return n;
+}
+
+// the end of a frame after its sub-steps: cell counts, whitewater advance, top height and ripples
+// (solver.py:720-728)
+void Tank::frame_end(double frame_dt) {
+  join();
   count_pass();
   if (d.whitewater) launch_whitewater(solo->ctx, frame_dt);
   ripple_frame(*this, frame_dt);
   CK(cudaGetLastError());
-  return n;
 }
 
 // Particles of A then E (the previous sub-step's output and the pending emissions), dead ones skipped. The

@@ -28,8 +28,24 @@ size_t ripple_state_bytes(Tank& t);
 void clear_ripple(Tank& t);
 void ripple_frame(Tank& t, double frame_dt);
 void read_ripple_field(Tank& t, int field, void* out, size_t bytes);
+void frame_maps(Tank& t, const double sun_dir[3], float* out, size_t bytes);   // W² float4 (top, slope x, slope z, light)
 void copy_ripple_state(Tank& t, void* dst_or_src, bool save);
 void free_ripple(Tank& t);
+
+const double* ripple_top(Tank& t, int* W);   // the last frame's top-view height map (W², -1 dry) or null
+
+// surface mesh of the liquid (mesh.cu)
+struct MeshInfo {
+  long long verts = 0, quads = 0, tris = 0, body_verts = 0, lone = 0;
+  int lattice[3] = {0, 0, 0};
+  int taps = 0;
+  double lo[3] = {0, 0, 0}, spacing = 0, smooth = 0;
+  double weights[33] = {};
+};
+MeshInfo build_surface_mesh(Tank& t, double smooth);
+void read_surface_mesh(Tank& t, float* pos, float* vel, int32_t* quads, int32_t* tris, long long max_verts,
+                       long long max_quads, long long max_tris);
+void free_mesh(Tank& t);
 
 uint32_t hash_host(uint32_t x);
 
@@ -101,6 +117,7 @@ struct Tank {
   Group* solo = nullptr;
   bool use_graphs = true;
   void* ripple = nullptr;          // ripple.cu state
+  void* mesh = nullptr;            // mesh.cu state (allocated by the first surface mesh)
   Snapshot snap;
   long long emit_cap = 0;
   EmitterDev* d_emitters = nullptr;
@@ -130,6 +147,7 @@ struct Tank {
   void reset();
   void substep(double dt);
   int step(double frame_dt);
+  void frame_end(double frame_dt);
   void count_pass();
   void source_emits(double dt);
   long long read_particles(float* pos4, float* vel4, long long cap);

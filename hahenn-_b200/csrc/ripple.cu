@@ -50,6 +50,8 @@ struct RippleState {
   double4* coef = nullptr;      // fixed depth: per mode the exact update over coef_dt as a 2×2 matrix
   double* kick = nullptr;       //   and the impulse kick factor
   double coef_dt = -1.0;
+  unsigned long long* light = nullptr;   // W² floor light in 2^-44 fixed point (frame maps)
+  float4* maps = nullptr;       // W²: top height, ripple slope x, slope z, floor light
   std::vector<void*> mem;
 };
 
@@ -336,6 +338,134 @@ __global__ void k_ripple_field(TankDev T, const float2* __restrict__ S, float2* 
   }
 }
 
+// ---------------------------------------------------------------------------------------------- frame maps
+// Per frame the bake exports two maps over the footprint (bake.py:241-249): the surface (top height and the
+// ripple slopes at texel centres) and the floor light (solver.py:796-846). The light is gathered by
+// splatting: the footprint is sampled 2×2 per texel, each wet sample refracts the sun (index 1.333) through
+// the normal of the height map's slope plus the ripple slope, keeps 1 - Fresnel of it and lands displaced by
+// its depth times the refracted ray's tilt less flat water's; a dry sample lands where it is with all of
+// its light. Its quarter of a texel's light is spread bilinearly over the four texels around the landing
+// point, in 2^-32 fixed point so that the sums do not depend on the order of the atomics (the whole map's
+// light is at most W², below 2^26 for W <= 8192, so no texel can overflow). A 5-point cross with wrap-around
+// then blurs it. Float64 throughout, on the float32 ripple field.
+constexpr double kLightFix = 4294967296.0;   // 2^32
+
+struct LightParams {
+  double sun[3];               // unit vector towards the sun
+  double flat[3];              // the refracted ray under flat water
+  double tex[2];               // texel size (footprint / W)
+  double Lx, Lz;               // footprint size (ripple vertex spacing Lx / rx)
+  double mtex[2];              // texel size of the surface map (nx·h / W)
+};
+
+// slope of the wet height map at texel (i, k): central differences with wrap-around neighbours, a dry
+// neighbour standing in as the centre, none on a dry texel (solver.py:813-819)
+__device__ __forceinline__ void height_slope(const double* __restrict__ H, int W, int i, int k, const LightParams& P,
+                                             double& gx, double& gz) {
+  const double c = H[(size_t)k * W + i];
+  gx = 0.0; gz = 0.0;
+  if (!(c >= 0.0)) return;
+  auto at = [&](int ii, int kk) { const double v = H[(size_t)kk * W + ii]; return v >= 0.0 ? v : c; };
+  const int ip = i + 1 < W ? i + 1 : 0, im = i > 0 ? i - 1 : W - 1;
+  const int kp = k + 1 < W ? k + 1 : 0, km = k > 0 ? k - 1 : W - 1;
+  gx = (at(ip, k) - at(im, k)) / (2 * P.tex[0]);
+  gz = (at(i, kp) - at(i, km)) / (2 * P.tex[1]);
+}
+
+// ripple slopes at (x, z) from the footprint corner, bilinear in the vertex field (solver.py:909-919)
+__device__ __forceinline__ void ripple_slope(const float4* __restrict__ F, int rx, int rz, double Lx, double Lz, double x,
+                                             double z, double& sx, double& sz) {
+  const double qx = fmin(fmax(x / Lx * rx, 0.0), (double)rx), qz = fmin(fmax(z / Lz * rz, 0.0), (double)rz);
+  const int bx = min((int)floor(qx), rx - 1), bz = min((int)floor(qz), rz - 1);
+  const double fx = qx - bx, fz = qz - bz;
+  const size_t o = (size_t)bz * (rx + 1) + bx;
+  const float4 a = F[o], b = F[o + 1], c = F[o + rx + 1], d = F[o + rx + 2];
+  sx = ((double)a.y * (1 - fx) + (double)b.y * fx) * (1 - fz) + ((double)c.y * (1 - fx) + (double)d.y * fx) * fz;
+  sz = ((double)a.z * (1 - fx) + (double)b.z * fx) * (1 - fz) + ((double)c.z * (1 - fx) + (double)d.z * fx) * fz;
+}
+
+__device__ __forceinline__ double fresnel_water(double c) {
+  const double x = fmin(fmax(1.0 - c, 0.0), 1.0);
+  const double x2 = x * x;
+  return 0.0204 + 0.9796 * (x2 * x2 * x);
+}
+
+// one thread per sample (2W × 2W)
+__global__ void __launch_bounds__(256) k_light_splat(const double* __restrict__ H, const float4* __restrict__ F, int W,
+                                                     int rx, int rz, LightParams P, unsigned long long* __restrict__ light) {
+  const int S = 2 * W;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= S * S) return;
+  const int si = e % S, sj = e / S;
+  const double u = (si + 0.5) / 2 - 0.5, w = (sj + 0.5) / 2 - 0.5;   // texel coordinates, centres at integers
+  // bilinear taps with held edges (solver.py:808-812)
+  const int i0 = min(max((int)floor(u), 0), W - 1), k0 = min(max((int)floor(w), 0), W - 1);
+  const int i1 = min(i0 + 1, W - 1), k1 = min(k0 + 1, W - 1);
+  const double ax = fmin(fmax(u - i0, 0.0), 1.0), az = fmin(fmax(w - k0, 0.0), 1.0);
+  auto lerp2 = [&](double a00, double a10, double a01, double a11) {
+    return (a00 * (1 - ax) + a10 * ax) * (1 - az) + (a01 * (1 - ax) + a11 * ax) * az;
+  };
+  const double h00 = H[(size_t)k0 * W + i0], h10 = H[(size_t)k0 * W + i1];
+  const double h01 = H[(size_t)k1 * W + i0], h11 = H[(size_t)k1 * W + i1];
+  auto dry = [](double v) { return v >= 0.0 ? v : -1.0; };
+  auto wetf = [](double v) { return v >= 0.0 ? 1.0 : 0.0; };
+  const double h = lerp2(dry(h00), dry(h10), dry(h01), dry(h11));
+  const bool wet = h >= 0.0 && lerp2(wetf(h00), wetf(h10), wetf(h01), wetf(h11)) > 0.999;
+  const double x = (u + 0.5) * P.tex[0], z = (w + 0.5) * P.tex[1];
+  double px = x, pz = z, energy = 1.0 / 4;
+  if (wet) {
+    double g[4][2];
+    height_slope(H, W, i0, k0, P, g[0][0], g[0][1]);
+    height_slope(H, W, i1, k0, P, g[1][0], g[1][1]);
+    height_slope(H, W, i0, k1, P, g[2][0], g[2][1]);
+    height_slope(H, W, i1, k1, P, g[3][0], g[3][1]);
+    double rsx, rsz;
+    ripple_slope(F, rx, rz, P.Lx, P.Lz, x, z, rsx, rsz);
+    double nx = -lerp2(g[0][0], g[1][0], g[2][0], g[3][0]) - rsx, ny = 1.0;
+    double nz = -lerp2(g[0][1], g[1][1], g[2][1], g[3][1]) - rsz;
+    const double len = sqrt(nx * nx + ny * ny + nz * nz);
+    nx /= len; ny /= len; nz /= len;
+    const double c = nx * P.sun[0] + ny * P.sun[1] + nz * P.sun[2];
+    const double eta = 1 / 1.333;
+    const double k = 1 - eta * eta * (1 - c * c);
+    const double q = eta * c - sqrt(fmax(k, 0.0));
+    const double r0 = -P.sun[0] * eta + nx * q, r1 = -P.sun[1] * eta + ny * q, r2 = -P.sun[2] * eta + nz * q;
+    const double fall = h / fmax(-r1, 0.05);
+    px = x + (r0 * fall - P.flat[0] * h / -P.flat[1]);
+    pz = z + (r2 * fall - P.flat[2] * h / -P.flat[1]);
+    energy = (1 - fresnel_water(c)) / 4;
+  }
+  const double lx = px / P.tex[0] - 0.5, lz = pz / P.tex[1] - 0.5;
+  const double fx0 = floor(lx), fz0 = floor(lz);
+  if (!(fx0 > -2.0 && fx0 < W && fz0 > -2.0 && fz0 < W)) return;     // no tap inside the map (NaN too)
+  const int x0 = (int)fx0, z0 = (int)fz0;
+  const double bx = lx - fx0, bz = lz - fz0;
+  const double wt[4] = {(1 - bx) * (1 - bz), bx * (1 - bz), (1 - bx) * bz, bx * bz};
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int xi = x0 + (t & 1), zi = z0 + (t >> 1);
+    if (xi < 0 || xi >= W || zi < 0 || zi >= W) continue;
+    const unsigned long long q = __double2ull_rn(energy * wt[t] * kLightFix);
+    if (q) atomicAdd(light + (size_t)zi * W + xi, q);
+  }
+}
+
+// one thread per texel: the blurred light and the surface map (top height, ripple slopes at the texel centre)
+__global__ void __launch_bounds__(256) k_light_maps(const unsigned long long* __restrict__ light, const double* __restrict__ H,
+                                                    const float4* __restrict__ F, int W, int rx, int rz, LightParams P,
+                                                    float4* __restrict__ maps) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= W * W) return;
+  const int i = e % W, k = e / W;
+  const int ip = i + 1 < W ? i + 1 : 0, im = i > 0 ? i - 1 : W - 1;
+  const int kp = k + 1 < W ? k + 1 : 0, km = k > 0 ? k - 1 : W - 1;
+  auto L = [&](int ii, int kk) { return (double)light[(size_t)kk * W + ii] / kLightFix; };
+  const double c = L(i, k) + L(i, km) + L(i, kp) + L(im, k) + L(ip, k);
+  double sx = 0.0, sz = 0.0;
+  if (rx > 0) ripple_slope(F, rx, rz, P.Lx, P.Lz, (i + 0.5) * P.mtex[0], (k + 0.5) * P.mtex[1], sx, sz);
+  maps[e] = make_float4((float)H[e], (float)sx, (float)sz, (float)(c / 5));
+}
+
 int ilog2(int x) { int l = 0; while ((1 << l) < x) ++l; return l; }
 
 void fft2(Tank& t, float2* data, float sign) {
@@ -519,6 +649,44 @@ void ripple_frame(Tank& t, double frame_dt) {
   CK(cudaGetLastError());
 }
 
+const double* ripple_top(Tank& t, int* W) {
+  if (t.d.rx <= 0 || !t.ripple) return nullptr;
+  *W = rs(t)->W;
+  return rs(t)->top;
+}
+
+void frame_maps(Tank& t, const double sun_dir[3], float* out, size_t bytes) {
+  const TankDev& D = t.d;
+  if (D.rx <= 0) throw Error(-6, "this tank has no ripple layer");
+  t.join();
+  RippleState& r = ensure(t);
+  const int W = r.W;
+  const size_t nt = (size_t)W * W;
+  if (bytes < nt * 16) throw Error(-1, "frame_maps: output buffer too small (" + std::to_string(nt * 16) + " bytes needed)");
+  const double sn = sqrt(sun_dir[0] * sun_dir[0] + sun_dir[1] * sun_dir[1] + sun_dir[2] * sun_dir[2]);
+  if (!(sn > 0) || !std::isfinite(sn)) throw Error(-1, "frame_maps: the sun direction must be a finite non-zero vector");
+  LightParams P{};
+  for (int a = 0; a < 3; ++a) P.sun[a] = sun_dir[a] / sn;
+  const double st = sqrt(std::max(1 - P.sun[1] * P.sun[1], 0.0)) / 1.333;
+  P.flat[0] = -P.sun[0] / 1.333; P.flat[1] = -sqrt(1 - st * st); P.flat[2] = -P.sun[2] / 1.333;
+  P.tex[0] = r.texel[0]; P.tex[1] = r.texel[1];
+  P.Lx = r.Lx; P.Lz = r.Lz;
+  P.mtex[0] = D.nx * D.h / W; P.mtex[1] = D.nz * D.h / W;
+  if (!r.light) {
+    r.light = (unsigned long long*)ralloc(t, r, nt * 8);
+    r.maps = (float4*)ralloc(t, r, nt * 16);
+  }
+  CK(cudaMemsetAsync(r.light, 0, nt * 8, t.stream));
+  const int ns = 4 * W * W;
+  k_light_splat<<<(ns + 255) / 256, 256, 0, t.stream>>>(r.top, r.field, W, D.rx, D.rz, P, r.light);
+  k_light_maps<<<(int)((nt + 255) / 256), 256, 0, t.stream>>>(r.light, r.top, r.field, W, D.rx, D.rz, P, r.maps);
+  CK(cudaGetLastError());
+  if (out) {
+    CK(cudaMemcpyAsync(out, r.maps, nt * 16, cudaMemcpyDeviceToHost, t.stream));
+    CK(cudaStreamSynchronize(t.stream));
+  }
+}
+
 void read_ripple_field(Tank& t, int field, void* out, size_t bytes) {
   const TankDev& D = t.d;
   if (D.rx <= 0) throw Error(-6, "this tank has no ripple layer");
@@ -550,6 +718,9 @@ void read_ripple_field(Tank& t, int field, void* out, size_t bytes) {
   } else if (field == 11) {
     need(nv * 4);
     CK(cudaMemcpy(out, r.mask, nv * 4, cudaMemcpyDeviceToHost));
+  } else if (field == 12) {
+    need((size_t)r.W * r.W * 8);
+    CK(cudaMemcpy(out, r.top, (size_t)r.W * r.W * 8, cudaMemcpyDeviceToHost));
   } else {
     throw Error(-1, "unknown grid field");
   }

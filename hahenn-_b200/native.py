@@ -14,7 +14,7 @@ ERR = {-1: 'invalid argument', -2: 'CUDA error', -3: 'out of memory', -4: 'capac
        -6: 'invalid state'}
 
 FIELD_CELL_COUNT, FIELD_FRAC, FIELD_VEL, FIELD_VELOLD, FIELD_MASK, FIELD_PRES, FIELD_RHS = range(7)
-FIELD_RIPPLE_SRC, FIELD_RIPPLE, FIELD_TOP, FIELD_RIPPLE_STATE, FIELD_RIPPLE_MASK = 7, 8, 9, 10, 11
+FIELD_RIPPLE_SRC, FIELD_RIPPLE, FIELD_TOP, FIELD_RIPPLE_STATE, FIELD_RIPPLE_MASK, FIELD_TOP64 = 7, 8, 9, 10, 11, 12
 
 
 class Params(C.Structure):
@@ -34,7 +34,8 @@ class Stats(C.Structure):
                 ('time', C.c_double), ('liters', C.c_double), ('full', C.c_int32), ('frame', C.c_int32),
                 ('errors', C.c_int32), ('pad', C.c_int32), ('nx', C.c_int32), ('ny', C.c_int32), ('nz', C.c_int32), ('h', C.c_double),
                 ('origin', C.c_double * 3), ('active_cells', C.c_int64), ('residual_max', C.c_double),
-                ('residual_rms', C.c_double), ('rhs_max', C.c_double)]
+                ('residual_rms', C.c_double), ('rhs_max', C.c_double), ('ripple_rx', C.c_int32), ('ripple_rz', C.c_int32),
+                ('wmap', C.c_int32), ('pad2', C.c_int32)]
 
 
 PHASES = ('bin_sort', 'p2g', 'grid_passes', 'pressure_solve', 'projection', 'g2p')
@@ -48,6 +49,12 @@ class Object(C.Structure):
 class Emitter(C.Structure):
     _fields_ = [('shape', C.c_int32), ('airborne', C.c_int32), ('pos', C.c_double * 3), ('dir', C.c_double * 3),
                 ('radius', C.c_double), ('speed', C.c_double), ('per_substep', C.c_double), ('radius_z', C.c_double)]
+
+
+class MeshInfo(C.Structure):
+    _fields_ = [('verts', C.c_int64), ('quads', C.c_int64), ('tris', C.c_int64), ('body_verts', C.c_int64),
+                ('lone', C.c_int64), ('lattice', C.c_int32 * 3), ('taps', C.c_int32), ('lo', C.c_double * 3),
+                ('spacing', C.c_double), ('smooth', C.c_double), ('weights', C.c_double * 33)]
 
 
 class Request(C.Structure):
@@ -99,6 +106,10 @@ SIGNATURES = {
     'suiri_read_particles': (C.c_int, [P, P, P, C.c_int64, C.POINTER(C.c_int64)]),
     'suiri_read_whitewater': (C.c_int, [P, P, P, C.c_int64, C.POINTER(C.c_int64)]),
     'suiri_read_grid': (C.c_int, [P, C.c_int32, P, C.c_size_t]),
+    'suiri_frame_maps': (C.c_int, [P, P, P, C.c_size_t]),
+    'suiri_frame_end': (C.c_int, [P, C.c_double]),
+    'suiri_surface_mesh': (C.c_int, [P, C.c_double, P]),
+    'suiri_surface_mesh_read': (C.c_int, [P, P, P, P, P, C.c_int64, C.c_int64, C.c_int64]),
     'suiri_get_stats': (C.c_int, [P, C.POINTER(Stats)]),
     'suiri_poll_stats': (C.c_int, [P, C.POINTER(Stats), C.POINTER(C.c_int32)]),
     'suiri_stats_readback_bytes': (C.c_size_t, []),

@@ -181,6 +181,10 @@ class Tank:
         self._c(N.lib().suiri_step(self._h, float(frame_dt), C.byref(n)))
         return n.value
 
+    def frame_end(self, frame_dt):
+        """The end of a frame after sub-steps taken with `substep` (counts, whitewater, top height, ripples)."""
+        self._c(N.lib().suiri_frame_end(self._h, float(frame_dt)))
+
     def sync(self):
         self._c(N.lib().suiri_sync(self._h))
 
@@ -302,12 +306,45 @@ class Tank:
         self._c(N.lib().suiri_read_grid(self._h, field, _ptr(out), out.nbytes))
         return out
 
+    def frame_maps(self, sun, out=None):
+        """The maps the bake writes per frame (``bake.py:241-249``) from the last frame: float32 (W, W, 4) =
+        top height (-1 dry), ripple slope d/dx, d/dz at texel centres, floor light (``Solver.caustics``,
+        ``solver.py:796-846``) for the sun direction `sun`. `out` may be a reused (W, W, 4) float32 array."""
+        W = self.stats()['wmap']
+        if out is None:
+            out = np.empty((W, W, 4), np.float32)
+        if out.dtype != np.float32 or out.shape != (W, W, 4) or not out.flags.c_contiguous:
+            raise ValueError(f'out must be a C-contiguous float32 array of shape {(W, W, 4)}')
+        s = np.ascontiguousarray(sun, np.float64)
+        if s.shape != (3,):
+            raise ValueError('sun is a 3-vector')
+        self._c(N.lib().suiri_frame_maps(self._h, _ptr(s), _ptr(out), out.nbytes))
+        return out
+
+    def surface_mesh(self, smooth=0.8):
+        """The liquid's surface mesh as the frame export writes it (``meshing.surface`` + ``settle_on_top`` +
+        the vertex velocity, ``meshing.py:52-199``, ``bake.py:228-235``): dict of verts (V, 3) float32, vel
+        (V, 3) float32, quads (Q, 4) int32, tris (T, 3) int32, and the build's info (lattice, blur weights)."""
+        info = N.MeshInfo()
+        self._c(N.lib().suiri_surface_mesh(self._h, float(smooth), C.byref(info)))
+        V, Q, T = info.verts, info.quads, info.tris
+        verts = np.empty((V, 3), np.float32); vel = np.empty((V, 3), np.float32)
+        quads = np.empty((Q, 4), np.int32); tris = np.empty((T, 3), np.int32)
+        self._c(N.lib().suiri_surface_mesh_read(self._h, _ptr(verts), _ptr(vel), _ptr(quads), _ptr(tris), V, Q, T))
+        return dict(verts=verts, vel=vel, quads=quads, tris=tris, body_verts=info.body_verts, lone=info.lone,
+                    lattice=tuple(info.lattice), lo=tuple(info.lo), spacing=info.spacing,
+                    weights=np.array(info.weights[:info.taps]))
+
+    def caustics(self, sun):
+        """Floor light relative to plain sunlight, (W, W) float32 (``Solver.caustics``)."""
+        return self.frame_maps(sun)[..., 3].copy()
+
     @staticmethod
     def _stats_dict(s):
         return dict(count=s.count, ww_count=s.ww_count, impacts=s.impacts, vmax=s.vmax, time=s.time, liters=s.liters,
                     full=bool(s.full), frame=s.frame, errors=s.errors, nx=s.nx, ny=s.ny, nz=s.nz, h=s.h, origin=tuple(s.origin),
                     active_cells=s.active_cells, residual_max=s.residual_max, residual_rms=s.residual_rms,
-                    rhs_max=s.rhs_max)
+                    rhs_max=s.rhs_max, ripple=(s.ripple_rx, s.ripple_rz), wmap=s.wmap)
 
     def stats(self):
         s = N.Stats()

@@ -106,6 +106,9 @@ typedef struct suiri_stats {
   double residual_max;     /* max |r| */
   double residual_rms;     /* sqrt(Σ r² / active_cells) */
   double rhs_max;          /* max |h²·div| over the same cells (the scale of r) */
+  int32_t ripple_rx, ripple_rz;   /* ripple layer vertices - 1 per side (0: none) */
+  int32_t wmap;            /* top-view height map texels per side */
+  int32_t pad2;
 } suiri_stats;
 
 /* An obstacle or drain in binary form (instead of scene JSON items). */
@@ -132,7 +135,8 @@ enum suiri_field {
   SUIRI_FIELD_RIPPLE = 8,      /* float32 [rz+1][rx+1][3]: ripple height, slope x, slope z */
   SUIRI_FIELD_TOP = 9,         /* float32 [wmap][wmap]: top-view water height, -1 dry */
   SUIRI_FIELD_RIPPLE_STATE = 10, /* float32 [2rz][2rx][2]: spectral state (height + i·velocity) */
-  SUIRI_FIELD_RIPPLE_MASK = 11 /* float32 [rz+1][rx+1]: absorption mask of the last frame */
+  SUIRI_FIELD_RIPPLE_MASK = 11, /* float32 [rz+1][rx+1]: absorption mask of the last frame */
+  SUIRI_FIELD_TOP64 = 12       /* float64 [wmap][wmap]: top-view water height as computed, -1 dry */
 };
 
 /* ---------------------------------------------------------------- one tank (the plain drop-in path) */
@@ -218,6 +222,9 @@ int suiri_substep(suiri_tank* t, double dt);
 /* one frame: CFL sub-steps, scene sources, whitewater, top height and ripples
    (FluidSim.step src/js/50-sim.js:300-336; Solver.step solver.py:716-728). *substeps may be NULL. */
 int suiri_step(suiri_tank* t, double frame_dt, int32_t* substeps);
+/* the end of a frame after sub-steps the caller took with suiri_substep: cell counts, whitewater advance over
+   frame_dt, top height and ripples (Solver.step solver.py:720-728, the part after the sub-step loop) */
+int suiri_frame_end(suiri_tank* t, double frame_dt);
 int suiri_sync(suiri_tank* t);
 
 /* liquid particles (alive) to host memory: pos4 = (x, y, z, airborne), vel4 = (vx, vy, vz, id as uint32 bits);
@@ -232,6 +239,36 @@ int suiri_read_whitewater(suiri_tank* t, float* pos4, float* vel4, int64_t cap, 
 int suiri_add_whitewater(suiri_tank* t, const float* pos4, const float* vel4, int64_t n);
 /* a grid field (enum suiri_field) into out (bytes long) */
 int suiri_read_grid(suiri_tank* t, int32_t field, void* out, size_t bytes);
+
+/* The per-frame maps over the footprint that the bake exports (blender_addon/suiri_lab/bake.py:241-249), from
+   the last frame's top-view height map and ripple field: float32 [wmap][wmap][4] = top height (-1 dry), ripple
+   slope d/dx and d/dz at the texel centre (solver.py:909-919), and the floor light relative to plain sunlight,
+   the sun (towards it, any length) refracted through the surface (Solver.caustics, solver.py:796-846).
+   bytes >= wmap²·16. SUIRI_ERR_INVALID for a zero or non-finite sun direction; -6 without a ripple layer. */
+int suiri_frame_maps(suiri_tank* t, const double sun_dir[3], float* out, size_t bytes);
+
+/* The liquid's surface mesh for the frame export (meshing.surface + settle_on_top + the vertex velocity,
+   blender_addon/suiri_lab/meshing.py:52-199, bake.py:228-235), built on the device from the particles as they
+   are: the body's distance field on a lattice of spacing h/2, blurred (Gaussian of sigma `smooth` lattice
+   nodes, the reference's default 0.8), meshed with surface nets (quads, outward); lone particles (at most 6
+   particles in the 3×3×3 cells around theirs) as 42-vertex icospheres (80 triangles each, after the body's
+   vertices, in particle order as suiri_read_particles returns them); vertices within 0.6h of the wet top-view
+   height map of the last frame settled onto it (none before the first frame or without a ripple layer); the
+   liquid's face velocity at every vertex. suiri_surface_mesh builds it and fills `info`; suiri_surface_mesh_read
+   copies it out: verts and vel float32 [verts][3], quads int32 [quads][4], tris int32 [tris][3]; any output may
+   be NULL; each array must hold the counts `info` gave (max_* are their capacities). */
+typedef struct suiri_mesh_info {
+  int64_t verts, quads, tris;
+  int64_t body_verts, lone;        /* surface-nets vertices; lone particles (42 vertices each) */
+  int32_t lattice[3];              /* distance-field lattice nodes per axis (0 without a body) */
+  int32_t taps;                    /* blur taps used, weights[0 .. taps) (normalised) */
+  double lo[3], spacing, smooth;   /* lattice origin [m], spacing h/2 [m], blur sigma [nodes] */
+  double weights[33];
+} suiri_mesh_info;
+
+int suiri_surface_mesh(suiri_tank* t, double smooth, suiri_mesh_info* info);
+int suiri_surface_mesh_read(suiri_tank* t, float* verts, float* vel, int32_t* quads, int32_t* tris, int64_t max_verts,
+                            int64_t max_quads, int64_t max_tris);
 int suiri_get_stats(suiri_tank* t, suiri_stats* s);
 /* Non-blocking stats, as the reference's FluidSim.pollStats (src/js/50-sim.js:346-363) maps its staging
    buffers asynchronously. One read of the device counters is in flight at a time. If it has finished, *s

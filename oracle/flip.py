@@ -699,6 +699,11 @@ class Tank:
         for _ in range(n):
             self.frame += 1
             self.substep(dt)
+        self.frame_end(frame_dt, ripple_layer, ripple_depth)
+        return n
+
+    def frame_end(self, frame_dt, ripple_layer=None, ripple_depth=0.0):
+        """The frame's tail after its sub-steps: counts, whitewater, top height, ripples (``solver.py:720-728``)."""
         self.count_cells()
         self.advance_whitewater(frame_dt)
         if ripple_layer is not None:
@@ -707,7 +712,6 @@ class Tank:
             mean_depth = min(max(len(self.pos) * self.vp / (self.nx * self.nz * self.h * self.h), 0.003), self.rim)
             ripple_layer.frame(frame_dt, ripple_depth if ripple_depth > 0 else mean_depth, self.rsrc, rp.ripple_mask(self))
             self.rsrc[:] = 0
-        return n
 
     @property
     def liters(self):

@@ -6,7 +6,7 @@ numpy) on seeded inputs and stores inputs and outputs as small ``.npz`` files in
 with the oracle and, where shapes allow, with these files directly.
 
 Usage, with REF the root of a checkout of the reference (given as the argument or in SUIRI_REFERENCE):
-    python tests/golden/make_golden.py REF
+    python tests/golden/make_golden.py REF [scenario ...]
 
 Obstacle lattices are the analytic shapes of ``oracle/sdf.py`` sampled at the solver's lattice points
 (``solver.py:106-110``) — the role the Blender host's mesh distance queries play (``bake.py:83-119``).
@@ -26,6 +26,17 @@ from oracle import sdf as sdfm            # noqa: E402
 def load_solver(ref):
     path = os.path.join(ref, 'blender_addon', 'suiri_lab', 'solver.py')
     spec = importlib.util.spec_from_file_location('ref_solver_%d' % np.random.randint(1 << 30), path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+MESHING = None                          # the reference's meshing module (main loads it)
+
+
+def load_meshing(ref):
+    path = os.path.join(ref, 'blender_addon', 'suiri_lab', 'meshing.py')
+    spec = importlib.util.spec_from_file_location('ref_meshing', path)
     mod = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mod)
     return mod
@@ -149,6 +160,9 @@ def scenario_drops(S):
     return out
 
 
+SUN = (0.35, 0.85, 0.25)      # a low sun from +x, +z: refracted rays leave the texel they enter
+
+
 def scenario_frame(S):
     """A whole frame (CFL sub-steps, whitewater advance, top height, ripple mask and ripple step) with
     obstacles, then a second frame."""
@@ -181,6 +195,17 @@ def scenario_frame(S):
         out[f'f{f}_wpos'], out[f'f{f}_wvel'], out[f'f{f}_wlife'] = sv.wpos.copy(), sv.wvel.copy(), sv.wlife.copy()
         out[f'f{f}_top'], out[f'f{f}_field'], out[f'f{f}_S'] = sv.top.copy(), sv.ripple.field.copy(), sv.ripple.S.copy()
         out[f'f{f}_frame'], out[f'f{f}_time'], out[f'f{f}_vmax'] = sv.frame, sv.time, sv.vmax
+        out[f'f{f}_caustics'] = sv.caustics(SUN)
+        # the frame's mesh export (bake.py:228-235)
+        v, q, tr = MESHING.surface(sv)
+        MESHING.settle_on_top(sv, v)
+        g = (v - sv.origin) / sv.h
+        vel = np.stack([sv._sample(g, a) for a in range(3)], 1) if len(v) else np.zeros((0, 3))
+        if len(v):
+            vel[~sv._in_grid(g)] = 0.0
+        out[f'f{f}_mesh_v'], out[f'f{f}_mesh_q'], out[f'f{f}_mesh_t'], out[f'f{f}_mesh_vel'] = v, q, tr, vel
+        out[f'f{f}_count'] = sv.count.copy()
+    out['sun'] = np.array(SUN)
     return out
 
 
@@ -219,8 +244,13 @@ def main():
     ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('SUIRI_REFERENCE')
     if not ref:
         sys.exit('usage: make_golden.py REF (the reference checkout; or set SUIRI_REFERENCE)')
+    only = set(sys.argv[2:])                 # scenario names to regenerate (all when none given)
+    global MESHING
+    MESHING = load_meshing(ref)
     for name, fn in (('dam16', scenario_dam), ('obstacles', scenario_obstacles), ('drops', scenario_drops),
                      ('frame', scenario_frame), ('ripple', scenario_ripple), ('dam32', scenario_dam32)):
+        if only and name not in only:
+            continue
         S = load_solver(ref)
         out = fn(S)
         path = os.path.join(HERE, f'{name}.npz')

@@ -67,8 +67,12 @@ def assert_particles(gpu, ora, what='', vel_rtol=RTOL, floor_y=None):
     assert len(gi) == len(oi), f'{what}: {len(gi)} particles on the GPU, {len(oi)} in the oracle'
     np.testing.assert_array_equal(gi, oi)
     np.testing.assert_array_equal(ga, oa, err_msg=f'{what}: airborne marks')
-    err = np.abs(gp - op)
-    assert np.all(err <= 1e-6 + 1e-6 * np.abs(op)), f'{what}: position err {err.max():.3e}'
+    perr = np.abs(gp - op) - (1e-6 + 1e-6 * np.abs(op))
+    if op.size and perr.max() > 0:
+        k = int(np.argmax(perr.max(1)))
+        raise AssertionError(f'{what}: position of particle id {int(oi[k])} (airborne {oa[k]:.0f}): {gp[k]} on the GPU, '
+                             f'{op[k]} in the oracle, velocity {gv[k]} / {ov[k]}; {int((perr.max(1) > 0).sum())} particles '
+                             f'beyond 1e-6 m + 1e-6 relative')
     verr = np.abs(gv - ov) - (vel_rtol * np.abs(ov) + vel_rtol * max(float(np.abs(ov).max()) if ov.size else 0.0, 1e-30))
     if floor_y is not None:
         verr[np.abs(op[:, 1] - floor_y) < 1e-9, 1] = -1.0
@@ -117,3 +121,35 @@ def objs_from_items(items):
         elif it['kind'] == 'drain':
             out.append(sdfm.make_drain(it['pos'], it['r'], tuple(it['rot'])))
     return out
+
+
+def assert_mesh_matches_oracle(pkg, gpu, ora, smooth=0.8):
+    """The GPU's surface mesh against the oracle's on the GPU's own state: the particles in the order the GPU
+    holds them (the order of its lone-particle spheres), its cell counts, top-view height map, projected face
+    velocity, and the blur weights it used (the reference forms them with NumPy's exp, which may differ from
+    the C library's in the last bit). Body vertices, quads, triangles and body velocities are equal; the
+    icosphere table of the drops is normalised by a different dot product, so their vertices and velocities
+    agree to float32 rounding."""
+    from oracle import meshing as om
+    m = gpu.surface_mesh(smooth)
+    P, V, A, ids = gpu.particles()
+    ora.pos, ora.vel, ora.air = P.astype(np.float64), V.astype(np.float64), A.astype(np.float64)
+    ora.pid = ids.astype(np.int64)
+    ora.count = gpu.grid(pkg.native.FIELD_CELL_COUNT).astype(np.int64)
+    W = gpu.stats()['wmap']
+    top = gpu.ripple_field(pkg.native.FIELD_TOP64, (W, W), np.float64)
+    velg = gpu.grid(pkg.native.FIELD_VEL).astype(np.float64)
+    verts, quads, tris = om.surface(ora, smooth, weights=m['weights'])
+    om.settle_on_top(ora, verts, top)
+    vel = om.vertex_velocity(ora, verts, velg)
+    nb = m['body_verts']
+    assert m['verts'].shape == verts.shape, (m['verts'].shape, verts.shape)
+    assert m['lone'] * 42 == len(verts) - nb
+    np.testing.assert_array_equal(m['quads'], quads)
+    np.testing.assert_array_equal(m['tris'], tris)
+    np.testing.assert_array_equal(m['verts'][:nb], verts[:nb].astype(np.float32))
+    np.testing.assert_array_equal(m['vel'][:nb], vel[:nb].astype(np.float32))
+    np.testing.assert_allclose(m['verts'][nb:], verts[nb:], rtol=2e-7, atol=1e-9)
+    np.testing.assert_allclose(m['vel'][nb:], vel[nb:], rtol=1e-6, atol=1e-9)
+    return m
+

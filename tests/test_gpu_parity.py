@@ -9,7 +9,7 @@ import pytest
 from conftest import GOLDEN
 from oracle import flip as of
 from oracle import ripple as orp
-from parity import (assert_close_field, assert_particles, f32, gpu_from, obstacle_items, oracle_from,
+from parity import (assert_close_field, assert_mesh_matches_oracle, assert_particles, f32, gpu_from, obstacle_items, oracle_from,
                     sync_oracle_particles)
 
 pytestmark = pytest.mark.gpu
@@ -242,6 +242,101 @@ def test_frame_step_whitewater_top_height_and_ripples(pkg):
     fld = gpu.ripple_field(pkg.native.FIELD_RIPPLE, (R + 1, R + 1, 3), np.float32)
     for c in range(3):     # heights in m, slopes: float32 FFT round-off floor 1e-12
         assert_close_field(fld[..., c], layer.field[..., c], rtol=1e-4, atol=1e-12, what=f'ripple field {c}')
+    # floor light of the frame: from the GPU's own maps as the oracle forms it, and against the oracle's frame
+    sun = d['sun']
+    maps = gpu.frame_maps(sun)
+    top64 = gpu.ripple_field(pkg.native.FIELD_TOP64, (W, W), np.float64)
+    _check_frame_maps(maps, top64, fld, nx * h, nz * h, sun)
+    assert_close_field(maps[..., 3], orp.caustics(ora.top, layer.field, nx * h, nz * h, sun), rtol=1e-4,
+                       what='floor light against the oracle frame')
+    # the frame's surface mesh: pool, obstacle walls and the lone drops in flight
+    m = assert_mesh_matches_oracle(pkg, gpu, ora)
+    assert m['quads'].shape[0] > 1000 and m['lone'] > 0
+    gpu.close()
+
+
+def _check_frame_maps(maps, top64, fld, Lx, Lz, sun):
+    """The frame maps against the oracle evaluated on the same height map and ripple field: top height
+    exactly (float32 of the float64 map), ripple slopes at texel centres and floor light within float32
+    rounding (both sides float64 on identical inputs; the light's fixed-point sums add 2^-32 per tap)."""
+    W = top64.shape[0]
+    np.testing.assert_array_equal(maps[..., 0], top64.astype(np.float32))
+    f64 = fld.astype(np.float64)
+    ii, jj = np.meshgrid(np.arange(W), np.arange(W))
+    sx, sz = orp.slope_at(f64, Lx, Lz, (ii + 0.5) * (Lx / W), (jj + 0.5) * (Lz / W))
+    np.testing.assert_allclose(maps[..., 1], sx, rtol=1e-6, atol=1e-9 * max(np.abs(sx).max(), 1e-30))
+    np.testing.assert_allclose(maps[..., 2], sz, rtol=1e-6, atol=1e-9 * max(np.abs(sz).max(), 1e-30))
+    light = orp.caustics(top64, f64, Lx, Lz, sun)
+    np.testing.assert_allclose(maps[..., 3], light, rtol=1e-6, atol=1e-7)
+
+
+def test_surface_mesh_under_rain(pkg):
+    """The surface mesh of the full scene's shape at a quarter of each axis after rain frames: a pool with
+    ripples and drops in flight (lone spheres), with the reference's blur (σ 0.8, 5 taps) and a wider one
+    (σ 1.6, 9 taps), each against the oracle on the GPU's state; then the mesh of an empty tank."""
+    w = pkg.workloads.full_scene(scale=4)
+    nx, ny, nz, h = w['nx'], w['ny'], w['nz'], w['h']
+    prm = w['params']
+    gpu = pkg.Tank(nx=nx, ny=ny, nz=nz, h=h, ripple=w['ripple'], wmap=128, capacity=len(w['pos']) + 20000,
+                   ripple_sigma=prm['sigma'], ripple_rho=prm['rho'], ripple_depth=prm['depth'], drop_d=prm['drop_d'],
+                   flip=prm['flip'], omega=prm['omega'], iters=40)
+    ora = oracle_from(nx, ny, nz, h, w['origin'], ripple=w['ripple'], wmap=128, flip=prm['flip'], omega=prm['omega'],
+                      iters=40)
+    gpu.add_particles(w['pos'])
+    rng = np.random.default_rng(8)
+    for f in range(2):
+        n = 300
+        drops = np.stack([rng.uniform(-0.45 * nx * h, 0.45 * nx * h, n), rng.uniform(0.5, 0.9, n) * ny * h,
+                          rng.uniform(-0.45 * nz * h, 0.45 * nz * h, n)], 1)
+        dv = np.zeros((n, 3)); dv[:, 1] = -2.0
+        gpu.add_particles(f32(drops), f32(dv), np.ones(n))
+        for _ in range(3):
+            gpu.step(1 / 60)
+    for smooth in (0.8, 1.6):
+        m = assert_mesh_matches_oracle(pkg, gpu, ora, smooth)
+        assert len(m['weights']) == 2 * max(1, int(np.ceil(2.5 * smooth))) + 1
+        assert m['quads'].shape[0] > 10000 and m['lone'] > 10
+    gpu.clear_water()
+    m = gpu.surface_mesh()
+    assert m['verts'].shape == (0, 3) and m['quads'].shape == (0, 4) and m['tris'].shape == (0, 3)
+    gpu.close()
+
+
+def test_frame_maps_floor_light_under_rain(pkg):
+    """The per-frame light and surface maps of the full scene's shape at a quarter of each axis (128² map,
+    256×128 ripple layer) after three frames of rain: ripples from the merged drops and the liquid's own
+    slope bend the light. Three suns (overhead, oblique, low from -x), each against the oracle on the GPU's
+    height map and ripple field."""
+    w = pkg.workloads.full_scene(scale=4)
+    nx, ny, nz, h = w['nx'], w['ny'], w['nz'], w['h']
+    Rx, Rz = w['ripple']
+    prm = w['params']
+    W = 128
+    gpu = pkg.Tank(nx=nx, ny=ny, nz=nz, h=h, ripple=(Rx, Rz), wmap=W, capacity=len(w['pos']) + 20000,
+                   ww_capacity=20000, ripple_sigma=prm['sigma'], ripple_rho=prm['rho'], ripple_depth=prm['depth'],
+                   drop_d=prm['drop_d'], flip=prm['flip'], omega=prm['omega'], iters=40)
+    gpu.add_particles(w['pos'])
+    rng = np.random.default_rng(5)
+    for f in range(3):
+        n = 200
+        drops = np.stack([rng.uniform(-0.45 * nx * h, 0.45 * nx * h, n), rng.uniform(0.3, 0.45, n) * ny * h,
+                          rng.uniform(-0.45 * nz * h, 0.45 * nz * h, n)], 1)
+        dv = np.zeros((n, 3)); dv[:, 1] = -4.0
+        gpu.add_particles(f32(drops), f32(dv), np.ones(n))
+        for _ in range(4):
+            gpu.step(1 / 60)
+    assert gpu.stats()['impacts'] > 0
+    top64 = gpu.ripple_field(pkg.native.FIELD_TOP64, (W, W), np.float64)
+    fld = gpu.ripple_field(pkg.native.FIELD_RIPPLE, (Rz + 1, Rx + 1, 3), np.float32)
+    assert np.abs(fld[..., 1]).max() > 0
+    out = np.empty((W, W, 4), np.float32)
+    for sun in ((0.0, 1.0, 0.0), (0.35, 0.85, 0.25), (-0.8, 0.45, 0.1)):
+        maps = gpu.frame_maps(sun, out)
+        assert maps is out
+        _check_frame_maps(maps, top64, fld, nx * h, nz * h, sun)
+        assert maps[..., 3].max() > maps[..., 3].min() + 1e-3          # the surface bends the light
+    with pytest.raises(pkg.native.SuiriError):
+        gpu.frame_maps((0.0, 0.0, 0.0))
     gpu.close()
 
 
@@ -539,14 +634,21 @@ def test_rectangular_ripple_layer_full_scene_quarter(pkg):
         gpu.add_particles(f32(drops), f32(dv), np.ones(n))
         ora.add_particles(f32(drops), f32(dv), np.ones(n))
         for _ in range(6):                    # the drops fall to the pool, then one frame is compared
-            n_gpu = gpu.step(1 / 60)
-            n_ora = ora.step(1 / 60, layer, ripple_depth=prm['depth'])
-            assert n_gpu == n_ora
-            # velocities within 1e-4: around landing drops the corner sums of faces with little total weight
-            # lose digits in float32 (the reference GPU path's own arithmetic), against float64 in the oracle;
-            # the vertical velocity of particles on the floor clamp is a tie (see assert_particles)
-            assert_particles(gpu, ora, f'burst {f}', vel_rtol=1e-4, floor_y=float(np.float32(0.32 * h)))
-            sync_oracle_particles(gpu, ora)
+            # each sub-step compared and the oracle continued from the GPU's particles: at 131k particles a few
+            # lie within the float32/float64 difference of a cell face after an unsynchronised sub-step, and
+            # the discrete cell counts (liquid cells, drift) then differ between the two
+            n = ora.substeps_for(1 / 60)
+            for _ in range(n):
+                gpu.substep(1 / 60 / n)
+                ora.frame += 1
+                ora.substep(1 / 60 / n)
+                # velocities within 1e-4: around landing drops the corner sums of faces with little total
+                # weight lose digits in float32 (the reference GPU path's own arithmetic), against float64 in
+                # the oracle; the vertical velocity of particles on the floor clamp is a tie (assert_particles)
+                assert_particles(gpu, ora, f'burst {f}', vel_rtol=1e-4, floor_y=float(np.float32(0.32 * h)))
+                sync_oracle_particles(gpu, ora)
+            gpu.frame_end(1 / 60)
+            ora.frame_end(1 / 60, layer, ripple_depth=prm['depth'])
         st = gpu.stats()
         assert st['impacts'] == ora.impacts
         assert ora.impacts > impacts, 'no drop merged in this burst'

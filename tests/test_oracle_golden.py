@@ -10,6 +10,7 @@ import pytest
 
 from conftest import GOLDEN
 from oracle import flip as of
+from oracle import meshing as om
 from oracle import ripple as orp
 from oracle import sdf as sdfm
 
@@ -109,6 +110,38 @@ def test_frame_step_whitewater_top_height_ripple():
         np.testing.assert_array_equal(t.top, d[f'f{f}_top'])
         close(layer.field, d[f'f{f}_field'], 1e-9, 1e-15)
         close(layer.S, d[f'f{f}_S'], 1e-9, 1e-15)
+        close(orp.caustics(t.top, layer.field, t.nx * t.h, t.nz * t.h, d['sun']), d[f'f{f}_caustics'], 1e-12, 1e-13)
+        np.testing.assert_array_equal(t.count, d[f'f{f}_count'])
+        v, q, tr = om.surface(t)
+        om.settle_on_top(t, v)
+        np.testing.assert_array_equal(v, d[f'f{f}_mesh_v'])
+        np.testing.assert_array_equal(q, d[f'f{f}_mesh_q'])
+        np.testing.assert_array_equal(tr, d[f'f{f}_mesh_t'])
+        np.testing.assert_array_equal(om.vertex_velocity(t, v), d[f'f{f}_mesh_vel'])
+
+
+def test_caustics_of_the_reference_frames():
+    """Floor light from the reference's own height map and ripple field after each fixture frame."""
+    d = load('frame')
+    h = float(d['h'])
+    for f in (1, 2):
+        light = orp.caustics(d[f'f{f}_top'], d[f'f{f}_field'], int(d['nx']) * h, int(d['nz']) * h, d['sun'])
+        close(light, d[f'f{f}_caustics'], 1e-12, 1e-13)
+        assert light.max() > 1.5 and light.min() < 0.5          # the surface focuses and shadows light
+
+
+@pytest.mark.parametrize('sun', [(0.0, 1.0, 0.0), (0.35, 0.85, 0.25), (-0.6, 0.5, 0.1)])
+def test_caustics_under_flat_water(sun):
+    """Flat water of any depth maps every texel onto itself: away from the edges (whose outer samples land
+    off the map) the light is the transmitted fraction 1 - Fresnel(cos θ_sun); dry floor takes it all."""
+    W, L = 24, 0.48
+    field = np.zeros((17, 17, 3))
+    s = np.asarray(sun) / np.linalg.norm(sun)
+    for depth in (0.0, 0.05, 0.2):
+        light = orp.caustics(np.full((W, W), depth), field, L, L, sun)
+        np.testing.assert_allclose(light[2:-2, 2:-2], 1 - orp.fresnel_w(s[1]), rtol=1e-12)
+    dry = orp.caustics(np.full((W, W), -1.0), field, L, L, sun)
+    np.testing.assert_allclose(dry[2:-2, 2:-2], 1.0, rtol=1e-12)
 
 
 def test_ripple_layer_alone():
