@@ -733,6 +733,135 @@ def run_full_scene(args, local):
     t.close()
 
 
+EXPORT_SUN = (0.35, 0.85, 0.25)
+
+
+def _export_bytes(info, particles, nodes, W):
+    """Algorithmic bytes of each phase of one frame export: what each kernel must read and write once.
+    classify 16 B/particle position + 1 B class (+ the 27 cell counts, cached); distance field 4 B/node
+    fill + 16 B/body particle; blur 3 passes × (4 B read + 4 B write)/node; surface nets 4 B/node phi
+    reads in the count, cell and quad passes + 4 B/cell vertex index + 24 B/vertex + 16 B/quad + 1 B/particle
+    class ×2; finish 24 B/body vertex + 24 B/vertex out; light maps 8 B/texel top + 16 B/ripple vertex
+    (cached) + 8 B/texel fixed-point sums ×3 + 16 B/texel maps."""
+    V, Q, nb, nl = len(info['verts']), len(info['quads']), int(info['body_verts']), int(info['lone'])
+    return dict(classify=17 * particles, distance_field=4 * nodes + 16 * particles, blur=24 * nodes,
+                surface_nets=12 * nodes + 4 * nodes + 24 * nb + 16 * Q + 2 * particles + 4 * nl,
+                finish=24 * nb + 24 * V, light_maps=(8 + 24 + 16) * W * W)
+
+
+def _cpu_export_rate(P, steps_frames=3):
+    """The oracle's export (surface mesh, settling, vertex velocity, floor light) timed on the host for the
+    same scene at a quarter of each axis, advanced on the GPU for the same frames: particles exported per
+    second on one core (NumPy)."""
+    from oracle import flip as of, meshing as om, ripple as orp
+    w = P.workloads.full_scene(scale=4)
+    prm = w['params']
+    t = P.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=prm['flip'], omega=prm['omega'], iters=prm['iters'],
+               whitewater=True, ripple=w['ripple'], wmap=128, capacity=len(w['pos']) + 20000,
+               ripple_sigma=prm['sigma'], ripple_rho=prm['rho'], ripple_depth=prm['depth'], drop_d=prm['drop_d'])
+    t.add_particles(w['pos'])
+    t.set_emitters(w['emitters'])
+    for _ in range(steps_frames):
+        t.step(prm['dt'])
+    ora = of.Tank(w['nx'], w['ny'], w['nz'], w['h'], origin=w['origin'], ripple=w['ripple'], wmap=128)
+    pos, vel, air, ids = t.particles()
+    ora.pos, ora.vel, ora.air, ora.pid = pos.astype(float), vel.astype(float), air.astype(float), ids.astype(np.int64)
+    ora.count = t.grid(P.native.FIELD_CELL_COUNT).astype(np.int64)
+    top = t.ripple_field(P.native.FIELD_TOP64, (128, 128), np.float64)
+    velg = t.grid(P.native.FIELD_VEL).astype(np.float64)
+    field = t.ripple_field(P.native.FIELD_RIPPLE, (w['ripple'][1] + 1, w['ripple'][0] + 1, 3), np.float32).astype(float)
+    n = len(pos)
+    t.close()
+    t0 = time.perf_counter()
+    v, q, tr = om.surface(ora)
+    om.settle_on_top(ora, v, top)
+    om.vertex_velocity(ora, v, velg)
+    orp.caustics(top, field, w['nx'] * w['h'], w['nz'] * w['h'], EXPORT_SUN)
+    sec = time.perf_counter() - t0
+    return n / sec, n, sec
+
+
+def run_frame_export(args, local):
+    """The per-frame export of the full scene (256×128(up)×128 cells at h = 1/128 m, ≈8.4M particles, rain,
+    1024×512 ripple layer, 512² maps) after 8 frames of 1/240 s: a step is one frame's export, the surface
+    mesh (lone drops as spheres, surface nets of the blurred distance field on the 2 mm lattice, settling,
+    vertex velocity) and the floor light and surface maps. `value` is the device time of the export's kernels
+    (the state resident in HBM); `e2e` is the export through the public calls into host arrays (mesh build,
+    its read-back, the maps' build and read-back)."""
+    import torch
+    P = pkg()
+    w = P.workloads.full_scene()
+    prm = w['params']
+    W = 512
+    t = P.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=prm['flip'], omega=prm['omega'], iters=prm['iters'],
+               whitewater=True, ripple=w['ripple'], wmap=W, capacity=int(len(w['pos']) * 1.1) + 200000,
+               ww_capacity=400000, ripple_sigma=prm['sigma'], ripple_rho=prm['rho'], ripple_depth=prm['depth'], device=local,
+               drop_d=prm['drop_d'])
+    t.add_particles(w['pos'])
+    t.set_emitters(w['emitters'])
+    for _ in range(8):
+        t.step(prm['dt'])
+    t.sync()
+    stream = torch.cuda.ExternalStream(t.stream())
+    particles = t.stats()['count']
+    for _ in range(args.warmup):
+        m = t.surface_mesh()
+        t.frame_maps(EXPORT_SUN)
+    phases = {k: 0.0 for k in P.native.MESH_PHASES}
+    light_ms = 0.0
+    clocks = Clocks(local)
+    clocks.start()
+    for _ in range(args.steps):
+        m = t.surface_mesh()
+        for k, v in m['phase_ms'].items():
+            phases[k] += v / args.steps
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        t.frame_maps(EXPORT_SUN, read=False)
+        b.record(stream)
+        b.synchronize()
+        light_ms += a.elapsed_time(b) / args.steps
+    clk = clocks.stop()
+    dev_ms = sum(phases.values()) + light_ms
+    # end to end: the public calls into host arrays
+    out = np.empty((W, W, 4), np.float32)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        m = t.surface_mesh()
+        t.frame_maps(EXPORT_SUN, out)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    d2h = m['verts'].nbytes + m['vel'].nbytes + m['quads'].nbytes + m['tris'].nbytes + out.nbytes
+    nodes = int(np.prod(m['lattice']))
+    alg = _export_bytes(m, particles, nodes, W)
+    times = dict(phases, light_maps=light_ms)
+    top = max(times, key=times.get)
+    peak, kind = peaks()
+    prof = profile_figure('frame_export_traffic.json') or {}
+    ach = alg[top] / (times[top] * 1e-3) / 1e9
+    cpu_rate, cpu_n, cpu_s = _cpu_export_rate(P)
+    line = dict(metric='exported particles/s', value=particles * 1000 / dev_ms, unit='particles/s', n_gpus=1,
+                steps=args.steps, warmup=args.warmup, ms_per_step=dev_ms, higher_is_better=True, scaling='weak',
+                vs_baseline=None, dtype='f32/f64', data='synthetic (seeded particles, rain)',
+                config=dict(workload='frame_export_256x128x128', particles=int(particles), wmap=W,
+                            lattice=list(m['lattice']), verts=int(len(m['verts'])), quads=int(len(m['quads'])),
+                            lone=int(m['lone']), l2='state larger than L2 (particles 268 MB, lattice '
+                            f'{nodes * 16 / 1e6:.0f} MB); no flush'),
+                phases_ms=times,
+                roofline=dict(bound='hbm', kernel=top, achieved=ach, peak=peak, unit='GB/s', frac=ach / peak,
+                              peak_kind=kind, traffic=prof.get(top), alg_bytes_per_launch=alg[top]),
+                alg_bytes=alg,
+                cpu_baseline=dict(value=cpu_rate, unit='particles/s', cores=1, kind='port',
+                                  sample=f'the oracle export (surface mesh, settling, vertex velocity, floor light) '
+                                         f'of the scene at a quarter of each axis ({cpu_n} particles, 128² maps), '
+                                         f'{cpu_s:.1f} s on one core'),
+                e2e=dict(value=particles / e2e_s, unit='particles/s', h2d_bytes_per_step=0, d2h_bytes_per_step=int(d2h)),
+                # per export: 4 of the cell count, 12 of the mesh (classify, fill, splat, 3 blur passes,
+                # count, scan, cells, quads, lone, finish), 2 of the light maps
+                gpu_launches=18 * args.steps, clocks=clk)
+    print(json.dumps(line), flush=True)
+    t.close()
+
+
 def run_serve(args, local):
     """Serving workload: Poisson arrivals of seeded scene solves (axes up to 128, 10 % with a faucet), each
     asking for `--req-steps` sub-steps, admitted under a 150 GB HBM budget and co-scheduled in shared
@@ -784,7 +913,8 @@ def main():
     ap.add_argument('--steps', type=int, default=20)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='suiri', choices=['suiri', 'reference'])
-    ap.add_argument('--workload', default='batch', choices=['batch', 'obstacles_inflow', 'serve', 'full_scene'])
+    ap.add_argument('--workload', default='batch',
+                    choices=['batch', 'obstacles_inflow', 'serve', 'full_scene', 'frame_export'])
     ap.add_argument('--cpu-steps', type=int, default=2, help='sub-steps of the single-tank CPU baseline sample')
     ap.add_argument('--tanks', type=int, default=64)
     ap.add_argument('--rate', type=float, default=200.0)
@@ -808,6 +938,8 @@ def main():
         return run_serve(args, local)
     if args.workload == 'full_scene':
         return run_full_scene(args, local)
+    if args.workload == 'frame_export':
+        return run_frame_export(args, local)
     return run_plain(args, rank, world, local)
 
 

@@ -465,7 +465,7 @@ int suiri_read_grid(suiri_tank* h, int32_t field, void* out, size_t bytes) {
 
 int suiri_frame_maps(suiri_tank* h, const double sun_dir[3], float* out, size_t bytes) {
   return guard(h ? &h->err : nullptr, [&] {
-    if (!sun_dir || !out) throw Error(SUIRI_ERR_INVALID, "null sun direction or output");
+    if (!sun_dir) throw Error(SUIRI_ERR_INVALID, "null sun direction");
     frame_maps(*T(h), sun_dir, out, bytes);
   });
 }
@@ -482,6 +482,7 @@ int suiri_surface_mesh(suiri_tank* h, double smooth, suiri_mesh_info* info) {
     info->taps = m.taps;
     info->spacing = m.spacing; info->smooth = m.smooth;
     for (int k = 0; k < m.taps && k < 33; ++k) info->weights[k] = m.weights[k];
+    for (int k = 0; k < 5; ++k) info->phase_ms[k] = m.phase_ms[k];
   });
 }
 

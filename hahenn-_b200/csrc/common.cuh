@@ -120,7 +120,8 @@ struct TankDev {
   double* flux;             // 3*nnodes cut-cell face fluxes (divergence operand)
   float* pres;              // 2*nhalf colour-split pressure
   float* pres2;             // 2*nhalf, the other buffer of the temporal-blocked solve
-  int* act;                 // 2*nhalf: per colour, the colour slots of the active cells (this sub-step)
+  int4* act;                // 2*nhalf: per colour, the active cells of this sub-step: (colour slot, SOR code,
+                            //   rhs bits, 1/ΣC bits), so a sweep reads a cell's constants in one load
   float* rhs;               // 2*nhalf h²·div
   uint32_t* code;           // 2*nhalf
   const Obj* objs;

@@ -313,7 +313,7 @@ Tank::Tank(const TankConfig& c) : cfg(c) {
   D.vv = (float2*)alloc(3 * nn * 8);
   D.pres = (float*)alloc(2 * nh * 4); D.rhs = (float*)alloc(2 * nh * 4); D.code = (uint32_t*)alloc(2 * nh * 4);
   D.pres2 = (float*)alloc(2 * nh * 4);
-  D.act = (int*)alloc(2 * nh * 4);
+  D.act = (int4*)alloc(2 * nh * 16);
   d_objs = (Obj*)alloc(kMaxObj * sizeof(Obj));
   D.objs = d_objs;
   D.ctr = (Counters*)alloc(sizeof(Counters));
@@ -359,7 +359,7 @@ size_t tank_bytes(const TankConfig& c) {
   size_t b = cap * 16 * 6 + cap * 2 * 4;                      // A, E, B (pos, vel), ranks
   b += (nc + 1) * 4 + (nc + 2) * 4;                           // counts, offsets
   b += nn * (6 * 8 + 4 * 16 + 2 * 3 * 8 + 3 * 8);            // accumulator, vel/velold/frac/svel, fracd/flux, vv
-  b += 2 * nh * 20;                                           // pressure (two buffers), rhs, code, active lists
+  b += 2 * nh * 32;                                           // pressure (two buffers), rhs, code, active lists
   b += kMaxObj * sizeof(Obj) + sizeof(Counters) + kMaxEmitters * sizeof(EmitterDev);
   b += 2 * (size_t)std::max(1LL, c.ww_cap) * 32;
   if (c.rx > 0) {

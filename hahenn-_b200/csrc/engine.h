@@ -41,6 +41,7 @@ struct MeshInfo {
   int taps = 0;
   double lo[3] = {0, 0, 0}, spacing = 0, smooth = 0;
   double weights[33] = {};
+  double phase_ms[5] = {};        // device time: classify, distance field, blur, surface nets, finish
 };
 MeshInfo build_surface_mesh(Tank& t, double smooth);
 void read_surface_mesh(Tank& t, float* pos, float* vel, int32_t* quads, int32_t* tris, long long max_verts,

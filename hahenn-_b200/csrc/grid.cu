@@ -348,7 +348,9 @@ __global__ void __launch_bounds__(kThreads) k_grid_cells(const TankDev* __restri
     int at = 0;
     if (lane == leader) at = atomicAdd(&T.ctr->n_act[cc], __popc(m));
     at = __shfl_sync(0xffffffffu, at, leader);
-    if (mine) T.act[(size_t)cc * T.nhalf + at + __popc(m & ((1u << lane) - 1))] = hs;
+    if (mine)
+      T.act[(size_t)cc * T.nhalf + at + __popc(m & ((1u << lane) - 1))] =
+          make_int4(hs, (int)code, __float_as_int(rhs), __float_as_int(__frcp_rn(den)));
   }
   // the last block: per colour, the prefix over tanks of the active counts (the sweeps' item → tank map)
   if (last_block(ticket)) {

@@ -31,6 +31,7 @@ namespace suiri {
 namespace {
 
 constexpr int kMeshThreads = 1024;   // one item per thread in the compaction tiles
+constexpr int kMeshPhases = 5;       // classify, distance field, blur, surface nets, finish (device time each)
 constexpr int kMaxTaps = 33;
 
 struct MeshCounters {
@@ -524,6 +525,7 @@ struct MeshState {
   float* vel = nullptr; size_t vel_cap = 0;
   MeshInfo info{};
   bool built = false;
+  cudaEvent_t ev[2 * kMeshPhases] = {};   // start and end of each phase
 };
 
 template <class T>
@@ -544,6 +546,7 @@ void free_mesh(Tank& t) {
   for (void* p : dev) if (p) cudaFree(p);
   if (m->h_mc) cudaFreeHost(m->h_mc);
   if (m->h_base) cudaFreeHost(m->h_base);
+  for (cudaEvent_t e : m->ev) if (e) cudaEventDestroy(e);
   delete m;
   t.mesh = nullptr;
 }
@@ -566,6 +569,7 @@ MeshInfo build_surface_mesh(Tank& t, double smooth) {
     CK(cudaMalloc(&m->d_ico, V.size() * 8));
     CK(cudaMemcpyAsync(m->d_ico, V.data(), V.size() * 8, cudaMemcpyHostToDevice, t.stream));
     CK(cudaStreamSynchronize(t.stream));
+    for (cudaEvent_t& e : m->ev) CK(cudaEventCreate(&e));
   }
   MeshState& M = *(MeshState*)t.mesh;
   M.built = false;
@@ -577,8 +581,10 @@ MeshInfo build_surface_mesh(Tank& t, double smooth) {
   for (int a = 0; a < 3; ++a) { init.lo_key[a] = ~0u; init.hi_key[a] = 0u; }
   *M.h_mc = init;
   CK(cudaMemcpyAsync(M.d_mc, M.h_mc, sizeof(MeshCounters), cudaMemcpyHostToDevice, t.stream));
+  CK(cudaEventRecord(M.ev[0], t.stream));
   if (n > 0) k_mesh_classify<<<grid, 256, 0, t.stream>>>(dT, M.kind, M.d_mc);
   CK(cudaGetLastError());
+  CK(cudaEventRecord(M.ev[1], t.stream));
   CK(cudaMemcpyAsync(M.h_mc, M.d_mc, sizeof(MeshCounters), cudaMemcpyDeviceToHost, t.stream));
   CK(cudaStreamSynchronize(t.stream));
   const MeshCounters mc = *M.h_mc;
@@ -623,13 +629,20 @@ MeshInfo build_surface_mesh(Tank& t, double smooth) {
     grow(M.phiA, M.phiA_cap, (size_t)nodes);
     grow(M.phiB, M.phiB_cap, (size_t)nodes);
     const unsigned far_key = [&] { unsigned b; memcpy(&b, &G.far32, 4); return (b & 0x80000000u) ? ~b : (b | 0x80000000u); }();
+    CK(cudaEventRecord(M.ev[2], t.stream));
     k_mesh_fill<<<grid, 256, 0, t.stream>>>(M.key, nodes, far_key);
     k_mesh_splat<<<grid, 256, 0, t.stream>>>(dT, M.kind, G, M.key);
+    CK(cudaEventRecord(M.ev[3], t.stream));
+    CK(cudaEventRecord(M.ev[4], t.stream));
     k_mesh_blur<0><<<grid, 256, 0, t.stream>>>(M.key, M.phiA, G, taps);
     k_mesh_blur<1><<<grid, 256, 0, t.stream>>>(M.phiA, M.phiB, G, taps);
     k_mesh_blur<2><<<grid, 256, 0, t.stream>>>(M.phiB, M.phiA, G, taps);
     CK(cudaGetLastError());
+    CK(cudaEventRecord(M.ev[5], t.stream));
+  } else {
+    for (int k = 2; k < 6; ++k) CK(cudaEventRecord(M.ev[k], t.stream));
   }
+  CK(cudaEventRecord(M.ev[6], t.stream));
   MeshSegs S{};
   if (mc.n_body > 0) {
     const long long X = G.X, Y = G.Y, Z = G.Z;
@@ -644,6 +657,7 @@ MeshInfo build_surface_mesh(Tank& t, double smooth) {
   const int B = S.first_block[5];
   if (B > 0) {
     grow(M.bcount, M.bcount_cap, (size_t)B + 1);
+    CK(cudaEventRecord(M.ev[6], t.stream));
     const float* phi = M.phiA;
     k_mesh_count<<<B, kMeshThreads, 0, t.stream>>>(phi, G, S, M.kind, M.bcount);
     k_mesh_scan<<<1, 1024, 0, t.stream>>>(M.bcount, B);
@@ -667,6 +681,7 @@ MeshInfo build_surface_mesh(Tank& t, double smooth) {
   }
   grow(M.lone_idx, M.lone_cap, (size_t)std::max<long long>(nl, 1));
   if (S.n[4] > 0) k_mesh_lone<<<nb_of(S.n[4]), kMeshThreads, 0, t.stream>>>(S, M.kind, M.bcount, M.lone_idx);
+  CK(cudaEventRecord(M.ev[7], t.stream));
   grow(M.pos, M.pos_cap, 3 * (size_t)std::max<long long>(nv, 1));
   grow(M.vel, M.vel_cap, 3 * (size_t)std::max<long long>(nv, 1));
   FinishParams F{};
@@ -678,9 +693,16 @@ MeshInfo build_surface_mesh(Tank& t, double smooth) {
   F.rim = D.rim;
   F.size_x = D.nx * D.h; F.size_z = D.nz * D.h;
   F.ico = M.d_ico;
+  CK(cudaEventRecord(M.ev[8], t.stream));
   if (nv > 0) k_mesh_finish<<<grid, 256, 0, t.stream>>>(dT, G, F, M.vtx, M.lone_idx, M.pos, M.vel);
   CK(cudaGetLastError());
+  CK(cudaEventRecord(M.ev[9], t.stream));
   CK(cudaStreamSynchronize(t.stream));
+  for (int k = 0; k < kMeshPhases; ++k) {     // the surface nets phase includes the read of the three counts
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, M.ev[2 * k], M.ev[2 * k + 1]));
+    info.phase_ms[k] = ms;
+  }
   info.verts = nv; info.quads = nq; info.tris = 80 * nl; info.body_verts = nbv; info.lone = nl;
   info.lattice[0] = G.X; info.lattice[1] = G.Y; info.lattice[2] = G.Z;
   for (int a = 0; a < 3; ++a) info.lo[a] = G.lo[a];

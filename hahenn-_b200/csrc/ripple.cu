@@ -662,7 +662,7 @@ void frame_maps(Tank& t, const double sun_dir[3], float* out, size_t bytes) {
   RippleState& r = ensure(t);
   const int W = r.W;
   const size_t nt = (size_t)W * W;
-  if (bytes < nt * 16) throw Error(-1, "frame_maps: output buffer too small (" + std::to_string(nt * 16) + " bytes needed)");
+  if (out && bytes < nt * 16) throw Error(-1, "frame_maps: output buffer too small (" + std::to_string(nt * 16) + " bytes needed)");
   const double sn = sqrt(sun_dir[0] * sun_dir[0] + sun_dir[1] * sun_dir[1] + sun_dir[2] * sun_dir[2]);
   if (!(sn > 0) || !std::isfinite(sn)) throw Error(-1, "frame_maps: the sun direction must be a finite non-zero vector");
   LightParams P{};

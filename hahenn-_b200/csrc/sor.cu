@@ -130,6 +130,36 @@ __device__ __forceinline__ void sor_cell(const TankDev& T, int color, int s) {
   T.pres[own] = sor_update(C, nb, rhs, p, T.omega);
 }
 
+// relax the listed cell of entry e (slot, code, rhs, 1/ΣC): its pressure and six neighbours in one round of
+// loads (cut cells also read their face fractions)
+__device__ __forceinline__ void sor_entry(const TankDev& T, int color, int4 e) {
+  const int hx = T.hx, nx = T.nx, ny = T.ny, nz = T.nz;
+  const int s = e.x;
+  const uint32_t code = (uint32_t)e.y;
+  const int row = divu(s, T.dhx), ti = s - row * hx;
+  const int k = divu(row, T.dny), j = row - k * ny;
+  const int i = 2 * ti + ((j + k + color) & 1);
+  const float* __restrict__ po = T.pres + (size_t)(1 - color) * T.nhalf;
+  const int rowb = hx * row;
+  float nb[6];
+  nb[0] = i > 0 ? po[((i - 1) >> 1) + rowb] : 0.f;
+  nb[1] = i + 1 < nx ? po[((i + 1) >> 1) + rowb] : 0.f;
+  nb[2] = j > 0 ? po[ti + rowb - hx] : 0.f;
+  nb[3] = j + 1 < ny ? po[ti + rowb + hx] : 0.f;
+  nb[4] = k > 0 ? po[ti + rowb - hx * ny] : 0.f;
+  nb[5] = k + 1 < nz ? po[ti + rowb + hx * ny] : 0.f;
+  const size_t own = (size_t)color * T.nhalf + s;
+  const float p = T.pres[own];
+  const float rhs = __int_as_float(e.z), inv = __int_as_float(e.w);
+  if (code & kCodePartial) {
+    float C[6];
+    cut_coeffs(T, i, j, k, C);
+    T.pres[own] = sor_update_inv(C, nb, rhs, p, T.omega, inv);
+  } else {
+    T.pres[own] = sor_update_open(code, nb, rhs, p, T.omega, inv);
+  }
+}
+
 // Launched with programmatic stream serialisation (all but the first sweep of a solve): the next sweep's
 // blocks may start as soon as every block of this one has started. Before griddepcontrol.wait a block
 // reads only what no sweep writes (its tank descriptor, the cell's code, rhs and cut-cell fractions, all
@@ -154,25 +184,17 @@ __global__ void __launch_bounds__(kSorThreads) k_sor(const TankDev* __restrict__
   const bool on = live && sweep < T.iters;
   float* const pres = T.pres;
   const float omega = T.omega;
-  int s = 0;
-  uint32_t code = 0;
-  float rhs = 0.f;
-  if (on) {
-    s = T.act[(size_t)color * nhalf + (q - pfx[t])];
-    code = T.code[(size_t)color * nhalf + s];
-    rhs = T.rhs[(size_t)color * nhalf + s];
-  }
+  // the cell's list entry carries its slot, code, rhs and 1/ΣC (written by the cell pass)
+  int4 e = make_int4(0, 0, 0, 0);
+  if (on) e = T.act[(size_t)color * nhalf + (q - pfx[t])];
+  const int s = e.x;
+  const uint32_t code = (uint32_t)e.y;
+  const float rhs = __int_as_float(e.z), inv = __int_as_float(e.w);
   const int row = divu(s, T.dhx), ti = s - row * hx;
   const int k = divu(row, T.dny), j = row - k * ny;
   const int i = 2 * ti + ((j + k + color) & 1);
   float C[6];
-  if (code & kCodePartial) {
-    cut_coeffs(T, i, j, k, C);
-  } else {
-#pragma unroll
-    for (int d = 0; d < 6; ++d) C[d] = (code >> d) & 1u ? 1.0f : 0.0f;
-  }
-  const float inv = coeff_inv(code & kCodePartial, code, C);
+  if (code & kCodePartial) cut_coeffs(T, i, j, k, C);
   asm volatile("griddepcontrol.wait;" ::: "memory");
   if (on) {
     const float* __restrict__ po = pres + (size_t)(1 - color) * nhalf;
@@ -185,13 +207,14 @@ __global__ void __launch_bounds__(kSorThreads) k_sor(const TankDev* __restrict__
     nb[4] = k > 0 ? po[ti + rowb - hx * ny] : 0.f;
     nb[5] = k + 1 < nz ? po[ti + rowb + hx * ny] : 0.f;
     const float p = pres[(size_t)color * nhalf + s];
-    pres[(size_t)color * nhalf + s] = sor_update_inv(C, nb, rhs, p, omega, inv);
+    pres[(size_t)color * nhalf + s] = (code & kCodePartial) ? sor_update_inv(C, nb, rhs, p, omega, inv)
+                                                            : sor_update_open(code, nb, rhs, p, omega, inv);
   }
   if (kLoop) {
     for (int r = q + (int)gridDim.x * kSorThreads; r < pfx[ntanks]; r += (int)gridDim.x * kSorThreads) {
       const int t2 = find_slot(pfx, ntanks, r);
       const TankDev& T2 = tanks[t2];
-      if (sweep < T2.iters) sor_cell(T2, color, T2.act[(size_t)color * T2.nhalf + (r - pfx[t2])]);
+      if (sweep < T2.iters) sor_entry(T2, color, T2.act[(size_t)color * T2.nhalf + (r - pfx[t2])]);
     }
   }
 }
@@ -999,7 +1022,7 @@ __global__ void __launch_bounds__(kThreads) k_sor_residual(const TankDev* __rest
   if (live) {
     const TankDev& T = tanks[t];
     const int hx = T.hx, nx = T.nx, ny = T.ny, nz = T.nz;
-    const int s = T.act[(size_t)color * T.nhalf + (q - pfx[t])];
+    const int s = T.act[(size_t)color * T.nhalf + (q - pfx[t])].x;
     const int row = divu(s, T.dhx), ti = s - row * hx;
     const int k = divu(row, T.dny), j = row - k * ny;
     const int i = 2 * ti + ((j + k + color) & 1);

@@ -54,7 +54,11 @@ class Emitter(C.Structure):
 class MeshInfo(C.Structure):
     _fields_ = [('verts', C.c_int64), ('quads', C.c_int64), ('tris', C.c_int64), ('body_verts', C.c_int64),
                 ('lone', C.c_int64), ('lattice', C.c_int32 * 3), ('taps', C.c_int32), ('lo', C.c_double * 3),
-                ('spacing', C.c_double), ('smooth', C.c_double), ('weights', C.c_double * 33)]
+                ('spacing', C.c_double), ('smooth', C.c_double), ('weights', C.c_double * 33),
+                ('phase_ms', C.c_double * 5)]
+
+
+MESH_PHASES = ('classify', 'distance_field', 'blur', 'surface_nets', 'finish')
 
 
 class Request(C.Structure):

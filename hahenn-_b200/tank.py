@@ -306,18 +306,21 @@ class Tank:
         self._c(N.lib().suiri_read_grid(self._h, field, _ptr(out), out.nbytes))
         return out
 
-    def frame_maps(self, sun, out=None):
+    def frame_maps(self, sun, out=None, read=True):
         """The maps the bake writes per frame (``bake.py:241-249``) from the last frame: float32 (W, W, 4) =
         top height (-1 dry), ripple slope d/dx, d/dz at texel centres, floor light (``Solver.caustics``,
         ``solver.py:796-846``) for the sun direction `sun`. `out` may be a reused (W, W, 4) float32 array."""
+        s = np.ascontiguousarray(sun, np.float64)
+        if s.shape != (3,):
+            raise ValueError('sun is a 3-vector')
+        if not read:                      # built on the device only (timing)
+            self._c(N.lib().suiri_frame_maps(self._h, _ptr(s), None, 0))
+            return None
         W = self.stats()['wmap']
         if out is None:
             out = np.empty((W, W, 4), np.float32)
         if out.dtype != np.float32 or out.shape != (W, W, 4) or not out.flags.c_contiguous:
             raise ValueError(f'out must be a C-contiguous float32 array of shape {(W, W, 4)}')
-        s = np.ascontiguousarray(sun, np.float64)
-        if s.shape != (3,):
-            raise ValueError('sun is a 3-vector')
         self._c(N.lib().suiri_frame_maps(self._h, _ptr(s), _ptr(out), out.nbytes))
         return out
 
@@ -333,7 +336,8 @@ class Tank:
         self._c(N.lib().suiri_surface_mesh_read(self._h, _ptr(verts), _ptr(vel), _ptr(quads), _ptr(tris), V, Q, T))
         return dict(verts=verts, vel=vel, quads=quads, tris=tris, body_verts=info.body_verts, lone=info.lone,
                     lattice=tuple(info.lattice), lo=tuple(info.lo), spacing=info.spacing,
-                    weights=np.array(info.weights[:info.taps]))
+                    weights=np.array(info.weights[:info.taps]),
+                    phase_ms=dict(zip(N.MESH_PHASES, info.phase_ms)))
 
     def caustics(self, sun):
         """Floor light relative to plain sunlight, (W, W) float32 (``Solver.caustics``)."""

@@ -78,7 +78,8 @@ typedef struct suiri_params {
   double drop_d_median;
   double drop_d_sigma_log;
   /* form of the pressure solve of the tank's own sub-steps, and of a batch or serving lane whose first tank
-     it is (sor_mode of suiri_tune; -1: cluster-resident where the lane's tanks fit, else one launch per sweep) */
+     it is (sor_mode of suiri_tune, 0..4; -1: cluster-resident where the lane's tanks fit, else one launch per
+     sweep) */
   int32_t sor_mode;
   /* polls of a bounded device wait (the cooperative solve's grid barrier) before it gives up, records error
      bit 1 in the tank's stats and returns (default 2^22; a batch or lane takes its tanks' smallest) */
@@ -244,7 +245,8 @@ int suiri_read_grid(suiri_tank* t, int32_t field, void* out, size_t bytes);
    the last frame's top-view height map and ripple field: float32 [wmap][wmap][4] = top height (-1 dry), ripple
    slope d/dx and d/dz at the texel centre (solver.py:909-919), and the floor light relative to plain sunlight,
    the sun (towards it, any length) refracted through the surface (Solver.caustics, solver.py:796-846).
-   bytes >= wmap²·16. SUIRI_ERR_INVALID for a zero or non-finite sun direction; -6 without a ripple layer. */
+   bytes >= wmap²·16; out NULL builds the maps on the device only (they are kept until the next call).
+   SUIRI_ERR_INVALID for a zero or non-finite sun direction; -6 without a ripple layer. */
 int suiri_frame_maps(suiri_tank* t, const double sun_dir[3], float* out, size_t bytes);
 
 /* The liquid's surface mesh for the frame export (meshing.surface + settle_on_top + the vertex velocity,
@@ -264,6 +266,7 @@ typedef struct suiri_mesh_info {
   int32_t taps;                    /* blur taps used, weights[0 .. taps) (normalised) */
   double lo[3], spacing, smooth;   /* lattice origin [m], spacing h/2 [m], blur sigma [nodes] */
   double weights[33];
+  double phase_ms[5];              /* device time of the build: classify, distance field, blur, surface nets, finish */
 } suiri_mesh_info;
 
 int suiri_surface_mesh(suiri_tank* t, double smooth, suiri_mesh_info* info);

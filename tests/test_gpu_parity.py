@@ -373,13 +373,14 @@ def test_ripple_layer_spectral_update(pkg, depth):
 
 def test_sor_bit_exact_when_the_sweep_grid_is_capped(pkg):
     """A tank with more active cells of one colour than the GPU has resident sweep threads (256×64×64, the
-    lower 7/8 liquid: ≈458k cells a colour against 148 SMs × 2048): the sweep grid is capped at what is
-    resident and each thread also relaxes the cells one grid further on. Pressures equal the reference's
-    float32 loop bit for bit."""
+    lower 7/8 liquid: ≈458k cells a colour against 148 SMs × 2048), with a sphere, a turned box and a tilted
+    cone cutting cells: the sweep grid is capped at what is resident and each thread also relaxes the cells one
+    grid further on, cut cells among them. Pressures equal the reference's float32 loop bit for bit."""
     nx, ny, nz, h = 256, 64, 64, 1.0 / 64
     cells = pkg.workloads.block_cells(nx, ny, nz, lambda i, j, k: j < 56)
     pos = pkg.workloads.fill_cells(cells, h, pkg.workloads.grid_origin(nx, nz, h), 1, 7)
     gpu = gpu_from(pkg, nx, ny, nz, h, flip=0.95, omega=1.7, iters=8, capacity=len(pos) + 1024)
+    gpu.set_objects(obstacle_items()[0][:3])
     gpu.add_particles(f32(pos))
     gpu.substep(1 / 240)
     assert gpu.stats()['errors'] == 0
