@@ -896,6 +896,26 @@ def run_for_profiler(args, local):
         for t in tanks:
             t.close()
         return
+    if args.workload == 'frame_export':
+        # the full scene's shape at a quarter of each axis (131k particles, 128² maps), 3 frames, then N
+        # exports (mesh and maps)
+        w = P.workloads.full_scene(scale=4)
+        prm = w['params']
+        t = P.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=prm['flip'], omega=prm['omega'],
+                   iters=prm['iters'], whitewater=True, ripple=w['ripple'], wmap=128, capacity=len(w['pos']) + 20000,
+                   ripple_sigma=prm['sigma'], ripple_rho=prm['rho'], ripple_depth=prm['depth'], drop_d=prm['drop_d'],
+                   device=local)
+        t.add_particles(w['pos'])
+        t.set_emitters(w['emitters'])
+        for _ in range(3):
+            t.step(prm['dt'])
+        for _ in range(args.ncu_steps):
+            t.surface_mesh()
+            t.frame_maps(EXPORT_SUN, read=False)
+        t.sync()
+        print('exports', args.ncu_steps, 'particles', t.stats()['count'])
+        t.close()
+        return
     w = P.workloads.obstacles_inflow()
     t = make_tank(P, w, local)
     t.tune(args.bps, args.sor_mode if args.sor_mode != 4 else 0)
