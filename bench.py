@@ -555,16 +555,20 @@ def run_batch(args, rank, world, local):
         sol = lanes[dom]['kernels']['pressure_solve']
         mode = best[dom][1]
         per_launch = 1 if mode in (1, 4) else 2 * iters
-        tr = profile_figure('sor_cluster_batch_traffic.json' if mode == 4 else 'sor_sweep_traffic.json')
+        tr = profile_figure('sor_cluster_batch_traffic.json' if mode == 4 else 'sor_batch_traffic.json') or {}
+        tr_kind = 'warm' if 'dram_bytes_per_launch' in tr else ('cold' if 'dram_bytes_per_launch_cold' in tr else None)
         roofline = dict(bound='hbm', kernel='k_sor_cluster (whole solve, one launch per lane)' if mode == 4 else
                         f'sor mode {mode}', achieved=sol['achieved_gbs'], peak=peak, unit='GB/s',
                         frac=sol['achieved_gbs'] / peak, peak_kind=kind,
-                        traffic=None if tr is None else tr.get('dram_bytes_per_launch'),
+                        traffic=tr.get('dram_bytes_per_launch', tr.get('dram_bytes_per_launch_cold')),
+                        traffic_kind=tr_kind, traffic_source='profiles/' + ('sor_cluster_batch_traffic.json' if mode == 4
+                                                                             else 'sor_batch_traffic.json'),
                         alg_bytes_per_launch=sol['alg_bytes'] / per_launch, launch_ms=sol['ms'] / per_launch,
                         lane=dom, active_cells=lanes[dom]['active_cells'], iters=iters,
                         unit_bytes='20 B per active cell per colour sweep',
                         note='the solve\'s operands stay on chip (shared memory) or in L2, so the algorithmic '
-                             'rate may exceed the HBM copy rate; traffic is the DRAM bytes ncu measured per launch')
+                             'rate may exceed the HBM copy rate; traffic is the DRAM bytes ncu measured per launch '
+                             '(warm: caches kept as in the step; cold: ncu flushed them before the launch)')
         cpu_rate, cpu_el, cpu_what = cpu_sample_rate(specs)
         launches = args.steps * sum(launches_per_substep(best[l][1], iters) for l in range(nlanes))
         line = dict(metric=METRIC, value=value, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
