@@ -9,8 +9,9 @@ Knobs (``suiri_tune`` / ``suiri_batch_tune``, ``suiri_tune_piece`` / ``suiri_bat
     cluster's shared memory;
   * the tile of sor_mode 4: the shared memory one CTA takes (piece_kb; 0 = the device's maximum), which
     sets the z planes per CTA and so the CTAs per tank and the cluster size;
-  * the form of the grid-to-particle pass (``suiri_tune_g2p``): a grid-stride walk, or one block per brick
-    with the brick's faces staged in shared memory; tried with the best of the other knobs.
+  * the form of the grid-to-particle pass (``suiri_tune_g2p``): a grid-stride walk, its common path with the
+    rare branches deferred to a second pass, or one block per brick with the brick's faces staged in shared
+    memory; tried with the best of the other knobs.
 
 A batch is tuned lane by lane (``autotune_batch``): its size lanes run concurrently, and small tanks may
 prefer another form than large ones.
@@ -25,7 +26,7 @@ CANDIDATES = ((2, 0, 0), (4, 0, 0), (8, 0, 0), (4, 2, 0), (4, 3, 0), (4, 1, 0),
               (2, 4, 0), (2, 4, 192), (2, 4, 128), (2, 4, 96), (2, 4, 64), (4, 4, 0))
 
 
-G2P_FORMS = (0, 1)
+G2P_FORMS = (0, 2, 1)
 
 
 def _time(target, dt, steps):

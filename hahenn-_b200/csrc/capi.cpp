@@ -602,7 +602,7 @@ static void tune_piece(Group& g, int32_t piece_kb) {
 }
 
 static void tune_g2p(Group& g, int32_t form) {
-  if (form != 0 && form != 1) throw Error(SUIRI_ERR_INVALID, "g2p form is 0 or 1");
+  if (form < 0 || form > 2) throw Error(SUIRI_ERR_INVALID, "g2p form is 0, 1 or 2");
   if (form == g.g2p_form) return;
   CK(cudaStreamSynchronize(g.stream));
   g.g2p_form = form;

@@ -962,6 +962,9 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
   CK(cudaMemsetAsync(d_barrier, 0, sizeof(GridBarrier), stream));
   CK(cudaMallocAsync(&d_ticket, 4 * sizeof(unsigned), stream));
   CK(cudaMemsetAsync(d_ticket, 0, 4 * sizeof(unsigned), stream));
+  size_t defer_cap = 1;                 // G2P form 2: every particle of the group may be deferred
+  for (Tank* x : tanks) defer_cap += (size_t)x->d.cap + (size_t)std::max(x->d.emit_cap, 0);
+  CK(cudaMallocAsync(&d_defer, defer_cap * sizeof(int) + 16, stream));
   // one block per SM: the grid barrier's cost grows with the number of arriving blocks
   sor_blocks = std::min(std::min(sor_persist_max_blocks(device), sm_count), std::max(1, (hp[n] + kThreads - 1) / kThreads));
   CK(cudaStreamSynchronize(stream));
@@ -969,6 +972,8 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
   ctx.apfx = d_apfx;
   ctx.barrier = d_barrier;
   ctx.ticket = d_ticket;
+  ctx.defer_n = d_defer;
+  ctx.defer_list = d_defer + 4;
   ctx.stream = stream;
   ctx.tanks = d_tanks;
   ctx.ntanks = n;
@@ -1009,7 +1014,7 @@ Group::~Group() {
   drop_cluster_classes();
   if (cl_fork) cudaEventDestroy(cl_fork);
   for (void* p : {(void*)d_hpfx, (void*)d_apfx, (void*)d_barrier, (void*)d_ticket, d_tbl, (void*)d_tanks, (void*)d_bpfx,
-                  (void*)d_ppfx, (void*)d_bsum, (void*)d_pieces})
+                  (void*)d_ppfx, (void*)d_bsum, (void*)d_pieces, (void*)d_defer})
     if (p) cudaFreeAsync(p, stream);
   delete[] h_tanks;
   if (own_stream) cudaStreamDestroy(stream);

@@ -179,6 +179,7 @@ struct Group {
   int* d_apfx = nullptr;          // per colour, prefix of the active cells over the tanks
   void* d_tbl = nullptr;          // per-tile lists of the two-sweeps-per-launch solve (allocated when tuned to it)
   unsigned* d_ticket = nullptr;   // last-block tickets of the kernels that end in a prefix over tanks
+  int* d_defer = nullptr;         // G2P form 2: the count, then the deferred particles' sorted indices
   void ensure_tbl();
   GridBarrier* d_barrier = nullptr;
   int sor_mode = 0;               // 0: one launch per colour sweep, 1: one cooperative launch per solve,
@@ -198,7 +199,8 @@ struct Group {
   int cl_piece_kb = 0;            // shared memory per CTA at most (tile knob; 0: the device maximum)
   void plan_cluster();            // throws if a tank cannot be held by one cluster
   bool residual = false;          // FP64 residual of every solve into the tank counters
-  int g2p_form = 0;               // 0 grid-stride walk, 1 per-brick with the faces in shared memory (tuner knob)
+  int g2p_form = 0;               // 0 grid-stride walk, 1 per-brick with the faces in shared memory, 2 the walk's
+                                  // common path with the rare branches deferred to a second pass (tuner knob)
   bool profile = false;           // record events between the phases of the sub-step (inside the graph too)
   static constexpr int kPhases = 6;   // binning+sort, P2G, node+cell passes, pressure solve, projection, G2P
   cudaEvent_t ev_ph[kPhases + 1] = {};

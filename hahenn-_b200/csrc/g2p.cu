@@ -197,9 +197,14 @@ __device__ inline void crown(const TankDev& T, double cx, double cy, double cz, 
 // `faces`, advection, collision, walls, drains, the free-flight mark and merging of sub-grid drops and
 // whitewater spawning; writes the new state to A at the same slot. Returns 1 + the float64 bits of its
 // capped speed when it is inside the grid (0 otherwise), for the speed maximum.
-template <class F>
+// kFast: the common path only. Where the particle needs a rare branch (RK2, an obstacle within reach, the
+// free-flight test of a sparse cell, a falling drop, a whitewater spawn) it sets *defer and returns without
+// writing; the full body then runs for it in a second pass (k_g2p_deferred), from the same inputs, so every
+// particle gets exactly the arithmetic of the full body. Without those branches the fast body needs far
+// fewer registers, and more warps fit per SM.
+template <class F, bool kFast = false>
 __device__ __forceinline__ unsigned long long g2p_particle(const TankDev& T, int local, const float4 P, const float4 V,
-                                                           const F& faces) {
+                                                           const F& faces, bool* defer = nullptr) {
   unsigned long long vbits = 0ull;
   const int flags = flags_of(P.w);
   const uint32_t id = __float_as_uint(V.w);
@@ -225,7 +230,8 @@ __device__ __forceinline__ unsigned long long g2p_particle(const TankDev& T, int
     v[1] -= T.g * dt;
   }
   double x[3] = {x0[0] + v[0] * dt, x0[1] + v[1] * dt, x0[2] + v[2] * dt};
-  if (T.advect && ing) {
+  if (kFast && T.advect && ing) { *defer = true; return 0ull; }
+  if (!kFast && T.advect && ing) {
     // midpoint rule through the grid velocity (no reference counterpart): xm = x0 + u0·dt/2, x = x0 +
     // u(xm)·dt; u falls back to u0 where no face took weight, Euler if the midpoint leaves the grid
     const double hd = 0.5 * dt;
@@ -241,7 +247,8 @@ __device__ __forceinline__ unsigned long long g2p_particle(const TankDev& T, int
     }
   }
   const double rc = 0.32 * h;
-  if (maybe_within(T, x[0], x[1], x[2], rc)) {
+  if (kFast && maybe_within(T, x[0], x[1], x[2], rc)) { *defer = true; return 0ull; }
+  if (!kFast && maybe_within(T, x[0], x[1], x[2], rc)) {
     const double d = tank_sdf(T, x[0], x[1], x[2]);
     if (d < rc) {
       double nx, ny, nz;
@@ -271,6 +278,7 @@ __device__ __forceinline__ unsigned long long g2p_particle(const TankDev& T, int
     if (n0 >= 4) {
       air = false;
     } else if (n0 <= 2 && c0[1] + 2 < T.ny) {
+      if (kFast) { *defer = true; return 0ull; }
       int around = 0, above = 0;
 #pragma unroll
       for (int dz = -1; dz <= 1; ++dz)
@@ -287,6 +295,7 @@ __device__ __forceinline__ unsigned long long g2p_particle(const TankDev& T, int
   const int frame = T.ctr->frame;
   double g1[3] = {-1.0, -1.0, -1.0};
   const bool falling = air && vold[1] < -0.3;
+  if (kFast && falling) { *defer = true; return 0ull; }
   if (falling) grid_pos(T, x[0], x[1], x[2], g1[0], g1[1], g1[2]);     // only a falling drop may merge
   if (falling && in_grid(T, g1[0], g1[1], g1[2])) {
     const int c1[3] = {(int)floor(g1[0]), (int)floor(g1[1]), (int)floor(g1[2])};
@@ -330,7 +339,8 @@ __device__ __forceinline__ unsigned long long g2p_particle(const TankDev& T, int
       if (near) {
         uint32_t s = hash_u32(id * 9781u + (uint32_t)frame * 6271u + 17u);
         const double e = fmin(fmax((sp - 0.75) / 1.6, 0.0), 1.0);
-        if (rnd(s) < T.ww_rate * e * e * dt) {
+        if (kFast && rnd(s) < T.ww_rate * e * e * dt) { *defer = true; return 0ull; }
+        if (!kFast && rnd(s) < T.ww_rate * e * e * dt) {
           const double j0 = rnd(s) - 0.5, j1 = rnd(s) - 0.5, j2 = rnd(s) - 0.5;
           const double life = 1.0 + 2.5 * rnd(s);
           const double f = 0.8 + 0.35 * rnd(s);
@@ -349,7 +359,9 @@ __device__ __forceinline__ unsigned long long g2p_particle(const TankDev& T, int
   return vbits;
 }
 
-__global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ pfx) {
+template <bool kSplit>
+__global__ void __launch_bounds__(kThreads, kSplit ? 3 : 1) k_g2p(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ pfx,
+                                                  int* __restrict__ defer_list, int* __restrict__ defer_n) {
   const int total = pfx[ntanks];
   const int stride = gridDim.x * blockDim.x;
   const int lane = threadIdx.x & 31;
@@ -376,7 +388,20 @@ __global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ ta
     fetch(base + stride + lane);
     unsigned long long vbits = 0ull;
     const int tt = t;
-    if (t >= 0) vbits = g2p_particle(tanks[t], local, P, V, GlobalFaces{});
+    if (kSplit) {
+      bool defer = false;
+      if (t >= 0) vbits = g2p_particle<GlobalFaces, true>(tanks[t], local, P, V, GlobalFaces{}, &defer);
+      // the deferred particles of the warp: one atomic, then consecutive entries
+      const unsigned m = __ballot_sync(0xffffffffu, defer);
+      if (m) {
+        int at = 0;
+        if (lane == __ffs(m) - 1) at = atomicAdd(defer_n, __popc(m));
+        at = __shfl_sync(0xffffffffu, at, __ffs(m) - 1);
+        if (defer) defer_list[at + __popc(m & ((1u << lane) - 1))] = base + lane;
+      }
+    } else if (t >= 0) {
+      vbits = g2p_particle(tanks[t], local, P, V, GlobalFaces{});
+    }
     // non-negative doubles order like their bit patterns: a warp max, then one atomic per warp and tank
     const int t0 = __shfl_sync(0xffffffffu, tt, 0);
     if (__all_sync(0xffffffffu, tt == t0 || tt < 0)) {
@@ -390,6 +415,22 @@ __global__ void __launch_bounds__(kThreads) k_g2p(const TankDev* __restrict__ ta
     } else if (vbits) {
       atomicMax((unsigned long long*)&tanks[tt].ctr->vmax_bits64, vbits);
     }
+  }
+}
+
+// the deferred particles of k_g2p<true> with the full body (sorted index q over all tanks); the list was
+// filled by the kernel before in the stream, so its count is read here
+__global__ void __launch_bounds__(kThreads) k_g2p_deferred(const TankDev* __restrict__ tanks, int ntanks,
+                                                           const int* __restrict__ pfx, const int* __restrict__ defer_list,
+                                                           const int* __restrict__ defer_n) {
+  const int n = *defer_n;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int q = defer_list[e];
+    const int t = find_slot(pfx, ntanks, q);
+    const int local = q - pfx[t];
+    const TankDev& T = tanks[t];
+    const unsigned long long vb = g2p_particle(T, local, __ldcs(T.pB + local), __ldcs(T.vB + local), GlobalFaces{});
+    if (vb) atomicMax((unsigned long long*)&T.ctr->vmax_bits64, vb);
   }
 }
 
@@ -581,14 +622,24 @@ __global__ void k_whitewater_end(const TankDev* __restrict__ tanks, int ntanks) 
 // than the other particle kernels), so that the grid-stride loop runs in one wave
 int g2p_blocks(const LaunchCtx& L) {
   static int resident[128] = {};
-  return std::min(L.particle_blocks, resident_grid((const void*)k_g2p, resident));
+  return std::min(L.particle_blocks, resident_grid((const void*)k_g2p<false>, resident));
 }
 
+// form 0: the grid-stride walk; 1: per brick with the faces in shared memory; 2: the walk's common path with
+// the rare branches deferred to a second pass over a list
 void launch_g2p(const LaunchCtx& L, int form) {
-  if (form == 1)
+  if (form == 1) {
     k_g2p_brick<<<L.nblocks[kFamG2P], kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.bpfx[kFamG2P]);
-  else
-    k_g2p<<<g2p_blocks(L), kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_sorted);
+  } else if (form == 2) {
+    static int resident[128] = {}, resident_d[128] = {};
+    cudaMemsetAsync(L.defer_n, 0, sizeof(int), L.stream);
+    const int nb = std::min(2 * L.particle_blocks, resident_grid((const void*)k_g2p<true>, resident));
+    k_g2p<true><<<nb, kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_sorted, L.defer_list, L.defer_n);
+    k_g2p_deferred<<<resident_grid((const void*)k_g2p_deferred, resident_d), kThreads, 0, L.stream>>>(
+        L.tanks, L.ntanks, L.ppfx_sorted, L.defer_list, L.defer_n);
+  } else {
+    k_g2p<false><<<g2p_blocks(L), kThreads, 0, L.stream>>>(L.tanks, L.ntanks, L.ppfx_sorted, nullptr, nullptr);
+  }
 }
 void launch_whitewater(const LaunchCtx& L, double frame_dt) {
   k_whitewater<<<L.particle_blocks, kThreads, 0, L.stream>>>(L.tanks, L.ntanks, frame_dt);

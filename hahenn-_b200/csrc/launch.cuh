@@ -32,6 +32,8 @@ struct LaunchCtx {
   uint2* tbl_list;          // device, two sweeps per launch: per tile the active-cell lists (k_tbl_lists)
   int* tbl_cnt;             //   per tile: entries of list A, B, C
   int2* tbl_c;              //   per tile: colour-0 cells with a constant pressure other than +0
+  int* defer_list;          // device, G2P form 2: sorted indices of the particles deferred to the full body
+  int* defer_n;             //   and their count
 };
 
 // One CTA of the cluster-resident solve: planes [k0, k0+nk) of tank `tank` (index into the launch's

@@ -321,6 +321,10 @@ int suiri_batch_tune_piece(suiri_batch* b, int32_t piece_kb);
 /* form of the grid-to-particle pass: 0 a grid-stride walk over the sorted particles (corner loads from the
    node arrays), 1 one block per 8×8×8-cell brick with the brick's face nodes copied to shared memory first.
    Both give the same particles bit for bit. */
+/* form of the grid-to-particle pass: 0 a grid-stride walk over the sorted particles; 1 one block per 8³ brick with
+   its faces staged in shared memory; 2 the walk's common path (fewer registers, more warps) with the particles
+   that need a rare branch (RK2, an obstacle within reach, a sparse cell's free-flight test, a falling drop, a
+   whitewater spawn) deferred to a second pass that runs the full update for them. All give the same particles. */
 int suiri_tune_g2p(suiri_tank* t, int32_t form);
 int suiri_batch_tune_g2p(suiri_batch* b, int32_t form);
 /* all knobs of one size lane of a batch (lane in [0, suiri_batch_lanes)): the lanes run concurrently and may

@@ -707,12 +707,15 @@ def test_full_size_obstacles_inflow_substeps(pkg):
     gpu.close()
 
 
+@pytest.mark.parametrize('form', [1, 2])
 @pytest.mark.parametrize('advect', ['euler', 'rk2'])
-def test_g2p_brick_form_equals_the_walk(pkg, advect):
-    """The per-brick grid-to-particle form (faces staged in shared memory, one block per 8×8×8 brick and one
-    for the particles outside the grid) gives the particles of the grid-stride walk bit for bit: a tank with
-    obstacles and an odd size, a pool with airborne drops falling into it, and particles above the rim
-    (outside the grid), with Euler and RK2 advection; whitewater counts and the speed maximum agree."""
+def test_g2p_brick_form_equals_the_walk(pkg, advect, form):
+    """The per-brick grid-to-particle form (1: faces staged in shared memory, one block per 8×8×8 brick and
+    one for the particles outside the grid) and the split form (2: the common path, with the particles that
+    need obstacles, the free-flight test, merging or a whitewater spawn deferred to a second pass) give the
+    particles of the grid-stride walk bit for bit: a tank with obstacles and an odd size, a pool with airborne
+    drops falling into it, and particles above the rim (outside the grid), with Euler and RK2 advection;
+    whitewater counts, impacts and the speed maximum agree."""
     w = pkg.workloads.random_tank(5, axes=(21, 37, 19))
     rng = np.random.default_rng(4)
     hi = np.array([w['nx'], w['ny'], w['nz']]) * w['h'] + w['origin']
@@ -738,7 +741,7 @@ def test_g2p_brick_form_equals_the_walk(pkg, advect):
         t.close()
         return out
 
-    walk, brick = run(0), run(1)
+    walk, brick = run(0), run(form)
     for x, y in zip(walk[:4], brick[:4]):
         np.testing.assert_array_equal(x, y)
     assert walk[4:] == brick[4:]

@@ -56,7 +56,7 @@ def test_autotune_keeps_the_fastest_and_skips_shapes_that_fail():
     best, timings = autotune.autotune(t, 1 / 240)
     assert best == (2, 4, 128, 1) and t.key() == (2, 4, 128, 1)
     assert timings[(4, 1, 0, 0)] == float('inf') and timings[(2, 4, 128, 0)] == pytest.approx(3.0)
-    assert set(timings) == {c + (0,) for c in autotune.CANDIDATES} | {(2, 4, 128, 1)}
+    assert set(timings) == {c + (0,) for c in autotune.CANDIDATES} | {(2, 4, 128, f) for f in autotune.G2P_FORMS}
     assert t.substeps == 7              # the tuning sub-steps were rolled back
     assert {c[1] for c in autotune.CANDIDATES} >= {0, 1, 2, 3, 4}
     assert len({c[2] for c in autotune.CANDIDATES if c[1] == 4}) >= 3     # tile sizes of the cluster solve
