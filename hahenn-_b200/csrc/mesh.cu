@@ -6,7 +6,9 @@
 //              bounding box (float32 positions, ordered-key atomics) sizes the lattice
 //   splat      the body's distance field on a lattice of spacing h/2 around that box: every particle
 //              lowers the 4×4×4 nodes around it to |node - x| - r (float64, kept float32 by an ordered-key
-//              minimum, so the field does not depend on the order of the atomics); far value 2·spacing
+//              minimum, so the field does not depend on the order of the atomics); far value 2·spacing. The
+//              particles are put in cell order first, and one block per tile of 8×4×4 cells takes its minima
+//              in shared memory and then one global minimum per node it lowered
 //   smooth     clipped to [-r, far], blurred along x, y, z with normalised Gaussian taps, each tap added in
 //              float64 and rounded to float32 as the reference's float32 array accumulates it
 //   nets       surface nets: a vertex per cell whose corners change sign (the mean of its edge crossings),
@@ -118,14 +120,99 @@ __global__ void k_mesh_fill(unsigned* __restrict__ key, long long n, unsigned v)
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) key[e] = v;
 }
 
-// the body's distance field (meshing.py:76-92): the 4×4×4 lattice nodes from floor(q) - 1 on
-__global__ void __launch_bounds__(256) k_mesh_splat(const TankDev* __restrict__ Tp, const uint8_t* __restrict__ kind,
-                                                    MeshGeom G, unsigned* __restrict__ key) {
+// Cell order of the in-grid particles of A∪E (the counts and offsets of the frame-end count pass): their
+// indices, grouped by cell, so that a tile of cells finds its particles as a few contiguous runs
+__global__ void __launch_bounds__(256) k_mesh_order(const TankDev* __restrict__ Tp, int* __restrict__ fill,
+                                                    int* __restrict__ order) {
   const TankDev& T = *Tp;
   const int n_live = T.ctr->n_live, n = n_live + T.ctr->n_emit;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-    if (kind[q] != 0) continue;
+  const int lane = threadIdx.x & 31;
+  for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += gridDim.x * blockDim.x) {
+    const int q = base + lane;
+    int cell = -1;
+    if (q < n) {
+      const float4 p = q < n_live ? T.pA[q] : T.pE[q - n_live];
+      if (!(flags_of(p.w) & kFlagDead)) {
+        double gx, gy, gz;
+        grid_pos(T, (double)p.x, (double)p.y, (double)p.z, gx, gy, gz);
+        if (in_grid(T, gx, gy, gz)) cell = cell_idx(T, (int)gx, (int)gy, (int)gz);
+      }
+    }
+    const unsigned act = __ballot_sync(0xffffffffu, cell >= 0);
+    if (cell >= 0) {
+      const unsigned peers = __match_any_sync(act, (unsigned)cell);
+      const int leader = __ffs(peers) - 1;
+      int first = 0;
+      if (lane == leader) first = atomicAdd(fill + cell, __popc(peers));
+      first = __shfl_sync(act, first, leader);
+      order[T.off[cell] + first + __popc(peers & ((1u << lane) - 1u))] = q;
+    }
+  }
+}
+
+// The body's distance field per tile of kTX×kTY×kTZ cells: the particles of the tile's cells that are not lone
+// (the same 27-cell count test as k_mesh_classify, per cell) lower the lattice nodes around them in a
+// shared-memory copy of the nodes the tile can reach, then each node the tile lowered takes one global
+// minimum. Same values as one global minimum per particle and node: a minimum does not depend on order.
+constexpr int kTX = 8, kTY = 4, kTZ = 4;
+constexpr int kBX = 2 * kTX + 6, kBY = 2 * kTY + 6, kBZ = 2 * kTZ + 6;   // node box: 2 nodes a cell + margins
+__global__ void __launch_bounds__(256) k_mesh_splat_tiles(const TankDev* __restrict__ Tp, const int* __restrict__ order,
+                                                          MeshGeom G, unsigned far_key, unsigned* __restrict__ key) {
+  __shared__ unsigned s_key[kBX * kBY * kBZ];
+  __shared__ int s_row0[kTY * kTZ], s_rowp[kTY * kTZ + 1];
+  __shared__ unsigned char s_lone[kTX * kTY * kTZ];
+  const TankDev& T = *Tp;
+  const int tnx = (T.nx + kTX - 1) / kTX, tny = (T.ny + kTY - 1) / kTY;
+  const int ci0 = (blockIdx.x % tnx) * kTX, cj0 = ((blockIdx.x / tnx) % tny) * kTY, ck0 = (blockIdx.x / (tnx * tny)) * kTZ;
+  const int ci1 = min(ci0 + kTX, T.nx);
+  if (threadIdx.x < kTY * kTZ) {
+    const int j = cj0 + threadIdx.x % kTY, k = ck0 + threadIdx.x / kTY;
+    int a = 0, b = 0;
+    if (j < T.ny && k < T.nz) {
+      a = T.off[cell_idx(T, ci0, j, k)];
+      b = T.off[cell_idx(T, ci1 - 1, j, k) + 1];
+    }
+    s_row0[threadIdx.x] = a;
+    s_rowp[threadIdx.x + 1] = b - a;
+  }
+  for (int c = threadIdx.x; c < kTX * kTY * kTZ; c += blockDim.x) {
+    const int i = ci0 + c % kTX, j = cj0 + (c / kTX) % kTY, k = ck0 + c / (kTX * kTY);
+    int near = 0;
+    if (i < T.nx && j < T.ny && k < T.nz)
+      for (int dk = -1; dk <= 1; ++dk)
+        for (int dj = -1; dj <= 1; ++dj)
+          for (int di = -1; di <= 1; ++di) near += cell_count(T, i + di, j + dj, k + dk);
+    s_lone[c] = near <= 6;
+  }
+  for (int e = threadIdx.x; e < kBX * kBY * kBZ; e += blockDim.x) s_key[e] = far_key;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_rowp[0] = 0;
+    for (int r = 1; r <= kTY * kTZ; ++r) s_rowp[r] += s_rowp[r - 1];
+  }
+  __syncthreads();
+  const int total = s_rowp[kTY * kTZ];
+  if (total == 0) return;
+  // the node box's first node per axis: two below the lattice node of the tile's low cell corner
+  const long long b0[3] = {(long long)floor(((T.ox + ci0 * T.h) - G.lo[0]) / G.sp) - 2,
+                           (long long)floor(((T.oy + cj0 * T.h) - G.lo[1]) / G.sp) - 2,
+                           (long long)floor(((T.oz + ck0 * T.h) - G.lo[2]) / G.sp) - 2};
+  const int n_live = T.ctr->n_live, n_all = n_live + T.ctr->n_emit;
+  for (int qq = threadIdx.x; qq < total; qq += blockDim.x) {
+    int lo = 0, hi = kTY * kTZ - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (s_rowp[mid] <= qq) lo = mid; else hi = mid - 1;
+    }
+    const int slot = s_row0[lo] + (qq - s_rowp[lo]);
+    const int q = order[slot];
+    if (q < 0 || q >= n_all) continue;
     const float4 p = q < n_live ? T.pA[q] : T.pE[q - n_live];
+    double gx, gy, gz;
+    grid_pos(T, (double)p.x, (double)p.y, (double)p.z, gx, gy, gz);
+    const int ci = (int)gx - ci0, cj = (int)gy - cj0, ck = (int)gz - ck0;
+    if (ci < 0 || ci >= kTX || cj < 0 || cj >= kTY || ck < 0 || ck >= kTZ) continue;
+    if (s_lone[ci + kTX * (cj + kTY * ck)]) continue;
     const double u[3] = {((double)p.x - G.lo[0]) / G.sp, ((double)p.y - G.lo[1]) / G.sp, ((double)p.z - G.lo[2]) / G.sp};
     const long long b[3] = {(long long)floor(u[0]), (long long)floor(u[1]), (long long)floor(u[2])};
     for (int ox = -1; ox <= 2; ++ox) {
@@ -142,10 +229,23 @@ __global__ void __launch_bounds__(256) k_mesh_splat(const TankDev* __restrict__ 
           const double ez = ((double)z - u[2]) * G.sp;
           const double d = sqrt(ex * ex + ey * ey + ez * ez) - G.r;
           if (!(d < G.far_)) continue;
-          atomicMin(key + (x * G.Y + y) * G.Z + z, okey(__double2float_rn(d)));
+          const unsigned kv = okey(__double2float_rn(d));
+          const long long lx = x - b0[0], ly = y - b0[1], lz = z - b0[2];
+          if (lx >= 0 && lx < kBX && ly >= 0 && ly < kBY && lz >= 0 && lz < kBZ)
+            atomicMin(s_key + lx + kBX * (ly + kBY * lz), kv);
+          else
+            atomicMin(key + (x * G.Y + y) * G.Z + z, kv);    // outside the box (not expected): directly
         }
       }
     }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < kBX * kBY * kBZ; e += blockDim.x) {
+    const unsigned v = s_key[e];
+    if (v == far_key) continue;
+    const long long x = b0[0] + e % kBX, y = b0[1] + (e / kBX) % kBY, z = b0[2] + e / (kBX * kBY);
+    if (x < 0 || x >= G.X || y < 0 || y >= G.Y || z < 0 || z >= G.Z) continue;
+    atomicMin(key + (x * G.Y + y) * G.Z + z, v);
   }
 }
 
@@ -521,6 +621,8 @@ struct MeshState {
   double* vtx = nullptr; size_t vtx_cap = 0;
   int4* quads = nullptr; size_t quad_cap = 0;
   int* lone_idx = nullptr; size_t lone_cap = 0;
+  int* fill = nullptr; size_t fill_cap = 0;          // per cell, the particles placed in cell order so far
+  int* order = nullptr; size_t order_cap = 0;        // in-grid particles in cell order
   float* pos = nullptr; size_t pos_cap = 0;
   float* vel = nullptr; size_t vel_cap = 0;
   MeshInfo info{};
@@ -542,7 +644,7 @@ void free_mesh(Tank& t) {
   MeshState* m = (MeshState*)t.mesh;
   if (!m) return;
   void* dev[] = {m->d_mc, m->d_ico, m->kind, m->key, m->phiA, m->phiB, m->vid, m->bcount, m->vtx, m->quads,
-                 m->lone_idx, m->pos, m->vel};
+                 m->lone_idx, m->pos, m->vel, m->fill, m->order};
   for (void* p : dev) if (p) cudaFree(p);
   if (m->h_mc) cudaFreeHost(m->h_mc);
   if (m->h_base) cudaFreeHost(m->h_base);
@@ -631,7 +733,13 @@ MeshInfo build_surface_mesh(Tank& t, double smooth) {
     const unsigned far_key = [&] { unsigned b; memcpy(&b, &G.far32, 4); return (b & 0x80000000u) ? ~b : (b | 0x80000000u); }();
     CK(cudaEventRecord(M.ev[2], t.stream));
     k_mesh_fill<<<grid, 256, 0, t.stream>>>(M.key, nodes, far_key);
-    k_mesh_splat<<<grid, 256, 0, t.stream>>>(dT, M.kind, G, M.key);
+    // the in-grid particles in cell order, then one block per tile of cells
+    grow(M.fill, M.fill_cap, (size_t)D.ncells);
+    grow(M.order, M.order_cap, (size_t)std::max<long long>(n, 1));
+    CK(cudaMemsetAsync(M.fill, 0, (size_t)D.ncells * sizeof(int), t.stream));
+    k_mesh_order<<<grid, 256, 0, t.stream>>>(dT, M.fill, M.order);
+    const int tiles = ((D.nx + kTX - 1) / kTX) * ((D.ny + kTY - 1) / kTY) * ((D.nz + kTZ - 1) / kTZ);
+    k_mesh_splat_tiles<<<tiles, 256, 0, t.stream>>>(dT, M.order, G, far_key, M.key);
     CK(cudaEventRecord(M.ev[3], t.stream));
     CK(cudaEventRecord(M.ev[4], t.stream));
     k_mesh_blur<0><<<grid, 256, 0, t.stream>>>(M.key, M.phiA, G, taps);
