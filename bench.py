@@ -859,9 +859,9 @@ def run_frame_export(args, local):
                                          f'of the scene at a quarter of each axis ({cpu_n} particles, 128² maps), '
                                          f'{cpu_s:.1f} s on one core'),
                 e2e=dict(value=particles / e2e_s, unit='particles/s', h2d_bytes_per_step=0, d2h_bytes_per_step=int(d2h)),
-                # per export: 4 of the cell count, 12 of the mesh (classify, fill, splat, 3 blur passes,
-                # count, scan, cells, quads, lone, finish), 2 of the light maps
-                gpu_launches=18 * args.steps, clocks=clk)
+                # per export: 4 of the cell count, 13 of the mesh (classify, fill, cell order, tile splat,
+                # 3 blur passes, count, scan, cells, quads, lone, finish), 2 of the light maps
+                gpu_launches=19 * args.steps, clocks=clk)
     print(json.dumps(line), flush=True)
     t.close()
 
