@@ -551,6 +551,27 @@ int suiri_batch_create(suiri_tank* const* tanks, int32_t n, suiri_batch** out) {
   return SUIRI_OK;
 }
 
+int suiri_batch_create_lanes(suiri_tank* const* tanks, int32_t n, const int32_t* lane_of, suiri_batch** out) {
+  if (!out || !tanks || n <= 0) { g_err = "batch needs tanks"; return SUIRI_ERR_INVALID; }
+  *out = nullptr;
+  std::unique_ptr<suiri_batch> b(new suiri_batch());
+  const int rc = guard(nullptr, [&] {
+    std::vector<Tank*> v;
+    std::vector<int> l;
+    for (int i = 0; i < n; ++i) {
+      v.push_back(T(tanks[i]));
+      if (lane_of) {
+        if (lane_of[i] < 0 || lane_of[i] >= kMaxLanes) throw Error(SUIRI_ERR_INVALID, "lane index in 0..7");
+        l.push_back(lane_of[i]);
+      }
+    }
+    b->b.reset(new Batch(v, lane_of ? l.data() : nullptr));
+  });
+  if (rc != SUIRI_OK) return rc;
+  *out = b.release();
+  return SUIRI_OK;
+}
+
 int suiri_batch_destroy(suiri_batch* b) {
   if (!b) return SUIRI_ERR_INVALID;
   const int rc = guard(nullptr, [&] { b->b.reset(); });

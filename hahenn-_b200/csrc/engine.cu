@@ -1098,12 +1098,16 @@ void Group::plan_cluster() {
   cl_classes = classes;
 }
 
-Batch::Batch(const std::vector<Tank*>& t) {
+Batch::Batch(const std::vector<Tank*>& t, const int* lane_of) {
   if (t.empty()) throw Error(-1, "a batch needs at least one tank");
   for (Tank* x : t)
     if (x->cfg.device != t[0]->cfg.device) throw Error(-1, "all tanks of a batch must be on one device");
-  std::vector<Tank*> by_lane[kSizeLanes];
-  for (Tank* x : t) by_lane[size_lane((long long)x->d.nx * x->d.ny * x->d.nz)].push_back(x);
+  std::vector<Tank*> by_lane[kMaxLanes];
+  for (size_t i = 0; i < t.size(); ++i) {
+    const int l = lane_of ? lane_of[i] : size_lane((long long)t[i]->d.nx * t[i]->d.ny * t[i]->d.nz);
+    if (l < 0 || l >= kMaxLanes) throw Error(-1, "lane index out of range");
+    by_lane[l].push_back(t[i]);
+  }
   for (auto& v : by_lane)
     if (!v.empty()) lanes.emplace_back(new Group(v, nullptr));
   if (lanes.size() == 1) {

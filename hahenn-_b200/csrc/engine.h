@@ -226,6 +226,7 @@ struct Group {
 // as its own group on its own stream, so a lane of small tanks does not wait for the largest tank's
 // kernels and the lanes' kernels overlap on the GPU.
 constexpr int kSizeLanes = 3;
+constexpr int kMaxLanes = 8;    // lanes a batch may be given explicitly
 inline int size_lane(long long cells) { return cells < (1LL << 16) ? 0 : (cells < (1LL << 19) ? 1 : 2); }
 
 // A batch of tanks: one group per occupied size lane. Every sub-step forks from the batch's stream to the
@@ -237,7 +238,7 @@ struct Batch {
   cudaEvent_t fork = nullptr;
   std::vector<cudaEvent_t> join;
 
-  explicit Batch(const std::vector<Tank*>& t);
+  explicit Batch(const std::vector<Tank*>& t, const int* lane_of = nullptr);   // lane_of: a lane per tank
   ~Batch();
   void substep(double dt);
 };

@@ -122,6 +122,7 @@ SIGNATURES = {
     'suiri_stream': (C.c_int, [P, C.POINTER(P)]),
     'suiri_use_graphs': (C.c_int, [P, C.c_int32]),
     'suiri_batch_create': (C.c_int, [C.POINTER(P), C.c_int32, C.POINTER(P)]),
+    'suiri_batch_create_lanes': (C.c_int, [C.POINTER(P), C.c_int32, P, C.POINTER(P)]),
     'suiri_batch_destroy': (C.c_int, [P]),
     'suiri_batch_substep': (C.c_int, [P, C.c_double]),
     'suiri_batch_sync': (C.c_int, [P]),

@@ -369,14 +369,41 @@ class Tank:
     liters = water_liters
 
 
+def balanced_lanes(cells, particles, k):
+    """Lane per tank for `k` lanes of tanks contiguous in size (cells), each lane with about the same number of
+    particles: small tanks stay together (their latency-bound sweeps do not wait for large tanks' kernels) and
+    no lane holds most of the work. Tanks of the same size share a lane."""
+    cells, particles = np.asarray(cells), np.asarray(particles, np.float64)
+    order = np.argsort(cells, kind='stable')
+    cum = np.cumsum(particles[order])
+    tot = cum[-1] if len(cum) else 0.0
+    lane = np.empty(len(cells), np.int32)
+    for rank, i in enumerate(order):
+        before = cum[rank] - particles[i]
+        lane[i] = min(k - 1, int(k * (before + 0.5 * particles[i]) / max(tot, 1.0)))
+    for rank in range(1, len(order)):
+        a, b = order[rank - 1], order[rank]
+        if cells[a] == cells[b]:
+            lane[b] = lane[a]
+    return lane
+
+
 class Batch:
     """Many tanks stepped by shared launches (one descriptor table, one CUDA graph per sub-step)."""
 
-    def __init__(self, tanks):
+    def __init__(self, tanks, lanes=None):
+        """`lanes`: None for the size lanes (under 2^16 cells, under 2^19, larger), or a lane index 0..7 per
+        tank (see `balanced_lanes`)."""
         self.tanks = list(tanks)
         arr = (C.c_void_p * len(self.tanks))(*[t.handle.value for t in self.tanks])
         h = C.c_void_p()
-        N.check(N.lib().suiri_batch_create(arr, len(self.tanks), C.byref(h)))
+        if lanes is None:
+            N.check(N.lib().suiri_batch_create(arr, len(self.tanks), C.byref(h)))
+        else:
+            lo = np.ascontiguousarray(lanes, np.int32)
+            if lo.shape != (len(self.tanks),):
+                raise ValueError('one lane per tank')
+            N.check(N.lib().suiri_batch_create_lanes(arr, len(self.tanks), _ptr(lo), C.byref(h)))
         self._h = h
 
     def close(self):

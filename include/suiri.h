@@ -299,6 +299,9 @@ int suiri_use_graphs(suiri_tank* t, int32_t on);
    from the batch's stream (suiri_batch_stream) to the lanes and joins back to it, so the lanes' kernels
    overlap and small tanks do not wait for the largest one's kernels. */
 int suiri_batch_create(suiri_tank* const* tanks, int32_t n, suiri_batch** out);
+/* as suiri_batch_create with the lanes given: lane_of[i] in 0..7 is tank i's lane (each occupied lane is a
+   group with its own stream and graph; NULL: the size lanes, under 2^16 cells, under 2^19, larger) */
+int suiri_batch_create_lanes(suiri_tank* const* tanks, int32_t n, const int32_t* lane_of, suiri_batch** out);
 int suiri_batch_destroy(suiri_batch* b);
 int suiri_batch_substep(suiri_batch* b, double dt);
 int suiri_batch_sync(suiri_batch* b);

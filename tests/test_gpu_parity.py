@@ -394,11 +394,12 @@ def test_sor_bit_exact_when_the_sweep_grid_is_capped(pkg):
     gpu.close()
 
 
-@pytest.mark.parametrize('axes,seeds', [((16, 24, 32), (1, 2, 3)), ((16, 48), (1, 2, 16))])
-def test_batch_equals_solo_bit_for_bit(pkg, axes, seeds):
+@pytest.mark.parametrize('axes,seeds,lanes', [((16, 24, 32), (1, 2, 3), None), ((16, 48), (1, 2, 16), None),
+                                              ((16, 24, 32), (1, 2, 3), (2, 0, 5))])
+def test_batch_equals_solo_bit_for_bit(pkg, axes, seeds, lanes):
     """Tanks of uneven sizes stepped in one batch give exactly the particles they give alone; with the 48³
     tank (seed 16) the batch spans two size lanes (its own stream and graph each, forked and joined every
-    sub-step)."""
+    sub-step); with lanes given explicitly, each tank in a lane of its own."""
     specs = [pkg.workloads.random_tank(s, axes=axes) for s in seeds]
     if axes == (16, 48):
         sizes = [w['nx'] * w['ny'] * w['nz'] for w in specs]
@@ -415,7 +416,7 @@ def test_batch_equals_solo_bit_for_bit(pkg, axes, seeds):
         return out
 
     solo, batched = make(), make()
-    b = pkg.Batch(batched)
+    b = pkg.Batch(batched, lanes)
     for _ in range(6):
         for t in solo:
             t.substep(1 / 240)

@@ -117,3 +117,16 @@ def test_batch_tuned_lane_by_lane():
     best, timings = autotune.autotune_batch(b, 1 / 240)
     assert [k[1] for k in best] == [4, 0] and b.knobs[0][1] == 4 and b.knobs[1][1] == 0
     assert b.substeps == 0 and set(timings) == {0, 1}
+
+
+def test_balanced_lanes_keep_sizes_together_and_balance_particles():
+    from importlib import import_module
+    tk = import_module('hahenn-_b200.tank')
+    cells = [100, 100, 200, 400, 800, 800, 1600, 3200]
+    parts = [c * 8 for c in cells]
+    lane = tk.balanced_lanes(cells, parts, 2)
+    assert lane[0] == lane[1] and lane[4] == lane[5]          # equal sizes share a lane
+    assert list(lane) == sorted(lane)                          # contiguous in size
+    assert set(lane) == {0, 1}
+    tot = [sum(p for p, l in zip(parts, lane) if l == k) for k in (0, 1)]
+    assert max(tot) <= 0.75 * sum(parts)
