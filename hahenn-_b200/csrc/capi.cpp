@@ -597,6 +597,7 @@ int suiri_batch_sync(suiri_batch* b) {
 static void tune_group(Group& g, int32_t particle_blocks_per_sm, int32_t sor_mode) {
   if (particle_blocks_per_sm < 1 || particle_blocks_per_sm > 32) throw Error(SUIRI_ERR_INVALID, "blocks per SM in 1..32");
   if (sor_mode < 0 || sor_mode > 4) throw Error(SUIRI_ERR_INVALID, "sor_mode is 0, 1, 2, 3 or 4");
+  if (sor_mode == 1 && g.tanks.size() > 65535) throw Error(SUIRI_ERR_INVALID, "sor_mode 1 takes at most 65535 tanks");
   CK(cudaStreamSynchronize(g.stream));
   if (sor_mode == 4) g.plan_cluster();     // throws (and changes nothing else) when a tank does not fit
   g.blocks_per_sm = particle_blocks_per_sm;
@@ -619,6 +620,8 @@ static void tune_piece(Group& g, int32_t piece_kb) {
       throw;
     }
     g.drop_graph();
+  } else if (g.sor_mode == 1) {
+    g.drop_graph();                         // the persistent solve's shared memory per block
   }
 }
 

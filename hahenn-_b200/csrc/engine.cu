@@ -965,8 +965,9 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
   size_t defer_cap = 1;                 // G2P form 2: every particle of the group may be deferred
   for (Tank* x : tanks) defer_cap += (size_t)x->d.cap + (size_t)std::max(x->d.emit_cap, 0);
   CK(cudaMallocAsync(&d_defer, defer_cap * sizeof(int) + 16, stream));
-  // one block per SM: the grid barrier's cost grows with the number of arriving blocks
-  sor_blocks = std::min(std::min(sor_persist_max_blocks(device), sm_count), std::max(1, (hp[n] + kThreads - 1) / kThreads));
+  // the persistent solve: one block of 1024 threads per SM at most, and no more blocks than ~4 cells a thread
+  // (the grid barrier's cost grows with the number of arriving blocks); a batch shares the SMs among its lanes
+  sor_blocks = std::min(std::min(sor_persist_max_blocks(device), sm_count), std::max(1, (2 * hp[n] + 4095) / 4096));
   CK(cudaStreamSynchronize(stream));
   ctx.hpfx = d_hpfx;
   ctx.apfx = d_apfx;
@@ -995,7 +996,7 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
     }
   } else {
     if (want == 2) ensure_tbl();
-    sor_mode = want;
+    sor_mode = (want == 1 && n > 65535) ? 0 : want;     // the persistent solve keys its entries by a 16-bit tank
   }
 }
 
@@ -1114,6 +1115,18 @@ Batch::Batch(const std::vector<Tank*>& t, const int* lane_of) {
     stream = lanes[0]->stream;
     return;
   }
+  // the lanes' persistent solves run at the same time: their blocks together fit on the SMs at once, each
+  // lane's share in proportion to its cells
+  long long all = 0;
+  std::vector<long long> cells(lanes.size(), 0);
+  for (size_t l = 0; l < lanes.size(); ++l) {
+    for (Tank* x : lanes[l]->tanks) cells[l] += (long long)x->d.nx * x->d.ny * x->d.nz;
+    all += cells[l];
+  }
+  for (size_t l = 0; l < lanes.size(); ++l) {
+    const int share = (int)(lanes[l]->sm_count * cells[l] / std::max(all, 1LL));
+    lanes[l]->sor_blocks = std::max(1, std::min(lanes[l]->sor_blocks, share));
+  }
   CK(cudaSetDevice(t[0]->cfg.device));
   CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   own_stream = true;
@@ -1230,7 +1243,7 @@ void Group::enqueue_body() {
   launch_grid_cells(ctx);
   mark(3);
   if (sor_mode == 1 && max_iters > 0) {
-    launch_sor_persist(ctx, max_iters, sor_blocks, watchdog_polls);
+    launch_sor_persist(ctx, max_iters, sor_blocks, watchdog_polls, cl_piece_kb * 1024);
     CK(cudaGetLastError());
   } else if (sor_mode == 2 || sor_mode == 3) {
     // S sweeps per launch; launch l reads pres (l even) or pres2 and writes the other; an odd count ends in pres2

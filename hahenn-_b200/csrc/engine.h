@@ -196,7 +196,7 @@ struct Group {
   std::vector<ClusterClass> cl_classes;
   cudaEvent_t cl_fork = nullptr;
   void drop_cluster_classes();
-  int cl_piece_kb = 0;            // shared memory per CTA at most (tile knob; 0: the device maximum)
+  int cl_piece_kb = 0;            // shared memory per CTA at most, modes 4 and 1 (tile knob; 0: the device maximum)
   void plan_cluster();            // throws if a tank cannot be held by one cluster
   bool residual = false;          // FP64 residual of every solve into the tank counters
   int g2p_form = 0;               // 0 grid-stride walk, 1 per-brick with the faces in shared memory, 2 the walk's

@@ -71,7 +71,8 @@ void launch_grid_nodes(const LaunchCtx& L);
 void launch_grid_cells(const LaunchCtx& L);
 void launch_sor_sweep(const LaunchCtx& L, int color, int sweep);
 // whole solve, one cooperative launch; a barrier wait gives up after `limit` polls (error bit in the counters)
-void launch_sor_persist(const LaunchCtx& L, int max_iters, int blocks, unsigned limit);
+// smem_cap > 0: at most that much shared memory per block for its resident entries (tile knob)
+void launch_sor_persist(const LaunchCtx& L, int max_iters, int blocks, unsigned limit, int smem_cap = 0);
 constexpr unsigned kWatchdogPolls = 1u << 22;                            // default poll limit of a bounded wait
 int sor_persist_max_blocks(int device);                                  // co-resident blocks of k_sor_persist
 cudaError_t sor_tb_prepare();                                            // once per device, outside capture

@@ -20,9 +20,10 @@
 //   k_sor          one colour of every tank per launch (2·iters launches per solve, in the sub-step graph),
 //                  with programmatic dependent launch between sweeps; over the listed active cells, the
 //                  grid capped at the blocks resident at once (threads loop past it)
-//   k_sor_persist  the whole solve in one cooperative launch: all blocks resident, a grid barrier after
-//                  every colour sweep. The barrier's wait is bounded: after kSpinLimit polls it records
-//                  an error in the tank counters and every block returns.
+//   k_sor_persist  the whole solve in one cooperative launch: all blocks resident, each holding its share of
+//                  the active-cell lists and their own pressures in shared memory for the whole solve, a
+//                  grid barrier after every colour sweep. The barrier's wait is bounded: after the
+//                  watchdog's polls it records an error in the tank counters and every block returns.
 //   k_sor_tbl      two sweeps per launch over per-tile lists of active cells (temporal blocking)
 //   k_sor_tb<4>    four sweeps per launch on shared-memory tiles with halos
 #include <type_traits>
@@ -219,25 +220,23 @@ __global__ void __launch_bounds__(kSorThreads) k_sor(const TankDev* __restrict__
   }
 }
 
-// sense-free generation barrier over all blocks of a cooperative launch; false if the wait gave up after
-// `limit` polls (or another block's did)
-__device__ __forceinline__ bool grid_barrier(GridBarrier* b, unsigned nblocks, unsigned limit) {
+// Barrier over all blocks of a cooperative launch on a count that only grows: block arrivals add 1, and the
+// n-th barrier of the solve (from 1) is passed once the count reaches n·blocks (the count is cleared before
+// the launch). The wait is bounded: after `limit` polls, or once another block has given up, it records the
+// failure and returns false.
+__device__ __forceinline__ bool grid_barrier(GridBarrier* b, unsigned target, unsigned limit) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    const unsigned g = *(volatile unsigned*)&b->gen;
     __threadfence();
-    if (atomicAdd(&b->count, 1u) == nblocks - 1) {
-      b->count = 0;
-      __threadfence();
-      atomicAdd(&b->gen, 1u);
-    } else {
-      unsigned spins = 0;
-      while (*(volatile unsigned*)&b->gen == g) {
-        if (++spins > limit || *(volatile int*)&b->err) { ok = 0; break; }
-        __nanosleep(32);
-      }
+    atomicAdd(&b->count, 1u);
+    unsigned spins = 0;
+    for (;;) {
+      unsigned c;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(c) : "l"(&b->count) : "memory");
+      if (c >= target) break;
+      if (++spins > limit || *(volatile int*)&b->err) { ok = 0; break; }
     }
     __threadfence();
     if (!ok) atomicExch(&b->err, 1);
@@ -247,19 +246,96 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* b, unsigned nblocks, u
   return s_ok;
 }
 
-__global__ void __launch_bounds__(kThreads) k_sor_persist(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ hpfx,
-                                                          int max_iters, GridBarrier* bar, unsigned limit) {
-  const int total = hpfx[ntanks];
-  const int stride = gridDim.x * blockDim.x;
-  for (int sweep = 0; sweep < 2 * max_iters; ++sweep) {
-    const int color = sweep & 1, it = sweep >> 1;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += stride) {
-      const int t = find_slot(hpfx, ntanks, q);
+// The whole solve in one cooperative launch. Block b owns a fixed share of each colour's active-cell list
+// (entries [b·N/G, (b+1)·N/G) of the lists over all tanks) and keeps as many of its entries as fit in shared
+// memory for the whole solve, with the tank in the code's upper bits and the cell's own pressure beside it:
+// its own pressures are written only by this block, so they are read from shared memory, and written to
+// global memory for the neighbours. A sweep then reads from global memory only the six neighbour pressures
+// of each cell (through L2: other SMs wrote them), and a grid barrier separates the sweeps. Entries beyond
+// the shared-memory share are read from the lists each sweep. Same updates as the per-sweep launches, in the
+// same colour order, so the same pressures bit for bit.
+constexpr int kResThreads = 1024;
+constexpr int kResEntryBytes = 20;      // int4 entry + the cell's own pressure
+__global__ void __launch_bounds__(kResThreads, 1) k_sor_persist(const TankDev* __restrict__ tanks, int ntanks,
+                                                                const int* __restrict__ apfx, int max_iters,
+                                                                GridBarrier* bar, unsigned limit, int cap) {
+  extern __shared__ int4 s_ent[];
+  float* s_p = reinterpret_cast<float*>(s_ent + cap);
+  const int G = gridDim.x, b = blockIdx.x;
+  int r0[2], n[2], cached[2], base[2];
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const long long N = apfx[c * (ntanks + 1) + ntanks];
+    r0[c] = (int)(N * b / G);
+    n[c] = (int)(N * (b + 1) / G) - r0[c];
+  }
+  // the shared share of each colour, in proportion to its entries
+  const int tot = n[0] + n[1];
+  cached[0] = tot <= cap ? n[0] : (int)((long long)cap * n[0] / max(tot, 1));
+  cached[1] = min(n[1], cap - cached[0]);
+  base[0] = 0; base[1] = cached[0];
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const int* __restrict__ pfx = apfx + c * (ntanks + 1);
+    for (int e = threadIdx.x; e < cached[c]; e += kResThreads) {
+      const int q = r0[c] + e;
+      const int t = find_slot(pfx, ntanks, q);
       const TankDev& T = tanks[t];
-      if (it < T.iters) sor_cell(T, color, q - hpfx[t]);
+      int4 ent = T.act[(size_t)c * T.nhalf + (q - pfx[t])];
+      s_p[base[c] + e] = T.pres[(size_t)c * T.nhalf + ent.x];
+      ent.y = (ent.y & 0xFFFF) | (t << 16);
+      s_ent[base[c] + e] = ent;
     }
-    if (sweep + 1 < 2 * max_iters && !grid_barrier(bar, gridDim.x, limit)) {
-      if (threadIdx.x == 0 && blockIdx.x == 0)
+  }
+  __syncthreads();
+  for (int sweep = 0; sweep < 2 * max_iters; ++sweep) {
+    const int c = sweep & 1, it = sweep >> 1;
+    const int* __restrict__ pfx = apfx + c * (ntanks + 1);
+    for (int e = threadIdx.x; e < n[c]; e += kResThreads) {
+      int4 ent;
+      int t;
+      const bool in_smem = e < cached[c];
+      if (in_smem) {
+        ent = s_ent[base[c] + e];
+        t = ent.y >> 16;
+      } else {
+        const int q = r0[c] + e;
+        t = find_slot(pfx, ntanks, q);
+        ent = tanks[t].act[(size_t)c * tanks[t].nhalf + (q - pfx[t])];
+      }
+      const TankDev& T = tanks[t];
+      if (it >= T.iters) continue;
+      const int hx = T.hx, nx = T.nx, ny = T.ny, nz = T.nz;
+      const int s = ent.x;
+      const uint32_t code = (uint32_t)ent.y & 0xFFFFu;
+      const int row = divu(s, T.dhx), ti = s - row * hx;
+      const int k = divu(row, T.dny), j = row - k * ny;
+      const int i = 2 * ti + ((j + k + c) & 1);
+      const float* __restrict__ po = T.pres + (size_t)(1 - c) * T.nhalf;
+      const int rowb = hx * row;
+      float nb[6];
+      nb[0] = i > 0 ? __ldcg(po + ((i - 1) >> 1) + rowb) : 0.f;
+      nb[1] = i + 1 < nx ? __ldcg(po + ((i + 1) >> 1) + rowb) : 0.f;
+      nb[2] = j > 0 ? __ldcg(po + ti + rowb - hx) : 0.f;
+      nb[3] = j + 1 < ny ? __ldcg(po + ti + rowb + hx) : 0.f;
+      nb[4] = k > 0 ? __ldcg(po + ti + rowb - hx * ny) : 0.f;
+      nb[5] = k + 1 < nz ? __ldcg(po + ti + rowb + hx * ny) : 0.f;
+      const size_t own = (size_t)c * T.nhalf + s;
+      const float p = in_smem ? s_p[base[c] + e] : __ldcg(T.pres + own);
+      const float rhs = __int_as_float(ent.z), inv = __int_as_float(ent.w);
+      float np;
+      if (code & kCodePartial) {
+        float C[6];
+        cut_coeffs(T, i, j, k, C);
+        np = sor_update_inv(C, nb, rhs, p, T.omega, inv);
+      } else {
+        np = sor_update_open(code, nb, rhs, p, T.omega, inv);
+      }
+      __stcg(T.pres + own, np);
+      if (in_smem) s_p[base[c] + e] = np;
+    }
+    if (sweep + 1 < 2 * max_iters && !grid_barrier(bar, (unsigned)G * (unsigned)(sweep + 1), limit)) {
+      if (threadIdx.x == 0)
         for (int t = 0; t < ntanks; ++t) atomicOr(&tanks[t].ctr->err, kErrBarrier);
       return;
     }
@@ -1080,27 +1156,47 @@ void launch_sor_residual(const LaunchCtx& L) {
     k_sor_residual<<<L.nblocks[kFamSor], kThreads, 0, L.stream>>>(L.tanks, L.ntanks, (const int*)L.apfx, c);
 }
 
+// shared memory a block of the persistent solve may take (the device's opt-in maximum less its static part)
+static int sor_persist_smem(int device) {
+  static int cache[128] = {};
+  if (device < 0 || device >= 128) return 0;
+  if (!cache[device]) {
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    const int bytes = optin - 1024;
+    cudaFuncSetAttribute(k_sor_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cache[device] = bytes;
+  }
+  return cache[device];
+}
+
 int sor_persist_max_blocks(int device) {
   int per_sm = 0, sms = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sor_persist, kThreads, 0);
+  const int smem = sor_persist_smem(device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sor_persist, kResThreads, smem);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   return per_sm * sms;
 }
 
-void launch_sor_persist(const LaunchCtx& L, int max_iters, int blocks, unsigned limit) {
+void launch_sor_persist(const LaunchCtx& L, int max_iters, int blocks, unsigned limit, int smem_cap) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const int smem = smem_cap > 0 ? std::min(smem_cap, sor_persist_smem(dev)) : sor_persist_smem(dev);
+  const int cap = smem / kResEntryBytes;
   // the barrier starts every solve cleared: a solve whose wait gave up leaves its counts behind
   cudaMemsetAsync(L.barrier, 0, sizeof(GridBarrier), L.stream);
   // cooperative launch: the runtime refuses it unless every block can be resident at once
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
-  cfg.blockDim = dim3(kThreads);
+  cfg.blockDim = dim3(kResThreads);
+  cfg.dynamicSmemBytes = (size_t)cap * kResEntryBytes;
   cfg.stream = L.stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k_sor_persist, L.tanks, L.ntanks, (const int*)L.hpfx, max_iters, L.barrier, limit);
+  cudaLaunchKernelEx(&cfg, k_sor_persist, L.tanks, L.ntanks, (const int*)L.apfx, max_iters, L.barrier, limit, cap);
 }
 
 }  // namespace suiri

@@ -108,14 +108,15 @@ def test_serving_budget_admission(pkg):
 
 
 def test_bounded_wait_gives_up_reports_and_serving_fails_the_request(pkg):
-    """The cooperative solve (sor_mode 1) with a poll limit of 0: the grid barrier's waits give up at once.
-    The sub-step returns, the tank's stats carry error bit 1, and with the per-sweep form the next sub-steps
-    run cleanly. In the server a request whose solve gave up is reported failed with the reason, and the
-    next request completes."""
+    """The cooperative solve (sor_mode 1) with a poll limit of 0: a block that finds a grid barrier not yet
+    passed gives up at once (32³ and 32–48-cell tanks, so the solve has several blocks to wait for). The
+    sub-step returns, the tank's stats carry error bit 1, and with the per-sweep form the next sub-steps run
+    cleanly. In the server a request whose solve gave up is reported failed with the reason, and the next
+    request completes."""
     from importlib import import_module
     serve = import_module('hahenn-_b200.serve')
-    w = pkg.workloads.dam_break(16)
-    t = pkg.Tank(nx=16, ny=16, nz=16, h=w['h'], iters=20, whitewater=False, ripple=None, capacity=len(w['pos']) * 2,
+    w = pkg.workloads.dam_break(32)
+    t = pkg.Tank(nx=32, ny=32, nz=32, h=w['h'], iters=20, whitewater=False, ripple=None, capacity=len(w['pos']) * 2,
                  sor_mode=1, watchdog_polls=0)
     t.add_particles(w['pos'])
     t.substep(1 / 240)
@@ -126,7 +127,7 @@ def test_bounded_wait_gives_up_reports_and_serving_fails_the_request(pkg):
     st = t.stats()
     assert st['count'] == len(w['pos']) and np.isfinite(t.grid(pkg.native.FIELD_PRES)).all()
     t.close()
-    sc, prm, em, _ = serve.scene_request(6, axes=(16, 24))
+    sc, prm, em, _ = serve.scene_request(6, axes=(32, 48))
     srv = serve.Server(budget_bytes=4e9)
     bad = srv.submit(sc, dict(prm, sor_mode=1, watchdog_polls=0), em, steps=3)
     with pytest.raises(pkg.native.SuiriError, match='grid-barrier wait'):
