@@ -709,6 +709,42 @@ def test_full_size_obstacles_inflow_substeps(pkg):
     gpu.close()
 
 
+def test_full_batch_of_64_tanks_one_substep(pkg):
+    """The batching workload at its full size: the 64 uneven tanks (11.7M particles, 80 SOR iterations,
+    0-3 analytic obstacles each) advanced one sub-step as one batch in its size lanes; every 8th tank (sizes
+    across both lanes) against the oracle run on that tank alone: counts and masks bit-exact, P2G velocity,
+    pressure, projected velocity and particles within the parity tolerances."""
+    from parity import objs_from_items
+    specs = pkg.workloads.batch_tanks(64)
+    tanks = []
+    for w in specs:
+        prm = w['params']
+        t = pkg.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=prm['flip'], omega=prm['omega'],
+                     iters=prm['iters'], gravity=prm['g'], whitewater=True, ripple=None,
+                     capacity=int(len(w['pos']) * 1.2) + 1000, ww_capacity=20000, sdf_mode='analytic')
+        t.set_objects(w['objects'])
+        t.add_particles(w['pos'])
+        tanks.append(t)
+    b = pkg.Batch(tanks)
+    assert b.lanes() >= 2
+    dt = 1 / 240
+    b.substep(dt)
+    b.sync()
+    for i in range(0, 64, 8):
+        w = specs[i]
+        prm = w['params']
+        ora = oracle_from(w['nx'], w['ny'], w['nz'], w['h'], w['origin'], flip=prm['flip'], omega=prm['omega'],
+                          iters=prm['iters'], g=prm['g'], whitewater=True, ww_cap=20000)
+        ora.set_objects(objs_from_items(w['objects']))
+        ora.add_particles(f32(w['pos']))
+        ora.frame = 1
+        ora.substep(dt)
+        compare_substep(pkg, tanks[i], ora, f'batch tank {i} ({w["nx"]}x{w["ny"]}x{w["nz"]})')
+    b.close()
+    for t in tanks:
+        t.close()
+
+
 @pytest.mark.parametrize('form', [1, 2])
 @pytest.mark.parametrize('advect', ['euler', 'rk2'])
 def test_g2p_brick_form_equals_the_walk(pkg, advect, form):
