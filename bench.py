@@ -909,12 +909,13 @@ def run_for_profiler(args, local):
             t.close()
         return
     if args.workload == 'frame_export':
-        # the full scene's shape at a quarter of each axis (131k particles, 128² maps), 3 frames, then N
-        # exports (mesh and maps)
-        w = P.workloads.full_scene(scale=4)
+        # the full scene's shape at 1/--scale of each axis (default a quarter: 131k particles, 128² maps),
+        # 3 frames, then N exports (mesh and maps)
+        w = P.workloads.full_scene(scale=args.scale)
         prm = w['params']
         t = P.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], flip=prm['flip'], omega=prm['omega'],
-                   iters=prm['iters'], whitewater=True, ripple=w['ripple'], wmap=128, capacity=len(w['pos']) + 20000,
+                   iters=prm['iters'], whitewater=True, ripple=w['ripple'], wmap=512 // args.scale,
+                   capacity=int(len(w['pos']) * 1.1) + 20000,
                    ripple_sigma=prm['sigma'], ripple_rho=prm['rho'], ripple_depth=prm['depth'], drop_d=prm['drop_d'],
                    device=local)
         t.add_particles(w['pos'])
@@ -957,6 +958,7 @@ def main():
     ap.add_argument('--bps', type=int, default=2, help='profiler run: particle blocks per SM')
     ap.add_argument('--g2p-form', type=int, default=0, help='profiler run: form of the grid-to-particle pass')
     ap.add_argument('--sor-mode', type=int, default=4, help='profiler run: form of the pressure solve')
+    ap.add_argument('--scale', type=int, default=4, help='profiler run of the frame export: 1/scale of each axis')
     args = ap.parse_args()
     rank, world = int(os.environ.get('RANK', 0)), int(os.environ.get('WORLD_SIZE', 1))
     local = int(os.environ.get('LOCAL_RANK', 0))

@@ -32,7 +32,8 @@ namespace suiri {
 
 namespace {
 
-constexpr int kMeshThreads = 1024;   // one item per thread in the compaction tiles
+constexpr int kMeshThreads = 1024;   // threads of a compaction block
+constexpr int kMeshItems = 8;        // consecutive items per thread: a block's tile is 8192 items
 constexpr int kMeshPhases = 5;       // classify, distance field, blur, surface nets, finish (device time each)
 constexpr int kMaxTaps = 33;
 
@@ -198,7 +199,19 @@ __global__ void __launch_bounds__(256) k_mesh_splat_tiles(const TankDev* __restr
                            (long long)floor(((T.oy + cj0 * T.h) - G.lo[1]) / G.sp) - 2,
                            (long long)floor(((T.oz + ck0 * T.h) - G.lo[2]) / G.sp) - 2};
   const int n_live = T.ctr->n_live, n_all = n_live + T.ctr->n_emit;
-  for (int qq = threadIdx.x; qq < total; qq += blockDim.x) {
+  // the tile's particles in a strided permutation j·P mod total (P about a warp's share, coprime to total):
+  // the lanes of a warp take particles of cells far apart, so their minima seldom hit the same node
+  __shared__ int s_P;
+  if (threadIdx.x == 0) {
+    int P = (total / 32) | 1;
+    auto gcd = [](int a, int b) { while (b) { const int t = a % b; a = b; b = t; } return a; };
+    while (total > 1 && gcd(P, total) != 1) ++P;
+    s_P = P;
+  }
+  __syncthreads();
+  const long long Pst = s_P;
+  for (int jj = threadIdx.x; jj < total; jj += blockDim.x) {
+    const int qq = (int)((jj * Pst) % total);
     int lo = 0, hi = kTY * kTZ - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
@@ -327,38 +340,52 @@ __device__ __forceinline__ bool seg_flag(int seg, long long item, const float* _
   return kind[item] == 1;
 }
 
-// exclusive rank of this thread's flag among the block's, in thread order; the block's total in *total
-__device__ __forceinline__ int block_rank(bool f, int* total) {
+// exclusive prefix of the threads' counts in thread order; the block's total in *total
+__device__ __forceinline__ int block_excl(int v, int* total) {
   __shared__ int s_w[32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const unsigned b = __ballot_sync(~0u, f);
-  if (lane == 0) s_w[w] = __popc(b);
+  int inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(~0u, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) s_w[w] = inc;
   __syncthreads();
   if (w == 0) {
     const int nw = blockDim.x >> 5;
-    const int v = lane < nw ? s_w[lane] : 0;
-    int inc = v;
+    const int x = lane < nw ? s_w[lane] : 0;
+    int iw = x;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(~0u, inc, o);
-      if (lane >= o) inc += y;
+      const int y = __shfl_up_sync(~0u, iw, o);
+      if (lane >= o) iw += y;
     }
-    if (lane < nw) s_w[lane] = inc - v;
-    if (lane == 31) *total = inc;
+    if (lane < nw) s_w[lane] = iw - x;
+    if (lane == 31) *total = iw;
   }
   __syncthreads();
-  const int r = s_w[w] + __popc(b & ((1u << lane) - 1u));
+  const int r = s_w[w] + inc - v;
   __syncthreads();
   return r;
+}
+
+// the first item of this thread's run of kMeshItems consecutive items in block `blk` of a segment
+__device__ __forceinline__ long long run_first(int blk_in_seg) {
+  return ((long long)blk_in_seg * kMeshThreads + threadIdx.x) * kMeshItems;
 }
 
 __global__ void __launch_bounds__(kMeshThreads) k_mesh_count(const float* __restrict__ phi, MeshGeom G, MeshSegs S,
                                                              const uint8_t* __restrict__ kind, int* __restrict__ bcount) {
   __shared__ int s_tot;
   const int seg = seg_of(S, blockIdx.x);
-  const long long item = (long long)(blockIdx.x - S.first_block[seg]) * kMeshThreads + threadIdx.x;
-  const bool f = item < S.n[seg] && seg_flag(seg, item, phi, G, kind);
-  block_rank(f, &s_tot);
+  const long long first = run_first(blockIdx.x - S.first_block[seg]);
+  int cnt = 0;
+  for (int m = 0; m < kMeshItems; ++m) {
+    const long long item = first + m;
+    if (item < S.n[seg] && seg_flag(seg, item, phi, G, kind)) ++cnt;
+  }
+  block_excl(cnt, &s_tot);
   if (threadIdx.x == 0) bcount[blockIdx.x] = s_tot;
 }
 
@@ -419,16 +446,22 @@ __global__ void __launch_bounds__(kMeshThreads) k_mesh_cells(const float* __rest
                                                              const int* __restrict__ bbase, int* __restrict__ vid,
                                                              double* __restrict__ vtx) {
   __shared__ int s_tot;
-  const long long c = (long long)blockIdx.x * kMeshThreads + threadIdx.x;
-  const bool f = c < S.n[0] && cell_mixed(phi, G, c);
-  const int r = block_rank(f, &s_tot);
-  if (c >= S.n[0]) return;
-  const int id = f ? bbase[blockIdx.x] + r : -1;
-  vid[c] = id;
-  if (f) {
+  const long long first = run_first(blockIdx.x);
+  unsigned mixed = 0;
+  for (int m = 0; m < kMeshItems; ++m) {
+    const long long c = first + m;
+    if (c < S.n[0] && cell_mixed(phi, G, c)) mixed |= 1u << m;
+  }
+  int id = bbase[blockIdx.x] + block_excl(__popc(mixed), &s_tot);
+  for (int m = 0; m < kMeshItems; ++m) {
+    const long long c = first + m;
+    if (c >= S.n[0]) break;
+    if (!((mixed >> m) & 1u)) { vid[c] = -1; continue; }
+    vid[c] = id;
     double v[3];
     nets_vertex(phi, G, c, v);
     vtx[3 * (size_t)id] = v[0]; vtx[3 * (size_t)id + 1] = v[1]; vtx[3 * (size_t)id + 2] = v[2];
+    ++id;
   }
 }
 
@@ -441,34 +474,48 @@ __global__ void __launch_bounds__(kMeshThreads) k_mesh_quads(const float* __rest
   const int blk = blockIdx.x + S.first_block[1];
   const int seg = seg_of(S, blk);
   const int ax = seg - 1;
-  const long long e = (long long)(blk - S.first_block[seg]) * kMeshThreads + threadIdx.x;
-  bool lo_in = false;
-  const bool f = e < S.n[seg] && edge_crossing(phi, G, ax, e, &lo_in);
-  const int r = block_rank(f, &s_tot);
-  if (!f) return;
-  const int id = bbase[blk] + r - bbase[S.first_block[1]];
-  int i, j, k;
-  edge_node(G, ax, e, i, j, k);
+  const long long first = run_first(blk - S.first_block[seg]);
+  unsigned cross = 0, low_in = 0;
+  for (int m = 0; m < kMeshItems; ++m) {
+    const long long e = first + m;
+    bool lo_in = false;
+    if (e < S.n[seg] && edge_crossing(phi, G, ax, e, &lo_in)) {
+      cross |= 1u << m;
+      if (lo_in) low_in |= 1u << m;
+    }
+  }
+  int id = bbase[blk] + block_excl(__popc(cross), &s_tot) - bbase[S.first_block[1]];
   const int a1 = ax == 0 ? 1 : 0, a2 = ax == 2 ? 1 : 2;
-  auto cell = [&](int o1, int o2) {
-    int c[3] = {i, j, k};
-    c[a1] -= o1; c[a2] -= o2;
-    return vid[((long long)c[0] * (G.Y - 1) + c[1]) * (G.Z - 1) + c[2]];
-  };
-  int4 q = make_int4(cell(1, 1), cell(0, 1), cell(0, 0), cell(1, 0));
-  const bool rev = ax == 1 ? lo_in : !lo_in;
-  if (rev) q = make_int4(q.w, q.z, q.y, q.x);
-  quads[id] = q;
+  for (int m = 0; m < kMeshItems; ++m) {
+    if (!((cross >> m) & 1u)) continue;
+    int i, j, k;
+    edge_node(G, ax, first + m, i, j, k);
+    auto cell = [&](int o1, int o2) {
+      int c[3] = {i, j, k};
+      c[a1] -= o1; c[a2] -= o2;
+      return vid[((long long)c[0] * (G.Y - 1) + c[1]) * (G.Z - 1) + c[2]];
+    };
+    int4 q = make_int4(cell(1, 1), cell(0, 1), cell(0, 0), cell(1, 0));
+    const bool lo_in = (low_in >> m) & 1u;
+    const bool rev = ax == 1 ? lo_in : !lo_in;
+    if (rev) q = make_int4(q.w, q.z, q.y, q.x);
+    quads[id++] = q;
+  }
 }
 
 __global__ void __launch_bounds__(kMeshThreads) k_mesh_lone(MeshSegs S, const uint8_t* __restrict__ kind,
                                                             const int* __restrict__ bbase, int* __restrict__ lone_idx) {
   __shared__ int s_tot;
   const int blk = blockIdx.x + S.first_block[4];
-  const long long q = (long long)blockIdx.x * kMeshThreads + threadIdx.x;
-  const bool f = q < S.n[4] && kind[q] == 1;
-  const int r = block_rank(f, &s_tot);
-  if (f) lone_idx[bbase[blk] + r - bbase[S.first_block[4]]] = (int)q;
+  const long long first = run_first(blockIdx.x);
+  unsigned lone = 0;
+  for (int m = 0; m < kMeshItems; ++m) {
+    const long long q = first + m;
+    if (q < S.n[4] && kind[q] == 1) lone |= 1u << m;
+  }
+  int id = bbase[blk] + block_excl(__popc(lone), &s_tot) - bbase[S.first_block[4]];
+  for (int m = 0; m < kMeshItems; ++m)
+    if ((lone >> m) & 1u) lone_idx[id++] = (int)(first + m);
 }
 
 struct FinishParams {
@@ -653,7 +700,10 @@ void free_mesh(Tank& t) {
   t.mesh = nullptr;
 }
 
-static int nb_of(long long n) { return (int)((n + kMeshThreads - 1) / kMeshThreads); }
+static int nb_of(long long n) {
+  const long long tile = (long long)kMeshThreads * kMeshItems;
+  return (int)((n + tile - 1) / tile);
+}
 
 MeshInfo build_surface_mesh(Tank& t, double smooth) {
   if (!(smooth > 0) || smooth > 6.0) throw Error(-1, "surface mesh: smooth (blur sigma in lattice nodes) in (0, 6]");
