@@ -11,7 +11,8 @@ form of the pressure solve picked by the autotuner. `value` is the batch's parti
 scenes stepped one by one on the plain path give `plain_sequential`. Synthetic seeded data.
 
 Other workloads: `obstacles_inflow` (one 128×64×64 tank with obstacles, a faucet and a drain),
-`full_scene` (256×128×128 with rain and the 1024×512 ripple layer), `serve` (Poisson scene requests).
+`full_scene` (256×128×128 with rain and the 1024×512 ripple layer), `frame_export` (that scene's per-frame
+surface mesh and light/surface maps), `serve` (Poisson scene requests).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl suiri|reference] [--workload ...]
 
@@ -211,10 +212,11 @@ def size_lanes(specs):
     return [occ.index(r) for r in raw], len(occ)
 
 
-def launches_per_substep(sor_mode, iters, residual=False):
-    """Kernels of one sub-step graph of a group (bin, scan ×2, scatter and the rest: 10) plus the solve's."""
+def launches_per_substep(sor_mode, iters, residual=False, g2p_form=0):
+    """Kernels of one sub-step graph of a group (bin, scan ×2, scatter and the rest: 10) plus the solve's, and
+    the deferred pass of G2P form 2."""
     sor = {0: 2 * iters, 1: 1, 2: 1 + iters + (iters & 1), 3: -(-2 * iters // 4) + (-(-2 * iters // 4) & 1), 4: 1}[sor_mode]
-    return 10 + (sor if iters > 0 else 0) + (2 if residual else 0)
+    return 10 + (sor if iters > 0 else 0) + (2 if residual else 0) + (1 if g2p_form == 2 else 0)
 
 
 # ------------------------------------------------------------------ the CPU oracle (reference arm, cpu_baseline)
@@ -578,7 +580,7 @@ def run_batch(args, rank, world, local):
                              'rate may exceed the HBM copy rate; traffic is the DRAM bytes ncu measured per launch '
                              '(warm: caches kept as in the step; cold: ncu flushed them before the launch)')
         cpu_rate, cpu_el, cpu_what = cpu_sample_rate(specs)
-        launches = args.steps * sum(launches_per_substep(best[l][1], iters) for l in range(nlanes))
+        launches = args.steps * sum(launches_per_substep(best[l][1], iters, g2p_form=best[l][3]) for l in range(nlanes))
         line = dict(metric=METRIC, value=value, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
                     ms_per_step=ms, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
                     data='synthetic (seeded particles, analytic obstacles)', config=cfg,
@@ -696,7 +698,8 @@ def run_plain(args, rank, world, local):
                                   unit_bytes='20 B per active cell per colour sweep'),
                     phases_ms=ph, tuned=dict(blocks_per_sm=best[0], sor_mode=best[1], piece_kb=best[2], g2p_form=best[3]),
                     cpu_baseline=dict(value=cpu_rate, unit=METRIC, cores=1, kind='port', sample=cpu_what),
-                    e2e=e2e, gpu_launches=launches_per_substep(best[1], prm['iters']) * args.steps, clocks=clk,
+                    e2e=e2e, gpu_launches=launches_per_substep(best[1], prm['iters'], g2p_form=best[3]) * args.steps,
+                    clocks=clk,
                     residual_f64=residual)
         print(json.dumps(line), flush=True)
     tank.close()
