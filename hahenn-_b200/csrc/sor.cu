@@ -904,10 +904,13 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_sor_cluster(const TankDe
   const size_t nh = T.nhalf;
   float* sp = reinterpret_cast<float*>(cl_smem);     // [2][PS]
   float* sr = sp + 2 * PS;                           // [2][US]
-  int* s_cnt = reinterpret_cast<int*>(sr + 2 * US);  // [8]
+  int* s_cnt = reinterpret_cast<int*>(sr + 2 * US);  // [8] (spare)
   uint8_t* sc = reinterpret_cast<uint8_t*>(s_cnt + 8);   // [2][US]
+  uint16_t* sl = reinterpret_cast<uint16_t*>(sc + 2 * US);   // [2][US]: the active slots, by colour and region
+  __shared__ int s_n[2][3], s_o[2][3], s_f[2][3];    // per colour and region (first plane, last plane, interior)
   const unsigned rank = cluster_ctarank();
-  if (threadIdx.x < 8) s_cnt[threadIdx.x] = 0;
+  if (threadIdx.x < 6) { (&s_n[0][0])[threadIdx.x] = 0; (&s_f[0][0])[threadIdx.x] = 0; }
+  __syncthreads();
   // pressure of the own planes and the ghost planes, zero in the padding and outside the tank
   for (int q = threadIdx.x; q < 2 * PS; q += kClusterThreads) {
     const int c = q >= PS, L = q - c * PS;
@@ -919,48 +922,54 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_sor_cluster(const TankDe
     sp[q] = v;
   }
   const size_t g0 = (size_t)hx * ny * k0;            // first slot of the piece in each colour's global array
+  const int iters = on ? T.iters : 0;
+  const float omega = T.omega;
+  const DivU dny = T.dny, dhx = T.dhx;
+  const bool below = on && k0 > 0, above = on && k0 + nk < nz;   // neighbour pieces (remote planes)
+  // rows [0, lo_r): first plane (it reads and feeds the piece below); [hi_r, nk·ny): last plane (the piece
+  // above); [lo_r, hi_r): interior. A single plane with neighbours on both sides is the first range.
+  const int lo_r = below ? ny : 0;
+  const int hi_r = (above && !(below && nk == 1)) ? (nk - 1) * ny : nk * ny;
+  auto region = [&](int l) { const int row = divu(l, dhx); return row < lo_r ? 0 : (row >= hi_r ? 1 : 2); };
   for (int q = threadIdx.x; q < 2 * U; q += kClusterThreads) {
     const int c = q >= U, l = q - c * U;
     const size_t g = c * nh + g0 + l;
     const uint32_t cd = T.code[g];
     sr[c * US + l] = T.rhs[g];
     sc[c * US + l] = (uint8_t)((cd & 0x3Fu) | ((cd & kCodePartial) ? 0x40u : 0u) | ((cd & kCodeActive) ? 0x80u : 0u));
+    if (cd & kCodeActive) atomicAdd(&s_n[c][region(l)], 1);
   }
-  const int iters = on ? T.iters : 0;
-  const float omega = T.omega;
-  const DivU dny = T.dny;
-  const bool below = on && k0 > 0, above = on && k0 + nk < nz;   // neighbour pieces (remote planes)
-  // rows [0, lo_r): first plane (it reads and feeds the piece below); [hi_r, nk·ny): last plane (the piece
-  // above); [lo_r, hi_r): interior. A single plane with neighbours on both sides is the first range.
-  const int lo_r = below ? ny : 0;
-  const int hi_r = (above && !(below && nk == 1)) ? (nk - 1) * ny : nk * ny;
-  // a warp's chunk: 32/hx whole rows (hx ≤ 32; lanes past them idle), or a 32-slot part of a row
-  const int lane = threadIdx.x & 31;
-  const bool narrow = hx <= 32;
-  const int rpc = narrow ? 32 / hx : 1, cpr = narrow ? 1 : (hx + 31) / 32;
-  const int my_r = narrow ? lane / hx : 0, my_t = narrow ? lane % hx : lane;
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    const int c = threadIdx.x;
+    s_o[c][0] = c * US; s_o[c][1] = s_o[c][0] + s_n[c][0]; s_o[c][2] = s_o[c][1] + s_n[c][1];
+  }
+  __syncthreads();
+  // the lists of active slots: the sweeps visit only liquid cells with an open face
+  for (int q = threadIdx.x; q < 2 * U; q += kClusterThreads) {
+    const int c = q >= U, l = q - c * U;
+    if (!(sc[c * US + l] & 0x80u)) continue;
+    const int r = region(l);
+    sl[s_o[c][r] + atomicAdd(&s_f[c][r], 1)] = (uint16_t)l;
+  }
+  __syncthreads();
   const int ghost_above_plane = np_ + 1;             // the piece below stores this piece's first plane here
   // 1/n for the cells without cut faces, n their open faces (the correctly rounded reciprocals)
   __shared__ float s_inv[8];
   if (threadIdx.x < 8) s_inv[threadIdx.x] = threadIdx.x ? __frcp_rn((float)threadIdx.x) : 0.f;
-  auto relax = [&](auto push, int c, int r0, int r1, int* ctr) {
+  __syncthreads();
+  auto relax = [&](auto push, int c, int reg) {
     const float* po = sp + (1 - c) * PS;
     float* pw = sp + c * PS;
     const float* rw = sr + c * US;
     const uint8_t* cw = sc + c * US;
-    const int nch = narrow ? (r1 - r0 + rpc - 1) / rpc : (r1 - r0) * cpr;
+    const uint16_t* lst = sl + s_o[c][reg];
+    const int cnt = s_n[c][reg];
 #pragma unroll 1
-    while (true) {
-      int ch = 0;
-      if (lane == 0) ch = atomicAdd(ctr, 1);
-      ch = __shfl_sync(0xffffffffu, ch, 0);
-      if (ch >= nch) break;
-      const int row = r0 + (narrow ? ch * rpc + my_r : ch / cpr);
-      const int ti = narrow ? my_t : (ch % cpr) * 32 + lane;
-      if ((narrow && my_r >= rpc) || ti >= hx || row >= r1) continue;
-      const int l = row * hx + ti;
+    for (int e = threadIdx.x; e < cnt; e += kClusterThreads) {
+      const int l = lst[e];
+      const int row = divu(l, dhx), ti = l - row * hx;
       const uint32_t cd = cw[l];
-      if (!(cd & 0x80u)) continue;
       const int kl = divu(row, dny), j = row - kl * ny, k = k0 + kl;
       const int s = (j + k + c) & 1;
       const int L = (ti + 1) + W * ((j + 1) + RY * (kl + 1));
@@ -994,15 +1003,13 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_sor_cluster(const TankDe
 #pragma unroll 1
     for (int c = 0; c < 2; ++c) {
       const bool go = it < iters;
-      int* ctr = s_cnt + 4 * c;           // this sweep's counters; the other set is zeroed for the next sweep
-      if (threadIdx.x < 3) s_cnt[4 * (1 - c) + threadIdx.x] = 0;
       cluster_wait();
       if (go) {
-        relax(with_push, c, 0, lo_r, ctr);
-        relax(with_push, c, hi_r, nk * ny, ctr + 1);
+        relax(with_push, c, 0);
+        relax(with_push, c, 1);
       }
       cluster_arrive();
-      if (go) relax(no_push, c, lo_r, hi_r, ctr + 2);
+      if (go) relax(no_push, c, 2);
       __syncthreads();
     }
   }
@@ -1018,7 +1025,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_sor_cluster(const TankDe
 // shared bytes of a piece of np planes: padded pressure, rhs, the work counters and the codes
 int cluster_smem_bytes(const TankDev& D, int np) {
   const ClusterLayout G = cluster_layout(D.hx, D.ny, np);
-  return ((8 * G.PS + 8 * G.US + 32 + 2 * G.US) + 15) & ~15;
+  return ((8 * G.PS + 8 * G.US + 32 + 2 * G.US + 4 * G.US) + 15) & ~15;
 }
 
 cudaError_t sor_cluster_prepare(int smem_bytes, int cluster) {

@@ -463,7 +463,7 @@ def test_solve_forms_equal_per_sweep_launches(pkg, mode, piece_kb):
         np.testing.assert_array_equal(a, b)
 
 
-@pytest.mark.parametrize('piece_kb', [11, 21, 46])
+@pytest.mark.parametrize('piece_kb', [12, 24, 54])
 def test_cluster_solve_pieces_across_ctas(pkg, piece_kb):
     """The cluster-resident solve with less shared memory per CTA, so the 32×16×16 tank is cut into pieces
     of 1 z plane (16 CTAs: every plane's z neighbours are ghost planes pushed by the next CTAs), 3 planes (six
