@@ -148,6 +148,9 @@ bool Server::advance(Lane& L) {
     std::vector<Tank*> ts;
     for (Request* r : L.active) ts.push_back(r->tank.get());
     L.group.reset(new Group(ts, L.stream));
+    // the lanes run at the same time: a lane's persistent solve (sor_mode 1) takes at most its share of the SMs,
+    // so that the cooperative launches of all lanes are resident together
+    L.group->sor_blocks = std::max(1, std::min(L.group->sor_blocks, L.group->sm_count / kSizeLanes));
     ++rebuilds;
     L.changed = false;
   }
