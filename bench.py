@@ -552,10 +552,17 @@ def run_batch(args, rank, world, local):
             parts = sum(st[i]['count'] for i in idx)
             nodes = sum((specs[i]['nx'] + 1) * (specs[i]['ny'] + 1) * (specs[i]['nz'] + 1) for i in idx)
             active = sum(st[i]['active_cells'] for i in idx)
+            cells = sum(specs[i]['nx'] * specs[i]['ny'] * specs[i]['nz'] for i in idx)
             ph = {k: float(np.mean([p[l][k] for p in phases])) for k in P.native.PHASES}
             fig = {}
-            for name, alg in (('p2g', 32.0 * parts + 48.0 * nodes), ('g2p', 64.0 * parts + 24.0 * nodes),
-                              ('pressure_solve', 20.0 * active * iters)):
+            # algorithmic bytes per phase: binning 32 B read + 4 B rank, scan 12 B per cell, scatter 64 + 4 B;
+            # P2G 32 B per particle + 48 B flush per node; node pass 88 B read + 104 B written per node, cell
+            # pass 40 B per cell + 16 B per active list entry; the solve 20 B per active cell and colour sweep;
+            # projection 40 B per node; G2P 64 B per particle + 24 B of node gathers per node
+            for name, alg in (('bin_sort', 104.0 * parts + 12.0 * cells), ('p2g', 32.0 * parts + 48.0 * nodes),
+                              ('grid_passes', 192.0 * nodes + 40.0 * cells + 16.0 * active),
+                              ('pressure_solve', 20.0 * active * iters), ('projection', 40.0 * nodes),
+                              ('g2p', 64.0 * parts + 24.0 * nodes)):
                 gbs = alg / (ph[name] * 1e-3) / 1e9
                 fig[name] = dict(alg_bytes=alg, ms=ph[name], achieved_gbs=gbs, frac=gbs / peak)
             lanes.append(dict(tanks=len(idx), particles=parts, nodes=nodes, active_cells=active, phases_ms=ph,
