@@ -19,7 +19,9 @@ prefer another form than large ones.
 Each candidate is timed on the device (events on the tank's or batch's stream) over a few sub-steps of the
 real state, after one sub-step that captures its graph. Targets that can save and restore their state
 (``save_state`` / ``restore_state``: the tanks' water copies) are put back afterwards, so tuning leaves the
-simulation where it found it.
+simulation where it found it. The first candidate is the default; a shape that beats it on its first
+reading is timed twice more beside it and kept only if its slowest reading still wins by MARGIN, since some
+forms (the cluster solve beside a busy lane) swing by a fifth from one graph launch to the next.
 """
 
 CANDIDATES = ((2, 0, 0), (4, 0, 0), (8, 0, 0), (4, 2, 0), (4, 3, 0), (4, 1, 0),
@@ -28,58 +30,85 @@ CANDIDATES = ((2, 0, 0), (4, 0, 0), (8, 0, 0), (4, 2, 0), (4, 3, 0), (4, 1, 0),
 
 G2P_FORMS = (0, 2, 1)
 
+MARGIN = 0.02       # a shape replaces the first (default) one only when it is faster by this fraction
+CONFIRM = 2         # extra readings of the two finalists before that choice
+
 
 def _time(target, dt, steps):
     target.time_substeps(dt, 1)                  # captures the graph of the new shape
     return target.time_substeps(dt, steps) / steps
 
 
-def autotune(target, dt, candidates=CANDIDATES, steps=3, g2p_forms=G2P_FORMS):
+def _settle(target, dt, steps, timings, keys, apply, confirm):
+    """The fastest of `keys` by its first reading, checked against the first key (the default): both are
+    timed `confirm` more times, interleaved, and each is scored by its slowest reading, so a form whose
+    sub-step time swings from one graph launch to the next is judged by its bad readings. The fastest
+    replaces the default only when it still wins by MARGIN."""
+    default, first = keys[0], min(keys, key=timings.get)
+    if first == default or timings[default] == float('inf') or confirm <= 0:
+        return first
+    score = {default: timings[default], first: timings[first]}
+    for _ in range(confirm):
+        for key in (default, first):
+            apply(key)
+            score[key] = max(score[key], _time(target, dt, steps))
+    return first if score[first] * (1 + MARGIN) < score[default] else default
+
+
+def autotune(target, dt, candidates=CANDIDATES, steps=3, g2p_forms=G2P_FORMS, confirm=CONFIRM):
     """Return ((blocks_per_sm, sor_mode, piece_kb, g2p_form), {candidate: ms per sub-step}) and leave the best
     set. The candidates (blocks per SM, solve form, tile) are timed with the first G2P form; the other G2P
-    forms are then timed with the best of them."""
+    forms are then timed with the best of them. The first candidate and the first G2P form are the
+    defaults: another shape is kept only when it stays faster by MARGIN over repeated readings. The timings
+    returned are the first readings."""
     timings = {}
     last = None
     saved = target.save_state() if hasattr(target, 'save_state') else None
     has_g2p = hasattr(target, 'tune_g2p')
+
+    def shape(key):
+        target.tune_piece(key[2])
+        target.tune(key[0], key[1])
+
     try:
         if has_g2p:
             target.tune_g2p(g2p_forms[0])
+        keys = []
         for cand in candidates:
             key = (cand[0], cand[1], cand[2] if len(cand) > 2 else 0, g2p_forms[0])
+            keys.append(key)
             try:
-                target.tune_piece(key[2])
-                target.tune(key[0], key[1])
+                shape(key)
                 timings[key] = _time(target, dt, steps)
             except Exception as e:      # a shape the device cannot launch (too large to be co-resident, …)
                 timings[key] = float('inf')
                 last = e
-        best = min(timings, key=timings.get)
-        if timings[best] == float('inf'):
+        if min(timings.values()) == float('inf'):
             raise last
+        best = _settle(target, dt, steps, timings, keys, shape, confirm)
         if has_g2p:
-            target.tune_piece(best[2])
-            target.tune(best[0], best[1])
+            shape(best)
+            forms = [best]
             for form in g2p_forms[1:]:
                 key = best[:3] + (form,)
+                forms.append(key)
                 try:
                     target.tune_g2p(form)
                     timings[key] = _time(target, dt, steps)
                 except Exception as e:
                     timings[key] = float('inf')
                     last = e
-            best = min((k for k in timings if k[:3] == best[:3]), key=timings.get)
+            best = _settle(target, dt, steps, timings, forms, lambda key: target.tune_g2p(key[3]), confirm)
     finally:
         if saved is not None:
             target.restore_state(saved)
-    target.tune_piece(best[2])
-    target.tune(best[0], best[1])
+    shape(best)
     if has_g2p:
         target.tune_g2p(best[3])
     return best, timings
 
 
-def autotune_batch(batch, dt, candidates=CANDIDATES, steps=3, g2p_forms=G2P_FORMS):
+def autotune_batch(batch, dt, candidates=CANDIDATES, steps=3, g2p_forms=G2P_FORMS, confirm=CONFIRM):
     """Tune each size lane of a batch in turn (the others keep their settings) on the batch's sub-step time,
     with the batch's state rolled back afterwards. Returns ([best per lane], {lane: timings})."""
     saved = batch.save_state()
@@ -89,7 +118,7 @@ def autotune_batch(batch, dt, candidates=CANDIDATES, steps=3, g2p_forms=G2P_FORM
         for k in range(n):
             batch.tune_lane(k, *CANDIDATES[0][:2], 0, g2p_forms[0])
         for k in range(n):
-            b, t = autotune(batch.lane(k), dt, candidates, steps, g2p_forms)
+            b, t = autotune(batch.lane(k), dt, candidates, steps, g2p_forms, confirm)
             best.append(b)
             timings[k] = t
     finally:
