@@ -8,7 +8,9 @@ iterations at ω = 1.7, FLIP 0.95, dt = 1/240 s (11.7M particles, 3.7M cells; se
 one sub-step of all 64 tanks: binning, P2G, forces and divergence, the pressure solve, projection, G2P with
 collisions and drop/whitewater logic, advanced together by the batched, graph-captured launches with the
 form of the pressure solve picked by the autotuner. `value` is the batch's particle-steps/s; the same 64
-scenes stepped one by one on the plain path give `plain_sequential`. Synthetic seeded data.
+scenes stepped one by one on the plain path give `plain_sequential`. At one GPU the line also carries
+`serving`: p50/p99 request latency of the serving loop over a short Poisson run at 10 requests/s
+(`--serve-sample` seconds). Synthetic seeded data.
 
 Other workloads: `obstacles_inflow` (one 128×64×64 tank with obstacles, a faucet and a drain),
 `full_scene` (256×128×128 with rain and the 1024×512 ripple layer), `frame_export` (that scene's per-frame
@@ -588,6 +590,7 @@ def run_batch(args, rank, world, local):
                              '(warm: caches kept as in the step; cold: ncu flushed them before the launch)')
         cpu_rate, cpu_el, cpu_what = cpu_sample_rate(specs)
         launches = args.steps * sum(launches_per_substep(best[l][1], iters, g2p_form=best[l][3]) for l in range(nlanes))
+        serving = serving_sample(args.serve_sample, local) if world == 1 and args.serve_sample > 0 else None
         line = dict(metric=METRIC, value=value, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
                     ms_per_step=ms, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
                     data='synthetic (seeded particles, analytic obstacles)', config=cfg,
@@ -600,10 +603,25 @@ def run_batch(args, rank, world, local):
                     batched_over_plain=ms_plain / ms if world == 1 else None,
                     roofline=roofline, kernels=dict(peak_gbs=peak, lanes=lanes),
                     cpu_baseline=dict(value=cpu_rate, unit=METRIC, cores=1, kind='port', sample=cpu_what),
-                    e2e=e2e, gpu_launches=launches, clocks=clk, residual_f64=residual)
+                    e2e=e2e, gpu_launches=launches, clocks=clk, residual_f64=residual, serving=serving)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def serving_sample(duration, local, rate=10.0):
+    """The metric's latency figures beside the batch: the serving loop (`--workload serve`) run for `duration`
+    seconds of Poisson arrivals at `rate` requests/s, the load one B200 serves as it comes (at the serving
+    configuration's 200/s the offered load is several times what it delivers, and the latencies measure the
+    queue: `--workload serve --rate 200`). Latencies are wall-clock request times from submission to the
+    finished result."""
+    from importlib import import_module
+    r = import_module('hahenn-_b200.serve').poisson_run(rate=rate, duration=duration, steps=120, budget_bytes=150e9,
+                                                        device=local)
+    keep = ('requests', 'completed', 'failed', 'p50_ms', 'p99_ms', 'particle_steps_per_s',
+            'offered_particle_steps_per_s', 'mean_active', 'wall_s')
+    return dict(workload='serving_poisson', rate_per_s=rate, duration_s=duration, steps_per_request=120,
+                budget_gb=150, **{k: r[k] for k in keep})
 
 
 # ------------------------------------------------------------------ the single-tank workload
@@ -963,6 +981,8 @@ def main():
     ap.add_argument('--rate', type=float, default=200.0)
     ap.add_argument('--duration', type=float, default=60.0)
     ap.add_argument('--req-steps', type=int, default=120)
+    ap.add_argument('--serve-sample', type=float, default=20.0,
+                    help='batch workload at one GPU: seconds of serving at 10 requests/s for its p50/p99 (0: none)')
     ap.add_argument('--ncu-steps', type=int, default=0,
                     help='profiler run: 3 warm-up and N more sub-steps of the workload, no timing, no JSON line')
     ap.add_argument('--bps', type=int, default=2, help='profiler run: particle blocks per SM')

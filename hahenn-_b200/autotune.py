@@ -30,7 +30,7 @@ CANDIDATES = ((2, 0, 0), (4, 0, 0), (8, 0, 0), (4, 2, 0), (4, 3, 0), (4, 1, 0),
 
 G2P_FORMS = (0, 2, 1)
 
-MARGIN = 0.02       # a shape replaces the first (default) one only when it is faster by this fraction
+MARGIN = 0.01       # a shape replaces the first (default) one only when it is faster by this fraction
 CONFIRM = 2         # extra readings of the two finalists before that choice
 
 
