@@ -148,11 +148,24 @@ __device__ __forceinline__ double tank_sdf(const TankDev& T, double px, double p
   return scene_sdf(T.objs, T.nobj, px, py, pz, true);
 }
 
+// Half extents, in the obstacle's own frame, of a box holding the shape (the outer part of the cup and the
+// trough: their distance is the max of the outer shape's and a carved one's).
+__device__ __forceinline__ void local_box(const Obj& o, double& bx, double& by, double& bz) {
+  const double* d = o.dims;
+  switch (o.type) {
+    case 0: case 6: bx = d[0]; by = d[1]; bz = d[2]; return;          // (round) box, trough
+    case 2: case 3: case 5: bx = d[0]; by = d[1]; bz = d[0]; return;  // cylinder, cone, cup
+    case 4: bx = d[0] + d[1]; by = d[1]; bz = d[0] + d[1]; return;    // torus
+    default: bx = by = bz = d[0]; return;                             // sphere
+  }
+}
+
 // False only where the scene distance is certainly at least `r`: in analytic mode, when the point lies
-// beyond r (+1e-6, far above rounding) of every obstacle's bounding sphere. Every shape but the gutter
-// (type 7) lies inside its bounding sphere and its distance function is at least the distance to the shape
-// (exact, or the max of exact ones), so then every term of the scene minimum, culled or not, is ≥ r. Lattice
-// mode, or any gutter, always answers true.
+// beyond r (+1e-6, far above rounding) of every obstacle's bounding sphere, or of the box in the obstacle's
+// frame that holds it. Every shape but the gutter (type 7) lies inside both and its distance function is at
+// least the distance to the shape (exact, or the max of exact ones), so then every term of the scene
+// minimum, culled or not, is ≥ r. Lattice mode, or any gutter, always answers true. (A sphere's box adds
+// nothing to its sphere; a rotated box's or a cylinder's takes a quarter of the points its sphere does.)
 __device__ __forceinline__ bool maybe_within(const TankDev& T, double px, double py, double pz, double r) {
   if (!T.has_obst) return false;
   if (T.sdf_mode != kSdfAnalytic) return true;
@@ -162,7 +175,14 @@ __device__ __forceinline__ bool maybe_within(const TankDev& T, double px, double
     if (o.type == 7) return true;
     const double ex = px - o.pos[0], ey = py - o.pos[1], ez = pz - o.pos[2];
     const double lim = r + o.bound + 1e-6;
-    if (ex * ex + ey * ey + ez * ez < lim * lim) return true;
+    if (ex * ex + ey * ey + ez * ez >= lim * lim) continue;
+    if (o.type == 1) return true;
+    double qx, qy, qz, bx, by, bz;
+    to_local(o, px, py, pz, qx, qy, qz);
+    local_box(o, bx, by, bz);
+    const double ox = fmax(fabs(qx) - bx, 0.0), oy = fmax(fabs(qy) - by, 0.0), oz = fmax(fabs(qz) - bz, 0.0);
+    const double rb = r + 1e-6;
+    if (ox * ox + oy * oy + oz * oz < rb * rb) return true;
   }
   return false;
 }

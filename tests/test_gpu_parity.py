@@ -184,6 +184,35 @@ def test_obstacle_distances_every_shape(pkg, mode):
     t.close()
 
 
+def test_collisions_near_every_shape(pkg):
+    """Particles within a few collision radii of all eight shapes (turned) and others anywhere in the tank,
+    one sub-step in analytic mode: they equal the oracle's, which tests every particle against the scene
+    distance, so the device's culls (the bounding sphere, then a box in the obstacle's frame) skip no
+    collision."""
+    from parity import objs_from_items
+    nx, ny, nz, h = 24, 12, 16, 1 / 40
+    kw = dict(flip=0.96, omega=1.6, iters=20)
+    gpu = gpu_from(pkg, nx, ny, nz, h, **kw)
+    gpu.set_objects(ALL_SHAPES)
+    ora = oracle_from(nx, ny, nz, h, gpu.origin, **kw)
+    ora.set_objects(objs_from_items(ALL_SHAPES))
+    rng = np.random.default_rng(21)
+    pts = gpu.origin + rng.random((400000, 3)) * np.array([nx, ny, nz]) * h
+    d = ora.sdf_at(pts)
+    rc = 0.32 * h
+    near = pts[(d > -rc) & (d < 3 * rc)][:8000]
+    pos = f32(np.concatenate([near, pts[-4000:]]))
+    vel = f32(rng.uniform(-0.6, 0.6, pos.shape))
+    assert len(near) == 8000
+    gpu.add_particles(pos, vel)
+    ora.add_particles(pos, vel)
+    gpu.substep(1 / 240)
+    ora.frame = 1
+    ora.substep(1 / 240)
+    assert_particles(gpu, ora, 'collisions near every shape')
+    gpu.close()
+
+
 def test_drops_merge_ripple_impulse_crown_and_spawn(pkg):
     d = load('drops')
     nx, ny, nz, h = int(d['nx']), int(d['ny']), int(d['nz']), float(d['h'])
