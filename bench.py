@@ -430,7 +430,7 @@ def e2e_batch(P, specs, device, best, steps, workers=8):
     def job(n_steps):
         t0 = time.perf_counter()
         list(pool.map(lambda tp: tp[0].add_particles(tp[1]), zip(tanks, host)))
-        h2d = sum(32 * len(p) for p in host)          # staged as two float4 per particle
+        h2d = sum(12 * len(p) for p in host)          # the positions, copied packed (3 float32 per particle)
         d2h = 0
         t1 = time.perf_counter()
         for _ in range(n_steps):
@@ -692,7 +692,7 @@ def run_plain(args, rank, world, local):
         for e in w['emitters']:
             p, v = faucet_particles(e, dt, rng)
             t2.add_particles(p, v)
-            h2d += 32 * len(p)
+            h2d += 24 * len(p)          # positions and velocities, copied packed (6 float32 per particle)
         t2.substep(dt)
         t2.poll_stats()
         d2h += readback

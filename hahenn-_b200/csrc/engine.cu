@@ -31,6 +31,18 @@ __global__ void k_set_dt(TankDev* tanks, int n, double dt) {
 }
 __global__ void k_set_emit(Counters* c, int n) { c->n_emit = n; }
 
+// particles added from the host, copied packed as the caller gave them (positions, then velocities and
+// airborne marks where given, float32), into E's pos+flags / vel+id layout; ids count on from `first`
+__global__ void k_unpack_added(float4* __restrict__ pE, float4* __restrict__ vE, const float* __restrict__ pos,
+                               const float* __restrict__ vel, const float* __restrict__ air, int n, uint32_t first) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float a = air ? air[i] : 0.f;
+  pE[i] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], a > 0.5f ? (float)kFlagAir : 0.f);
+  const float vx = vel ? vel[3 * i] : 0.f, vy = vel ? vel[3 * i + 1] : 0.f, vz = vel ? vel[3 * i + 2] : 0.f;
+  vE[i] = make_float4(vx, vy, vz, __uint_as_float(first + (uint32_t)i));
+}
+
 __device__ __forceinline__ uint32_t hash32(uint32_t x) {
   x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
   return x;
@@ -329,13 +341,14 @@ Tank::~Tank() {
   cudaSetDevice(cfg.device);
   if (stream) cudaStreamSynchronize(stream);
   for (void* p : dmem) cudaFreeAsync(p, stream);
+  if (d_stage) cudaFreeAsync(d_stage, stream);
   if (stream) cudaStreamSynchronize(stream);
   if (snap.p) { cudaFree(snap.p); cudaFree(snap.v); cudaFree(snap.wp); cudaFree(snap.wv); cudaFree(snap.pres); cudaFree(snap.ripple); }
   free_ripple(*this);
   free_mesh(*this);
   delete h_ctr;
   for (int k = 0; k < 2; ++k) {
-    if (h_stage_p[k]) { cudaFreeHost(h_stage_p[k]); cudaFreeHost(h_stage_v[k]); }
+    if (h_stage[k]) cudaFreeHost(h_stage[k]);
     if (stage_ev[k]) cudaEventDestroy(stage_ev[k]);
   }
   if (h_poll) cudaFreeHost(h_poll);
@@ -463,11 +476,21 @@ bool Tank::poll_counters(Counters& out) {
   return fresh;
 }
 
-void Tank::stage(const float4* p, const float4* v, long long n) {
-  join();
+// n packed particles in pinned memory (positions, then velocities and marks where given) to the device in one
+// copy, unpacked into E after the particles staged before them
+void Tank::stage(const unsigned char* src, size_t bytes, long long n, bool has_vel, bool has_air) {
   if (n <= 0) return;
-  CK(cudaMemcpyAsync(d.pE + n_emit_host, p, n * 16, cudaMemcpyHostToDevice, stream));
-  CK(cudaMemcpyAsync(d.vE + n_emit_host, v, n * 16, cudaMemcpyHostToDevice, stream));
+  if (bytes > d_stage_cap) {
+    if (d_stage) CK(cudaFreeAsync(d_stage, stream));
+    d_stage_cap = bytes;
+    CK(cudaMallocAsync((void**)&d_stage, d_stage_cap, stream));
+  }
+  CK(cudaMemcpyAsync(d_stage, src, bytes, cudaMemcpyHostToDevice, stream));
+  const float* pos = reinterpret_cast<const float*>(d_stage);
+  const float* vel = has_vel ? pos + 3 * n : nullptr;
+  const float* air = has_air ? pos + (has_vel ? 6 : 3) * n : nullptr;
+  k_unpack_added<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(d.pE + n_emit_host, d.vE + n_emit_host, pos, vel,
+                                                                   air, (int)n, next_id);
   n_emit_host += n;
   k_set_emit<<<1, 1, 0, stream>>>(d.ctr, (int)n_emit_host);
   CK(cudaGetLastError());
@@ -485,30 +508,25 @@ void Tank::add_particles(const float* pos, const float* vel, const float* air, l
     room = std::min<long long>(cfg.cap - n_upper, emit_cap - n_emit_host);
   }
   long long take = std::max(0LL, std::min(n, room));
-  // two pinned staging buffers in turn: a buffer is refilled once the copies out of it two calls ago have
+  // two pinned staging buffers in turn: a buffer is refilled once the copy out of it two calls ago has
   // finished (an event, not a wait for the whole stream, so the host stays ahead of the device)
   const int k = stage_k;
   stage_k ^= 1;
   if (stage_ev[k]) CK(cudaEventSynchronize(stage_ev[k]));
   else CK(cudaEventCreateWithFlags(&stage_ev[k], cudaEventDisableTiming));
-  if ((size_t)take > stage_cap[k]) {
-    if (h_stage_p[k]) { cudaFreeHost(h_stage_p[k]); cudaFreeHost(h_stage_v[k]); }
-    stage_cap[k] = (size_t)take;
-    CK(cudaMallocHost(&h_stage_p[k], stage_cap[k] * 16));
-    CK(cudaMallocHost(&h_stage_v[k], stage_cap[k] * 16));
+  const size_t bp = (size_t)take * 12, bv = vel ? bp : 0, ba = air ? (size_t)take * 4 : 0;
+  if (bp + bv + ba > stage_cap[k]) {
+    if (h_stage[k]) cudaFreeHost(h_stage[k]);
+    h_stage[k] = nullptr;
+    stage_cap[k] = bp + bv + ba;
+    CK(cudaMallocHost((void**)&h_stage[k], stage_cap[k]));
   }
-  float4* sp = h_stage_p[k];
-  float4* sv = h_stage_v[k];
-  for (long long i = 0; i < take; ++i) {
-    const float a = air ? air[i] : 0.f;
-    sp[i] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], a > 0.5f ? (float)kFlagAir : 0.f);
-    const float vx = vel ? vel[3 * i] : 0.f, vy = vel ? vel[3 * i + 1] : 0.f, vz = vel ? vel[3 * i + 2] : 0.f;
-    uint32_t id = next_id + (uint32_t)i;
-    float idf;
-    memcpy(&idf, &id, 4);
-    sv[i] = make_float4(vx, vy, vz, idf);
+  if (take > 0) {
+    memcpy(h_stage[k], pos, bp);
+    if (vel) memcpy(h_stage[k] + bp, vel, bv);
+    if (air) memcpy(h_stage[k] + bp + bv, air, ba);
   }
-  stage(sp, sv, take);
+  stage(h_stage[k], bp + bv + ba, take, vel != nullptr, air != nullptr);
   CK(cudaEventRecord(stage_ev[k], stream));
   next_id += (uint32_t)take;
   if (take < n) {

@@ -105,8 +105,10 @@ struct Tank {
   uint32_t next_id = 0;
   long long n_emit_host = 0;      // particles staged in E for the next sub-step
   long long n_upper = 0;          // upper bound of live particles (exact after a stats read)
-  float4 *h_stage_p[2] = {}, *h_stage_v[2] = {};   // pinned staging of added particles, used in turn
-  size_t stage_cap[2] = {};
+  unsigned char* h_stage[2] = {};  // pinned staging of added particles (packed as given), used in turn
+  size_t stage_cap[2] = {};        // bytes
+  unsigned char* d_stage = nullptr;  // their device copy, unpacked into E by a kernel
+  size_t d_stage_cap = 0;
   cudaEvent_t stage_ev[2] = {};   // the copies out of each staging buffer have finished
   int stage_k = 0;
   Counters* h_poll = nullptr;     // pinned target of the asynchronous counter read
@@ -142,7 +144,7 @@ struct Tank {
   void read_counters();           // synchronous
   bool poll_counters(Counters& out);   // non-blocking: the last finished read into out (true); starts the next
   void add_particles(const float* pos, const float* vel, const float* air, long long n, uint32_t* first);
-  void stage(const float4* p, const float4* v, long long n);
+  void stage(const unsigned char* src, size_t bytes, long long n, bool has_vel, bool has_air);
   void emit_block(const double lo[3], const double hi[3], bool fill);
   void clear();
   void reset();
