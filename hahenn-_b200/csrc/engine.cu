@@ -31,6 +31,108 @@ __global__ void k_set_dt(TankDev* tanks, int n, double dt) {
 }
 __global__ void k_set_emit(Counters* c, int n) { c->n_emit = n; }
 
+// Read-back compaction: the live particles of A then E, in that order, into the sorted buffers B (scratch
+// between sub-steps: the binning of the next one rewrites them) in the layout of the C ABI, pos4 (x, y, z,
+// airborne 0/1) and vel4 (vx, vy, vz, id bits). Tiles of kReadTile particles: a count per tile, one scan of
+// the counts, then each tile writes its live particles at its prefix, ranked by warp ballots.
+constexpr int kReadThreads = 256, kReadPer = 4, kReadTile = kReadThreads * kReadPer;
+
+__device__ __forceinline__ float4 read_src(const float4* __restrict__ a, const float4* __restrict__ e, int nl, int i) {
+  return i < nl ? a[i] : e[i - nl];
+}
+
+__global__ void __launch_bounds__(kReadThreads) k_read_count(const float4* __restrict__ pA, const float4* __restrict__ pE,
+                                                             int nl, int tot, int* __restrict__ cnt) {
+  __shared__ int s_w[kReadThreads / 32];
+  int c = 0;
+#pragma unroll
+  for (int r = 0; r < kReadPer; ++r) {
+    const int i = blockIdx.x * kReadTile + r * kReadThreads + threadIdx.x;
+    if (i < tot) c += ((int)read_src(pA, pE, nl, i).w & kFlagDead) ? 0 : 1;
+  }
+  c = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+#pragma unroll
+    for (int w = 0; w < kReadThreads / 32; ++w) t += s_w[w];
+    cnt[blockIdx.x] = t;
+  }
+}
+
+// exclusive prefix of cnt[0, n) in place, the total in cnt[n]; one block of 1024 threads
+__global__ void __launch_bounds__(1024) k_read_scan(int* __restrict__ cnt, int n) {
+  __shared__ int s_w[32];
+  __shared__ int s_carry;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (int base = 0; base < n; base += 1024) {
+    const int i = base + threadIdx.x;
+    const int v = i < n ? cnt[i] : 0;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_w[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      int w = s_w[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      s_w[lane] = w;
+    }
+    __syncthreads();
+    const int before = s_carry + (warp ? s_w[warp - 1] : 0);
+    if (i < n) cnt[i] = before + x - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) s_carry = before + x;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) cnt[n] = s_carry;
+}
+
+__global__ void __launch_bounds__(kReadThreads) k_read_write(const float4* __restrict__ pA, const float4* __restrict__ vA,
+                                                             const float4* __restrict__ pE, const float4* __restrict__ vE,
+                                                             int nl, int tot, const int* __restrict__ pfx,
+                                                             float4* __restrict__ outp, float4* __restrict__ outv) {
+  __shared__ int s_w[kReadThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int off = pfx[blockIdx.x];
+  for (int r = 0; r < kReadPer; ++r) {
+    const int i = blockIdx.x * kReadTile + r * kReadThreads + threadIdx.x;
+    float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
+    bool live = false;
+    if (i < tot) {
+      P = read_src(pA, pE, nl, i);
+      live = !((int)P.w & kFlagDead);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, live);
+    if (lane == 0) s_w[warp] = __popc(m);
+    __syncthreads();
+    int before = 0, all = 0;
+#pragma unroll
+    for (int w = 0; w < kReadThreads / 32; ++w) {
+      const int c = s_w[w];
+      before += w < warp ? c : 0;
+      all += c;
+    }
+    if (live) {
+      const int k = off + before + __popc(m & ((1u << lane) - 1));
+      outp[k] = make_float4(P.x, P.y, P.z, ((int)P.w & kFlagAir) ? 1.f : 0.f);
+      if (outv) outv[k] = read_src(vA, vE, nl, i);
+    }
+    off += all;
+    __syncthreads();
+  }
+}
+
 // particles added from the host, copied packed as the caller gave them (positions, then velocities and
 // airborne marks where given, float32), into E's pos+flags / vel+id layout; ids count on from `first`
 __global__ void k_unpack_added(float4* __restrict__ pE, float4* __restrict__ vE, const float* __restrict__ pos,
@@ -342,6 +444,7 @@ Tank::~Tank() {
   if (stream) cudaStreamSynchronize(stream);
   for (void* p : dmem) cudaFreeAsync(p, stream);
   if (d_stage) cudaFreeAsync(d_stage, stream);
+  if (d_rcnt) cudaFreeAsync(d_rcnt, stream);
   if (stream) cudaStreamSynchronize(stream);
   if (snap.p) { cudaFree(snap.p); cudaFree(snap.v); cudaFree(snap.wp); cudaFree(snap.wv); cudaFree(snap.pres); cudaFree(snap.ripple); }
   free_ripple(*this);
@@ -353,6 +456,8 @@ Tank::~Tank() {
   }
   if (h_poll) cudaFreeHost(h_poll);
   if (h_read_p) { cudaFreeHost(h_read_p); cudaFreeHost(h_read_v); }
+  if (h_rcount) cudaFreeHost(h_rcount);
+  for (cudaEvent_t e : read_ev) cudaEventDestroy(e);
   if (poll_ev) cudaEventDestroy(poll_ev);
   if (ev_own) cudaEventDestroy(ev_own);
   if (stream && own_stream) cudaStreamDestroy(stream);
@@ -759,42 +864,57 @@ void Tank::frame_end(double frame_dt) {
   CK(cudaGetLastError());
 }
 
-// Particles of A then E (the previous sub-step's output and the pending emissions), dead ones skipped. The
-// device copies land in pinned buffers kept by the tank (one copy each of what is needed: positions only for a
-// count), then one pass converts them into the caller's arrays.
+// Particles of A then E (the previous sub-step's output and the pending emissions), dead ones skipped, in that
+// order: compacted on the device into the ABI layout (k_read_*), then the live count and as many particles as
+// the caller takes are copied into pinned buffers kept by the tank, in chunks whose copy into the caller's
+// arrays overlaps the transfer of the next.
 long long Tank::read_particles(float* pos4, float* vel4, long long cap) {
   read_counters();
   const long long nl = h_ctr->n_live, ne = h_ctr->n_emit, tot = nl + ne;
-  if ((size_t)tot > read_cap) {
-    if (h_read_p) { cudaFreeHost(h_read_p); cudaFreeHost(h_read_v); h_read_p = h_read_v = nullptr; read_cap = 0; }
-    CK(cudaMallocHost(&h_read_p, std::max<size_t>(tot, 1) * 16));
-    CK(cudaMallocHost(&h_read_v, std::max<size_t>(tot, 1) * 16));
-    read_cap = std::max<size_t>(tot, 1);
+  if (tot <= 0) return 0;
+  if (tot > cfg.cap) throw Error(-2, "particle counters above the capacity");   // B holds the compacted copy
+  const int nb = (int)((tot + kReadTile - 1) / kReadTile);
+  if ((size_t)nb + 1 > rcnt_cap) {
+    if (d_rcnt) CK(cudaFreeAsync(d_rcnt, stream));
+    rcnt_cap = (size_t)nb + 1;
+    CK(cudaMallocAsync((void**)&d_rcnt, rcnt_cap * sizeof(int), stream));
   }
-  float4* P = h_read_p;
-  float4* V = h_read_v;
-  const bool want_v = vel4 != nullptr && cap > 0;
-  if (nl) {
-    CK(cudaMemcpyAsync(P, d.pA, nl * 16, cudaMemcpyDeviceToHost, stream));
-    if (want_v) CK(cudaMemcpyAsync(V, d.vA, nl * 16, cudaMemcpyDeviceToHost, stream));
-  }
-  if (ne) {
-    CK(cudaMemcpyAsync(P + nl, d.pE, ne * 16, cudaMemcpyDeviceToHost, stream));
-    if (want_v) CK(cudaMemcpyAsync(V + nl, d.vE, ne * 16, cudaMemcpyDeviceToHost, stream));
-  }
+  if (!h_rcount) CK(cudaMallocHost((void**)&h_rcount, sizeof(int)));
+  const bool want_p = pos4 != nullptr && cap > 0, want_v = vel4 != nullptr && cap > 0;
+  k_read_count<<<nb, kReadThreads, 0, stream>>>(d.pA, d.pE, (int)nl, (int)tot, d_rcnt);
+  k_read_scan<<<1, 1024, 0, stream>>>(d_rcnt, nb);
+  if (want_p || want_v)
+    k_read_write<<<nb, kReadThreads, 0, stream>>>(d.pA, d.vA, d.pE, d.vE, (int)nl, (int)tot, d_rcnt, d.pB,
+                                                  want_v ? d.vB : nullptr);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h_rcount, d_rcnt + nb, sizeof(int), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
-  long long k = 0;
-  for (long long i = 0; i < tot; ++i) {
-    const int fl = (int)P[i].w;
-    if (fl & kFlagDead) continue;
-    if (k < cap) {
-      if (pos4) {
-        float* o = pos4 + 4 * k;
-        o[0] = P[i].x; o[1] = P[i].y; o[2] = P[i].z; o[3] = (fl & kFlagAir) ? 1.f : 0.f;
-      }
-      if (want_v) memcpy(vel4 + 4 * k, &V[i], 16);
-    }
-    ++k;
+  const long long k = *h_rcount, m = std::min(k, want_p || want_v ? cap : 0LL);
+  if (m <= 0) return k;
+  if ((size_t)m > read_cap) {
+    if (h_read_p) { cudaFreeHost(h_read_p); cudaFreeHost(h_read_v); h_read_p = h_read_v = nullptr; read_cap = 0; }
+    CK(cudaMallocHost(&h_read_p, (size_t)m * 16));
+    CK(cudaMallocHost(&h_read_v, (size_t)m * 16));
+    read_cap = (size_t)m;
+  }
+  constexpr long long kChunk = 1 << 20;
+  const int nch = (int)((m + kChunk - 1) / kChunk);
+  while ((int)read_ev.size() < nch) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    read_ev.push_back(e);
+  }
+  for (int c = 0; c < nch; ++c) {
+    const long long a = c * kChunk, n = std::min(kChunk, m - a);
+    if (want_p) CK(cudaMemcpyAsync(h_read_p + a, d.pB + a, n * 16, cudaMemcpyDeviceToHost, stream));
+    if (want_v) CK(cudaMemcpyAsync(h_read_v + a, d.vB + a, n * 16, cudaMemcpyDeviceToHost, stream));
+    CK(cudaEventRecord(read_ev[c], stream));
+  }
+  for (int c = 0; c < nch; ++c) {
+    const long long a = c * kChunk, n = std::min(kChunk, m - a);
+    CK(cudaEventSynchronize(read_ev[c]));
+    if (want_p) memcpy(pos4 + 4 * a, h_read_p + a, n * 16);
+    if (want_v) memcpy(vel4 + 4 * a, h_read_v + a, n * 16);
   }
   return k;
 }

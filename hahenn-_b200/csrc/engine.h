@@ -114,6 +114,10 @@ struct Tank {
   Counters* h_poll = nullptr;     // pinned target of the asynchronous counter read
   float4 *h_read_p = nullptr, *h_read_v = nullptr;   // pinned landing buffers of particle read-back
   size_t read_cap = 0;
+  int* d_rcnt = nullptr;          // per-block live counts of the read-back compaction, then their prefix
+  size_t rcnt_cap = 0;
+  int* h_rcount = nullptr;        // pinned: the live count
+  std::vector<cudaEvent_t> read_ev;   // one per copied chunk of the read-back
   cudaEvent_t poll_ev = nullptr;
   bool poll_pending = false;
   std::string err;
