@@ -451,12 +451,13 @@ Tank::~Tank() {
   free_mesh(*this);
   delete h_ctr;
   for (int k = 0; k < 2; ++k) {
-    if (h_stage[k]) cudaFreeHost(h_stage[k]);
+    pinned_put(h_stage[k], stage_cap[k]);
     if (stage_ev[k]) cudaEventDestroy(stage_ev[k]);
   }
-  if (h_poll) cudaFreeHost(h_poll);
-  if (h_read_p) { cudaFreeHost(h_read_p); cudaFreeHost(h_read_v); }
-  if (h_rcount) cudaFreeHost(h_rcount);
+  pinned_put(h_poll, sizeof(Counters));
+  pinned_put(h_read_p, read_cap * 16);
+  pinned_put(h_read_v, read_cap * 16);
+  pinned_put(h_rcount, sizeof(int));
   for (cudaEvent_t e : read_ev) cudaEventDestroy(e);
   if (poll_ev) cudaEventDestroy(poll_ev);
   if (ev_own) cudaEventDestroy(ev_own);
@@ -469,6 +470,50 @@ void Tank::join() {
     dep = nullptr;
   }
   dirty = true;
+}
+
+namespace {
+std::mutex g_pin_m;
+std::map<size_t, std::vector<void*>> g_pin_free;
+size_t g_pin_cached = 0;
+constexpr size_t kPinCacheMax = 2ull << 30;
+size_t pin_class(size_t b) {
+  size_t c = 4096;
+  while (c < b) c <<= 1;
+  return c;
+}
+}  // namespace
+
+void* pinned_get(size_t bytes, size_t* got) {
+  const size_t c = pin_class(bytes);
+  if (got) *got = c;
+  {
+    std::lock_guard<std::mutex> g(g_pin_m);
+    auto it = g_pin_free.find(c);
+    if (it != g_pin_free.end() && !it->second.empty()) {
+      void* p = it->second.back();
+      it->second.pop_back();
+      g_pin_cached -= c;
+      return p;
+    }
+  }
+  void* p = nullptr;
+  CK(cudaHostAlloc(&p, c, cudaHostAllocPortable));
+  return p;
+}
+
+void pinned_put(void* p, size_t bytes) {
+  if (!p) return;
+  const size_t c = pin_class(bytes);
+  {
+    std::lock_guard<std::mutex> g(g_pin_m);
+    if (g_pin_cached + c <= kPinCacheMax) {
+      g_pin_free[c].push_back(p);
+      g_pin_cached += c;
+      return;
+    }
+  }
+  cudaFreeHost(p);
 }
 
 size_t tank_bytes(const TankConfig& c) {
@@ -571,7 +616,7 @@ bool Tank::poll_counters(Counters& out) {
   }
   if (!poll_pending) {
     if (!h_poll) {
-      CK(cudaMallocHost(&h_poll, sizeof(Counters)));
+      h_poll = (Counters*)pinned_get(sizeof(Counters));
       CK(cudaEventCreateWithFlags(&poll_ev, cudaEventDisableTiming));
     }
     CK(cudaMemcpyAsync(h_poll, d.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
@@ -621,10 +666,10 @@ void Tank::add_particles(const float* pos, const float* vel, const float* air, l
   else CK(cudaEventCreateWithFlags(&stage_ev[k], cudaEventDisableTiming));
   const size_t bp = (size_t)take * 12, bv = vel ? bp : 0, ba = air ? (size_t)take * 4 : 0;
   if (bp + bv + ba > stage_cap[k]) {
-    if (h_stage[k]) cudaFreeHost(h_stage[k]);
+    pinned_put(h_stage[k], stage_cap[k]);
     h_stage[k] = nullptr;
-    stage_cap[k] = bp + bv + ba;
-    CK(cudaMallocHost((void**)&h_stage[k], stage_cap[k]));
+    stage_cap[k] = 0;
+    h_stage[k] = (unsigned char*)pinned_get(bp + bv + ba, &stage_cap[k]);
   }
   if (take > 0) {
     memcpy(h_stage[k], pos, bp);
@@ -879,7 +924,7 @@ long long Tank::read_particles(float* pos4, float* vel4, long long cap) {
     rcnt_cap = (size_t)nb + 1;
     CK(cudaMallocAsync((void**)&d_rcnt, rcnt_cap * sizeof(int), stream));
   }
-  if (!h_rcount) CK(cudaMallocHost((void**)&h_rcount, sizeof(int)));
+  if (!h_rcount) h_rcount = (int*)pinned_get(sizeof(int));
   const bool want_p = pos4 != nullptr && cap > 0, want_v = vel4 != nullptr && cap > 0;
   k_read_count<<<nb, kReadThreads, 0, stream>>>(d.pA, d.pE, (int)nl, (int)tot, d_rcnt);
   k_read_scan<<<1, 1024, 0, stream>>>(d_rcnt, nb);
@@ -892,10 +937,14 @@ long long Tank::read_particles(float* pos4, float* vel4, long long cap) {
   const long long k = *h_rcount, m = std::min(k, want_p || want_v ? cap : 0LL);
   if (m <= 0) return k;
   if ((size_t)m > read_cap) {
-    if (h_read_p) { cudaFreeHost(h_read_p); cudaFreeHost(h_read_v); h_read_p = h_read_v = nullptr; read_cap = 0; }
-    CK(cudaMallocHost(&h_read_p, (size_t)m * 16));
-    CK(cudaMallocHost(&h_read_v, (size_t)m * 16));
-    read_cap = (size_t)m;
+    pinned_put(h_read_p, read_cap * 16);
+    pinned_put(h_read_v, read_cap * 16);
+    h_read_p = h_read_v = nullptr;
+    read_cap = 0;
+    size_t got = 0;
+    h_read_p = (float4*)pinned_get((size_t)m * 16, &got);
+    h_read_v = (float4*)pinned_get((size_t)m * 16);
+    read_cap = got / 16;
   }
   constexpr long long kChunk = 1 << 20;
   const int nch = (int)((m + kChunk - 1) / kChunk);
@@ -1065,7 +1114,7 @@ int blocks_for(int fam, const TankDev& D) {
 }
 }  // namespace
 
-Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
+Group::Group(const std::vector<Tank*>& t, cudaStream_t s, bool async_setup) : tanks(t) {
   if (tanks.empty()) throw Error(-1, "a batch needs at least one tank");
   device = tanks[0]->cfg.device;
   for (Tank* x : tanks)
@@ -1073,13 +1122,18 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
   CK(cudaSetDevice(device));
   if (s) { stream = s; } else { CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)); own_stream = true; }
   CK(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device));
+  if (async_setup) {
+    CK(cudaStreamCreateWithFlags(&setup, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&setup_done, cudaEventDisableTiming));
+  }
+  const cudaStream_t q = async_setup ? setup : stream;   // where the tables are allocated and filled
   CK(sor_tb_prepare());
   const int n = (int)tanks.size();
-  CK(cudaMallocAsync(&d_tanks, n * sizeof(TankDev), stream));
+  CK(cudaMallocAsync(&d_tanks, n * sizeof(TankDev), q));
   h_tanks = new TankDev[n];
-  CK(cudaMallocAsync(&d_bpfx, kFamCount * (n + 1) * sizeof(int), stream));
-  CK(cudaMallocAsync(&d_ppfx, 2 * (n + 1) * sizeof(int), stream));
-  CK(cudaMemsetAsync(d_ppfx, 0, 2 * (n + 1) * sizeof(int), stream));
+  CK(cudaMallocAsync(&d_bpfx, kFamCount * (n + 1) * sizeof(int), q));
+  CK(cudaMallocAsync(&d_ppfx, 2 * (n + 1) * sizeof(int), q));
+  CK(cudaMemsetAsync(d_ppfx, 0, 2 * (n + 1) * sizeof(int), q));
   std::vector<int> pf(kFamCount * (n + 1));
   for (int f = 0; f < kFamCount; ++f) {
     int acc = 0;
@@ -1088,25 +1142,30 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
     ctx.nblocks[f] = acc;
     ctx.bpfx[f] = d_bpfx + f * (n + 1);
   }
-  CK(cudaMallocAsync(&d_bsum, std::max(1, ctx.nblocks[kFamScan]) * sizeof(long long), stream));
-  CK(cudaMemcpyAsync(d_bpfx, pf.data(), pf.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+  CK(cudaMallocAsync(&d_bsum, std::max(1, ctx.nblocks[kFamScan]) * sizeof(long long), q));
+  CK(cudaMemcpyAsync(d_bpfx, pf.data(), pf.size() * sizeof(int), cudaMemcpyHostToDevice, q));
   std::vector<int> hp(n + 1, 0);
   for (int i = 0; i < n; ++i) hp[i + 1] = hp[i] + tanks[i]->d.nhalf;
-  CK(cudaMallocAsync(&d_hpfx, (n + 1) * sizeof(int), stream));
-  CK(cudaMallocAsync(&d_apfx, 2 * (n + 1) * sizeof(int), stream));
-  CK(cudaMemsetAsync(d_apfx, 0, 2 * (n + 1) * sizeof(int), stream));
-  CK(cudaMemcpyAsync(d_hpfx, hp.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
-  CK(cudaMallocAsync(&d_barrier, sizeof(GridBarrier), stream));
-  CK(cudaMemsetAsync(d_barrier, 0, sizeof(GridBarrier), stream));
-  CK(cudaMallocAsync(&d_ticket, 4 * sizeof(unsigned), stream));
-  CK(cudaMemsetAsync(d_ticket, 0, 4 * sizeof(unsigned), stream));
+  CK(cudaMallocAsync(&d_hpfx, (n + 1) * sizeof(int), q));
+  CK(cudaMallocAsync(&d_apfx, 2 * (n + 1) * sizeof(int), q));
+  CK(cudaMemsetAsync(d_apfx, 0, 2 * (n + 1) * sizeof(int), q));
+  CK(cudaMemcpyAsync(d_hpfx, hp.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, q));
+  CK(cudaMallocAsync(&d_barrier, sizeof(GridBarrier), q));
+  CK(cudaMemsetAsync(d_barrier, 0, sizeof(GridBarrier), q));
+  CK(cudaMallocAsync(&d_ticket, 4 * sizeof(unsigned), q));
+  CK(cudaMemsetAsync(d_ticket, 0, 4 * sizeof(unsigned), q));
   size_t defer_cap = 1;                 // G2P form 2: every particle of the group may be deferred
   for (Tank* x : tanks) defer_cap += (size_t)x->d.cap + (size_t)std::max(x->d.emit_cap, 0);
-  CK(cudaMallocAsync(&d_defer, defer_cap * sizeof(int) + 16, stream));
+  CK(cudaMallocAsync(&d_defer, defer_cap * sizeof(int) + 16, q));
   // the persistent solve: one block of 1024 threads per SM at most, and no more blocks than ~4 cells a thread
   // (the grid barrier's cost grows with the number of arriving blocks); a batch shares the SMs among its lanes
   sor_blocks = std::min(std::min(sor_persist_max_blocks(device), sm_count), std::max(1, (2 * hp[n] + 4095) / 4096));
-  CK(cudaStreamSynchronize(stream));
+  if (async_setup) {
+    CK(cudaEventRecord(setup_done, setup));
+    CK(cudaStreamWaitEvent(stream, setup_done, 0));
+  } else {
+    CK(cudaStreamSynchronize(stream));
+  }
   ctx.hpfx = d_hpfx;
   ctx.apfx = d_apfx;
   ctx.barrier = d_barrier;
@@ -1140,7 +1199,7 @@ Group::Group(const std::vector<Tank*>& t, cudaStream_t s) : tanks(t) {
 
 Group::~Group() {
   cudaSetDevice(device);
-  cudaStreamSynchronize(stream);
+  if (!settled) cudaStreamSynchronize(stream);
   drop_graph();
   for (cudaEvent_t e : ev_ph)
     if (e) cudaEventDestroy(e);
@@ -1156,6 +1215,8 @@ Group::~Group() {
                   (void*)d_ppfx, (void*)d_bsum, (void*)d_pieces, (void*)d_defer})
     if (p) cudaFreeAsync(p, stream);
   delete[] h_tanks;
+  if (setup) cudaStreamDestroy(setup);
+  if (setup_done) cudaEventDestroy(setup_done);
   if (own_stream) cudaStreamDestroy(stream);
 }
 
@@ -1324,15 +1385,25 @@ void Group::ensure_uploaded() {
   bool stale = false;
   for (size_t i = 0; i < tanks.size(); ++i) stale |= uploaded[i] != tanks[i]->version;
   if (!stale) return;
-  CK(cudaStreamSynchronize(stream));
+  // the first upload of a group set up on its own stream goes the same way (nothing has used the table yet);
+  // later ones wait until the sub-steps queued with the old table have run
+  const bool first_async = setup && !uploaded_once;
+  if (!first_async) CK(cudaStreamSynchronize(stream));
   int mi = 0;
   for (size_t i = 0; i < tanks.size(); ++i) {
     h_tanks[i] = tanks[i]->d;
     uploaded[i] = tanks[i]->version;
     mi = std::max(mi, tanks[i]->d.iters);
   }
-  CK(cudaMemcpyAsync(d_tanks, h_tanks, tanks.size() * sizeof(TankDev), cudaMemcpyHostToDevice, stream));
-  CK(cudaStreamSynchronize(stream));
+  if (first_async) {
+    CK(cudaMemcpyAsync(d_tanks, h_tanks, tanks.size() * sizeof(TankDev), cudaMemcpyHostToDevice, setup));
+    CK(cudaEventRecord(setup_done, setup));
+    CK(cudaStreamWaitEvent(stream, setup_done, 0));
+  } else {
+    CK(cudaMemcpyAsync(d_tanks, h_tanks, tanks.size() * sizeof(TankDev), cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+  uploaded_once = true;
   dt_on_device = false;                          // the host images carry no sub-step dt
   // the graph's shape depends only on the iteration count (the emitter kernel reads nemit on the device)
   if (mi != max_iters) { max_iters = mi; drop_graph(); }

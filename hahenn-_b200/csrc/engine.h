@@ -70,6 +70,13 @@ struct TankConfig {
 // device bytes a tank of this configuration allocates (admission by HBM budget)
 size_t tank_bytes(const TankConfig& c);
 
+// Pinned host memory through a process-wide cache of blocks (powers of two from 4 KB, up to 2 GB cached):
+// handing pinned memory back to the driver synchronises the device, which would stall every batch running
+// on it whenever a scene is released (serving). pinned_get returns a block of at least `bytes` (its size in
+// *got when given); pinned_put takes it back with the same request size.
+void* pinned_get(size_t bytes, size_t* got = nullptr);
+void pinned_put(void* p, size_t bytes);
+
 struct PrevXf { double pos[3]; double R[9]; };
 
 struct Snapshot {
@@ -217,8 +224,15 @@ struct Group {
   bool use_graphs = true;
   int sm_count = 148;
 
-  Group(const std::vector<Tank*>& t, cudaStream_t s);
+  // async_setup: the group's tables are set up on a stream of its own that the group's stream then waits for,
+  // so building a group does not wait for work already queued on that stream (a serving lane replaces its
+  // group while the previous one's sub-steps run)
+  Group(const std::vector<Tank*>& t, cudaStream_t s, bool async_setup = false);
   ~Group();
+  cudaStream_t setup = nullptr;   // async_setup: the stream of the first uploads
+  cudaEvent_t setup_done = nullptr;
+  bool uploaded_once = false;
+  bool settled = false;           // the owner saw every launch of this group finish: no wait when destroyed
   void ensure_uploaded();
   void set_dt(double dt);
   double dev_dt = 0;              // the sub-step dt the device descriptors hold, when dt_on_device

@@ -37,7 +37,15 @@ Server::~Server() {
   cv.notify_all();
   if (worker.joinable()) worker.join();
   cudaSetDevice(dev);
-  for (Lane& L : lanes) L.group.reset();
+  for (Lane& L : lanes) {
+    try {
+      settle(L, true);
+    } catch (const Error&) {
+      for (auto& r : L.retired) if (r.ev) cudaEventDestroy(r.ev);
+      L.retired.clear();
+    }
+    L.group.reset();
+  }
   for (auto& kv : reqs) kv.second->tank.reset();
   for (Lane& L : lanes) {
     cudaStreamSynchronize(L.stream);
@@ -133,7 +141,38 @@ void Server::finish_request(Request* r) {
   cv.notify_all();
 }
 
+// a lane's group is replaced without waiting for its queued sub-steps: it is kept, with the requests that
+// ended with it, until an event after its last sub-step has completed
+void Server::retire(Lane& L, std::vector<Request*> done) {
+  Lane::Retired r;
+  r.group = std::move(L.group);
+  r.done = std::move(done);
+  CK(cudaEventCreateWithFlags(&r.ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(r.ev, L.stream));
+  L.retired.push_back(std::move(r));
+}
+
+void Server::settle(Lane& L, bool wait) {
+  while (!L.retired.empty()) {
+    Lane::Retired& r = L.retired.front();
+    if (wait) {
+      CK(cudaEventSynchronize(r.ev));
+    } else {
+      const cudaError_t q = cudaEventQuery(r.ev);
+      if (q == cudaErrorNotReady) break;
+      CK(q);
+    }
+    if (r.group) r.group->settled = true;
+    r.group.reset();
+    cudaEventDestroy(r.ev);
+    std::vector<Request*> done = std::move(r.done);
+    L.retired.pop_front();
+    for (Request* q : done) finish_request(q);
+  }
+}
+
 bool Server::advance(Lane& L) {
+  settle(L, false);
   // sub-steps of this lane that have finished on the device free their places
   while (!L.inflight.empty()) {
     const cudaError_t q = cudaEventQuery(L.inflight.front());
@@ -144,10 +183,10 @@ bool Server::advance(Lane& L) {
   }
   if ((int)L.inflight.size() >= kLaneRunAhead) return false;
   if (L.changed || !L.group) {
-    L.group.reset();
+    if (L.group) retire(L, {});
     std::vector<Tank*> ts;
     for (Request* r : L.active) ts.push_back(r->tank.get());
-    L.group.reset(new Group(ts, L.stream));
+    L.group.reset(new Group(ts, L.stream, true));
     // the lanes run at the same time: a lane's persistent solve (sor_mode 1) takes at most its share of the SMs,
     // so that the cooperative launches of all lanes are resident together
     L.group->sor_blocks = std::max(1, std::min(L.group->sor_blocks, L.group->sm_count / kSizeLanes));
@@ -190,8 +229,7 @@ bool Server::advance(Lane& L) {
   std::vector<Request*> still, done;
   for (Request* r : L.active) (++r->steps_done >= r->steps ? done : still).push_back(r);
   if (!done.empty()) {
-    L.group.reset();                 // the batch refers to the tanks that are about to be freed
-    for (Request* r : done) finish_request(r);
+    retire(L, std::move(done));      // the group refers to the tanks, which are freed once it has run
     L.changed = true;
   }
   L.active.swap(still);
@@ -203,7 +241,7 @@ void Server::loop() {
   while (true) {
     std::vector<Request*> admitted;
     bool idle = true;
-    for (Lane& L : lanes) idle &= L.active.empty();
+    for (Lane& L : lanes) idle &= L.active.empty() && L.retired.empty();
     {
       std::unique_lock<std::mutex> g(m);
       if (idle && queue.empty()) cv.wait_for(g, std::chrono::milliseconds(20));
@@ -222,11 +260,17 @@ void Server::loop() {
     long long resident = 0;
     for (Lane& L : lanes) resident += (long long)L.active.size();
     for (Lane& L : lanes) {
-      if (L.active.empty()) continue;
+      if (L.active.empty()) {
+        settle(L, false);
+        continue;
+      }
       any = true;
       moved |= advance(L);
     }
-    if (!any) continue;
+    if (!any) {
+      std::this_thread::sleep_for(std::chrono::microseconds(20));   // only retired groups left to finish
+      continue;
+    }
     if (moved) {
       ++rounds;
       sum_active += (double)resident;

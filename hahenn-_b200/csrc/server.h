@@ -50,6 +50,14 @@ struct Lane {
   bool changed = false;
   std::deque<cudaEvent_t> inflight;   // one per queued sub-step, oldest first
   std::vector<cudaEvent_t> spare;
+  // groups replaced while their sub-steps were still queued: each is destroyed, and the requests that ended
+  // with it are finished, once the event recorded after its last sub-step has completed
+  struct Retired {
+    std::unique_ptr<Group> group;
+    cudaEvent_t ev = nullptr;
+    std::vector<Request*> done;
+  };
+  std::deque<Retired> retired;
 };
 
 struct Server {
@@ -68,6 +76,8 @@ struct Server {
 
   Server(int device, double budget_bytes, double dt);
   ~Server();
+  void retire(Lane& L, std::vector<Request*> done);
+  void settle(Lane& L, bool wait);    // destroy the retired groups whose work has run (wait: all of them)
   long long submit(std::unique_ptr<Request> r);
   ServerStats stats();
 

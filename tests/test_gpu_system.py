@@ -234,6 +234,41 @@ def test_empty_tank_steps_cleanly(pkg):
     t.close()
 
 
+def test_read_back_skips_the_drained_and_keeps_pending_adds(pkg):
+    """The read-back (compacted on the device): particles a drain took in the last sub-step are left out, the
+    rest keep their order, particles added since come after them with their ids, marks and velocities, and a
+    read with no arrays returns the same count."""
+    import ctypes as C
+    w = pkg.workloads.dam_break()
+    t = pkg.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], whitewater=False, ripple=None,
+                 capacity=len(w['pos']) + 4096, iters=20)
+    t.set_objects([dict(kind='drain', pos=[-0.3, 0.0, 0.0], rot=[0, 0, 0], r=0.12)])
+    t.add_particles(w['pos'])
+    n0 = len(w['pos'])
+    for _ in range(3):
+        t.substep(1 / 240)
+    p1, v1 = t.particles4()
+    assert 0 < len(p1) < n0                                    # the drain took some
+    assert len(np.unique(v1[:, 3].view(np.uint32))) == len(p1)
+    rng = np.random.default_rng(5)
+    add = (np.array([0.1, 0.6, 0.1]) + rng.uniform(-0.05, 0.05, (1000, 3))).astype(np.float32)
+    vel = rng.uniform(-1, 1, (1000, 3)).astype(np.float32)
+    air = (rng.random(1000) < 0.5).astype(np.float32)
+    first = t.add_particles(add, vel, air)
+    p2, v2 = t.particles4()
+    assert len(p2) == len(p1) + 1000
+    np.testing.assert_array_equal(p2[:len(p1)], p1)
+    np.testing.assert_array_equal(v2[:len(p1)], v1)
+    np.testing.assert_array_equal(p2[len(p1):, :3], add)
+    np.testing.assert_array_equal(p2[len(p1):, 3], air)
+    np.testing.assert_array_equal(v2[len(p1):, :3], vel)
+    np.testing.assert_array_equal(v2[len(p1):, 3].view(np.uint32), first + np.arange(1000, dtype=np.uint32))
+    n = C.c_int64()
+    pkg.native.check(pkg.native.lib().suiri_read_particles(t.handle, None, None, 0, C.byref(n)))
+    assert n.value == len(p2)
+    t.close()
+
+
 def test_poll_stats_and_pipelined_particle_adds(pkg):
     """Non-blocking stats (pollStats): the first call only starts a read; a read started once the stream is
     idle returns exactly what the blocking read returns. Particles added every sub-step through the two
