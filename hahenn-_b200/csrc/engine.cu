@@ -502,6 +502,19 @@ void* pinned_get(size_t bytes, size_t* got) {
   return p;
 }
 
+bool host_pinned(const void* p, size_t bytes) {
+  if (!p || !bytes) return false;
+  for (const char* q : {(const char*)p, (const char*)p + bytes - 1}) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    if (a.type != cudaMemoryTypeHost) return false;
+  }
+  return true;
+}
+
 void pinned_put(void* p, size_t bytes) {
   if (!p) return;
   const size_t c = pin_class(bytes);
@@ -936,6 +949,13 @@ long long Tank::read_particles(float* pos4, float* vel4, long long cap) {
   CK(cudaStreamSynchronize(stream));
   const long long k = *h_rcount, m = std::min(k, want_p || want_v ? cap : 0LL);
   if (m <= 0) return k;
+  // caller arrays in page-locked memory: the copy engine writes them directly
+  if ((!want_p || host_pinned(pos4, (size_t)m * 16)) && (!want_v || host_pinned(vel4, (size_t)m * 16))) {
+    if (want_p) CK(cudaMemcpyAsync(pos4, d.pB, (size_t)m * 16, cudaMemcpyDeviceToHost, stream));
+    if (want_v) CK(cudaMemcpyAsync(vel4, d.vB, (size_t)m * 16, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    return k;
+  }
   if ((size_t)m > read_cap) {
     pinned_put(h_read_p, read_cap * 16);
     pinned_put(h_read_v, read_cap * 16);

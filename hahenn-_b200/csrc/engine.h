@@ -76,6 +76,8 @@ size_t tank_bytes(const TankConfig& c);
 // *got when given); pinned_put takes it back with the same request size.
 void* pinned_get(size_t bytes, size_t* got = nullptr);
 void pinned_put(void* p, size_t bytes);
+// true when both ends of [p, p + bytes) are page-locked host memory (registered or allocated by CUDA)
+bool host_pinned(const void* p, size_t bytes);
 
 struct PrevXf { double pos[3]; double R[9]; };
 

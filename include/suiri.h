@@ -231,7 +231,9 @@ int suiri_frame_end(suiri_tank* t, double frame_dt);
 int suiri_sync(suiri_tank* t);
 
 /* liquid particles (alive) to host memory: pos4 = (x, y, z, airborne), vel4 = (vx, vy, vz, id as uint32 bits);
-   either pointer may be NULL; *n = number available (written even when cap is too small) */
+   either pointer may be NULL; *n = number available (written even when cap is too small). Arrays in
+   page-locked memory (cudaHostRegister, cudaMallocHost) are written by the copy engine directly; others
+   through the tank's pinned buffers. */
 int suiri_read_particles(suiri_tank* t, float* pos4, float* vel4, int64_t cap, int64_t* n);
 /* whitewater: pos4 = (x, y, z, life), vel4 = (vx, vy, vz, kind) */
 int suiri_read_whitewater(suiri_tank* t, float* pos4, float* vel4, int64_t cap, int64_t* n);

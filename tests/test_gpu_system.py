@@ -236,8 +236,8 @@ def test_empty_tank_steps_cleanly(pkg):
 
 def test_read_back_skips_the_drained_and_keeps_pending_adds(pkg):
     """The read-back (compacted on the device): particles a drain took in the last sub-step are left out, the
-    rest keep their order, particles added since come after them with their ids, marks and velocities, and a
-    read with no arrays returns the same count."""
+    rest keep their order, particles added since come after them with their ids, marks and velocities, a
+    read with no arrays returns the same count, and a read into page-locked arrays gives the same particles."""
     import ctypes as C
     w = pkg.workloads.dam_break()
     t = pkg.Tank(nx=w['nx'], ny=w['ny'], nz=w['nz'], h=w['h'], whitewater=False, ripple=None,
@@ -266,6 +266,14 @@ def test_read_back_skips_the_drained_and_keeps_pending_adds(pkg):
     n = C.c_int64()
     pkg.native.check(pkg.native.lib().suiri_read_particles(t.handle, None, None, 0, C.byref(n)))
     assert n.value == len(p2)
+    # into page-locked arrays (written by the copy engine directly): the same particles
+    import torch
+    pp = torch.full((len(p2) + 10, 4), -7.0, dtype=torch.float32, pin_memory=True).numpy()
+    pv = torch.full((len(p2) + 10, 4), -7.0, dtype=torch.float32, pin_memory=True).numpy()
+    p3, v3 = t.particles4((pp, pv))
+    np.testing.assert_array_equal(p3, p2)
+    np.testing.assert_array_equal(v3, v2)
+    assert np.all(pp[len(p2):] == -7.0)
     t.close()
 
 
