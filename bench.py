@@ -409,7 +409,7 @@ def init_ranks(world, local):
 # ------------------------------------------------------------------ the batching workload (default)
 def e2e_batch(P, specs, device, best, steps, workers=8):
     """The job end to end through the public API with host buffers: every scene's particles added from host
-    arrays (staged through pinned memory into the device), `steps` batched sub-steps with each scene's stats
+    arrays (page-locked, copied by the copy engine), `steps` batched sub-steps with each scene's stats
     read back every sub-step (pollStats), and every scene's particles read back into page-locked host arrays
     (the ABI's pos4/vel4 layout) at the end. The scenes are uploaded and read back from `workers` host threads, one
     scene per thread at a time (handles are per thread; the ctypes calls release the interpreter lock).
@@ -421,9 +421,10 @@ def e2e_batch(P, specs, device, best, steps, workers=8):
     for k, knobs in enumerate(best):
         b.tune_lane(k, *knobs)
     import torch
-    host = [np.ascontiguousarray(w['pos'], np.float32) for w in specs]
-    # the read-back lands in page-locked arrays, allocated once as a client reading every run keeps them: the
-    # copy engine writes them directly (pageable arrays go through the tanks' pinned buffers and a host copy)
+    # the scenes' positions and the read-back live in page-locked arrays, allocated once as a client that
+    # uploads and reads every run keeps them: the copy engine reads and writes them directly (pageable arrays
+    # go through the tanks' pinned buffers and a host copy)
+    host = [torch.from_numpy(np.ascontiguousarray(w['pos'], np.float32)).pin_memory().numpy() for w in specs]
     pinned = [tuple(torch.empty((len(p) + 64, 4), dtype=torch.float32, pin_memory=True) for _ in range(2)) for p in host]
     outs = [(a.numpy(), b.numpy()) for a, b in pinned]
     readback = int(P.native.lib().suiri_stats_readback_bytes())

@@ -454,6 +454,7 @@ Tank::~Tank() {
     pinned_put(h_stage[k], stage_cap[k]);
     if (stage_ev[k]) cudaEventDestroy(stage_ev[k]);
   }
+  if (copy_ev) cudaEventDestroy(copy_ev);
   pinned_put(h_poll, sizeof(Counters));
   pinned_put(h_read_p, read_cap * 16);
   pinned_put(h_read_v, read_cap * 16);
@@ -639,16 +640,9 @@ bool Tank::poll_counters(Counters& out) {
   return fresh;
 }
 
-// n packed particles in pinned memory (positions, then velocities and marks where given) to the device in one
-// copy, unpacked into E after the particles staged before them
-void Tank::stage(const unsigned char* src, size_t bytes, long long n, bool has_vel, bool has_air) {
-  if (n <= 0) return;
-  if (bytes > d_stage_cap) {
-    if (d_stage) CK(cudaFreeAsync(d_stage, stream));
-    d_stage_cap = bytes;
-    CK(cudaMallocAsync((void**)&d_stage, d_stage_cap, stream));
-  }
-  CK(cudaMemcpyAsync(d_stage, src, bytes, cudaMemcpyHostToDevice, stream));
+// n packed particles (positions, then velocities and marks where given) copied to d_stage are unpacked into E
+// after the particles staged before them
+void Tank::unpack_staged(long long n, bool has_vel, bool has_air) {
   const float* pos = reinterpret_cast<const float*>(d_stage);
   const float* vel = has_vel ? pos + 3 * n : nullptr;
   const float* air = has_air ? pos + (has_vel ? 6 : 3) * n : nullptr;
@@ -658,6 +652,13 @@ void Tank::stage(const unsigned char* src, size_t bytes, long long n, bool has_v
   k_set_emit<<<1, 1, 0, stream>>>(d.ctr, (int)n_emit_host);
   CK(cudaGetLastError());
   n_upper += n;
+}
+
+void Tank::ensure_d_stage(size_t bytes) {
+  if (bytes <= d_stage_cap) return;
+  if (d_stage) CK(cudaFreeAsync(d_stage, stream));
+  d_stage_cap = bytes;
+  CK(cudaMallocAsync((void**)&d_stage, d_stage_cap, stream));
 }
 
 void Tank::add_particles(const float* pos, const float* vel, const float* air, long long n, uint32_t* first) {
@@ -671,26 +672,40 @@ void Tank::add_particles(const float* pos, const float* vel, const float* air, l
     room = std::min<long long>(cfg.cap - n_upper, emit_cap - n_emit_host);
   }
   long long take = std::max(0LL, std::min(n, room));
-  // two pinned staging buffers in turn: a buffer is refilled once the copy out of it two calls ago has
-  // finished (an event, not a wait for the whole stream, so the host stays ahead of the device)
-  const int k = stage_k;
-  stage_k ^= 1;
-  if (stage_ev[k]) CK(cudaEventSynchronize(stage_ev[k]));
-  else CK(cudaEventCreateWithFlags(&stage_ev[k], cudaEventDisableTiming));
   const size_t bp = (size_t)take * 12, bv = vel ? bp : 0, ba = air ? (size_t)take * 4 : 0;
-  if (bp + bv + ba > stage_cap[k]) {
-    pinned_put(h_stage[k], stage_cap[k]);
-    h_stage[k] = nullptr;
-    stage_cap[k] = 0;
-    h_stage[k] = (unsigned char*)pinned_get(bp + bv + ba, &stage_cap[k]);
-  }
-  if (take > 0) {
+  if (take > 0 && host_pinned(pos, bp) && (!vel || host_pinned(vel, bv)) && (!air || host_pinned(air, ba)) &&
+      cudaStreamQuery(stream) == cudaSuccess) {
+    // page-locked arrays and nothing queued on the tank's stream: the copy engine reads them directly, and
+    // the call returns once it has (the caller may then reuse them)
+    ensure_d_stage(bp + bv + ba);
+    CK(cudaMemcpyAsync(d_stage, pos, bp, cudaMemcpyHostToDevice, stream));
+    if (vel) CK(cudaMemcpyAsync(d_stage + bp, vel, bv, cudaMemcpyHostToDevice, stream));
+    if (air) CK(cudaMemcpyAsync(d_stage + bp + bv, air, ba, cudaMemcpyHostToDevice, stream));
+    if (!copy_ev) CK(cudaEventCreateWithFlags(&copy_ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(copy_ev, stream));
+    unpack_staged(take, vel != nullptr, air != nullptr);
+    CK(cudaEventSynchronize(copy_ev));
+  } else if (take > 0) {
+    // two pinned staging buffers in turn: a buffer is refilled once the copy out of it two calls ago has
+    // finished (an event, not a wait for the whole stream, so the host stays ahead of the device)
+    const int k = stage_k;
+    stage_k ^= 1;
+    if (stage_ev[k]) CK(cudaEventSynchronize(stage_ev[k]));
+    else CK(cudaEventCreateWithFlags(&stage_ev[k], cudaEventDisableTiming));
+    if (bp + bv + ba > stage_cap[k]) {
+      pinned_put(h_stage[k], stage_cap[k]);
+      h_stage[k] = nullptr;
+      stage_cap[k] = 0;
+      h_stage[k] = (unsigned char*)pinned_get(bp + bv + ba, &stage_cap[k]);
+    }
     memcpy(h_stage[k], pos, bp);
     if (vel) memcpy(h_stage[k] + bp, vel, bv);
     if (air) memcpy(h_stage[k] + bp + bv, air, ba);
+    ensure_d_stage(bp + bv + ba);
+    CK(cudaMemcpyAsync(d_stage, h_stage[k], bp + bv + ba, cudaMemcpyHostToDevice, stream));
+    CK(cudaEventRecord(stage_ev[k], stream));
+    unpack_staged(take, vel != nullptr, air != nullptr);
   }
-  stage(h_stage[k], bp + bv + ba, take, vel != nullptr, air != nullptr);
-  CK(cudaEventRecord(stage_ev[k], stream));
   next_id += (uint32_t)take;
   if (take < n) {
     h_ctr->full = 1;

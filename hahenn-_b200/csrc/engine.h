@@ -118,6 +118,7 @@ struct Tank {
   size_t stage_cap[2] = {};        // bytes
   unsigned char* d_stage = nullptr;  // their device copy, unpacked into E by a kernel
   size_t d_stage_cap = 0;
+  cudaEvent_t copy_ev = nullptr;  // a direct copy from page-locked caller arrays has finished
   cudaEvent_t stage_ev[2] = {};   // the copies out of each staging buffer have finished
   int stage_k = 0;
   Counters* h_poll = nullptr;     // pinned target of the asynchronous counter read
@@ -157,7 +158,8 @@ struct Tank {
   void read_counters();           // synchronous
   bool poll_counters(Counters& out);   // non-blocking: the last finished read into out (true); starts the next
   void add_particles(const float* pos, const float* vel, const float* air, long long n, uint32_t* first);
-  void stage(const unsigned char* src, size_t bytes, long long n, bool has_vel, bool has_air);
+  void ensure_d_stage(size_t bytes);
+  void unpack_staged(long long n, bool has_vel, bool has_air);
   void emit_block(const double lo[3], const double hi[3], bool fill);
   void clear();
   void reset();

@@ -196,8 +196,10 @@ int suiri_estimate_bytes(const char* scene_json, const suiri_params* params, dou
 
 /* particles from host arrays, appended before the next sub-step (emit_block/_add, solver.py:304-343).
    pos, vel: n×3 float32 (vel NULL: at rest); airborne: n floats (0/1) or NULL. The arrays cross to the
-   device packed as given (12 B a particle for positions alone) through pinned staging, and a kernel lays
-   them out. *first_id (may be NULL) = id of the first. */
+   device packed as given (12 B a particle for positions alone), and a kernel lays them out: arrays in
+   page-locked memory are read by the copy engine directly when nothing is queued on the tank's stream (the
+   call returns once they have been read), others are copied into pinned staging first. Either way the
+   caller may reuse the arrays on return. *first_id (may be NULL) = id of the first. */
 int suiri_add_particles(suiri_tank* t, const float* pos, const float* vel, const float* airborne, int64_t n,
                         uint32_t* first_id);
 /* Fixed-rate emitters run on the device inside every sub-step (also inside a captured CUDA graph): shape 0

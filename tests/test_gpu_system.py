@@ -277,6 +277,39 @@ def test_read_back_skips_the_drained_and_keeps_pending_adds(pkg):
     t.close()
 
 
+def test_adds_from_page_locked_arrays_equal_adds_from_pageable_ones(pkg):
+    """Particles added from page-locked arrays (read by the copy engine directly) arrive exactly as those added
+    from ordinary arrays (staged first), with their velocities, marks and ids, and the caller's arrays are
+    left as they were."""
+    import torch
+    rng = np.random.default_rng(8)
+    pos = (np.array([0.0, 0.3, 0.0]) + rng.uniform(-0.2, 0.2, (5000, 3))).astype(np.float32)
+    vel = rng.uniform(-1, 1, (5000, 3)).astype(np.float32)
+    air = (rng.random(5000) < 0.3).astype(np.float32)
+    out = []
+    for pinned in (False, True):
+        t = pkg.Tank(nx=32, ny=32, nz=32, h=1 / 32, whitewater=False, ripple=None, capacity=8192, iters=20)
+        args = [torch.from_numpy(a.copy()).pin_memory().numpy() if pinned else a.copy() for a in (pos, vel, air)]
+        t.sync()                       # nothing queued: the page-locked arrays go to the device directly
+        first = t.add_particles(*args)
+        for a, b in zip(args, (pos, vel, air)):
+            np.testing.assert_array_equal(a, b)
+        out.append((first,) + t.particles4())
+        t.substep(1 / 240)
+        out[-1] += t.particles4()
+        t.close()
+    assert out[0][0] == out[1][0]
+    np.testing.assert_array_equal(out[0][1], out[1][1])          # as added: in the order given
+    np.testing.assert_array_equal(out[0][2], out[1][2])
+    np.testing.assert_array_equal(out[1][1][:, :3], pos)
+    np.testing.assert_array_equal(out[1][2][:, :3], vel)
+    np.testing.assert_array_equal(out[1][1][:, 3], air)
+    # after a sub-step the order within a cell follows the binning's atomics: compare by id
+    o0, o1 = (np.argsort(o[4][:, 3].view(np.uint32)) for o in out)
+    np.testing.assert_array_equal(out[0][3][o0], out[1][3][o1])
+    np.testing.assert_array_equal(out[0][4][o0], out[1][4][o1])
+
+
 def test_poll_stats_and_pipelined_particle_adds(pkg):
     """Non-blocking stats (pollStats): the first call only starts a read; a read started once the stream is
     idle returns exactly what the blocking read returns. Particles added every sub-step through the two
