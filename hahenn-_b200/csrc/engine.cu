@@ -424,6 +424,8 @@ Tank::Tank(const TankConfig& c) : cfg(c) {
   D.vel = (float4*)alloc(nn * 16); D.velold = (float4*)alloc(nn * 16);
   D.frac = (float4*)alloc(nn * 16); D.svel = (float4*)alloc(nn * 16);
   D.fracd = (double*)alloc(3 * nn * 8); D.flux = (double*)alloc(3 * nn * 8);
+  D.near = (uint8_t*)alloc(nc);
+  CK(cudaMemsetAsync(D.near, 1, nc, stream));      // 1 (test the obstacles) until the geometry pass builds it
   D.vv = (float2*)alloc(3 * nn * 8);
   D.pres = (float*)alloc(2 * nh * 4); D.rhs = (float*)alloc(2 * nh * 4); D.code = (uint32_t*)alloc(2 * nh * 4);
   D.pres2 = (float*)alloc(2 * nh * 4);
@@ -536,6 +538,7 @@ size_t tank_bytes(const TankConfig& c) {
   size_t b = cap * 16 * 6 + cap * 2 * 4;                      // A, E, B (pos, vel), ranks
   b += (nc + 1) * 4 + (nc + 2) * 4;                           // counts, offsets
   b += nn * (6 * 8 + 4 * 16 + 2 * 3 * 8 + 3 * 8);            // accumulator, vel/velold/frac/svel, fracd/flux, vv
+  b += nc;                                                    // obstacle reach per cell
   b += 2 * nh * 32;                                           // pressure (two buffers), rhs, code, active lists
   b += kMaxObj * sizeof(Obj) + sizeof(Counters) + kMaxEmitters * sizeof(EmitterDev);
   b += 2 * (size_t)std::max(1LL, c.ww_cap) * 32;

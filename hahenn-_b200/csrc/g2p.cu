@@ -247,8 +247,17 @@ __device__ __forceinline__ unsigned long long g2p_particle(const TankDev& T, int
     }
   }
   const double rc = 0.32 * h;
-  if (kFast && maybe_within(T, x[0], x[1], x[2], rc)) { *defer = true; return 0ull; }
-  if (!kFast && maybe_within(T, x[0], x[1], x[2], rc)) {
+  // a particle of a cell that no obstacle can reach, moving less than kNearMove·h, skips the obstacle tests
+  // (they would all fail: see cell_near)
+  bool may = T.has_obst;
+  if (may && ing) {
+    const double dx = x[0] - x0[0], dy = x[1] - x0[1], dz = x[2] - x0[2];
+    const double lim = kNearMove * h;
+    may = !(dx * dx + dy * dy + dz * dz <= lim * lim && T.near[cell_idx(T, c0[0], c0[1], c0[2])] == 0);
+  }
+  may = may && maybe_within(T, x[0], x[1], x[2], rc);
+  if (kFast && may) { *defer = true; return 0ull; }
+  if (!kFast && may) {
     const double d = tank_sdf(T, x[0], x[1], x[2]);
     if (d < rc) {
       double nx, ny, nz;

@@ -97,6 +97,10 @@ __global__ void __launch_bounds__(kThreads) k_geom(const TankDev* __restrict__ t
   T.fracd[n] = f[0];
   T.fracd[T.nnodes + n] = f[1];
   T.fracd[2 * T.nnodes + n] = f[2];
+  // whether a particle of this cell may come within a collision radius (0.32h, the grid-to-particle pass's)
+  // of an obstacle this sub-step
+  if (i < nx && j < ny && k < nz)
+    T.near[cell_idx(T, i, j, k)] = cell_near(T, T.ox + h * (i + 0.5), T.oy + h * (j + 0.5), T.oz + h * (k + 0.5), 0.32 * h);
   T.frac[n] = make_float4((float)f[0], (float)f[1], (float)f[2], 0.f);
   T.svel[n] = make_float4((float)sv[0], (float)sv[1], (float)sv[2], 0.f);
 }
