@@ -258,10 +258,13 @@ __device__ __forceinline__ unsigned long long g2p_particle(const TankDev& T, int
   may = may && maybe_within(T, x[0], x[1], x[2], rc);
   if (kFast && may) { *defer = true; return 0ull; }
   if (!kFast && may) {
-    const double d = tank_sdf(T, x[0], x[1], x[2]);
+    int near = -1;
+    double other = -kBig;
+    const double d = T.sdf_mode == kSdfAnalytic ? scene_sdf_nearest(T.objs, T.nobj, x[0], x[1], x[2], near, other)
+                                                : tank_sdf(T, x[0], x[1], x[2]);
     if (d < rc) {
       double nx, ny, nz;
-      tank_normal(T, x[0], x[1], x[2], nx, ny, nz);
+      tank_normal_near(T, x[0], x[1], x[2], d, near, other, nx, ny, nz);
       x[0] += nx * (rc - d); x[1] += ny * (rc - d); x[2] += nz * (rc - d);
       double vs[3];
       tank_solid_vel(T, x[0], x[1], x[2], vs[0], vs[1], vs[2]);
@@ -369,7 +372,7 @@ __device__ __forceinline__ unsigned long long g2p_particle(const TankDev& T, int
 }
 
 template <bool kSplit>
-__global__ void __launch_bounds__(kThreads, kSplit ? 3 : 1) k_g2p(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ pfx,
+__global__ void __launch_bounds__(kThreads, kSplit ? 3 : 2) k_g2p(const TankDev* __restrict__ tanks, int ntanks, const int* __restrict__ pfx,
                                                   int* __restrict__ defer_list, int* __restrict__ defer_n) {
   const int total = pfx[ntanks];
   const int stride = gridDim.x * blockDim.x;

@@ -83,6 +83,36 @@ __device__ inline double scene_sdf(const Obj* __restrict__ objs, int n, double p
   return best;
 }
 
+// scene_sdf(…, cull = true), also giving the obstacle that holds the minimum (`near`, -1: none) and a lower
+// bound on every other obstacle's distance (`other`: its distance where the loop computed it, its
+// bounding-sphere distance where the cull skipped it; -kBig with a gutter, whose distance that sphere does not
+// bound). The same loop and fmin order, so the same value.
+__device__ inline double scene_sdf_nearest(const Obj* __restrict__ objs, int n, double px, double py, double pz, int& near,
+                                           double& other) {
+  double best = kBig;
+  near = -1;
+  other = kBig;
+  for (int i = 0; i < n; ++i) {
+    const Obj& o = objs[i];
+    if (o.flag != 1) continue;
+    if (o.type == 7) other = -kBig;
+    const double c = len3(px - o.pos[0], py - o.pos[1], pz - o.pos[2]) - o.bound;
+    if (c > best) {
+      other = fmin(other, c);
+      continue;
+    }
+    const double d = shape_sdf(o, px, py, pz);
+    if (d < best) {
+      if (near >= 0) other = fmin(other, best);
+      best = d;
+      near = i;
+    } else {
+      other = fmin(other, d);
+    }
+  }
+  return best;
+}
+
 // velocity of the nearest obstacle (src/js/30-wgsl-sim.js:96-106)
 __device__ inline void solid_vel_analytic(const Obj* __restrict__ objs, int n, double px, double py, double pz,
                                           double& vx, double& vy, double& vz) {
@@ -219,13 +249,33 @@ __device__ __forceinline__ uint8_t cell_near(const TankDev& T, double cx, double
 }
 
 // central differences, e = 6e-4 (solver.py:142-151, 30-wgsl-sim.js:88-95)
-__device__ inline void tank_normal(const TankDev& T, double px, double py, double pz, double& nx, double& ny, double& nz) {
-  const double e = 0.0006;
-  nx = tank_sdf(T, px + e, py, pz) - tank_sdf(T, px - e, py, pz);
-  ny = tank_sdf(T, px, py + e, pz) - tank_sdf(T, px, py - e, pz);
-  nz = tank_sdf(T, px, py, pz + e) - tank_sdf(T, px, py, pz - e);
+constexpr double kNormalStep = 0.0006;
+__device__ __forceinline__ void normal_from(double nx, double ny, double nz, double& ox, double& oy, double& oz) {
   const double l = sqrt(nx * nx + ny * ny + nz * nz);
-  if (l > 1e-9) { nx /= l; ny /= l; nz /= l; } else { nx = 0.0; ny = 1.0; nz = 0.0; }
+  if (l > 1e-9) { ox = nx / l; oy = ny / l; oz = nz / l; } else { ox = 0.0; oy = 1.0; oz = 0.0; }
+}
+__device__ inline void tank_normal(const TankDev& T, double px, double py, double pz, double& nx, double& ny, double& nz) {
+  const double e = kNormalStep;
+  normal_from(tank_sdf(T, px + e, py, pz) - tank_sdf(T, px - e, py, pz),
+              tank_sdf(T, px, py + e, pz) - tank_sdf(T, px, py - e, pz),
+              tank_sdf(T, px, py, pz + e) - tank_sdf(T, px, py, pz - e), nx, ny, nz);
+}
+
+// tank_normal at p, where the scene distance d came from scene_sdf_nearest: when every other obstacle is more
+// than d + 2e (+1e-6) away, each of the six samples (within e of p, the distances 1-Lipschitz) has its minimum
+// at obstacle `near` and no cull skips it, so the scene distance there is that obstacle's own: six shape
+// evaluations instead of six scene loops, the same values
+__device__ inline void tank_normal_near(const TankDev& T, double px, double py, double pz, double d, int near, double other,
+                                        double& nx, double& ny, double& nz) {
+  const double e = kNormalStep;
+  if (T.sdf_mode == kSdfAnalytic && near >= 0 && other > d + 2 * e + 1e-6) {
+    const Obj& o = T.objs[near];
+    normal_from(shape_sdf(o, px + e, py, pz) - shape_sdf(o, px - e, py, pz),
+                shape_sdf(o, px, py + e, pz) - shape_sdf(o, px, py - e, pz),
+                shape_sdf(o, px, py, pz + e) - shape_sdf(o, px, py, pz - e), nx, ny, nz);
+  } else {
+    tank_normal(T, px, py, pz, nx, ny, nz);
+  }
 }
 
 __device__ inline void tank_solid_vel(const TankDev& T, double px, double py, double pz, double& vx, double& vy, double& vz) {
