@@ -115,8 +115,8 @@ struct TankDev {
   float4* velold;           // P2G velocity, .w = valid-face mask bits
   float4* frac;             // face open fractions, float32
   double* fracd;            // 3*nnodes, float64 (divergence)
-  uint8_t* near;            // ncells: 0 where no obstacle's cull can hold for a point within kNearReach of the
-                            // cell's centre (built with the face fractions), 1 elsewhere
+  uint8_t* near;            // ncells: whether an obstacle's cull (bit 1) or a drain (bit 2) can hold for a
+                            // point within kNearReach·h of the cell's centre (built with the face fractions)
   float4* svel;             // solid velocity at faces
   float2* vv;               // 3*nnodes: per component (projected v, P2G v or NaN where the face took no weight)
   double* flux;             // 3*nnodes cut-cell face fluxes (divergence operand)

@@ -425,7 +425,7 @@ Tank::Tank(const TankConfig& c) : cfg(c) {
   D.frac = (float4*)alloc(nn * 16); D.svel = (float4*)alloc(nn * 16);
   D.fracd = (double*)alloc(3 * nn * 8); D.flux = (double*)alloc(3 * nn * 8);
   D.near = (uint8_t*)alloc(nc);
-  CK(cudaMemsetAsync(D.near, 1, nc, stream));      // 1 (test the obstacles) until the geometry pass builds it
+  CK(cudaMemsetAsync(D.near, 3, nc, stream));      // test obstacles and drains until the geometry pass builds it
   D.vv = (float2*)alloc(3 * nn * 8);
   D.pres = (float*)alloc(2 * nh * 4); D.rhs = (float*)alloc(2 * nh * 4); D.code = (uint32_t*)alloc(2 * nh * 4);
   D.pres2 = (float*)alloc(2 * nh * 4);

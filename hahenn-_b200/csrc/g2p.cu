@@ -247,15 +247,15 @@ __device__ __forceinline__ unsigned long long g2p_particle(const TankDev& T, int
     }
   }
   const double rc = 0.32 * h;
-  // a particle of a cell that no obstacle can reach, moving less than kNearMove·h, skips the obstacle tests
-  // (they would all fail: see cell_near)
-  bool may = T.has_obst;
-  if (may && ing) {
+  // a particle of a cell that no obstacle (drain) can reach, moving less than kNearMove·h, skips the obstacle
+  // (drain) tests: they would all fail (see cell_near)
+  uint8_t reach = kNearObst | kNearDrain;
+  if (T.nobj && ing) {
     const double dx = x[0] - x0[0], dy = x[1] - x0[1], dz = x[2] - x0[2];
     const double lim = kNearMove * h;
-    may = !(dx * dx + dy * dy + dz * dz <= lim * lim && T.near[cell_idx(T, c0[0], c0[1], c0[2])] == 0);
+    if (dx * dx + dy * dy + dz * dz <= lim * lim) reach = T.near[cell_idx(T, c0[0], c0[1], c0[2])];
   }
-  may = may && maybe_within(T, x[0], x[1], x[2], rc);
+  const bool may = T.has_obst && (reach & kNearObst) && maybe_within(T, x[0], x[1], x[2], rc);
   if (kFast && may) { *defer = true; return 0ull; }
   if (!kFast && may) {
     int near = -1;
@@ -281,7 +281,7 @@ __device__ __forceinline__ unsigned long long g2p_particle(const TankDev& T, int
   tank_clamp(T, x0, x, v, rc);
   const Fp fp = footprint(T);
   bool alive = true;
-  if (T.nobj && in_drain(T.objs, T.nobj, x[0], x[1], x[2])) alive = false;
+  if (T.nobj && (reach & kNearDrain) && in_drain(T.objs, T.nobj, x[0], x[1], x[2])) alive = false;
   if (!in_fp(fp, x[0], x[2]) && x[1] < 0.002) alive = false;
   if (fabs(x[0]) > 20 || fabs(x[2]) > 20 || x[1] < -1 || x[1] > 30) alive = false;
   // free-flight mark of sub-grid drops (solver.py:565-583)

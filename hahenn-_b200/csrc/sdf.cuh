@@ -222,30 +222,39 @@ __device__ __forceinline__ bool maybe_within(const TankDev& T, double px, double
 constexpr double kNearMove = 0.98;
 constexpr double kNearReach = 0.8660254037844387 + kNearMove + 1e-3;
 
-// The cell's entry of T.near (k_geom): 0 only when maybe_within(p, r) is false for every p within kNearReach·h
-// of the centre c, i.e. when c is beyond r + 1e-6 + kNearReach·h (+1e-6) of every obstacle's bounding sphere
-// or of its box in its own frame. Both distances change by at most |p − c| between c and p (the distance to a
-// ball or to a box is 1-Lipschitz, and the rotation keeps lengths), so maybe_within's tests fail at every such p.
+// The cell's entry of T.near (k_geom), two bits. Bit kNearObst is clear only when maybe_within(p, r) is false
+// for every p within kNearReach·h of the centre c, i.e. when c is beyond r + 1e-6 + kNearReach·h (+1e-6) of
+// every obstacle's bounding sphere or of its box in its own frame. Both distances change by at most |p − c|
+// between c and p (the distance to a ball or to a box is 1-Lipschitz, and the rotation keeps lengths), so
+// maybe_within's tests fail at every such p. Bit kNearDrain is clear only when c is beyond every drain's
+// bound + kNearReach·h (+1e-6), so in_drain(p) is false at every such p.
+constexpr uint8_t kNearObst = 1, kNearDrain = 2;
 __device__ __forceinline__ uint8_t cell_near(const TankDev& T, double cx, double cy, double cz, double r) {
-  if (!T.has_obst) return 0;
-  if (T.sdf_mode != kSdfAnalytic) return 1;
   const double reach = kNearReach * T.h + 1e-6;
+  uint8_t bits = 0;
+  if (T.has_obst && T.sdf_mode != kSdfAnalytic) bits |= kNearObst;
   for (int i = 0; i < T.nobj; ++i) {
     const Obj& o = T.objs[i];
-    if (o.flag != 1) continue;
-    if (o.type == 7) return 1;
     const double ex = cx - o.pos[0], ey = cy - o.pos[1], ez = cz - o.pos[2];
+    const double e2 = ex * ex + ey * ey + ez * ez;
+    if (o.flag == 2) {
+      const double lim = o.bound + reach;
+      if (e2 <= lim * lim) bits |= kNearDrain;
+      continue;
+    }
+    if (o.flag != 1 || (bits & kNearObst)) continue;
+    if (o.type == 7) { bits |= kNearObst; continue; }
     const double lim = r + o.bound + 1e-6 + reach;
-    if (ex * ex + ey * ey + ez * ez >= lim * lim) continue;
-    if (o.type == 1) return 1;
+    if (e2 >= lim * lim) continue;
+    if (o.type == 1) { bits |= kNearObst; continue; }
     double qx, qy, qz, bx, by, bz;
     to_local(o, cx, cy, cz, qx, qy, qz);
     local_box(o, bx, by, bz);
     const double ox = fmax(fabs(qx) - bx, 0.0), oy = fmax(fabs(qy) - by, 0.0), oz = fmax(fabs(qz) - bz, 0.0);
     const double rb = r + 1e-6 + reach;
-    if (ox * ox + oy * oy + oz * oz < rb * rb) return 1;
+    if (ox * ox + oy * oy + oz * oz < rb * rb) bits |= kNearObst;
   }
-  return 0;
+  return bits;
 }
 
 // central differences, e = 6e-4 (solver.py:142-151, 30-wgsl-sim.js:88-95)
