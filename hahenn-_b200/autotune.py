@@ -41,9 +41,9 @@ def _time(target, dt, steps):
 
 def _settle(target, dt, steps, timings, keys, apply, confirm):
     """The fastest of `keys` by its first reading, checked against the first key (the default): both are
-    timed `confirm` more times, interleaved, and each is scored by its slowest reading, so a form whose
-    sub-step time swings from one graph launch to the next is scored by its bad readings. The fastest
-    replaces the default only when it still wins by MARGIN."""
+    timed `confirm` more times, interleaved, and each is scored by its slowest reading: a form whose sub-step
+    time swings from one graph launch to the next counts with its bad readings. The fastest replaces the
+    default only when it still wins by MARGIN."""
     default, first = keys[0], min(keys, key=timings.get)
     if first == default or timings[default] == float('inf') or confirm <= 0:
         return first
