@@ -160,3 +160,116 @@ def test_balanced_lanes_keep_sizes_together_and_balance_particles():
     assert set(lane) == {0, 1}
     tot = [sum(p for p, l in zip(parts, lane) if l == k) for k in (0, 1)]
     assert max(tot) <= 0.75 * sum(parts)
+
+
+def _local_box(o):
+    d = o['dims']
+    t = o['type']
+    if t in (0, 6):
+        return np.array([d[0], d[1], d[2]])
+    if t in (2, 3, 5):
+        return np.array([d[0], d[1], d[0]])
+    if t == 4:
+        return np.array([d[0] + d[1], d[1], d[0] + d[1]])
+    return np.array([d[0], d[0], d[0]])
+
+
+def _reach_bits(objs, c, h, rc):
+    """The per-cell reach rule of the geometry pass, restated: bit 1 an obstacle's cull may hold within
+    reach·h of the centre c, bit 2 a drain's bound may (reach = √3/2 + 0.98 + 1e-3)."""
+    from oracle import sdf as sdfm
+    reach = (0.8660254037844387 + 0.98 + 1e-3) * h + 1e-6
+    bits = np.zeros(len(c), np.uint8)
+    for o in objs:
+        e2 = ((c - o['pos']) ** 2).sum(1)
+        if o['flag'] == 2:
+            bits |= np.where(e2 <= (o['bound'] + reach) ** 2, 2, 0).astype(np.uint8)
+            continue
+        if o['type'] == 7:
+            bits |= 1
+            continue
+        inside = e2 < (rc + o['bound'] + 1e-6 + reach) ** 2
+        if o['type'] != 1:
+            q = sdfm.to_local(o, c)
+            out = np.maximum(np.abs(q) - _local_box(o), 0.0)
+            inside &= (out ** 2).sum(1) < (rc + 1e-6 + reach) ** 2
+        bits |= inside.astype(np.uint8)
+    return bits
+
+
+def _ball(rng, n, r):
+    v = rng.normal(size=(n, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    return v * (r * rng.random((n, 1)) ** (1 / 3))
+
+
+def test_reach_rule_leaves_out_only_cells_no_collision_or_drain_can_come_from():
+    """The reach map's rule on the reference's own shape distances (the oracle's restatement of the WGSL
+    library): from a cell it leaves out, no point a particle can reach in the sub-step (within √3/2·h of the
+    centre, then at most 0.98h) is within the collision radius of an obstacle or inside a drain. A gutter
+    anywhere marks every cell."""
+    from oracle import sdf as sdfm
+    from parity import objs_from_items
+    from test_gpu_parity import ALL_SHAPES
+    h = 1 / 40
+    rc = 0.32 * h
+    items = [it for it in ALL_SHAPES if it['shape'] != 'gutter']
+    objs = objs_from_items(items) + [sdfm.make_drain([0.05, 0.0, 0.1], 0.05)]
+    rng = np.random.default_rng(4)
+    lo, hi = np.array([-0.3, 0.0, -0.2]), np.array([0.3, 0.3, 0.2])
+    cells = lo + rng.random((6000, 3)) * (hi - lo)
+    bits = _reach_bits(objs, cells, h, rc)
+    assert 0 < (bits & 1).sum() < len(cells) and 0 < (bits & 2).sum() < len(cells)
+    far_o, far_d = cells[(bits & 1) == 0], cells[(bits & 2) == 0]
+    reach = (0.8660254037844387 + 0.98) * h
+    for c0, test in ((far_o, lambda p: sdfm.scene_sdf(objs, p, cull=True) >= rc),
+                     (far_d, lambda p: ~sdfm.in_drain_analytic(objs, p))):
+        p = np.repeat(c0, 16, 0) + _ball(rng, len(c0) * 16, reach)
+        assert np.all(test(p))
+    # the cells it keeps include ones a collision does come from
+    near = cells[(bits & 1) == 1][:2000]
+    p = np.repeat(near, 16, 0) + _ball(rng, len(near) * 16, reach)
+    assert np.any(sdfm.scene_sdf(objs, p, cull=True) < rc)
+    gut = objs_from_items([it for it in ALL_SHAPES if it['shape'] == 'gutter'])
+    assert np.all(_reach_bits(gut, cells[:100], h, rc) & 1)
+
+
+def test_nearest_obstacle_normal_samples_equal_the_scene_distance():
+    """The collision normal's shortcut, on the reference's shape distances: where the culled scene loop at p
+    puts every obstacle but the nearest more than d + 2e (+1e-6) away (computed distance, or bounding-sphere
+    distance where the cull skipped it), the scene distance at each of the six samples p ± e·axis equals the
+    nearest obstacle's own distance bit for bit."""
+    from oracle import sdf as sdfm
+    from parity import objs_from_items
+    from test_gpu_parity import ALL_SHAPES
+    objs = [o for o in objs_from_items([it for it in ALL_SHAPES if it['shape'] != 'gutter'])]
+    rng = np.random.default_rng(6)
+    lo, hi = np.array([-0.3, 0.0, -0.2]), np.array([0.3, 0.3, 0.2])
+    p = lo + rng.random((200000, 3)) * (hi - lo)
+    d_all = np.stack([sdfm.shape_sdf(o, p) for o in objs], 1)
+    p = p[np.abs(d_all.min(1)) < 0.01][:20000]             # near a surface, as colliding particles are
+    e = 0.0006
+    # the culled loop, tracking the nearest and a lower bound on the others
+    best = np.full(len(p), sdfm.BIG)
+    near = np.full(len(p), -1)
+    other = np.full(len(p), sdfm.BIG)
+    for i, o in enumerate(objs):
+        c = np.linalg.norm(p - o['pos'], axis=1) - o['bound']
+        d = sdfm.shape_sdf(o, p)
+        culled = c > best
+        other = np.where(culled, np.minimum(other, c), other)
+        better = ~culled & (d < best)
+        other = np.where(better & (near >= 0), np.minimum(other, best), other)
+        other = np.where(~culled & ~better, np.minimum(other, d), other)
+        near = np.where(better, i, near)
+        best = np.where(better, d, best)
+    np.testing.assert_array_equal(best, sdfm.scene_sdf(objs, p, cull=True))
+    ok = (near >= 0) & (other > best + 2 * e + 1e-6)
+    assert ok.mean() > 0.5 and (~ok).any()
+    for axis in range(3):
+        for sgn in (1.0, -1.0):
+            q = p.copy()
+            q[:, axis] = p[:, axis] + sgn * e
+            scene = sdfm.scene_sdf(objs, q, cull=True)
+            own = np.choose(near.clip(0), [sdfm.shape_sdf(o, q) for o in objs])
+            np.testing.assert_array_equal(scene[ok], own[ok])
