@@ -3,7 +3,9 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 
 #include "../../include/suiri.h"
 #include "engine.h"
@@ -329,6 +331,37 @@ int suiri_eval_sdf(suiri_tank* h, const double* pts, int64_t n, double* out) {
   return guard(h ? &h->err : nullptr, [&] {
     if (n < 0 || (n > 0 && (!pts || !out))) throw Error(SUIRI_ERR_INVALID, "bad point arrays");
     T(h)->eval_sdf(pts, n, out);
+  });
+}
+
+namespace {
+std::mutex g_host_m;
+std::map<void*, size_t> g_host_blocks;   // blocks handed out by suiri_host_alloc and their request sizes
+}  // namespace
+
+int suiri_host_alloc(size_t bytes, void** out) {
+  return guard(nullptr, [&] {
+    if (!out || bytes == 0) throw Error(SUIRI_ERR_INVALID, "bad host allocation arguments");
+    *out = nullptr;
+    void* p = pinned_get(bytes);
+    std::lock_guard<std::mutex> g(g_host_m);
+    g_host_blocks[p] = bytes;
+    *out = p;
+  });
+}
+
+int suiri_host_free(void* p) {
+  return guard(nullptr, [&] {
+    if (!p) return;
+    size_t bytes = 0;
+    {
+      std::lock_guard<std::mutex> g(g_host_m);
+      auto it = g_host_blocks.find(p);
+      if (it == g_host_blocks.end()) throw Error(SUIRI_ERR_INVALID, "not a block of suiri_host_alloc");
+      bytes = it->second;
+      g_host_blocks.erase(it);
+    }
+    pinned_put(p, bytes);
   });
 }
 

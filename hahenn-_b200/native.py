@@ -125,6 +125,8 @@ SIGNATURES = {
     'suiri_batch_create_lanes': (C.c_int, [C.POINTER(P), C.c_int32, P, C.POINTER(P)]),
     'suiri_batch_destroy': (C.c_int, [P]),
     'suiri_batch_substep': (C.c_int, [P, C.c_double]),
+    'suiri_host_alloc': (C.c_int, [C.c_size_t, C.POINTER(C.c_void_p)]),
+    'suiri_host_free': (C.c_int, [P]),
     'suiri_batch_sync': (C.c_int, [P]),
     'suiri_batch_tune': (C.c_int, [P, C.c_int32, C.c_int32]),
     'suiri_batch_stream': (C.c_int, [P, C.POINTER(P)]),
@@ -178,6 +180,21 @@ def validate_scene(scene, clamp_tank=True):
     buf = C.create_string_buffer(n.value + 1)
     check(lib().suiri_scene_validate(js, 1 if clamp_tank else 0, buf, n.value + 1, C.byref(n)))
     return json.loads(buf.value.decode())
+
+
+def host_empty(shape, dtype='float32'):
+    """An uninitialised NumPy array in page-locked host memory from the library (suiri_host_alloc), released
+    to the library's cache when the array and its views are gone. Particle adds and read-backs with such
+    arrays are copied by the copy engine directly."""
+    import weakref
+    import numpy as np
+    dt = np.dtype(dtype)
+    n = max(1, int(np.prod(shape)) * dt.itemsize)
+    ptr = C.c_void_p()
+    check(lib().suiri_host_alloc(n, C.byref(ptr)))
+    buf = (C.c_char * n).from_address(ptr.value)
+    weakref.finalize(buf, lib().suiri_host_free, C.c_void_p(ptr.value))
+    return np.frombuffer(buf, dtype=dt, count=int(np.prod(shape))).reshape(shape)
 
 
 def check(rc, handle=None):

@@ -232,10 +232,17 @@ int suiri_step(suiri_tank* t, double frame_dt, int32_t* substeps);
 int suiri_frame_end(suiri_tank* t, double frame_dt);
 int suiri_sync(suiri_tank* t);
 
+/* page-locked host memory for the arrays of suiri_add_particles and suiri_read_particles, so that a host
+   without CUDA headers (a Node addon) gets the direct copies: at least `bytes`, from the library's cache of
+   pinned blocks (handing pinned memory back to the driver synchronises the device, so freed blocks are kept
+   for reuse, up to 2 GB); suiri_host_free takes back a block suiri_host_alloc gave */
+int suiri_host_alloc(size_t bytes, void** out);
+int suiri_host_free(void* p);
+
 /* liquid particles (alive) to host memory: pos4 = (x, y, z, airborne), vel4 = (vx, vy, vz, id as uint32 bits);
    either pointer may be NULL; *n = number available (written even when cap is too small). Arrays in
-   page-locked memory (cudaHostRegister, cudaMallocHost) are written by the copy engine directly; others
-   through the tank's pinned buffers. */
+   page-locked memory (suiri_host_alloc, cudaHostRegister, cudaMallocHost) are written by the copy engine
+   directly; others through the tank's pinned buffers. */
 int suiri_read_particles(suiri_tank* t, float* pos4, float* vel4, int64_t cap, int64_t* n);
 /* whitewater: pos4 = (x, y, z, life), vel4 = (vx, vy, vz, kind) */
 int suiri_read_whitewater(suiri_tank* t, float* pos4, float* vel4, int64_t cap, int64_t* n);

@@ -308,6 +308,19 @@ def test_adds_from_page_locked_arrays_equal_adds_from_pageable_ones(pkg):
     o0, o1 = (np.argsort(o[4][:, 3].view(np.uint32)) for o in out)
     np.testing.assert_array_equal(out[0][3][o0], out[1][3][o1])
     np.testing.assert_array_equal(out[0][4][o0], out[1][4][o1])
+    # the library's own page-locked arrays (suiri_host_alloc) for both directions
+    t = pkg.Tank(nx=32, ny=32, nz=32, h=1 / 32, whitewater=False, ripple=None, capacity=8192, iters=20)
+    hp = pkg.native.host_empty((5000, 3))
+    hp[:] = pos
+    t.sync()
+    t.add_particles(hp, vel, air)
+    rp, rv = pkg.native.host_empty((5010, 4)), pkg.native.host_empty((5010, 4))
+    p4, v4 = t.particles4((rp, rv))
+    np.testing.assert_array_equal(p4, out[1][1])
+    np.testing.assert_array_equal(v4, out[1][2])
+    t.close()
+    with pytest.raises(pkg.native.SuiriError):
+        pkg.native.check(pkg.native.lib().suiri_host_free(pkg.native.C.c_void_p(hp.ctypes.data + 16)))
 
 
 def test_poll_stats_and_pipelined_particle_adds(pkg):
